@@ -1,0 +1,412 @@
+"""Benchmark of the FP64 Cg/Bicg drop-in on one synthetic workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--size 200]
+
+Workload (a "step"): one Cg solve of the pressure-correction Poisson system
+and one Bicg solve of a momentum system, both FP64 with Jacobi
+preconditioning, on a 200^3 hexahedral grid (8.0 M cells) stretched
+geometrically (ratio 1.02) toward both y walls.  Seeded synthetic inputs;
+the reference ships no benchmark meshes.  See the DESIGN notes for the
+momentum system's Peclet number.
+
+Metric: Mcell-iters/s = sum over solves of (cells x iterations) / time.
+
+* value   -- solves through the library with val/x/b already in device
+             memory (tf_solve_device), timed with CUDA events on the
+             library's stream, max over ranks.
+* e2e     -- the same solves through tf_solve with pinned host buffers:
+             every step copies val, x, b host->device and back.
+* roofline-- the dominant kernel (the tiled SpMV) timed alone on the same
+             matrix with CUDA events; algorithmic bytes per launch
+             12*nnz + 4*(n+1) + 16*n; peak = measured HBM copy bandwidth.
+* cpu_baseline -- the oracle (C++ restatement of the reference, all host
+             threads) on a bounded number of iterations of the same system.
+
+`--impl reference` runs the oracle instead, on rank 0 only.
+Multi-GPU runs are replicas (independent systems per rank, weak scaling).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "t-flows_b200"))
+
+SPMV_BYTES = lambda n, nnz: 12 * nnz + 4 * (n + 1) + 16 * n  # noqa: E731
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=200)
+    ap.add_argument("--peclet", type=float, default=1.0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_workload(size, peclet):
+    from tflows_b200 import systems
+    p, m = systems.stretched_pair(n=size, seed=2, tol=1e-10, miter=20000, ratio=1.02,
+                                  peclet=peclet, momentum_miter=2000)
+    return [p, m]
+
+
+def workload_config(sysl, size, peclet):
+    p = sysl[0]
+    return {
+        "workload": f"stretched-hex-{size}^3 (ratio 1.02 toward both y walls): Cg pressure "
+                    f"Poisson (one pressure-boundary face pins the level) + Bicg upwind "
+                    f"momentum (cell Peclet {peclet:g}, CFL 0.5); FP64, Jacobi, tol 1e-10 "
+                    f"(reference NRMS with norm=1)",
+        "n_cells": p.n, "nnz": p.nnz, "solves_per_step": len(sysl),
+        "l2_policy": f"inputs larger than L2 (val {8 * p.nnz / 1e6:.0f} MB per system)",
+        "parallelism": "replicas",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(size):
+    """DRAM bytes per SpMV launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"spmv_fp64_stretched{size}.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(sysl, seconds, threads):
+    """Oracle Cg on a bounded number of iterations of the pressure system."""
+    from oracle import oracle as O
+    s = sysl[0]
+
+    def run(k):
+        v, x, b = s.val.copy(), s.x0.copy(), s.b.copy()
+        t0 = time.perf_counter()
+        r = O.solve_native("cg", "jacobi", s.csr.row, s.csr.col, s.csr.dia, v, x, b, k, 0.0,
+                           norm=1.0, threads=threads)
+        return time.perf_counter() - t0, r["niter"]
+
+    t1, _ = run(2)
+    t3, _ = run(6)
+    per_it = max((t3 - t1) / 4, 1e-6)
+    k = int(max(4, min(2000, seconds / per_it)))
+    t, it = run(k)
+    return {"value": s.n * it / t / 1e6, "unit": "Mcell-iters/s", "cores": threads,
+            "kind": "port",
+            "sample": f"oracle Cg+Jacobi, {it} iterations of the {s.n}-cell pressure system "
+                      f"(tol 0 -> fixed count), {t:.1f} s wall, OpenMP {threads} threads"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    sysl = make_workload(args.size, args.peclet)
+    threads = O.max_threads()
+    sample_iters = int(os.environ.get("TF_REF_ITERS", "40"))
+
+    def step():
+        tot = 0
+        for s in sysl:
+            v, x, b = s.val.copy(), s.x0.copy(), s.b.copy()
+            r = O.solve_native(s.solver, s.prec, s.csr.row, s.csr.col, s.csr.dia, v, x, b,
+                               sample_iters, s.tol, norm=s.norm, threads=threads)
+            tot += s.n * r["niter"]
+        return tot
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    cells = sum(step() for _ in range(args.steps))
+    dt = time.perf_counter() - t0
+    val = cells / dt / 1e6
+    line = {
+        "impl": "reference", "metric": "Mcell-iters/s", "value": val, "unit": "Mcell-iters/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": workload_config(sysl, args.size, args.peclet),
+        "cpu_baseline": {"value": val, "unit": "Mcell-iters/s", "cores": threads,
+                         "kind": "port",
+                         "sample": f"each step: {sample_iters} iterations (bounded) of "
+                                   f"each of the {len(sysl)} solves"},
+        "e2e": {"value": val, "unit": "Mcell-iters/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    from tflows_b200 import native
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def allsum(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    sysl = make_workload(args.size, args.peclet)
+    ctx = native.Context(local)
+    mats = [native.Matrix(ctx, s.csr.row, s.csr.col, s.csr.dia) for s in sysl]
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    # Device-resident inputs (pristine copies) and work buffers.
+    dev = []
+    for s in sysl:
+        d = {k: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+             for k, a in (("val0", s.val), ("b0", s.b), ("x0", s.x0))}
+        d.update(val=d["val0"].clone(), b=d["b0"].clone(), x=d["x0"].clone())
+        dev.append(d)
+    torch.cuda.synchronize()
+
+    results = {}
+
+    def device_step():
+        cells, its = 0, []
+        with torch.cuda.stream(stream):
+            for s, m, d in zip(sysl, mats, dev):
+                d["x"].copy_(d["x0"])
+                it, res = native.solve_device(ctx, m, s.solver, s.prec, d["val"].data_ptr(),
+                                              d["x"].data_ptr(), d["b"].data_ptr(), s.miter,
+                                              s.tol, s.norm)
+                cells += s.n * it
+                its.append((it, res))
+        return cells, its
+
+    for _ in range(args.warmup):
+        device_step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    per_solve = []
+    ev0.record(stream)
+    cells = 0
+    iters = None
+    for _ in range(args.steps):
+        e_a = torch.cuda.Event(enable_timing=True)
+        e_a.record(stream)
+        c, its = device_step()
+        e_b = torch.cuda.Event(enable_timing=True)
+        e_b.record(stream)
+        per_solve.append((e_a, e_b))
+        cells += c
+        iters = its
+    ev1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    t_dev = ev0.elapsed_time(ev1) / 1e3
+    t_dev_max = allmax(t_dev)
+    cells_all = allsum(cells)
+    step_ms = [a.elapsed_time(b) for a, b in per_solve]
+
+    # End-to-end through tf_solve with pinned host buffers.
+    host = []
+    for s in sysl:
+        h = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+             for k, a in (("val", s.val), ("b", s.b), ("x", s.x0))}
+        host.append(h)
+    h2d = sum(8 * s.nnz + 16 * s.n for s in sysl)
+    d2h = h2d
+
+    def e2e_step():
+        c = 0
+        for s, m, h in zip(sysl, mats, host):
+            np.copyto(h["val"], s.val)
+            np.copyto(h["b"], s.b)
+            np.copyto(h["x"], s.x0)
+            it, res = native.solve(ctx, m, s.solver, s.prec, h["val"], h["x"], h["b"],
+                                   s.miter, s.tol, s.norm)
+            c += s.n * it
+        return c
+
+    e2e_step()
+    barrier()
+    e2e_cells, t_e2e = 0, 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        e2e_cells += e2e_step()
+        t_e2e += time.perf_counter() - t0
+    t_e2e_max = allmax(t_e2e)
+    e2e_all = allsum(e2e_cells)
+
+    # Accuracy of the last device solve: true relative residual in FP64.
+    import scipy.sparse as sps
+    acc = []
+    for s, d, (it, res) in zip(sysl, dev, iters):
+        A = sps.csr_matrix((s.val, s.csr.col - 1, s.csr.row - 1), shape=(s.n, s.n))
+        x = d["x"].cpu().numpy()
+        rr = np.linalg.norm(s.b - A @ x) / np.linalg.norm(s.b)
+        acc.append({"system": s.name, "solver": s.solver, "niter": it, "fin_res": res,
+                    "true_rel_residual": float(rr)})
+
+    # Roofline of the dominant kernel: the tiled SpMV on the pressure matrix.
+    s0, m0, d0 = sysl[0], mats[0], dev[0]
+    p = torch.randn(s0.n, dtype=torch.float64, device="cuda")
+    q = torch.empty_like(p)
+    torch.cuda.synchronize()
+    nrep = 20
+    for _ in range(3):
+        native.spmv(ctx, m0, d0["val0"].data_ptr(), p.data_ptr(), q.data_ptr())
+    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r0.record(stream)
+    for _ in range(nrep):
+        native.spmv(ctx, m0, d0["val0"].data_ptr(), p.data_ptr(), q.data_ptr())
+    r1.record(stream)
+    r1.synchronize()
+    t_spmv = r0.elapsed_time(r1) / 1e3 / nrep
+    peak, peak_kind = measured_peak()
+    bytes_spmv = SPMV_BYTES(s0.n, s0.nnz)
+    achieved = bytes_spmv / t_spmv / 1e9
+
+    launches = sum(args.steps * (4 + 3 * it) for it, _ in iters)
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            from oracle import oracle as O
+            cpu = cpu_baseline(sysl, args.cpu_seconds, O.max_threads())
+        ms = np.array(step_ms)
+        solve_count = args.steps * len(sysl) * world
+        line = {
+            "metric": "Mcell-iters/s", "value": cells_all / t_dev_max / 1e6,
+            "unit": "Mcell-iters/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_dev_max / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded stretched hex grid; no reference dataset exists)",
+            "config": workload_config(sysl, args.size, args.peclet),
+            "solves_per_s": solve_count / t_dev_max,
+            "step_ms_p50": float(np.percentile(ms, 50)),
+            "step_ms_p99": float(np.percentile(ms, 99)),
+            "accuracy": acc,
+            "e2e": {"value": e2e_all / t_e2e_max / 1e6, "unit": "Mcell-iters/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "kernel": "k_spmv_alpha (tiled CSR SpMV + p.q)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "bytes_per_launch": bytes_spmv, "launch_ms": t_spmv * 1e3,
+                         "traffic": ncu_traffic(args.size)},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+
+    for m in mats:
+        m.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

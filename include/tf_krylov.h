@@ -1,0 +1,145 @@
+/* ==========================================================================
+ *  tf_krylov.h -- C ABI of the B200 native Krylov solvers for T-Flows.
+ *
+ *  Drop-in replacement for the body of Native_Type % Solve_Native
+ *  (Sources/Process/Cpu/Native_Mod/Solve_Native.f90:2-46) and the solvers it
+ *  dispatches to (Native_Mod/Cg.f90, Native_Mod/Bicg.f90) with the
+ *  preconditioners of Native_Mod/Prec_Form.f90 and Prec_Solve.f90.
+ *
+ *  Conventions (those of Matrix_Type, Sources/Process/Cpu/Matrix_Mod.f90:57-76):
+ *    - row(1..n+1), col(1..nnz), dia(1..n) hold 1-based indices, exactly as
+ *      Create_Matrix builds them; the diagonal is the first entry of a row;
+ *    - every real is double (the REAL=double build);
+ *    - x points at x(1) of the Fortran array x(-nb:n); boundary entries
+ *      x(-nb:0) are never referenced because col >= 1.
+ *  Every function returns an int status (TF_OK = 0).  Non-convergence is not
+ *  an error: it is reported as niter == miter with fin_res >= tol, as the
+ *  reference does.
+ *
+ *  Threading: one CUDA stream per context; calls on one context must not
+ *  overlap.  Different contexts may be used from different threads.
+ * ========================================================================== */
+#ifndef TF_KRYLOV_H
+#define TF_KRYLOV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  64 and 72 are the codes the reference passes to
+ * Message % Error for an unknown solver (Solve_Native.f90:38) and an unknown
+ * preconditioner (Shared/Control_Mod/Native/Preconditioner_For_System_Matrix.f90:36). */
+enum tf_status {
+  TF_OK = 0,
+  TF_ERR_CUDA = 1,           /* a CUDA runtime call failed                       */
+  TF_ERR_OOM = 2,            /* device allocation failed or over memory budget   */
+  TF_ERR_ARG = 3,            /* bad argument (null pointer, size, index range)   */
+  TF_ERR_TIMEOUT = 4,        /* a bounded device-side wait gave up               */
+  TF_ERR_LAYOUT = 5,         /* CSR layout violates Matrix_Type's contract       */
+  TF_ERR_NO_DEVICE = 6,      /* no CUDA device / driver                          */
+  TF_ERR_BUSY = 7,           /* serving queue full or handle in use              */
+  TF_ERR_CANCELLED = 8,      /* request cancelled before it finished             */
+  TF_ERR_UNKNOWN_SOLVER = 64,
+  TF_ERR_UNKNOWN_PREC = 72
+};
+
+enum tf_solver { TF_SOLVER_CG = 0, TF_SOLVER_BICG = 1 };
+enum tf_prec { TF_PREC_NONE = 0, TF_PREC_JACOBI = 1, TF_PREC_ICC = 2 };
+
+typedef struct tf_ctx_s* tf_ctx;        /* device, stream, Krylov workspace   */
+typedef struct tf_matrix_s* tf_matrix;  /* device-resident CSR structure      */
+
+/* Human-readable text for a status code (static storage). */
+const char* tf_status_string(int status);
+
+/* Library version, e.g. "tfkrylov 0.1 sm_100a". */
+const char* tf_version(void);
+
+/* Context on CUDA device `device` (-1: current device).  Replaces the
+ * Work_Mod scratch arrays that Cg/Bicg connect (Cg.f90:44, Bicg.f90:45)
+ * and the Nat object made by Create_Native (Native_Mod/Create_Native.f90:2-25). */
+int tf_ctx_create(int device, tf_ctx* out);
+int tf_ctx_destroy(tf_ctx ctx);
+
+/* Upload the structure of one Matrix_Type (row, col, dia) once; values are
+ * passed per solve because Process assembles them on the host each time.
+ * Replaces Matrix_Mod/Create_Matrix.f90's result being visible to the
+ * solver.  n_cells = Grid % n_cells (nt), n_own = nt - n_buff_cells (ni),
+ * nnz = row(n_cells+1) - 1.  The arrays are copied; the caller keeps them. */
+int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own, int64_t nnz,
+                       const int* row, const int* col, const int* dia,
+                       tf_matrix* out);
+int tf_matrix_release(tf_matrix m);
+int tf_matrix_info(tf_matrix m, int* n_cells, int* n_own, int64_t* nnz,
+                   int* max_row_len);
+
+/* Solve A x = b.  Replaces Native_Type % Solve_Native (Solve_Native.f90:2-46)
+ * and so Cg.f90:2-257 / Bicg.f90:2-269.  val, x and b are host arrays of
+ * nnz, n_cells and n_cells doubles and are updated exactly as the reference
+ * updates them: x is overwritten with the solution, val and b come back as
+ * (v*fn)/fn where fn = 1/mean(diag) (Cg.f90:62-84, 245-250).  norm == NULL
+ * means the optional argument `norm` is absent (Fortran bind(C) passes NULL
+ * for an absent OPTIONAL).  niter/fin_res follow Cg.f90:101-123, 220-228. */
+int tf_solve(tf_ctx ctx, tf_matrix m, int solver, int prec, double* val,
+             double* x, double* b, int miter, int* niter, double tol,
+             double* fin_res, const double* norm);
+
+/* Same, with the solver and preconditioner given by name as in
+ * Solve_Native.f90:33-44 ('cg', 'bicg') and Prec_Form.f90:47-89 ('jacobi',
+ * 'icc', anything else = none).  The control-file spellings 'diagonal' and
+ * 'incomplete_cholesky' are mapped as Preconditioner_For_System_Matrix.f90:43-44
+ * maps them.  Unknown solver -> TF_ERR_UNKNOWN_SOLVER (the reference's 64). */
+int tf_solve_native(tf_ctx ctx, tf_matrix m, const char* solver,
+                    const char* prec, double* val, double* x, double* b,
+                    int miter, int* niter, double tol, double* fin_res,
+                    const double* norm);
+
+/* Same as tf_solve with val, x and b already in device memory (e.g. an
+ * OpenACC `host_data use_device` region).  Nothing crosses PCIe except the
+ * two result scalars. */
+int tf_solve_device(tf_ctx ctx, tf_matrix m, int solver, int prec,
+                    double* d_val, double* d_x, double* d_b, int miter,
+                    int* niter, double tol, double* fin_res,
+                    const double* norm);
+
+/* Per-iteration residual history of the last solve on ctx: hist[0] is the
+ * residual before the loop, hist[k] after iteration k, for k <= niter.
+ * Enabled by tf_ctx_set_history(ctx, 1) (off by default: it costs nothing
+ * on the device, one extra copy on the host). */
+int tf_ctx_set_history(tf_ctx ctx, int enable);
+int tf_last_history(tf_ctx ctx, double* hist, int cap, int* count);
+
+/* Pin (page-lock) a host array the caller will pass to tf_solve on every
+ * call, e.g. A % val, so its copies run at full PCIe/C2C bandwidth.
+ * Wraps cudaHostRegister / cudaHostUnregister. */
+int tf_host_pin(void* ptr, size_t bytes);
+int tf_host_unpin(void* ptr);
+
+/* ---------------------------------------------------------------------------
+ *  Building blocks exposed for testing and for callers that keep their own
+ *  Krylov loop.  All pointers are device pointers; vectors have n_cells
+ *  entries; val has nnz entries.  Each call is asynchronous on ctx's stream;
+ *  tf_ctx_sync waits for it.
+ * ------------------------------------------------------------------------- */
+/* q = A p over rows 1..n_own, in the row order and summation order of
+ * Cg.f90:177-185.  If pq != NULL, *pq (device) receives sum_i p_i q_i. */
+int tf_spmv(tf_ctx ctx, tf_matrix m, const double* d_val, const double* d_p,
+            double* d_q, double* d_pq);
+/* r = b - A x (Residual_Vector.f90:34-42). */
+int tf_residual(tf_ctx ctx, tf_matrix m, const double* d_val,
+                const double* d_b, const double* d_x, double* d_r);
+/* Normalized_Root_Mean_Square.f90:33-63 of r, on device; result to *d_out. */
+int tf_nrms(tf_ctx ctx, tf_matrix m, const double* d_val, const double* d_r,
+            const double* d_x, const double* norm, double* d_out);
+int tf_ctx_sync(tf_ctx ctx);
+/* The CUDA stream of ctx (a cudaStream_t), for callers that order their
+ * own work with it. */
+void* tf_ctx_stream(tf_ctx ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TF_KRYLOV_H */

@@ -1,0 +1,480 @@
+// tf_api.cu -- the C ABI (include/tf_krylov.h): contexts, matrix
+// registration, the Solve_Native drop-in and the building blocks.
+#include <cuda_runtime.h>
+#include <limits.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "tf_internal.h"
+#include "tf_tile.cuh"
+
+namespace {
+std::mutex g_err_mu;
+std::string g_last_err;
+}  // namespace
+
+void tf_set_last_cuda_error(cudaError_t e, const char* what, const char* file,
+                            int line) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  char buf[512];
+  snprintf(buf, sizeof buf, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e),
+           file, line);
+  g_last_err = buf;
+}
+
+extern "C" const char* tf_last_error_message(void) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  return g_last_err.c_str();
+}
+
+extern "C" const char* tf_status_string(int status) {
+  switch (status) {
+    case TF_OK: return "ok";
+    case TF_ERR_CUDA: return "CUDA runtime error";
+    case TF_ERR_OOM: return "out of device memory";
+    case TF_ERR_ARG: return "invalid argument";
+    case TF_ERR_TIMEOUT: return "bounded device wait timed out";
+    case TF_ERR_LAYOUT: return "CSR layout violates Matrix_Type contract";
+    case TF_ERR_NO_DEVICE: return "no CUDA device";
+    case TF_ERR_BUSY: return "busy";
+    case TF_ERR_CANCELLED: return "cancelled";
+    case TF_ERR_UNKNOWN_SOLVER: return "unknown native solver";
+    case TF_ERR_UNKNOWN_PREC: return "unknown preconditioner";
+    default: return "unknown status";
+  }
+}
+
+extern "C" const char* tf_version(void) { return "tfkrylov 0.1 sm_100a"; }
+
+// ---------------------------------------------------------------------------
+// Contexts
+// ---------------------------------------------------------------------------
+extern "C" int tf_ctx_create(int device, tf_ctx* out) {
+  if (!out) return TF_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return TF_ERR_NO_DEVICE;
+  }
+  if (device < 0) TF_CUDA_TRY(cudaGetDevice(&device));
+  if (device >= ndev) return TF_ERR_ARG;
+  TF_CUDA_TRY(cudaSetDevice(device));
+  tf_ctx_s* c = new tf_ctx_s();
+  c->device = device;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) {
+    c->sm_count = prop.multiProcessorCount;
+    c->l2_bytes = prop.l2CacheSize;
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    TF_CUDA_TRY(e);
+  }
+  *out = c;
+  return TF_OK;
+}
+
+extern "C" int tf_ctx_destroy(tf_ctx ctx) {
+  if (!ctx) return TF_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return TF_OK;
+}
+
+extern "C" int tf_ctx_sync(tf_ctx ctx) {
+  if (!ctx) return TF_ERR_ARG;
+  TF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return TF_OK;
+}
+
+extern "C" void* tf_ctx_stream(tf_ctx ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+extern "C" int tf_ctx_set_history(tf_ctx ctx, int enable) {
+  if (!ctx) return TF_ERR_ARG;
+  ctx->history = enable ? 1 : 0;
+  return TF_OK;
+}
+
+extern "C" int tf_last_history(tf_ctx ctx, double* hist, int cap, int* count) {
+  if (!ctx || !count || (cap > 0 && !hist)) return TF_ERR_ARG;
+  const int n = std::min(cap, ctx->last_count);
+  for (int i = 0; i < n; ++i) hist[i] = ctx->last_hist[i];
+  *count = ctx->last_count;
+  return TF_OK;
+}
+
+extern "C" int tf_host_pin(void* ptr, size_t bytes) {
+  if (!ptr || bytes == 0) return TF_ERR_ARG;
+  TF_CUDA_TRY(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+  return TF_OK;
+}
+
+extern "C" int tf_host_unpin(void* ptr) {
+  if (!ptr) return TF_ERR_ARG;
+  TF_CUDA_TRY(cudaHostUnregister(ptr));
+  return TF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Matrices
+// ---------------------------------------------------------------------------
+namespace {
+
+template <class T>
+int dev_alloc(T** p, size_t count) {
+  *p = nullptr;
+  TF_CUDA_TRY(cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T)));
+  TF_CUDA_TRY(cudaMemset(*p, 0, std::max<size_t>(count, 1) * sizeof(T)));
+  return TF_OK;
+}
+
+void free_matrix(tf_matrix_s* m) {
+  if (!m) return;
+  cudaSetDevice(m->ctx->device);
+  for (auto& g : m->graph)
+    if (g) cudaGraphExecDestroy(g);
+  void* ptrs[] = {m->d_row, m->d_col, m->d_dia, m->d_val, m->d_x, m->d_b,
+                  m->d_r, m->d_p, m->d_q, m->d_z, m->d_adiag, m->d_part,
+                  m->d_hist, m->d_state, m->d_params, m->d_lev_ptr, m->d_lev_rows};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (m->h_state) cudaFreeHost(m->h_state);
+  if (m->h_params) cudaFreeHost(m->h_params);
+  delete m;
+}
+
+// Largest nnz of any tile of `rows` consecutive rows among the first ni.
+int64_t max_tile_nnz(const std::vector<int>& row0, int ni, int rows) {
+  int64_t mx = 0;
+  for (int r0 = 0; r0 < ni; r0 += rows) {
+    const int r1 = std::min(r0 + rows, ni);
+    mx = std::max<int64_t>(mx, (int64_t)row0[r1] - row0[r0]);
+  }
+  return mx;
+}
+
+}  // namespace
+
+extern "C" int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own,
+                                  int64_t nnz, const int* row, const int* col,
+                                  const int* dia, tf_matrix* out) {
+  if (!ctx || !out) return TF_ERR_ARG;
+  *out = nullptr;
+  if (n_cells < 0 || n_own < 0 || n_own > n_cells || nnz < 0) return TF_ERR_ARG;
+  if (n_cells > 0 && (n_own < 1 || !row || !col || !dia)) return TF_ERR_ARG;
+  if (nnz > (int64_t)INT_MAX - 64) return TF_ERR_ARG;
+
+  // Validate the Matrix_Type contract (Create_Matrix.f90:87-119).
+  int max_len = 0, diag_first = 1;
+  if (n_cells > 0) {
+    if (row[0] != 1 || (int64_t)row[n_cells] - 1 != nnz) return TF_ERR_LAYOUT;
+    for (int i = 0; i < n_cells; ++i) {
+      if (row[i + 1] < row[i]) return TF_ERR_LAYOUT;
+      max_len = std::max(max_len, row[i + 1] - row[i]);
+      const int d = dia[i];
+      if (d < row[i] || d >= row[i + 1] || col[d - 1] != i + 1) return TF_ERR_LAYOUT;
+      if (col[row[i] - 1] != i + 1) diag_first = 0;
+    }
+    for (int64_t j = 0; j < nnz; ++j)
+      if (col[j] < 1 || col[j] > n_cells) return TF_ERR_LAYOUT;
+  }
+
+  TF_CUDA_TRY(cudaSetDevice(ctx->device));
+  tf_matrix_s* m = new tf_matrix_s();
+  m->ctx = ctx;
+  m->nt = n_cells;
+  m->ni = n_own;
+  m->nnz = nnz;
+  m->max_row_len = max_len;
+  m->diag_first = diag_first;
+
+  std::vector<int> row0((size_t)n_cells + 1 + 8, 0), col0((size_t)nnz + 8, 0),
+      dia0((size_t)n_cells + 8, 0);
+  if (n_cells > 0) {
+    for (int i = 0; i <= n_cells; ++i) row0[i] = row[i] - 1;
+    for (int i = n_cells + 1; i < (int)row0.size(); ++i) row0[i] = row0[n_cells];
+    for (int64_t j = 0; j < nnz; ++j) col0[j] = col[j] - 1;
+    for (int i = 0; i < n_cells; ++i) dia0[i] = dia[i] - 1;
+  }
+
+  const size_t nv = (size_t)n_cells + 8, nz = (size_t)nnz + 8;
+  int st = TF_OK;
+#define TRY_ALLOC(p, n)                          \
+  if (st == TF_OK) st = dev_alloc(&(p), (n));
+  TRY_ALLOC(m->d_row, row0.size());
+  TRY_ALLOC(m->d_col, nz);
+  TRY_ALLOC(m->d_dia, nv);
+  TRY_ALLOC(m->d_val, nz);
+  TRY_ALLOC(m->d_x, nv);
+  TRY_ALLOC(m->d_b, nv);
+  TRY_ALLOC(m->d_r, nv);
+  TRY_ALLOC(m->d_p, nv);
+  TRY_ALLOC(m->d_q, nv);
+  TRY_ALLOC(m->d_adiag, nv);
+  TRY_ALLOC(m->d_part, (size_t)8 * tf::kMaxBlocks + 16);
+  TRY_ALLOC(m->d_state, 1);
+  TRY_ALLOC(m->d_params, 1);
+#undef TRY_ALLOC
+  if (st == TF_OK) {
+    cudaError_t e = cudaMallocHost((void**)&m->h_state, sizeof(tf::SolveState));
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&m->h_params, sizeof(tf::SolveParams));
+    if (e != cudaSuccess) {
+      tf_set_last_cuda_error(e, "cudaMallocHost", __FILE__, __LINE__);
+      st = TF_ERR_OOM;
+    }
+  }
+  if (st == TF_OK) {
+    cudaError_t e = cudaMemcpy(m->d_row, row0.data(), row0.size() * sizeof(int),
+                               cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(m->d_col, col0.data(), col0.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(m->d_dia, dia0.data(), dia0.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      tf_set_last_cuda_error(e, "cudaMemcpy(structure)", __FILE__, __LINE__);
+      st = TF_ERR_CUDA;
+    }
+  }
+  if (st == TF_OK) {
+    // Tile configuration: the widest tile whose nnz fits its stage.
+    m->tile_cfg = tf::kTileNone;
+    for (int c = 0; c < 3 && n_cells > 0; ++c) {
+      if (max_tile_nnz(row0, n_own, tf::kTileRows[c]) <= tf::kTileNnzCap[c]) {
+        m->tile_cfg = c;
+        break;
+      }
+    }
+    if (const char* f = getenv("TF_TILE_CFG")) {
+      const int c = atoi(f);
+      if (c >= 0 && c <= 3 &&
+          (c == 3 || max_tile_nnz(row0, n_own, tf::kTileRows[c]) <= tf::kTileNnzCap[c]))
+        m->tile_cfg = c;
+    }
+    if (n_cells > 0) st = tf_fp64_prepare(m);
+  }
+  if (st == TF_OK && n_cells > 0 && getenv("TF_NO_ICC_BUILD") == nullptr) {
+    // nothing: the ICC level schedule is built on first ICC solve
+  }
+  if (st != TF_OK) {
+    free_matrix(m);
+    return st;
+  }
+  *out = m;
+  return TF_OK;
+}
+
+extern "C" int tf_matrix_release(tf_matrix m) {
+  if (!m) return TF_ERR_ARG;
+  cudaSetDevice(m->ctx->device);
+  cudaStreamSynchronize(m->ctx->stream);
+  free_matrix(m);
+  return TF_OK;
+}
+
+extern "C" int tf_matrix_info(tf_matrix m, int* n_cells, int* n_own,
+                              int64_t* nnz, int* max_row_len) {
+  if (!m) return TF_ERR_ARG;
+  if (n_cells) *n_cells = m->nt;
+  if (n_own) *n_own = m->ni;
+  if (nnz) *nnz = m->nnz;
+  if (max_row_len) *max_row_len = m->max_row_len;
+  return TF_OK;
+}
+
+extern "C" int tf_matrix_tile_config(tf_matrix m) { return m ? m->tile_cfg : -1; }
+
+// ---------------------------------------------------------------------------
+// Solves
+// ---------------------------------------------------------------------------
+namespace {
+
+int ensure_hist(tf_matrix_s* m, int need) {
+  if (m->hist_cap >= need) return TF_OK;
+  if (m->d_hist) cudaFree(m->d_hist);
+  m->d_hist = nullptr;
+  m->hist_cap = 0;
+  TF_CUDA_TRY(cudaMalloc((void**)&m->d_hist, (size_t)need * sizeof(double)));
+  m->hist_cap = need;
+  return TF_OK;
+}
+
+int run_solve_core(tf_matrix_s* m, int prec, int miter, double tol,
+                   const double* norm) {
+  tf_ctx_s* c = m->ctx;
+  tf::SolveParams* hp = m->h_params;
+  hp->tol = tol;
+  hp->norm = norm ? *norm : 0.0;
+  hp->has_norm = norm ? 1 : 0;
+  hp->miter = miter;
+  hp->hist = nullptr;
+  hp->hist_cap = 0;
+  if (c->history && miter >= 0) {
+    int st = ensure_hist(m, miter + 1);
+    if (st != TF_OK) return st;
+    hp->hist = m->d_hist;
+    hp->hist_cap = miter + 1;
+  }
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_params, hp, sizeof(*hp), cudaMemcpyHostToDevice, c->stream));
+  int st = (prec == tf::kPrecIcc) ? tf_icc_run_solve(m) : tf_fp64_run(m, prec);
+  if (st != TF_OK) return st;
+  TF_CUDA_TRY(cudaMemcpyAsync(m->h_state, m->d_state, sizeof(tf::SolveState),
+                              cudaMemcpyDeviceToHost, c->stream));
+  return TF_OK;
+}
+
+int finish_solve(tf_matrix_s* m, int* niter, double* fin_res) {
+  tf_ctx_s* c = m->ctx;
+  TF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const tf::SolveState& s = *m->h_state;
+  if (s.status != 0) return s.status;
+  *niter = s.niter;
+  *fin_res = s.res;
+  c->last_count = 0;
+  if (c->history && m->hist_cap > 0) {
+    const bool early_b = s.bnrm2 < m->h_params->tol;
+    const int cnt = early_b ? 0 : std::min(s.niter + 1, m->hist_cap);
+    c->last_hist.resize(std::max(cnt, 1));
+    if (cnt > 0)
+      TF_CUDA_TRY(cudaMemcpy(c->last_hist.data(), m->d_hist, cnt * sizeof(double),
+                             cudaMemcpyDeviceToHost));
+    c->last_count = cnt;
+  }
+  return TF_OK;
+}
+
+int check_solve_args(tf_ctx ctx, tf_matrix m, int solver, int prec, int* niter,
+                     double* fin_res) {
+  if (!ctx || !m || m->ctx != ctx || !niter || !fin_res) return TF_ERR_ARG;
+  if (solver != TF_SOLVER_CG && solver != TF_SOLVER_BICG) return TF_ERR_UNKNOWN_SOLVER;
+  if (prec < TF_PREC_NONE || prec > TF_PREC_ICC) return TF_ERR_UNKNOWN_PREC;
+  return TF_OK;
+}
+
+}  // namespace
+
+extern "C" int tf_solve(tf_ctx ctx, tf_matrix m, int solver, int prec,
+                        double* val, double* x, double* b, int miter,
+                        int* niter, double tol, double* fin_res,
+                        const double* norm) {
+  int st = check_solve_args(ctx, m, solver, prec, niter, fin_res);
+  if (st != TF_OK) return st;
+  if (m->nt == 0) {
+    *niter = 0;
+    *fin_res = 0.0;
+    return TF_OK;
+  }
+  if (!val || !x || !b) return TF_ERR_ARG;
+  std::lock_guard<std::mutex> lk(m->mu);
+  TF_CUDA_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const size_t vb = (size_t)m->nnz * sizeof(double), nb = (size_t)m->nt * sizeof(double);
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_val, val, vb, cudaMemcpyHostToDevice, s));
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_x, x, nb, cudaMemcpyHostToDevice, s));
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_b, b, nb, cudaMemcpyHostToDevice, s));
+  st = run_solve_core(m, prec, miter, tol, norm);
+  if (st != TF_OK) {
+    cudaStreamSynchronize(s);
+    return st;
+  }
+  TF_CUDA_TRY(cudaMemcpyAsync(val, m->d_val, vb, cudaMemcpyDeviceToHost, s));
+  TF_CUDA_TRY(cudaMemcpyAsync(x, m->d_x, nb, cudaMemcpyDeviceToHost, s));
+  TF_CUDA_TRY(cudaMemcpyAsync(b, m->d_b, nb, cudaMemcpyDeviceToHost, s));
+  return finish_solve(m, niter, fin_res);
+}
+
+extern "C" int tf_solve_device(tf_ctx ctx, tf_matrix m, int solver, int prec,
+                               double* d_val, double* d_x, double* d_b,
+                               int miter, int* niter, double tol,
+                               double* fin_res, const double* norm) {
+  int st = check_solve_args(ctx, m, solver, prec, niter, fin_res);
+  if (st != TF_OK) return st;
+  if (m->nt == 0) {
+    *niter = 0;
+    *fin_res = 0.0;
+    return TF_OK;
+  }
+  if (!d_val || !d_x || !d_b) return TF_ERR_ARG;
+  std::lock_guard<std::mutex> lk(m->mu);
+  TF_CUDA_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const size_t vb = (size_t)m->nnz * sizeof(double), nb = (size_t)m->nt * sizeof(double);
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_val, d_val, vb, cudaMemcpyDeviceToDevice, s));
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_x, d_x, nb, cudaMemcpyDeviceToDevice, s));
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_b, d_b, nb, cudaMemcpyDeviceToDevice, s));
+  st = run_solve_core(m, prec, miter, tol, norm);
+  if (st != TF_OK) {
+    cudaStreamSynchronize(s);
+    return st;
+  }
+  TF_CUDA_TRY(cudaMemcpyAsync(d_val, m->d_val, vb, cudaMemcpyDeviceToDevice, s));
+  TF_CUDA_TRY(cudaMemcpyAsync(d_x, m->d_x, nb, cudaMemcpyDeviceToDevice, s));
+  TF_CUDA_TRY(cudaMemcpyAsync(d_b, m->d_b, nb, cudaMemcpyDeviceToDevice, s));
+  return finish_solve(m, niter, fin_res);
+}
+
+namespace {
+// Fortran-style comparison: trailing blanks are not significant.
+bool name_is(const char* s, const char* want) {
+  size_t n = strlen(s);
+  while (n > 0 && s[n - 1] == ' ') --n;
+  return n == strlen(want) && strncmp(s, want, n) == 0;
+}
+}  // namespace
+
+extern "C" int tf_solve_native(tf_ctx ctx, tf_matrix m, const char* solver,
+                               const char* prec, double* val, double* x,
+                               double* b, int miter, int* niter, double tol,
+                               double* fin_res, const double* norm) {
+  if (!solver || !prec) return TF_ERR_ARG;
+  int s;
+  if (name_is(solver, "bicg")) s = TF_SOLVER_BICG;        // Solve_Native.f90:33
+  else if (name_is(solver, "cg")) s = TF_SOLVER_CG;       // Solve_Native.f90:35
+  else return TF_ERR_UNKNOWN_SOLVER;                      // Solve_Native.f90:38
+  int p;
+  if (name_is(prec, "jacobi") || name_is(prec, "diagonal")) p = TF_PREC_JACOBI;
+  else if (name_is(prec, "icc") || name_is(prec, "incomplete_cholesky")) p = TF_PREC_ICC;
+  else if (name_is(prec, "none")) p = TF_PREC_NONE;
+  else return TF_ERR_UNKNOWN_PREC;
+  return tf_solve(ctx, m, s, p, val, x, b, miter, niter, tol, fin_res, norm);
+}
+
+// ---------------------------------------------------------------------------
+// Building blocks
+// ---------------------------------------------------------------------------
+extern "C" int tf_spmv(tf_ctx ctx, tf_matrix m, const double* d_val,
+                       const double* d_p, double* d_q, double* d_pq) {
+  if (!ctx || !m || m->ctx != ctx) return TF_ERR_ARG;
+  if (m->nt == 0) return TF_OK;
+  if (!d_val || !d_p || !d_q) return TF_ERR_ARG;
+  if (((uintptr_t)d_val & 15) != 0) return TF_ERR_ARG;  // bulk copies need 16 B
+  TF_CUDA_TRY(cudaSetDevice(ctx->device));
+  return tf_fp64_spmv(m, d_val, d_p, d_q, d_pq);
+}
+
+extern "C" int tf_residual(tf_ctx ctx, tf_matrix m, const double* d_val,
+                           const double* d_b, const double* d_x, double* d_r) {
+  if (!ctx || !m || m->ctx != ctx) return TF_ERR_ARG;
+  if (m->nt == 0) return TF_OK;
+  if (!d_val || !d_b || !d_x || !d_r) return TF_ERR_ARG;
+  if (((uintptr_t)d_val & 15) != 0) return TF_ERR_ARG;
+  TF_CUDA_TRY(cudaSetDevice(ctx->device));
+  return tf_fp64_residual(m, d_val, d_b, d_x, d_r);
+}
+
+extern "C" int tf_nrms(tf_ctx ctx, tf_matrix m, const double* d_val,
+                       const double* d_r, const double* d_x,
+                       const double* norm, double* d_out) {
+  if (!ctx || !m || m->ctx != ctx || !d_val || !d_r || !d_x || !d_out) return TF_ERR_ARG;
+  if (m->nt == 0) return TF_ERR_ARG;
+  TF_CUDA_TRY(cudaSetDevice(ctx->device));
+  return tf_fp64_nrms(m, d_val, d_r, d_x, norm ? 1 : 0, norm ? *norm : 0.0, d_out);
+}

@@ -1,0 +1,745 @@
+// tf_fp64.cu -- FP64 drop-in for Native_Mod's Cg and Bicg (Jacobi / none /
+// ICC preconditioning) on one B200.
+//
+// One solve is one CUDA graph:
+//
+//   k_diag -> k_scale -> k_residual -> WHILE(cond) { k_pupdate -> k_spmv_alpha
+//                                                     -> k_update [-> ICC z] }
+//          -> k_unscale
+//
+// k_diag/k_scale      normalisation of Cg.f90:62-84 (+ NRMS(b), :95-104)
+// k_residual          r = b - A x and NRMS(r) (:109-123), rho of iteration 1
+// k_pupdate           z = M^-1 r (Prec_Solve) and p = z + beta p (:145-171)
+// k_spmv_alpha        q = A p, p.q, alfa = rho/(p.q)          (:176-198)
+// k_update            x += alfa p, r -= alfa q, NRMS(r,x), next rho, the
+//                     convergence test (:204-222) and the loop condition
+// k_unscale           de-normalisation (:245-250)
+//
+// Convergence is decided on the device: k_update's last CTA writes the
+// WHILE node's condition with cudaGraphSetConditional, so a whole solve is
+// one graph launch with no host round trip per iteration.
+//
+// Bicg (Bicg.f90) is served by the same graph: its shadow sequence starts as
+// r2 = r1 (:129-133) and is updated by exactly the operations applied to the
+// primary sequence with A in place of A^T (:143-145, 178-181), so r2, z2, p2
+// and q2 equal r1, z1, p1 and q1 bit for bit at every iteration, rho = z1.r1
+// and alfa's denominator p2.q1 = p1.q1.  Computing the shadow would double
+// the vector traffic and change no output.
+//
+// Rounding: every product and sum that the reference writes as a*b+c is
+// issued as __dmul_rn then __dadd_rn (no FMA contraction), matching the
+// reference's gnu build (-O3, x86-64 baseline, no FMA).  Row sums of the
+// SpMV and of r = b - A x are accumulated in storage order, so q and r agree
+// with the reference bit for bit given the same inputs; only the grid-wide
+// dot products are summed in a different (fixed, deterministic) order.
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include <algorithm>
+
+#include "tf_internal.h"
+#include "tf_tile.cuh"
+
+namespace tf {
+
+struct VecArgs {
+  int nt, ni;
+  long long nnz;
+  const int* dia;
+  double* val;
+  double* x;
+  double* b;
+  double* r;
+  double* p;
+  double* q;
+  double* z;
+  double* adiag;
+  double* part;
+  SolveState* st;
+  const SolveParams* prm;
+  cudaGraphConditionalHandle cond;
+  int use_cond;
+};
+
+__device__ __forceinline__ void set_cond(const VecArgs& a, int v) {
+  if (a.use_cond) cudaGraphSetConditional(a.cond, (unsigned)v);
+}
+
+// Fortran min/max as the reference's loops evaluate them.
+__device__ __forceinline__ double fmin_ref(double a, double b) {
+  return (b < a) ? b : a;
+}
+__device__ __forceinline__ double fmax_ref(double a, double b) {
+  return (b > a) ? b : a;
+}
+
+// ---------------------------------------------------------------------------
+// Normalisation (Cg.f90:62-76): adiag = diagonal, sum_a, fn = 1/(sum_a/ni)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_diag(VecArgs a) {
+  __shared__ double scratch[32];
+  double s = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.ni; i += stride) {
+    const double d = a.val[a.dia[i]];
+    a.adiag[i] = d;
+    s = __dadd_rn(s, d);
+  }
+  s = block_red<kSum>(s, scratch);
+  double v[1] = {s};
+  const int ops[1] = {kSum};
+  if (grid_reduce_last<1>(v, ops, a.part, &a.st->counter[kCntDiag], scratch) &&
+      threadIdx.x == 0) {
+    SolveState* st = a.st;
+    st->sum_a = v[0];
+    const double mean = __ddiv_rn(v[0], (double)a.ni);
+    st->fn = __ddiv_rn(1.0, mean);
+    st->done = 0;
+    st->iter = 0;
+    st->niter = 0;
+    st->status = 0;
+    st->res = 0.0;
+    st->rho = 0.0;
+    st->rho_old = 0.0;
+    st->alpha = 0.0;
+  }
+}
+
+// val *= fn, b *= fn (Cg.f90:77-84); adiag *= fn; NRMS(b) (Cg.f90:95-104)
+__global__ void __launch_bounds__(256) k_scale(VecArgs a) {
+  __shared__ double scratch[32];
+  const double fn = a.st->fn;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll 4
+  for (long long j = tid; j < a.nnz; j += stride) a.val[j] = __dmul_rn(a.val[j], fn);
+  const int has_norm = a.prm->has_norm;
+  double s = 0.0, mn = kHuge, mx = -kHuge;
+  for (long long i = tid; i < a.nt; i += stride) {
+    const double bi = __dmul_rn(a.b[i], fn);
+    a.b[i] = bi;
+    if (i < a.ni) {
+      const double ai = __dmul_rn(a.adiag[i], fn);
+      a.adiag[i] = ai;
+      s = __dadd_rn(s, nrms_term(bi, ai));
+      if (!has_norm) {
+        const double xi = a.x[i];
+        mn = fmin_ref(mn, xi);
+        mx = fmax_ref(mx, xi);
+      }
+    }
+  }
+  s = block_red<kSum>(s, scratch);
+  mn = block_red<kMin>(mn, scratch);
+  mx = block_red<kMax>(mx, scratch);
+  double v[3] = {s, mn, mx};
+  const int ops[3] = {kSum, kMin, kMax};
+  if (grid_reduce_last<3>(v, ops, a.part, &a.st->counter[kCntScale], scratch) &&
+      threadIdx.x == 0) {
+    SolveState* st = a.st;
+    st->xmin = v[1];
+    st->xmax = v[2];
+    const double bnrm2 = nrms_finish(v[0], has_norm, a.prm->norm, v[1], v[2]);
+    st->bnrm2 = bnrm2;
+    if (bnrm2 < a.prm->tol) {   // Cg.f90:101-104: iter = 0, res stays 0.0
+      st->done = 1;
+      st->niter = 0;
+      st->res = 0.0;
+      set_cond(a, 0);
+    }
+  }
+}
+
+// val /= fn, b /= fn (Cg.f90:245-250)
+__global__ void __launch_bounds__(256) k_unscale(VecArgs a) {
+  const double fn = a.st->fn;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll 4
+  for (long long j = tid; j < a.nnz; j += stride) a.val[j] = __ddiv_rn(a.val[j], fn);
+  for (long long i = tid; i < a.nt; i += stride) a.b[i] = __ddiv_rn(a.b[i], fn);
+}
+
+// ---------------------------------------------------------------------------
+// Per-row operators for the tile streamer
+// ---------------------------------------------------------------------------
+// q_i = sum_j a_ij p_j (Cg.f90:179-183), accumulates p_i q_i (:190-195)
+struct OpSpmvDot {
+  const double* __restrict__ p;
+  double* __restrict__ q;
+  double pq;
+  __device__ __forceinline__ void operator()(int i, const double* v,
+                                             const int* c, int len) {
+    double acc = 0.0;
+#pragma unroll 1
+    for (int k0 = 0; k0 < len; k0 += 8) {
+      double pv[8], vv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (k0 + u < len) {
+          vv[u] = v[k0 + u];
+          pv[u] = __ldg(p + c[k0 + u]);
+        }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (k0 + u < len) acc = __dadd_rn(acc, __dmul_rn(vv[u], pv[u]));
+    }
+    q[i] = acc;
+    pq = __dadd_rn(pq, __dmul_rn(__ldg(p + i), acc));
+  }
+};
+
+// r_i = b_i - sum_j a_ij x_j (Residual_Vector.f90:35-41), accumulates the
+// NRMS term and rho = z.r for Jacobi / none.
+template <int PREC>
+struct OpResidual {
+  const double* __restrict__ x;
+  const double* __restrict__ b;
+  double* __restrict__ r;
+  const double* __restrict__ adiag;
+  double s, rho;
+  __device__ __forceinline__ void operator()(int i, const double* v,
+                                             const int* c, int len) {
+    double acc = b[i];
+#pragma unroll 1
+    for (int k0 = 0; k0 < len; k0 += 8) {
+      double xv[8], vv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (k0 + u < len) {
+          vv[u] = v[k0 + u];
+          xv[u] = __ldg(x + c[k0 + u]);
+        }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (k0 + u < len) acc = __dsub_rn(acc, __dmul_rn(vv[u], xv[u]));
+    }
+    r[i] = acc;
+    const double ai = adiag[i];
+    s = __dadd_rn(s, nrms_term(acc, ai));
+    if (PREC == kPrecJacobi) {
+      const double zi = __dmul_rn(acc, __drcp_rn(ai));
+      rho = __dadd_rn(rho, __dmul_rn(zi, acc));
+    } else if (PREC == kPrecNone) {
+      rho = __dadd_rn(rho, __dmul_rn(acc, acc));
+    }
+  }
+};
+
+struct SpArgs {
+  const int* row;
+  const int* col;
+  const double* val;
+  int nrows;
+  VecArgs v;
+  double* out_scalar;  // building-block mode: receives the dot product
+};
+
+// Rows through shared-memory tiles (CFG < kTileNone) or straight from
+// global memory (kTileNone: rows too long for any tile).
+template <int CFG, class Op>
+__device__ __forceinline__ bool run_rows(const SpArgs& a, Op& op) {
+  if constexpr (CFG == kTileNone) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nrows; i += stride) {
+      const int js = a.row[i], je = a.row[i + 1];
+      op(i, a.val + js, a.col + js, je - js);
+    }
+    return true;
+  } else {
+    return stream_tiles<kTileRows[CFG], kTileNnzCap[CFG], double, 2>(
+        a.row, a.col, a.val, a.nrows, op);
+  }
+}
+
+template <int CFG>
+constexpr int cfg_threads() { return CFG == kTileNone ? 256 : kTileRows[CFG]; }
+
+__device__ __forceinline__ void flag_timeout(SolveState* st) {
+  if (st) atomicExch(&st->status, (int)TF_ERR_TIMEOUT);
+}
+
+// r = b - A x, NRMS(r) (Cg.f90:109-123), rho of iteration 1.
+template <int CFG, int PREC>
+__global__ void __launch_bounds__(cfg_threads<CFG>()) k_residual(SpArgs a) {
+  __shared__ double scratch[32];
+  SolveState* st = a.v.st;
+  if (st && st->done) return;
+  OpResidual<PREC> op{a.v.x, a.v.b, a.v.r, a.v.adiag, 0.0, 0.0};
+  if (!run_rows<CFG>(a, op) && threadIdx.x == 0) flag_timeout(st);
+  double v[2] = {block_red<kSum>(op.s, scratch), block_red<kSum>(op.rho, scratch)};
+  const int ops[2] = {kSum, kSum};
+  unsigned* cnt = st ? &st->counter[kCntResid] : reinterpret_cast<unsigned*>(a.out_scalar + 1);
+  if (grid_reduce_last<2>(v, ops, a.v.part, cnt, scratch) && threadIdx.x == 0) {
+    if (!st) return;
+    const SolveParams* prm = a.v.prm;
+    const double res = nrms_finish(v[0], prm->has_norm, prm->norm, st->xmin, st->xmax);
+    st->res = res;
+    if (prm->hist && prm->hist_cap > 0) prm->hist[0] = res;
+    if (st->status != 0 || res < prm->tol || prm->miter < 1) {
+      st->done = 1;   // Cg.f90:120-123 (iter = 0), or a zero-trip loop
+      st->niter = 0;
+      set_cond(a.v, 0);
+    } else {
+      if (PREC != kPrecIcc) st->rho = v[1];
+      st->iter = 1;
+      set_cond(a.v, 1);
+    }
+  }
+}
+
+// z = M^-1 r (Prec_Solve.f90:44-49 / :97-102) and p = z + beta p
+// (Cg.f90:158-171).  ICC reads z from the triangular solves.
+template <int PREC>
+__global__ void __launch_bounds__(256) k_pupdate(VecArgs a) {
+  const SolveState* st = a.st;
+  if (st->done) return;
+  const int k = st->iter;
+  const double beta = (k == 1) ? 0.0 : __ddiv_rn(st->rho, st->rho_old);
+  const int stride = gridDim.x * blockDim.x;
+#pragma unroll 4
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.ni; i += stride) {
+    double zi;
+    if (PREC == kPrecJacobi) zi = __dmul_rn(a.r[i], __drcp_rn(a.adiag[i]));
+    else if (PREC == kPrecNone) zi = a.r[i];
+    else zi = a.z[i];
+    a.p[i] = (k == 1) ? zi : __dadd_rn(zi, __dmul_rn(beta, a.p[i]));
+  }
+}
+
+// q = A p, p.q, alfa = rho / p.q (Cg.f90:176-198)
+template <int CFG>
+__global__ void __launch_bounds__(cfg_threads<CFG>()) k_spmv_alpha(SpArgs a) {
+  __shared__ double scratch[32];
+  SolveState* st = a.v.st;
+  if (st && st->done) return;
+  OpSpmvDot op{a.v.p, a.v.q, 0.0};
+  if (!run_rows<CFG>(a, op) && threadIdx.x == 0) flag_timeout(st);
+  double v[1] = {block_red<kSum>(op.pq, scratch)};
+  const int ops[1] = {kSum};
+  unsigned* cnt = st ? &st->counter[kCntSpmv] : reinterpret_cast<unsigned*>(a.out_scalar + 1);
+  if (grid_reduce_last<1>(v, ops, a.v.part, cnt, scratch) && threadIdx.x == 0) {
+    if (a.out_scalar) a.out_scalar[0] = v[0];
+    if (st) {
+      st->pq = v[0];
+      st->alpha = __ddiv_rn(st->rho, v[0]);
+    }
+  }
+}
+
+// x += alfa p; r -= alfa q (Cg.f90:204-209); NRMS(r, x) and the test
+// (:214-222); rho for the next iteration (Jacobi / none).
+template <int PREC>
+__global__ void __launch_bounds__(256) k_update(VecArgs a) {
+  __shared__ double scratch[32];
+  SolveState* st = a.st;
+  if (st->done) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(a, 0);
+    return;
+  }
+  const double alpha = st->alpha;
+  const SolveParams* prm = a.prm;
+  const int has_norm = prm->has_norm;
+  double s = 0.0, rho = 0.0, mn = kHuge, mx = -kHuge;
+  const int stride = gridDim.x * blockDim.x;
+#pragma unroll 2
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.ni; i += stride) {
+    const double xi = __dadd_rn(a.x[i], __dmul_rn(alpha, a.p[i]));
+    const double ri = __dsub_rn(a.r[i], __dmul_rn(alpha, a.q[i]));
+    a.x[i] = xi;
+    a.r[i] = ri;
+    const double ai = a.adiag[i];
+    s = __dadd_rn(s, nrms_term(ri, ai));
+    if (PREC == kPrecJacobi) {
+      const double zi = __dmul_rn(ri, __drcp_rn(ai));
+      rho = __dadd_rn(rho, __dmul_rn(zi, ri));
+    } else if (PREC == kPrecNone) {
+      rho = __dadd_rn(rho, __dmul_rn(ri, ri));
+    }
+    if (!has_norm) {
+      mn = fmin_ref(mn, xi);
+      mx = fmax_ref(mx, xi);
+    }
+  }
+  double v[4] = {block_red<kSum>(s, scratch), block_red<kSum>(rho, scratch),
+                 block_red<kMin>(mn, scratch), block_red<kMax>(mx, scratch)};
+  const int ops[4] = {kSum, kSum, kMin, kMax};
+  if (grid_reduce_last<4>(v, ops, a.part, &st->counter[kCntUpdate], scratch) &&
+      threadIdx.x == 0) {
+    const double res = nrms_finish(v[0], has_norm, prm->norm, v[2], v[3]);
+    st->res = res;
+    const int k = st->iter;
+    if (prm->hist && k < prm->hist_cap) prm->hist[k] = res;
+    if (st->status != 0) {
+      st->done = 1;
+      st->niter = k;
+    } else if (res < prm->tol) {         // Cg.f90:220
+      st->done = 1;
+      st->niter = k;
+    } else if (k >= prm->miter) {        // loop exhausted: niter = miter
+      st->done = 1;
+      st->niter = prm->miter;
+    } else {
+      if (PREC != kPrecIcc) {            // Cg.f90:222 and :150-156
+        st->rho_old = st->rho;
+        st->rho = v[1];
+      }
+      st->iter = k + 1;
+    }
+    set_cond(a, st->done ? 0 : 1);
+  }
+}
+
+}  // namespace tf
+
+using namespace tf;
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace {
+
+template <int CFG>
+size_t cfg_smem() {
+  if constexpr (CFG == kTileNone) return 0;
+  else return TileLayout<kTileRows[CFG], kTileNnzCap[CFG], double, 2>::kSmemBytes;
+}
+
+template <int CFG, int PREC>
+int set_attrs_cfg() {
+  const size_t sm = cfg_smem<CFG>();
+  if (sm > 48 * 1024) {
+    TF_CUDA_TRY(cudaFuncSetAttribute(k_residual<CFG, PREC>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    TF_CUDA_TRY(cudaFuncSetAttribute(k_spmv_alpha<CFG>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  }
+  return TF_OK;
+}
+
+VecArgs make_vec_args(tf_matrix_s* m) {
+  VecArgs a{};
+  a.nt = m->nt;
+  a.ni = m->ni;
+  a.nnz = (long long)m->nnz;
+  a.dia = m->d_dia;
+  a.val = m->d_val;
+  a.x = m->d_x;
+  a.b = m->d_b;
+  a.r = m->d_r;
+  a.p = m->d_p;
+  a.q = m->d_q;
+  a.z = m->d_z;
+  a.adiag = m->d_adiag;
+  a.part = m->d_part;
+  a.st = m->d_state;
+  a.prm = m->d_params;
+  a.cond = 0;
+  a.use_cond = 0;
+  return a;
+}
+
+SpArgs make_sp_args(tf_matrix_s* m, const VecArgs& v) {
+  SpArgs s{};
+  s.row = m->d_row;
+  s.col = m->d_col;
+  s.val = m->d_val;
+  s.nrows = m->ni;
+  s.v = v;
+  s.out_scalar = nullptr;
+  return s;
+}
+
+struct NodeBuilder {
+  cudaGraph_t g;
+  int status = TF_OK;
+  cudaGraphNode_t add(const void* fn, dim3 grid, dim3 block, size_t smem,
+                      void** args, cudaGraphNode_t dep) {
+    if (status != TF_OK) return nullptr;
+    cudaKernelNodeParams p{};
+    p.func = const_cast<void*>(fn);
+    p.gridDim = grid;
+    p.blockDim = block;
+    p.sharedMemBytes = (unsigned)smem;
+    p.kernelParams = args;
+    p.extra = nullptr;
+    cudaGraphNode_t node = nullptr;
+    cudaError_t e = cudaGraphAddKernelNode(&node, g, dep ? &dep : nullptr, dep ? 1 : 0, &p);
+    if (e != cudaSuccess) {
+      tf_set_last_cuda_error(e, "cudaGraphAddKernelNode", __FILE__, __LINE__);
+      status = TF_ERR_CUDA;
+    }
+    return node;
+  }
+};
+
+template <int CFG, int PREC>
+int build_graph_t(tf_matrix_s* m, cudaGraphExec_t* out) {
+  int st = set_attrs_cfg<CFG, PREC>();
+  if (st != TF_OK) return st;
+  cudaGraph_t g = nullptr;
+  TF_CUDA_TRY(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h = 0;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    TF_CUDA_TRY(e);
+  }
+  VecArgs va = make_vec_args(m);
+  va.cond = h;
+  va.use_cond = 1;
+  SpArgs sa = make_sp_args(m, va);
+  const dim3 vb(256), vg(m->vec_grid);
+  const dim3 sb(cfg_threads<CFG>()), sg(m->spmv_grid);
+  const size_t ssm = cfg_smem<CFG>();
+
+  NodeBuilder nb{g};
+  void* vargs[] = {&va};
+  void* sargs[] = {&sa};
+  cudaGraphNode_t n1 = nb.add((const void*)k_diag, vg, vb, 0, vargs, nullptr);
+  cudaGraphNode_t n2 = nb.add((const void*)k_scale, vg, vb, 0, vargs, n1);
+  cudaGraphNode_t n3 = nb.add((const void*)k_residual<CFG, PREC>, sg, sb, ssm, sargs, n2);
+  cudaGraphNode_t last = n3;
+  cudaGraphNode_t cnode = nullptr;
+  if (nb.status == TF_OK) {
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&cnode, g, &last, 1, &cp);
+    if (e != cudaSuccess) {
+      tf_set_last_cuda_error(e, "cudaGraphAddNode(conditional)", __FILE__, __LINE__);
+      nb.status = TF_ERR_CUDA;
+    } else {
+      NodeBuilder body{cp.conditional.phGraph_out[0]};
+      cudaGraphNode_t b1 = body.add((const void*)k_pupdate<PREC>, vg, vb, 0, vargs, nullptr);
+      cudaGraphNode_t b2 = body.add((const void*)k_spmv_alpha<CFG>, sg, sb, ssm, sargs, b1);
+      body.add((const void*)k_update<PREC>, vg, vb, 0, vargs, b2);
+      if (body.status != TF_OK) nb.status = body.status;
+    }
+  }
+  nb.add((const void*)k_unscale, vg, vb, 0, vargs, cnode);
+  if (nb.status != TF_OK) {
+    cudaGraphDestroy(g);
+    return nb.status;
+  }
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  TF_CUDA_TRY(e);
+  return TF_OK;
+}
+
+template <int PREC>
+int build_graph_p(tf_matrix_s* m, cudaGraphExec_t* out) {
+  switch (m->tile_cfg) {
+    case kTile512: return build_graph_t<kTile512, PREC>(m, out);
+    case kTile256: return build_graph_t<kTile256, PREC>(m, out);
+    case kTile128: return build_graph_t<kTile128, PREC>(m, out);
+    default: return build_graph_t<kTileNone, PREC>(m, out);
+  }
+}
+
+template <int CFG>
+int occupancy_grid(tf_matrix_s* m, const void* fn, int threads, size_t smem,
+                   int nrows, int* grid) {
+  int per_sm = 0;
+  TF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+  if (per_sm < 1) per_sm = 1;
+  int units = (CFG == kTileNone) ? (nrows + threads - 1) / threads
+                                 : (nrows + kTileRows[CFG > 2 ? 0 : CFG] - 1) / kTileRows[CFG > 2 ? 0 : CFG];
+  int g = std::min(units, per_sm * m->ctx->sm_count);
+  g = std::max(1, std::min(g, kMaxBlocks));
+  *grid = g;
+  return TF_OK;
+}
+
+template <int CFG>
+int prepare_cfg(tf_matrix_s* m) {
+  int st = set_attrs_cfg<CFG, kPrecJacobi>();
+  if (st != TF_OK) return st;
+  st = set_attrs_cfg<CFG, kPrecNone>();
+  if (st != TF_OK) return st;
+  st = set_attrs_cfg<CFG, kPrecIcc>();
+  if (st != TF_OK) return st;
+  return occupancy_grid<CFG>(m, (const void*)k_spmv_alpha<CFG>, cfg_threads<CFG>(),
+                             cfg_smem<CFG>(), m->ni, &m->spmv_grid);
+}
+
+}  // namespace
+
+int tf_fp64_prepare(tf_matrix_s* m) {
+  const int n = std::max(m->nt, 1);
+  m->vec_grid = std::max(1, std::min({(n + 1023) / 1024, m->ctx->sm_count * 4, kMaxBlocks}));
+  switch (m->tile_cfg) {
+    case kTile512: return prepare_cfg<kTile512>(m);
+    case kTile256: return prepare_cfg<kTile256>(m);
+    case kTile128: return prepare_cfg<kTile128>(m);
+    default: return prepare_cfg<kTileNone>(m);
+  }
+}
+
+namespace {
+// Host-driven loop: the same kernels launched directly, the loop condition
+// read back every kChunk iterations (kernels after convergence return at
+// once).  Used when TF_NO_GRAPH is set.
+template <int CFG, int PREC>
+int run_host_loop_t(tf_matrix_s* m) {
+  int st = set_attrs_cfg<CFG, PREC>();
+  if (st != TF_OK) return st;
+  cudaStream_t s = m->ctx->stream;
+  VecArgs va = make_vec_args(m);
+  SpArgs sa = make_sp_args(m, va);
+  const int vg = m->vec_grid, sg = m->spmv_grid;
+  const size_t ssm = cfg_smem<CFG>();
+  k_diag<<<vg, 256, 0, s>>>(va);
+  k_scale<<<vg, 256, 0, s>>>(va);
+  k_residual<CFG, PREC><<<sg, cfg_threads<CFG>(), ssm, s>>>(sa);
+  TF_CUDA_TRY(cudaGetLastError());
+  constexpr int kChunk = 16;
+  for (;;) {
+    TF_CUDA_TRY(cudaMemcpyAsync(m->h_state, m->d_state, sizeof(SolveState),
+                                cudaMemcpyDeviceToHost, s));
+    TF_CUDA_TRY(cudaStreamSynchronize(s));
+    if (m->h_state->done) break;
+    for (int k = 0; k < kChunk; ++k) {
+      k_pupdate<PREC><<<vg, 256, 0, s>>>(va);
+      k_spmv_alpha<CFG><<<sg, cfg_threads<CFG>(), ssm, s>>>(sa);
+      k_update<PREC><<<vg, 256, 0, s>>>(va);
+    }
+    TF_CUDA_TRY(cudaGetLastError());
+  }
+  k_unscale<<<vg, 256, 0, s>>>(va);
+  TF_CUDA_TRY(cudaGetLastError());
+  return TF_OK;
+}
+
+template <int PREC>
+int run_host_loop_p(tf_matrix_s* m) {
+  switch (m->tile_cfg) {
+    case kTile512: return run_host_loop_t<kTile512, PREC>(m);
+    case kTile256: return run_host_loop_t<kTile256, PREC>(m);
+    case kTile128: return run_host_loop_t<kTile128, PREC>(m);
+    default: return run_host_loop_t<kTileNone, PREC>(m);
+  }
+}
+}  // namespace
+
+int tf_fp64_run(tf_matrix_s* m, int prec) {
+  if (prec < 0 || prec > 2) return TF_ERR_ARG;
+  static const bool no_graph = getenv("TF_NO_GRAPH") != nullptr;
+  if (no_graph) {
+    if (prec == kPrecJacobi) return run_host_loop_p<kPrecJacobi>(m);
+    if (prec == kPrecNone) return run_host_loop_p<kPrecNone>(m);
+    return TF_ERR_ARG;
+  }
+  if (!m->graph[prec]) {
+    int st;
+    if (prec == kPrecJacobi) st = build_graph_p<kPrecJacobi>(m, &m->graph[prec]);
+    else if (prec == kPrecNone) st = build_graph_p<kPrecNone>(m, &m->graph[prec]);
+    else return TF_ERR_ARG;  // ICC runs through tf_icc_run
+    if (st != TF_OK) return st;
+  }
+  TF_CUDA_TRY(cudaGraphLaunch(m->graph[prec], m->ctx->stream));
+  return TF_OK;
+}
+
+// ---- building blocks (direct launches, no solve state) --------------------
+namespace {
+template <int CFG>
+int launch_spmv(tf_matrix_s* m, const double* val, const double* p, double* q,
+                double* scal) {
+  VecArgs va = make_vec_args(m);
+  va.st = nullptr;
+  va.p = const_cast<double*>(p);
+  va.q = q;
+  SpArgs sa = make_sp_args(m, va);
+  sa.val = val;
+  sa.out_scalar = scal;
+  k_spmv_alpha<CFG><<<m->spmv_grid, cfg_threads<CFG>(), cfg_smem<CFG>(), m->ctx->stream>>>(sa);
+  TF_CUDA_TRY(cudaGetLastError());
+  return TF_OK;
+}
+template <int CFG>
+int launch_resid(tf_matrix_s* m, const double* val, const double* b,
+                 const double* x, double* r, double* scal) {
+  VecArgs va = make_vec_args(m);
+  va.st = nullptr;
+  va.x = const_cast<double*>(x);
+  va.b = const_cast<double*>(b);
+  va.r = r;
+  SpArgs sa = make_sp_args(m, va);
+  sa.val = val;
+  sa.out_scalar = scal;
+  k_residual<CFG, kPrecNone><<<m->spmv_grid, cfg_threads<CFG>(), cfg_smem<CFG>(), m->ctx->stream>>>(sa);
+  TF_CUDA_TRY(cudaGetLastError());
+  return TF_OK;
+}
+}  // namespace
+
+// The building-block kernels need a scratch scalar pair: [0] result,
+// [1] reinterpreted as the last-block counter.  d_part's tail holds it.
+static double* bb_scalar(tf_matrix_s* m) { return m->d_part + 8 * kMaxBlocks; }
+
+int tf_fp64_spmv(tf_matrix_s* m, const double* val, const double* p, double* q,
+                 double* pq) {
+  double* scal = bb_scalar(m);
+  int st;
+  switch (m->tile_cfg) {
+    case kTile512: st = launch_spmv<kTile512>(m, val, p, q, scal); break;
+    case kTile256: st = launch_spmv<kTile256>(m, val, p, q, scal); break;
+    case kTile128: st = launch_spmv<kTile128>(m, val, p, q, scal); break;
+    default: st = launch_spmv<kTileNone>(m, val, p, q, scal); break;
+  }
+  if (st == TF_OK && pq)
+    TF_CUDA_TRY(cudaMemcpyAsync(pq, scal, sizeof(double), cudaMemcpyDeviceToDevice,
+                                m->ctx->stream));
+  return st;
+}
+
+int tf_fp64_residual(tf_matrix_s* m, const double* val, const double* b,
+                     const double* x, double* r) {
+  double* scal = bb_scalar(m);
+  switch (m->tile_cfg) {
+    case kTile512: return launch_resid<kTile512>(m, val, b, x, r, scal);
+    case kTile256: return launch_resid<kTile256>(m, val, b, x, r, scal);
+    case kTile128: return launch_resid<kTile128>(m, val, b, x, r, scal);
+    default: return launch_resid<kTileNone>(m, val, b, x, r, scal);
+  }
+}
+
+namespace tf {
+// NRMS of r with the diagonal of `val` (Normalized_Root_Mean_Square.f90).
+__global__ void __launch_bounds__(256) k_nrms(int ni, const int* dia, const double* val,
+                                              const double* r, const double* x,
+                                              int has_norm, double norm,
+                                              double* part, double* out) {
+  __shared__ double scratch[32];
+  double s = 0.0, mn = kHuge, mx = -kHuge;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ni; i += stride) {
+    s = __dadd_rn(s, nrms_term(r[i], val[dia[i]]));
+    if (!has_norm) {
+      mn = fmin_ref(mn, x[i]);
+      mx = fmax_ref(mx, x[i]);
+    }
+  }
+  double v[3] = {block_red<kSum>(s, scratch), block_red<kMin>(mn, scratch),
+                 block_red<kMax>(mx, scratch)};
+  const int ops[3] = {kSum, kMin, kMax};
+  if (grid_reduce_last<3>(v, ops, part, reinterpret_cast<unsigned*>(out + 1), scratch) &&
+      threadIdx.x == 0)
+    out[0] = nrms_finish(v[0], has_norm, norm, v[1], v[2]);
+}
+}  // namespace tf
+
+int tf_fp64_nrms(tf_matrix_s* m, const double* val, const double* r,
+                 const double* x, int has_norm, double norm, double* out) {
+  double* scal = bb_scalar(m);
+  k_nrms<<<m->vec_grid, 256, 0, m->ctx->stream>>>(m->ni, m->d_dia, val, r, x, has_norm,
+                                                  norm, m->d_part, scal);
+  TF_CUDA_TRY(cudaGetLastError());
+  TF_CUDA_TRY(cudaMemcpyAsync(out, scal, sizeof(double), cudaMemcpyDeviceToDevice,
+                              m->ctx->stream));
+  return TF_OK;
+}

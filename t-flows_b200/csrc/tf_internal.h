@@ -1,0 +1,88 @@
+// tf_internal.h -- host-side structures shared by the library's .cu files.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/tf_krylov.h"
+#include "tf_common.cuh"
+#include "tf_tile.cuh"
+
+#define TF_CUDA_TRY(expr)                                       \
+  do {                                                          \
+    cudaError_t _e = (expr);                                    \
+    if (_e != cudaSuccess) {                                    \
+      tf_set_last_cuda_error(_e, #expr, __FILE__, __LINE__);    \
+      return (_e == cudaErrorMemoryAllocation) ? TF_ERR_OOM     \
+                                               : TF_ERR_CUDA;   \
+    }                                                           \
+  } while (0)
+
+void tf_set_last_cuda_error(cudaError_t e, const char* what, const char* file,
+                            int line);
+
+struct tf_ctx_s {
+  int device = 0;
+  int sm_count = 148;
+  size_t l2_bytes = 0;
+  cudaStream_t stream = nullptr;
+  int history = 0;
+  std::vector<double> last_hist;
+  int last_count = 0;
+};
+
+// Device mirror of one Matrix_Type plus the Krylov workspace of its solves.
+struct tf_matrix_s {
+  tf_ctx_s* ctx = nullptr;
+  int nt = 0, ni = 0;
+  int64_t nnz = 0;
+  int max_row_len = 0;
+  int diag_first = 1;
+  // structure, 0-based, padded for 16-byte bulk copies
+  int* d_row = nullptr;
+  int* d_col = nullptr;
+  int* d_dia = nullptr;
+  // FP64 values and vectors (nt entries, padded)
+  double* d_val = nullptr;
+  double* d_x = nullptr;
+  double* d_b = nullptr;
+  double* d_r = nullptr;
+  double* d_p = nullptr;
+  double* d_q = nullptr;
+  double* d_z = nullptr;      // preconditioned residual (ICC only)
+  double* d_adiag = nullptr;  // diagonal of the scaled matrix
+  double* d_part = nullptr;   // grid-reduction partials
+  double* d_hist = nullptr;
+  int hist_cap = 0;
+  tf::SolveState* d_state = nullptr;
+  tf::SolveParams* d_params = nullptr;
+  tf::SolveState* h_state = nullptr;    // pinned
+  tf::SolveParams* h_params = nullptr;  // pinned
+  // SpMV tiling picked at registration
+  int tile_cfg = tf::kTileNone;
+  int spmv_grid = 1;
+  int vec_grid = 1;
+  // ICC level schedule (built on first use)
+  int icc_ready = 0;
+  int icc_nlev = 0;
+  int* d_lev_ptr = nullptr;   // forward levels: rows d_lev_rows[lev_ptr[l]..]
+  int* d_lev_rows = nullptr;
+  std::vector<int> h_lev_ptr;
+  // cached graphs, one per preconditioner
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  std::mutex mu;
+};
+
+// FP64 drop-in entry points implemented in tf_fp64.cu
+int tf_fp64_prepare(tf_matrix_s* m);
+int tf_fp64_run(tf_matrix_s* m, int prec);   // runs on m->ctx->stream
+int tf_fp64_spmv(tf_matrix_s* m, const double* val, const double* p,
+                 double* q, double* pq);
+int tf_fp64_residual(tf_matrix_s* m, const double* val, const double* b,
+                     const double* x, double* r);
+int tf_fp64_nrms(tf_matrix_s* m, const double* val, const double* r,
+                 const double* x, int has_norm, double norm, double* out);
+int tf_icc_build(tf_matrix_s* m, const int* h_row0, const int* h_col0);
+int tf_icc_run_solve(tf_matrix_s* m);        // ICC-preconditioned graph

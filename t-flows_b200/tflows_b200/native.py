@@ -1,0 +1,238 @@
+"""ctypes binding of libtfkrylov.so (the C ABI declared in include/tf_krylov.h).
+
+This is the Python counterpart of the Fortran ``bind(C)`` shim: it exposes
+the same entry points with the same argument meaning as
+``Native_Type % Solve_Native`` (Sources/Process/Cpu/Native_Mod/Solve_Native.f90).
+There is no fallback: if the shared library or a CUDA device is missing, every
+call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG, "lib", "libtfkrylov.so")
+
+TF_OK = 0
+STATUS = {
+    0: "TF_OK", 1: "TF_ERR_CUDA", 2: "TF_ERR_OOM", 3: "TF_ERR_ARG",
+    4: "TF_ERR_TIMEOUT", 5: "TF_ERR_LAYOUT", 6: "TF_ERR_NO_DEVICE",
+    7: "TF_ERR_BUSY", 8: "TF_ERR_CANCELLED", 64: "TF_ERR_UNKNOWN_SOLVER",
+    72: "TF_ERR_UNKNOWN_PREC",
+}
+SOLVERS = {"cg": 0, "bicg": 1}
+PRECS = {"none": 0, "jacobi": 1, "diagonal": 1, "icc": 2, "incomplete_cholesky": 2}
+
+# Every symbol include/tf_krylov.h declares; tests check the library exports them.
+EXPORTS = [
+    "tf_status_string", "tf_version", "tf_ctx_create", "tf_ctx_destroy",
+    "tf_matrix_register", "tf_matrix_release", "tf_matrix_info", "tf_solve",
+    "tf_solve_native", "tf_solve_device", "tf_ctx_set_history", "tf_last_history",
+    "tf_host_pin", "tf_host_unpin", "tf_spmv", "tf_residual", "tf_nrms",
+    "tf_ctx_sync", "tf_ctx_stream",
+]
+
+
+class TFError(RuntimeError):
+    def __init__(self, status, where=""):
+        self.status = status
+        msg = f"{where}: {STATUS.get(status, status)}"
+        try:
+            detail = _lib.tf_last_error_message().decode()
+            if detail and status in (1, 2):
+                msg += f" ({detail})"
+        except Exception:
+            pass
+        super().__init__(msg)
+
+
+_lib = None
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_dbl_p = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+
+def load(path=LIB_PATH):
+    """Load libtfkrylov.so (once).  Raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} not built; run `python t-flows_b200/build.py --lib`")
+    L = ctypes.CDLL(path)
+    L.tf_status_string.restype = ctypes.c_char_p
+    L.tf_status_string.argtypes = [ctypes.c_int]
+    L.tf_version.restype = ctypes.c_char_p
+    L.tf_last_error_message.restype = ctypes.c_char_p
+    L.tf_ctx_create.argtypes = [ctypes.c_int, ctypes.POINTER(_vp)]
+    L.tf_ctx_destroy.argtypes = [_vp]
+    L.tf_ctx_sync.argtypes = [_vp]
+    L.tf_ctx_stream.argtypes = [_vp]
+    L.tf_ctx_stream.restype = _vp
+    L.tf_ctx_set_history.argtypes = [_vp, ctypes.c_int]
+    L.tf_last_history.argtypes = [_vp, _c_dbl_p, ctypes.c_int, _c_int_p]
+    L.tf_matrix_register.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int64,
+                                     _c_int_p, _c_int_p, _c_int_p, ctypes.POINTER(_vp)]
+    L.tf_matrix_release.argtypes = [_vp]
+    L.tf_matrix_info.argtypes = [_vp, _c_int_p, _c_int_p,
+                                 ctypes.POINTER(ctypes.c_int64), _c_int_p]
+    L.tf_matrix_tile_config.argtypes = [_vp]
+    solve_args = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int,
+                  _c_int_p, ctypes.c_double, _c_dbl_p, _c_dbl_p]
+    L.tf_solve.argtypes = solve_args
+    L.tf_solve_device.argtypes = solve_args
+    L.tf_solve_native.argtypes = [_vp, _vp, ctypes.c_char_p, ctypes.c_char_p, _vp, _vp,
+                                  _vp, ctypes.c_int, _c_int_p, ctypes.c_double,
+                                  _c_dbl_p, _c_dbl_p]
+    L.tf_host_pin.argtypes = [_vp, ctypes.c_size_t]
+    L.tf_host_unpin.argtypes = [_vp]
+    L.tf_spmv.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
+    L.tf_residual.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
+    L.tf_nrms.argtypes = [_vp, _vp, _vp, _vp, _vp, _c_dbl_p, _vp]
+    _lib = L
+    return L
+
+
+def _check(st, where):
+    if st != TF_OK:
+        raise TFError(st, where)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_vp)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Context:
+    """One device + CUDA stream + Krylov workspace (tf_ctx)."""
+
+    def __init__(self, device=-1, history=False):
+        L = load()
+        h = _vp()
+        _check(L.tf_ctx_create(device, ctypes.byref(h)), "tf_ctx_create")
+        self.h = h
+        self.set_history(history)
+
+    def set_history(self, on):
+        _check(load().tf_ctx_set_history(self.h, 1 if on else 0), "tf_ctx_set_history")
+
+    def history(self):
+        cnt = ctypes.c_int(0)
+        _check(load().tf_last_history(self.h, None, 0, ctypes.byref(cnt)), "tf_last_history")
+        out = np.zeros(max(cnt.value, 1))
+        _check(load().tf_last_history(self.h, out.ctypes.data_as(_c_dbl_p), cnt.value,
+                                      ctypes.byref(cnt)), "tf_last_history")
+        return out[:cnt.value]
+
+    def sync(self):
+        _check(load().tf_ctx_sync(self.h), "tf_ctx_sync")
+
+    @property
+    def stream(self):
+        return load().tf_ctx_stream(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().tf_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Matrix:
+    """Device-resident structure of one Matrix_Type (tf_matrix)."""
+
+    def __init__(self, ctx, row, col, dia, n_own=None):
+        L = load()
+        self.row, self.col, self.dia = _i32(row), _i32(col), _i32(dia)
+        self.n = len(self.row) - 1
+        self.nnz = int(self.row[-1] - 1) if self.n > 0 else 0
+        self.n_own = self.n if n_own is None else int(n_own)
+        h = _vp()
+        _check(L.tf_matrix_register(ctx.h, self.n, self.n_own, self.nnz,
+                                    self.row.ctypes.data_as(_c_int_p),
+                                    self.col.ctypes.data_as(_c_int_p),
+                                    self.dia.ctypes.data_as(_c_int_p), ctypes.byref(h)),
+               "tf_matrix_register")
+        self.h = h
+        self.ctx = ctx
+
+    @property
+    def tile_config(self):
+        return load().tf_matrix_tile_config(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().tf_matrix_release(self.h)
+            self.h = None
+
+
+def _norm_arg(norm):
+    return None if norm is None else ctypes.byref(ctypes.c_double(norm))
+
+
+def solve(ctx, mat, solver, prec, val, x, b, miter, tol, norm=None):
+    """tf_solve: updates val, x, b in place like the reference; returns (niter, fin_res)."""
+    for a in (val, x, b):
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+    s = SOLVERS[solver] if isinstance(solver, str) else solver
+    p = PRECS[prec] if isinstance(prec, str) else prec
+    niter, res = ctypes.c_int(0), ctypes.c_double(0.0)
+    _check(load().tf_solve(ctx.h, mat.h, s, p, _ptr(val), _ptr(x), _ptr(b), int(miter),
+                           ctypes.byref(niter), float(tol), ctypes.byref(res),
+                           _norm_arg(norm)), "tf_solve")
+    return niter.value, res.value
+
+
+def solve_native(ctx, mat, solver, prec, val, x, b, miter, tol, norm=None):
+    """tf_solve_native: solver/prec by name, as Solve_Native dispatches them."""
+    niter, res = ctypes.c_int(0), ctypes.c_double(0.0)
+    st = load().tf_solve_native(ctx.h, mat.h, solver.encode(), prec.encode(), _ptr(val),
+                                _ptr(x), _ptr(b), int(miter), ctypes.byref(niter),
+                                float(tol), ctypes.byref(res), _norm_arg(norm))
+    _check(st, "tf_solve_native")
+    return niter.value, res.value
+
+
+def solve_device(ctx, mat, solver, prec, d_val, d_x, d_b, miter, tol, norm=None):
+    """tf_solve_device with raw device pointers (ints)."""
+    s = SOLVERS[solver] if isinstance(solver, str) else solver
+    p = PRECS[prec] if isinstance(prec, str) else prec
+    niter, res = ctypes.c_int(0), ctypes.c_double(0.0)
+    _check(load().tf_solve_device(ctx.h, mat.h, s, p, _vp(d_val), _vp(d_x), _vp(d_b),
+                                  int(miter), ctypes.byref(niter), float(tol),
+                                  ctypes.byref(res), _norm_arg(norm)), "tf_solve_device")
+    return niter.value, res.value
+
+
+def spmv(ctx, mat, d_val, d_p, d_q, d_pq=None):
+    _check(load().tf_spmv(ctx.h, mat.h, _vp(d_val), _vp(d_p), _vp(d_q),
+                          _vp(d_pq) if d_pq else None), "tf_spmv")
+
+
+def residual(ctx, mat, d_val, d_b, d_x, d_r):
+    _check(load().tf_residual(ctx.h, mat.h, _vp(d_val), _vp(d_b), _vp(d_x), _vp(d_r)),
+           "tf_residual")
+
+
+def nrms(ctx, mat, d_val, d_r, d_x, d_out, norm=None):
+    _check(load().tf_nrms(ctx.h, mat.h, _vp(d_val), _vp(d_r), _vp(d_x), _norm_arg(norm),
+                          _vp(d_out)), "tf_nrms")
+
+
+def pin(arr):
+    _check(load().tf_host_pin(_ptr(arr), arr.nbytes), "tf_host_pin")
+
+
+def unpin(arr):
+    _check(load().tf_host_unpin(_ptr(arr)), "tf_host_unpin")

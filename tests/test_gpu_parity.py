@@ -1,0 +1,276 @@
+"""GPU parity of the FP64 drop-in against the oracle, through the C ABI.
+
+Bars: per-row kernels (SpMV, residual) bit-exact with the oracle; a whole
+solve within rel-L2 1e-8 of the oracle's x, iteration count within 2 %
+(exact on the small fixtures), fin_res below tol whenever the oracle's is.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import golden_cases
+from oracle import oracle as O
+from tflows_b200 import native, systems
+
+pytestmark = pytest.mark.gpu
+
+REL_L2 = 1e-8      # FP64 solution agreement with the oracle
+ITER_TOL = 0.02    # |niter - niter_oracle| <= 2 %
+
+
+def torch_dev():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch
+
+
+def rel_l2(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def gpu_solve(ctx, row, col, dia, val, b, x0, solver, prec, miter, tol, norm):
+    m = native.Matrix(ctx, row, col, dia)
+    try:
+        v, x, bb = val.copy(), x0.copy(), b.copy()
+        niter, res = native.solve(ctx, m, solver, prec, v, x, bb, miter, tol, norm)
+        return x, v, bb, niter, res
+    finally:
+        m.close()
+
+
+def oracle_solve(row, col, dia, val, b, x0, solver, prec, miter, tol, norm, threads=8):
+    v, x, bb = val.copy(), x0.copy(), b.copy()
+    r = O.solve_native(solver, prec, row, col, dia, v, x, bb, miter, tol, norm=norm,
+                       threads=threads)
+    return x, v, bb, r["niter"], r["fin_res"]
+
+
+def check_parity(g, o, tol, exact_iters=False):
+    x, v, b, it, res = g
+    ox, ov, ob, oit, ores = o
+    if exact_iters:
+        assert it == oit, (it, oit)
+    else:
+        assert abs(it - oit) <= max(1, ITER_TOL * oit), (it, oit)
+    assert rel_l2(x, ox) <= REL_L2, rel_l2(x, ox)
+    if ores < tol:
+        assert res < tol
+    # val and b come back as (v*fn)/fn: within an ulp or two of the input
+    assert np.allclose(v, ov, rtol=4e-16, atol=0)
+    assert np.allclose(b, ob, rtol=4e-16, atol=0)
+
+
+@pytest.mark.parametrize("case", golden_cases(), ids=lambda c: c["name"])
+def test_golden_fixture_parity(gpu_ctx, case):
+    g = gpu_solve(gpu_ctx, case["row"], case["col"], case["dia"], case["val"], case["b"],
+                  case["x0"], case["solver"], case["prec"], case["miter"], case["tol"],
+                  case["norm"])
+    o = (case["x_out"], case["val_out"], case["b_out"], case["niter"], case["fin_res"])
+    if "diverging" in case["name"]:
+        # The reference's Bicg diverges here: the drop-in must too, same count.
+        assert g[3] == case["niter"] == case["miter"]
+        assert g[4] == pytest.approx(case["fin_res"], rel=1e-3)
+        return
+    check_parity(g, o, case["tol"], exact_iters=True)
+
+
+def _dev_arrays(torch, *arrs):
+    return [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in arrs]
+
+
+@pytest.mark.parametrize("kind,n,ratio", [("hex", 13, 1.0), ("hex", 40, 1.02),
+                                          ("poly", 3000, None)])
+def test_spmv_and_residual_bitwise(gpu_ctx, kind, n, ratio):
+    torch = torch_dev()
+    if kind == "hex":
+        s = systems.small_hex(n, seed=3, kind="momentum", ratio=ratio)
+    else:
+        s = systems.poly_system(n, seed=3, kind="pressure")
+    rng = np.random.default_rng(7)
+    p = rng.standard_normal(s.n)
+    xx = rng.standard_normal(s.n)
+    m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia)
+    try:
+        dval, dp, dq, db, dx, dr = _dev_arrays(torch, s.val, p, np.zeros(s.n), s.b, xx,
+                                               np.zeros(s.n))
+        dpq = torch.zeros(1, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        native.spmv(gpu_ctx, m, dval.data_ptr(), dp.data_ptr(), dq.data_ptr(), dpq.data_ptr())
+        native.residual(gpu_ctx, m, dval.data_ptr(), db.data_ptr(), dx.data_ptr(),
+                        dr.data_ptr())
+        gpu_ctx.sync()
+        q = dq.cpu().numpy()
+        r = dr.cpu().numpy()
+        assert np.array_equal(q, O.spmv(s.csr.row, s.csr.col, s.csr.dia, s.val, p))
+        assert np.array_equal(r, O.residual(s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, xx))
+        assert dpq.item() == pytest.approx(float(np.dot(p, q)), rel=1e-13)
+    finally:
+        m.close()
+
+
+@pytest.mark.parametrize("cfg", [0, 1, 2, 3])
+def test_every_tile_configuration(gpu_ctx, cfg, monkeypatch):
+    """Tile widths 512/256/128 and the direct-from-global path agree."""
+    torch = torch_dev()
+    monkeypatch.setenv("TF_TILE_CFG", str(cfg))
+    s = systems.small_hex(17, seed=5, kind="pressure", ratio=1.05)
+    m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia)
+    try:
+        assert m.tile_config == cfg
+        p = np.random.default_rng(1).standard_normal(s.n)
+        dval, dp, dq = _dev_arrays(torch, s.val, p, np.zeros(s.n))
+        torch.cuda.synchronize()
+        native.spmv(gpu_ctx, m, dval.data_ptr(), dp.data_ptr(), dq.data_ptr())
+        gpu_ctx.sync()
+        assert np.array_equal(dq.cpu().numpy(), O.spmv(s.csr.row, s.csr.col, s.csr.dia,
+                                                        s.val, p))
+    finally:
+        m.close()
+
+
+def test_long_rows_fall_back_to_global_path(gpu_ctx):
+    """A row longer than any tile stage (a dense coupling row) still works."""
+    n = 3000
+    rows, cols = [], []
+    for i in range(n):
+        nb = list(range(n)) if i == 7 else [j for j in (i - 1, i + 1, 7) if 0 <= j < n]
+        nb = sorted(set(nb) - {i})
+        rows.append([i] + nb)
+    row = np.zeros(n + 1, np.int32)
+    row[1:] = np.cumsum([len(r) for r in rows])
+    row += 1
+    col = np.concatenate([np.array(r) + 1 for r in rows]).astype(np.int32)
+    dia = row[:-1].copy()
+    val = np.where(col == np.repeat(np.arange(1, n + 1), np.diff(row)), 4.0 * n, -1.0)
+    m = native.Matrix(gpu_ctx, row, col, dia)
+    try:
+        assert m.tile_config == 3
+    finally:
+        m.close()
+    b = np.random.default_rng(2).uniform(-1, 1, n)
+    g = gpu_solve(gpu_ctx, row, col, dia, val, b, np.zeros(n), "cg", "jacobi", 200, 1e-12, 1.0)
+    o = oracle_solve(row, col, dia, val, b, np.zeros(n), "cg", "jacobi", 200, 1e-12, 1.0)
+    check_parity(g, o, 1e-12)
+
+
+@pytest.mark.parametrize("solver", ["cg", "bicg"])
+@pytest.mark.parametrize("prec", ["jacobi", "none"])
+@pytest.mark.parametrize("norm", [None, 1.0])
+def test_solve_variants_small(gpu_ctx, solver, prec, norm):
+    s = systems.small_hex(12, seed=6, kind="pressure", ratio=1.03)
+    x0 = np.random.default_rng(4).uniform(-0.5, 0.5, s.n)
+    args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, x0, solver, prec, 2000, 1e-10, norm)
+    check_parity(gpu_solve(gpu_ctx, *args), oracle_solve(*args), 1e-10)
+
+
+def test_bicg_equals_cg_on_gpu(gpu_ctx):
+    s = systems.small_hex(16, seed=7, kind="momentum", peclet=1.0, ratio=1.02)
+    a = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0)
+    g1 = gpu_solve(gpu_ctx, *a, "cg", "jacobi", 1000, 1e-10, 1.0)
+    g2 = gpu_solve(gpu_ctx, *a, "bicg", "jacobi", 1000, 1e-10, 1.0)
+    assert g1[3] == g2[3] and g1[4] == g2[4]
+    for u, w in zip(g1[:3], g2[:3]):
+        assert np.array_equal(u, w)
+
+
+@pytest.mark.parametrize("n", [30, 64])
+def test_pressure_parity_medium(gpu_ctx, n):
+    s = systems.small_hex(n, seed=1, kind="pressure", ratio=1.02)
+    args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, "cg", "jacobi", 5000, 1e-10, 1.0)
+    check_parity(gpu_solve(gpu_ctx, *args), oracle_solve(*args), 1e-10)
+
+
+def test_ldc_30_set_singular(gpu_ctx):
+    s = systems.ldc_pressure_30(singular="set_singular")
+    args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, "cg", "jacobi", 500, 1e-8, 1.0)
+    check_parity(gpu_solve(gpu_ctx, *args), oracle_solve(*args), 1e-8)
+
+
+def test_poly_parity(gpu_ctx):
+    s = systems.poly_system(20000, seed=3, kind="pressure", tol=1e-10, miter=5000, norm=1.0)
+    args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, "cg", "jacobi", 5000, 1e-10, 1.0)
+    check_parity(gpu_solve(gpu_ctx, *args), oracle_solve(*args), 1e-10)
+
+
+def test_early_exits(gpu_ctx):
+    s = systems.small_hex(6, seed=2, kind="pressure")
+    a = (s.csr.row, s.csr.col, s.csr.dia)
+    # b == 0 -> niter 0, fin_res exactly 0.0, x untouched
+    x0 = np.full(s.n, 0.25)
+    x, v, b, it, res = gpu_solve(gpu_ctx, *a, s.val, np.zeros(s.n), x0, "cg", "jacobi", 100,
+                                 1e-6, 1.0)
+    assert (it, res) == (0, 0.0) and np.all(x == 0.25)
+    # miter = 0 -> niter 0, fin_res = initial residual
+    x, v, b, it, res = gpu_solve(gpu_ctx, *a, s.val, s.b, s.x0, "cg", "jacobi", 0, 1e-6, 1.0)
+    o = oracle_solve(*a, s.val, s.b, s.x0, "cg", "jacobi", 0, 1e-6, 1.0)
+    assert it == 0 and res == pytest.approx(o[4], rel=1e-12) and np.all(x == 0.0)
+    # already converged x -> niter 0
+    ox = oracle_solve(*a, s.val, s.b, s.x0, "cg", "jacobi", 500, 1e-13, 1.0)[0]
+    x, v, b, it, res = gpu_solve(gpu_ctx, *a, s.val, s.b, ox, "cg", "jacobi", 500, 1e-11, 1.0)
+    assert it == 0 and res < 1e-11
+
+
+def test_error_codes(gpu_ctx):
+    s = systems.small_hex(4, seed=2, kind="pressure")
+    m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia)
+    try:
+        v, x, b = s.val.copy(), s.x0.copy(), s.b.copy()
+        with pytest.raises(native.TFError) as e:
+            native.solve_native(gpu_ctx, m, "gmres", "jacobi", v, x, b, 10, 1e-6)
+        assert e.value.status == 64
+        with pytest.raises(native.TFError) as e:
+            native.solve_native(gpu_ctx, m, "cg", "ilu", v, x, b, 10, 1e-6)
+        assert e.value.status == 72
+        it, res = native.solve_native(gpu_ctx, m, "cg   ", "diagonal", v, x, b, 100, 1e-8, 1.0)
+        assert it > 0
+    finally:
+        m.close()
+    bad_dia = s.csr.dia.copy()
+    bad_dia[3] += 1
+    with pytest.raises(native.TFError) as e:
+        native.Matrix(gpu_ctx, s.csr.row, s.csr.col, bad_dia)
+    assert e.value.status == 5
+
+
+def test_empty_system(gpu_ctx):
+    m = native.Matrix(gpu_ctx, np.array([1], np.int32), np.zeros(0, np.int32),
+                      np.zeros(0, np.int32))
+    try:
+        e = np.zeros(0)
+        assert native.solve(gpu_ctx, m, "cg", "jacobi", e, e.copy(), e.copy(), 10, 1e-6) == (0, 0.0)
+    finally:
+        m.close()
+
+
+def test_solve_device_pointers(gpu_ctx):
+    torch = torch_dev()
+    s = systems.small_hex(10, seed=9, kind="pressure")
+    dval, dx, db = _dev_arrays(torch, s.val, s.x0, s.b)
+    torch.cuda.synchronize()
+    m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia)
+    try:
+        it, res = native.solve_device(gpu_ctx, m, "cg", "jacobi", dval.data_ptr(),
+                                      dx.data_ptr(), db.data_ptr(), 1000, 1e-10, 1.0)
+    finally:
+        m.close()
+    o = oracle_solve(s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, "cg", "jacobi", 1000,
+                     1e-10, 1.0)
+    check_parity((dx.cpu().numpy(), dval.cpu().numpy(), db.cpu().numpy(), it, res), o, 1e-10)
+
+
+def test_history_matches_oracle(gpu_ctx):
+    s = systems.small_hex(9, seed=5, kind="pressure")
+    gpu_ctx.set_history(True)
+    try:
+        g = gpu_solve(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, "cg",
+                      "jacobi", 500, 1e-10, 1.0)
+        h = gpu_ctx.history()
+    finally:
+        gpu_ctx.set_history(False)
+    v, x, b = s.val.copy(), s.x0.copy(), s.b.copy()
+    r = O.solve_native("cg", "jacobi", s.csr.row, s.csr.col, s.csr.dia, v, x, b, 500, 1e-10,
+                       norm=1.0, history=True)
+    assert len(h) == g[3] + 1 == r["niter"] + 1
+    assert np.allclose(h, r["hist"], rtol=1e-9, atol=0)
