@@ -53,7 +53,40 @@ def parse():
     ap.add_argument("--peclet", type=float, default=1.0)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="solve", choices=["solve", "spmv"],
+                    help="spmv: only the pressure matrix and `--steps` SpMV launches "
+                         "(the small case profiled with ncu)")
     return ap.parse_args()
+
+
+def run_spmv_only(args):
+    """Register the pressure matrix and launch the tiled SpMV --steps times."""
+    import torch
+    from tflows_b200 import native, systems
+    from tflows_b200.grids import hex_grid
+    g = hex_grid(args.size, args.size, args.size, stretch_y=1.02)
+    s = systems.pressure_system(g, 2, tol=1e-10, miter=1, singular="pin", norm=1.0)
+    ctx = native.Context(0)
+    m = native.Matrix(ctx, s.csr.row, s.csr.col, s.csr.dia)
+    val = torch.from_numpy(s.val).cuda()
+    p = torch.randn(s.n, dtype=torch.float64, device="cuda")
+    q = torch.empty_like(p)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    native.spmv(ctx, m, val.data_ptr(), p.data_ptr(), q.data_ptr())
+    e0.record(stream)
+    for _ in range(args.steps):
+        native.spmv(ctx, m, val.data_ptr(), p.data_ptr(), q.data_ptr())
+    e1.record(stream)
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / max(args.steps, 1)
+    by = SPMV_BYTES(s.n, s.nnz)
+    print(json.dumps({"mode": "spmv", "n": s.n, "nnz": s.nnz, "tile_cfg": m.tile_config,
+                      "launch_ms": t * 1e3, "bytes_per_launch": by,
+                      "achieved_gbs": by / t / 1e9}), flush=True)
+    m.close()
+    ctx.close()
 
 
 def dist_env():
@@ -223,6 +256,9 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.mode == "spmv":
+        run_spmv_only(args)
         return
 
     import torch

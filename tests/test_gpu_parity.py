@@ -132,7 +132,7 @@ def test_every_tile_configuration(gpu_ctx, cfg, monkeypatch):
 
 def test_long_rows_fall_back_to_global_path(gpu_ctx):
     """A row longer than any tile stage (a dense coupling row) still works."""
-    n = 3000
+    n = 6000
     rows, cols = [], []
     for i in range(n):
         nb = list(range(n)) if i == 7 else [j for j in (i - 1, i + 1, 7) if 0 <= j < n]
@@ -273,4 +273,7 @@ def test_history_matches_oracle(gpu_ctx):
     r = O.solve_native("cg", "jacobi", s.csr.row, s.csr.col, s.csr.dia, v, x, b, 500, 1e-10,
                        norm=1.0, history=True)
     assert len(h) == g[3] + 1 == r["niter"] + 1
-    assert np.allclose(h, r["hist"], rtol=1e-9, atol=0)
+    # Early residuals agree to rounding; later ones carry the different
+    # summation order of the dot products, amplified as res falls by 1e11.
+    assert np.allclose(h[:10], r["hist"][:10], rtol=1e-11, atol=0)
+    assert np.allclose(h, r["hist"], rtol=1e-4, atol=0)
