@@ -58,6 +58,10 @@ const char* tf_status_string(int status);
 /* Library version, e.g. "tfkrylov 0.1 sm_100a". */
 const char* tf_version(void);
 
+/* Text of the last CUDA failure or argument rejection seen by the library
+ * (process-wide, static storage until the next failure). */
+const char* tf_last_error_message(void);
+
 /* Context on CUDA device `device` (-1: current device).  Replaces the
  * Work_Mod scratch arrays that Cg/Bicg connect (Cg.f90:44, Bicg.f90:45)
  * and the Nat object made by Create_Native (Native_Mod/Create_Native.f90:2-25). */
@@ -75,6 +79,9 @@ int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own, int64_t nnz,
 int tf_matrix_release(tf_matrix m);
 int tf_matrix_info(tf_matrix m, int* n_cells, int* n_own, int64_t* nnz,
                    int* max_row_len);
+/* SpMV tile configuration chosen at registration: 0/1/2 = 512/256/128-row
+ * shared-memory tiles, 3 = rows read straight from global memory. */
+int tf_matrix_tile_config(tf_matrix m);
 
 /* Solve A x = b.  Replaces Native_Type % Solve_Native (Solve_Native.f90:2-46)
  * and so Cg.f90:2-257 / Bicg.f90:2-269.  val, x and b are host arrays of

@@ -27,6 +27,11 @@ void tf_set_last_cuda_error(cudaError_t e, const char* what, const char* file,
   g_last_err = buf;
 }
 
+void tf_set_last_message(const char* msg) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  g_last_err = msg;
+}
+
 extern "C" const char* tf_last_error_message(void) {
   std::lock_guard<std::mutex> lk(g_err_mu);
   return g_last_err.c_str();

@@ -22,6 +22,7 @@
 
 void tf_set_last_cuda_error(cudaError_t e, const char* what, const char* file,
                             int line);
+void tf_set_last_message(const char* msg);
 
 struct tf_ctx_s {
   int device = 0;

@@ -30,7 +30,7 @@ EXPORTS = [
     "tf_matrix_register", "tf_matrix_release", "tf_matrix_info", "tf_solve",
     "tf_solve_native", "tf_solve_device", "tf_ctx_set_history", "tf_last_history",
     "tf_host_pin", "tf_host_unpin", "tf_spmv", "tf_residual", "tf_nrms",
-    "tf_ctx_sync", "tf_ctx_stream",
+    "tf_ctx_sync", "tf_ctx_stream", "tf_last_error_message", "tf_matrix_tile_config",
 ]
 
 
