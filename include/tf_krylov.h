@@ -146,6 +146,36 @@ int tf_ctx_sync(tf_ctx ctx);
  * own work with it. */
 void* tf_ctx_stream(tf_ctx ctx);
 
+/* ---------------------------------------------------------------------------
+ *  q = A p and p.q for callers that cannot allocate device memory.
+ *  No counterpart in the reference: T-Flows has no device code of its own.
+ *
+ *  Meant for code whose device memory belongs to someone else -- an OpenACC
+ *  data region (T-Flows' GPU layer), a caching or pooled allocator, a
+ *  process held to a fixed device-memory budget -- or that cannot pay for
+ *  the device synchronisation cudaFree brings.  Nothing is allocated: no
+ *  context, no registration, no cudaMalloc/cudaFree.  All arguments are
+ *  device pointers the caller owns: row (n+1) and col (nnz) are 1-based as
+ *  Matrix_Type stores them, val (nnz), p and q (n), and *d_pq receives
+ *  sum_i p_i q_i.  q's rows are summed in storage order, as tf_spmv does.
+ *
+ *  The kernel's only scratch, one partial sum per 256-row tile and a
+ *  counter, is a fixed 512 KiB array inside the library that every GPU which
+ *  loads the library keeps until exit.  It bounds n to
+ *  TF_SPMV_NOALLOC_MAX_ROWS; larger n returns TF_ERR_ARG (the reason is in
+ *  tf_last_error_message).  The first call on a device looks up the array's
+ *  device address (cudaGetSymbolAddress, with that device current); make
+ *  that first call before any stream capture.  Work is queued on `stream`
+ *  (a cudaStream_t, NULL = legacy default stream) and the call returns
+ *  without waiting.  Every call shares the one array: calls that can
+ *  overlap on the GPU (different streams, or different host threads on one
+ *  device) race and must be serialised by the caller.
+ * ------------------------------------------------------------------------- */
+#define TF_SPMV_NOALLOC_MAX_ROWS 16777216
+int tf_spmv_noalloc(int n, const int* d_row, const int* d_col,
+                    const double* d_val, const double* d_p, double* d_q,
+                    double* d_pq, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
