@@ -43,8 +43,8 @@ def nrms(ni, r, a_val, a_dia, x, norm):
 
 
 def solve(solver, prec, row, col, dia, val, x, b, miter, tol, norm=None):
-    """Cg.f90:2-257 and Bicg.f90:2-269 with Prec_Form (jacobi/none) and
-    Prec_Solve (jacobi/none).  Returns (x, val, b, niter, fin_res) as
+    """Cg.f90:2-257 and Bicg.f90:2-269 with Prec_Form and Prec_Solve
+    (jacobi, icc, none).  Returns (x, val, b, niter, fin_res) as
     0-based lists."""
     a_row, a_col, a_dia = _i(row), _i(col), _i(dia)
     a_val, x, b = _f(val), _f(x), _f(b)
@@ -67,15 +67,47 @@ def solve(solver, prec, row, col, dia, val, x, b, miter, tol, norm=None):
         for j in range(a_row[i], a_row[i + 1]):
             a_val[j] = a_val[j] * fn
         b[i] = b[i] * fn
-    # Prec_Form.f90:47-53 / 83-89
-    for i in range(1, ni + 1):
-        if prec == "jacobi":
-            d[i] = a_val[a_dia[i]]
-            d_inv[i] = 1.0 / d[i]
-        else:
-            d[i] = 1.0
+    # Prec_Form.f90:47-89
+    if prec == "icc":
+        for i in range(1, ni + 1):
+            sm = a_val[a_dia[i]]
+            for j in range(a_row[i] + 1, a_row[i + 1]):
+                k = a_col[j]
+                if k > i:
+                    break
+                sm = sm - d[k] * a_val[j] * a_val[j]
+            d_inv[i] = sm
+            d[i] = 1.0 / sm
+    else:
+        for i in range(1, ni + 1):
+            if prec == "jacobi":
+                d[i] = a_val[a_dia[i]]
+                d_inv[i] = 1.0 / d[i]
+            else:
+                d[i] = 1.0
 
-    def prec_solve(out, inp):   # Prec_Solve.f90:44-49 / 97-102
+    def prec_solve(out, inp):   # Prec_Solve.f90:44-102
+        if prec == "icc":
+            for i in range(1, ni + 1):                       # forward
+                sm = inp[i]
+                for j in range(a_row[i] + 1, a_row[i + 1]):
+                    k = a_col[j]
+                    if k > i:
+                        break
+                    sm = sm - a_val[j] * out[k]
+                out[i] = sm * d[i]
+            for i in range(1, ni + 1):
+                out[i] = out[i] * d_inv[i]
+            for i in range(ni, 0, -1):                       # backward
+                sm = out[i]
+                for j in range(a_row[i + 1] - 1, a_row[i], -1):
+                    k = a_col[j]
+                    if k < i:
+                        break
+                    if k <= ni:
+                        sm = sm - a_val[j] * out[k]
+                out[i] = sm * d[i]
+            return
         for i in range(1, ni + 1):
             out[i] = inp[i] * d_inv[i] if prec == "jacobi" else inp[i]
 

@@ -149,7 +149,8 @@ void free_matrix(tf_matrix_s* m) {
     if (g) cudaGraphExecDestroy(g);
   void* ptrs[] = {m->d_row, m->d_col, m->d_dia, m->d_val, m->d_x, m->d_b,
                   m->d_r, m->d_p, m->d_q, m->d_z, m->d_adiag, m->d_part,
-                  m->d_hist, m->d_state, m->d_params, m->d_lev_ptr, m->d_lev_rows};
+                  m->d_hist, m->d_state, m->d_params, m->d_levf_rows, m->d_levb_rows,
+                  m->d_icc_d, m->d_icc_dinv};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (m->h_state) cudaFreeHost(m->h_state);
@@ -266,9 +267,7 @@ extern "C" int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own,
     }
     if (n_cells > 0) st = tf_fp64_prepare(m);
   }
-  if (st == TF_OK && n_cells > 0 && getenv("TF_NO_ICC_BUILD") == nullptr) {
-    // nothing: the ICC level schedule is built on first ICC solve
-  }
+  if (st == TF_OK && n_cells > 0 && diag_first) st = tf_icc_build(m, row0.data(), col0.data());
   if (st != TF_OK) {
     free_matrix(m);
     return st;
@@ -329,7 +328,8 @@ int run_solve_core(tf_matrix_s* m, int prec, int miter, double tol,
     hp->hist_cap = miter + 1;
   }
   TF_CUDA_TRY(cudaMemcpyAsync(m->d_params, hp, sizeof(*hp), cudaMemcpyHostToDevice, c->stream));
-  int st = (prec == tf::kPrecIcc) ? tf_icc_run_solve(m) : tf_fp64_run(m, prec);
+  if (prec == tf::kPrecIcc && !m->icc_ready) return TF_ERR_LAYOUT;  // needs diagonal first
+  int st = tf_fp64_run(m, prec);
   if (st != TF_OK) return st;
   TF_CUDA_TRY(cudaMemcpyAsync(m->h_state, m->d_state, sizeof(tf::SolveState),
                               cudaMemcpyDeviceToHost, c->stream));

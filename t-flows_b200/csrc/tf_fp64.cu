@@ -36,7 +36,9 @@
 #include <stdio.h>
 
 #include <algorithm>
+#include <vector>
 
+#include "tf_icc.cuh"
 #include "tf_internal.h"
 #include "tf_tile.cuh"
 
@@ -473,6 +475,54 @@ struct NodeBuilder {
   }
 };
 
+IccArgs icc_args(tf_matrix_s* m) {
+  IccArgs a{};
+  a.row = m->d_row;
+  a.col = m->d_col;
+  a.val = m->d_val;
+  a.ni = m->ni;
+  a.d = m->d_icc_d;
+  a.d_inv = m->d_icc_dinv;
+  a.r = m->d_r;
+  a.y = m->d_q;   // q is free between k_update and the next SpMV
+  a.z = m->d_z;
+  a.st = m->d_state;
+  return a;
+}
+
+// Per-level kernel arguments, kept alive while a graph is built.
+struct IccLevelArgs {
+  std::vector<IccArgs> form, fwd, bwd;
+};
+
+IccLevelArgs icc_level_args(tf_matrix_s* m) {
+  IccLevelArgs L;
+  const IccArgs base = icc_args(m);
+  for (size_t l = 0; l + 1 < m->h_levf_ptr.size(); ++l) {
+    IccArgs a = base;
+    a.rows = m->d_levf_rows + m->h_levf_ptr[l];
+    a.count = m->h_levf_ptr[l + 1] - m->h_levf_ptr[l];
+    L.fwd.push_back(a);
+    a.st = nullptr;
+    L.form.push_back(a);
+  }
+  for (size_t l = 0; l + 1 < m->h_levb_ptr.size(); ++l) {
+    IccArgs a = base;
+    a.rows = m->d_levb_rows + m->h_levb_ptr[l];
+    a.count = m->h_levb_ptr[l + 1] - m->h_levb_ptr[l];
+    L.bwd.push_back(a);
+  }
+  return L;
+}
+
+struct RhoArgs {
+  int ni;
+  const double* z;
+  const double* r;
+  double* part;
+  SolveState* st;
+};
+
 template <int CFG, int PREC>
 int build_graph_t(tf_matrix_s* m, cudaGraphExec_t* out) {
   int st = set_attrs_cfg<CFG, PREC>();
@@ -496,10 +546,36 @@ int build_graph_t(tf_matrix_s* m, cudaGraphExec_t* out) {
   NodeBuilder nb{g};
   void* vargs[] = {&va};
   void* sargs[] = {&sa};
+  IccLevelArgs lv;
+  RhoArgs ra{m->ni, m->d_z, m->d_r, m->d_part, m->d_state};
+  void* rargs[] = {&ra.ni, &ra.z, &ra.r, &ra.part, &ra.st};
+  std::vector<void*> form_args, fwd_args, bwd_args;
+  if (PREC == kPrecIcc) {
+    lv = icc_level_args(m);
+    for (auto& a : lv.form) form_args.push_back(&a);
+    for (auto& a : lv.fwd) fwd_args.push_back(&a);
+    for (auto& a : lv.bwd) bwd_args.push_back(&a);
+  }
+  auto lgrid = [](int count) { return dim3(std::max(1, (count + 255) / 256)); };
+  // z = M^-1 r by the two level-scheduled sweeps, then rho = z.r
+  auto add_icc_apply = [&](NodeBuilder& b, cudaGraphNode_t dep) {
+    for (size_t l = 0; l < lv.fwd.size(); ++l)
+      dep = b.add((const void*)k_icc_fwd_level, lgrid(lv.fwd[l].count), dim3(256), 0,
+                  &fwd_args[l], dep);
+    for (size_t l = 0; l < lv.bwd.size(); ++l)
+      dep = b.add((const void*)k_icc_bwd_level, lgrid(lv.bwd[l].count), dim3(256), 0,
+                  &bwd_args[l], dep);
+    return b.add((const void*)k_icc_rho, vg, vb, 0, rargs, dep);
+  };
   cudaGraphNode_t n1 = nb.add((const void*)k_diag, vg, vb, 0, vargs, nullptr);
   cudaGraphNode_t n2 = nb.add((const void*)k_scale, vg, vb, 0, vargs, n1);
+  if (PREC == kPrecIcc)   // Prec_Form (Cg.f90:89) on the scaled matrix
+    for (size_t l = 0; l < lv.form.size(); ++l)
+      n2 = nb.add((const void*)k_icc_form_level, lgrid(lv.form[l].count), dim3(256), 0,
+                  &form_args[l], n2);
   cudaGraphNode_t n3 = nb.add((const void*)k_residual<CFG, PREC>, sg, sb, ssm, sargs, n2);
   cudaGraphNode_t last = n3;
+  if (PREC == kPrecIcc) last = add_icc_apply(nb, last);
   cudaGraphNode_t cnode = nullptr;
   if (nb.status == TF_OK) {
     cudaGraphNodeParams cp{};
@@ -515,7 +591,8 @@ int build_graph_t(tf_matrix_s* m, cudaGraphExec_t* out) {
       NodeBuilder body{cp.conditional.phGraph_out[0]};
       cudaGraphNode_t b1 = body.add((const void*)k_pupdate<PREC>, vg, vb, 0, vargs, nullptr);
       cudaGraphNode_t b2 = body.add((const void*)k_spmv_alpha<CFG>, sg, sb, ssm, sargs, b1);
-      body.add((const void*)k_update<PREC>, vg, vb, 0, vargs, b2);
+      cudaGraphNode_t b3 = body.add((const void*)k_update<PREC>, vg, vb, 0, vargs, b2);
+      if (PREC == kPrecIcc) add_icc_apply(body, b3);
       if (body.status != TF_OK) nb.status = body.status;
     }
   }
@@ -592,9 +669,20 @@ int run_host_loop_t(tf_matrix_s* m) {
   SpArgs sa = make_sp_args(m, va);
   const int vg = m->vec_grid, sg = m->spmv_grid;
   const size_t ssm = cfg_smem<CFG>();
+  IccLevelArgs lv;
+  if (PREC == kPrecIcc) lv = icc_level_args(m);
+  auto lgrid = [](int count) { return std::max(1, (count + 255) / 256); };
+  auto icc_apply = [&]() {
+    for (auto& a : lv.fwd) k_icc_fwd_level<<<lgrid(a.count), 256, 0, s>>>(a);
+    for (auto& a : lv.bwd) k_icc_bwd_level<<<lgrid(a.count), 256, 0, s>>>(a);
+    k_icc_rho<<<vg, 256, 0, s>>>(m->ni, m->d_z, m->d_r, m->d_part, m->d_state);
+  };
   k_diag<<<vg, 256, 0, s>>>(va);
   k_scale<<<vg, 256, 0, s>>>(va);
+  if (PREC == kPrecIcc)
+    for (auto& a : lv.form) k_icc_form_level<<<lgrid(a.count), 256, 0, s>>>(a);
   k_residual<CFG, PREC><<<sg, cfg_threads<CFG>(), ssm, s>>>(sa);
+  if (PREC == kPrecIcc) icc_apply();
   TF_CUDA_TRY(cudaGetLastError());
   constexpr int kChunk = 16;
   for (;;) {
@@ -606,6 +694,7 @@ int run_host_loop_t(tf_matrix_s* m) {
       k_pupdate<PREC><<<vg, 256, 0, s>>>(va);
       k_spmv_alpha<CFG><<<sg, cfg_threads<CFG>(), ssm, s>>>(sa);
       k_update<PREC><<<vg, 256, 0, s>>>(va);
+      if (PREC == kPrecIcc) icc_apply();
     }
     TF_CUDA_TRY(cudaGetLastError());
   }
@@ -631,13 +720,13 @@ int tf_fp64_run(tf_matrix_s* m, int prec) {
   if (no_graph) {
     if (prec == kPrecJacobi) return run_host_loop_p<kPrecJacobi>(m);
     if (prec == kPrecNone) return run_host_loop_p<kPrecNone>(m);
-    return TF_ERR_ARG;
+    return run_host_loop_p<kPrecIcc>(m);
   }
   if (!m->graph[prec]) {
     int st;
     if (prec == kPrecJacobi) st = build_graph_p<kPrecJacobi>(m, &m->graph[prec]);
     else if (prec == kPrecNone) st = build_graph_p<kPrecNone>(m, &m->graph[prec]);
-    else return TF_ERR_ARG;  // ICC runs through tf_icc_run
+    else st = build_graph_p<kPrecIcc>(m, &m->graph[prec]);
     if (st != TF_OK) return st;
   }
   TF_CUDA_TRY(cudaGraphLaunch(m->graph[prec], m->ctx->stream));

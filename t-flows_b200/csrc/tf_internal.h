@@ -65,12 +65,13 @@ struct tf_matrix_s {
   int tile_cfg = tf::kTileNone;
   int spmv_grid = 1;
   int vec_grid = 1;
-  // ICC level schedule (built on first use)
+  // ICC level schedule (built at registration for diagonal-first matrices)
   int icc_ready = 0;
-  int icc_nlev = 0;
-  int* d_lev_ptr = nullptr;   // forward levels: rows d_lev_rows[lev_ptr[l]..]
-  int* d_lev_rows = nullptr;
-  std::vector<int> h_lev_ptr;
+  int* d_levf_rows = nullptr;  // forward-sweep rows grouped by level
+  int* d_levb_rows = nullptr;  // backward-sweep rows grouped by level
+  std::vector<int> h_levf_ptr, h_levb_ptr;
+  double* d_icc_d = nullptr;     // Prec_Form's d
+  double* d_icc_dinv = nullptr;  // Prec_Form's d_inv
   // cached graphs, one per preconditioner
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   std::mutex mu;
@@ -86,4 +87,4 @@ int tf_fp64_residual(tf_matrix_s* m, const double* val, const double* b,
 int tf_fp64_nrms(tf_matrix_s* m, const double* val, const double* r,
                  const double* x, int has_norm, double norm, double* out);
 int tf_icc_build(tf_matrix_s* m, const int* h_row0, const int* h_col0);
-int tf_icc_run_solve(tf_matrix_s* m);        // ICC-preconditioned graph
+

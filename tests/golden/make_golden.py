@@ -53,6 +53,9 @@ def cases():
     out.append(dict(name="hex5_pressure_cg_none_nonorm", row=s.csr.row, col=s.csr.col,
                     dia=s.csr.dia, val=s.val, b=s.b, x0=s.x0, solver="cg", prec="none",
                     miter=500, tol=1e-9, norm=None))
+    out.append(dict(name="hex5_pressure_cg_icc", row=s.csr.row, col=s.csr.col,
+                    dia=s.csr.dia, val=s.val, b=s.b, x0=s.x0, solver="cg", prec="icc",
+                    miter=500, tol=1e-10, norm=1.0))
     m = systems.small_hex(4, seed=12, kind="momentum", tol=1e-10, miter=400, peclet=1.0,
                           ratio=1.1)
     out.append(dict(name="hex4_momentum_bicg_jacobi", row=m.csr.row, col=m.csr.col,
@@ -63,6 +66,9 @@ def cases():
     out.append(dict(name="hex4_momentum_pe10_bicg_diverging", row=m10.csr.row,
                     col=m10.csr.col, dia=m10.csr.dia, val=m10.val, b=m10.b, x0=m10.x0,
                     solver="bicg", prec="jacobi", miter=60, tol=1e-10, norm=1.0))
+    out.append(dict(name="hex4_momentum_bicg_icc", row=m.csr.row, col=m.csr.col,
+                    dia=m.csr.dia, val=m.val, b=m.b, x0=m.x0, solver="bicg", prec="icc",
+                    miter=400, tol=1e-10, norm=None))
     p = systems.poly_system(150, seed=14, kind="pressure", tol=1e-10, miter=500, norm=1.0)
     x0 = np.random.default_rng(15).uniform(-0.1, 0.1, p.n)
     out.append(dict(name="poly150_pressure_cg_jacobi_x0", row=p.csr.row, col=p.csr.col,

@@ -277,3 +277,37 @@ def test_history_matches_oracle(gpu_ctx):
     # summation order of the dot products, amplified as res falls by 1e11.
     assert np.allclose(h[:10], r["hist"][:10], rtol=1e-11, atol=0)
     assert np.allclose(h, r["hist"], rtol=1e-4, atol=0)
+
+
+@pytest.mark.parametrize("solver,kind", [("cg", "pressure"), ("bicg", "momentum")])
+@pytest.mark.parametrize("norm", [None, 1.0])
+def test_icc_parity(gpu_ctx, solver, kind, norm):
+    """Level-scheduled IC(0) (Prec_Form.f90:68-78, Prec_Solve.f90:64-92)."""
+    kw = {"peclet": 1.0} if kind == "momentum" else {}
+    s = systems.small_hex(14, seed=8, kind=kind, ratio=1.04, **kw)
+    args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, solver, "icc", 1000, 1e-10, norm)
+    check_parity(gpu_solve(gpu_ctx, *args), oracle_solve(*args), 1e-10, exact_iters=True)
+
+
+def test_icc_parity_medium_and_poly(gpu_ctx):
+    s = systems.small_hex(30, seed=2, kind="pressure", ratio=1.02)
+    args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, "cg", "icc", 3000, 1e-10, 1.0)
+    check_parity(gpu_solve(gpu_ctx, *args), oracle_solve(*args), 1e-10)
+    p = systems.poly_system(4000, seed=6, kind="pressure", tol=1e-10, miter=3000, norm=1.0)
+    args = (p.csr.row, p.csr.col, p.csr.dia, p.val, p.b, p.x0, "cg", "icc", 3000, 1e-10, 1.0)
+    check_parity(gpu_solve(gpu_ctx, *args), oracle_solve(*args), 1e-10)
+
+
+def test_icc_needs_diagonal_first(gpu_ctx):
+    """The 4x4 example of Matrix_Mod.f90 stores rows in column order."""
+    from golden.make_golden import example_4x4
+    row, col, dia, val = example_4x4()
+    m = native.Matrix(gpu_ctx, row, col, dia)
+    try:
+        v, x, b = val.copy(), np.zeros(4), np.ones(4)
+        with pytest.raises(native.TFError) as e:
+            native.solve(gpu_ctx, m, "cg", "icc", v, x, b, 10, 1e-8)
+        assert e.value.status == 5
+        assert native.solve(gpu_ctx, m, "cg", "jacobi", v, x, b, 10, 1e-8)[0] > 0
+    finally:
+        m.close()

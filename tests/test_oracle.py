@@ -26,7 +26,7 @@ def test_oracle_reproduces_golden(case):
 
 
 @pytest.mark.parametrize("solver", ["cg", "bicg"])
-@pytest.mark.parametrize("prec", ["jacobi", "none"])
+@pytest.mark.parametrize("prec", ["jacobi", "none", "icc"])
 @pytest.mark.parametrize("norm", [None, 1.0])
 def test_oracle_matches_python_transliteration(solver, prec, norm):
     s = systems.small_hex(4, seed=21, kind="momentum" if solver == "bicg" else "pressure",
