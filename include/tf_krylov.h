@@ -126,6 +126,69 @@ int tf_host_pin(void* ptr, size_t bytes);
 int tf_host_unpin(void* ptr);
 
 /* ---------------------------------------------------------------------------
+ *  Batched and served solves (C++ engine behind a C ABI).
+ *
+ *  No single reference counterpart: T-Flows solves its systems one at a
+ *  time through Solve_Native.  A batch holds many independent systems of
+ *  uneven size (Matrix_Type layout, 1-based); all of them iterate together
+ *  on the device, each with its own scalars, until each reaches
+ *  ||b - A x||_2 <= tol ||b||_2 (FP64) or its iteration limit.  The Krylov
+ *  recurrence is Cg's (Cg.f90:139-224, which Bicg.f90 also computes) with
+ *  Jacobi preconditioning (Prec_Form.f90:47-53), Krylov vectors in FP32 or
+ *  FP64, FP64 reductions, and FP64 reliable updates (iterative refinement).
+ * ------------------------------------------------------------------------- */
+typedef struct tf_batch_opts {
+  int vec_fp32;       /* 1: Krylov vectors stored in FP32; 0: FP64            */
+  int val_fp32;       /* 1: the SpMV streams an FP32 copy of the values       */
+  int sweep_iters;    /* iterations per captured graph launch (default 8)     */
+  int max_systems;    /* system slots (default 1024)                          */
+  double ru_delta;    /* refinement when |r| fell by this factor (0.1)        */
+  size_t mem_budget;  /* device bytes for all systems' data (default 4 GiB)   */
+} tf_batch_opts;
+
+typedef struct tf_batch_s* tf_batch;
+typedef struct tf_server_s* tf_server;
+
+/* Status of a system in a batch / request in a server. */
+enum tf_sys_status {
+  TF_SYS_FREE = 0, TF_SYS_INIT = 1, TF_SYS_ACTIVE = 2, TF_SYS_CONVERGED = 3,
+  TF_SYS_MAXITER = 4, TF_SYS_BREAKDOWN = 5
+};
+
+int tf_batch_create(tf_ctx ctx, const tf_batch_opts* opts, tf_batch* out);
+int tf_batch_destroy(tf_batch b);
+/* Copy one system in (host arrays; x0 may be NULL for zeros).  Returns
+ * TF_ERR_BUSY when the memory budget or the slots are exhausted. */
+int tf_batch_add(tf_batch b, int n, int64_t nnz, const int* row, const int* col,
+                 const int* dia, const double* val, const double* rhs,
+                 const double* x0, double tol, int maxit, int* sys);
+/* Iterate until every system has converged or stopped. */
+int tf_batch_run(tf_batch b);
+/* x (host, n doubles) may be NULL; true_rel_res = ||b-Ax||_2/||b||_2 in FP64;
+ * n_updates counts FP64 residual evaluations (initial one included). */
+int tf_batch_result(tf_batch b, int sys, double* x, int* iters,
+                    double* true_rel_res, int* status, int* n_updates);
+int tf_batch_remove(tf_batch b, int sys);
+int tf_batch_info(tf_batch b, int* sweeps, int* work_items, size_t* free_bytes);
+
+/* Continuous batching: a worker thread admits queued requests whenever the
+ * memory budget and slots allow, runs sweeps over everything admitted,
+ * and retires finished systems; requests arriving while others run join at
+ * the next sweep.  Submit copies the system; wait blocks until done and
+ * reports end-to-end and queueing latency in milliseconds. */
+int tf_server_create(tf_ctx ctx, const tf_batch_opts* opts, tf_server* out);
+int tf_server_submit(tf_server s, int n, int64_t nnz, const int* row,
+                     const int* col, const int* dia, const double* val,
+                     const double* rhs, const double* x0, double tol, int maxit,
+                     int64_t* req);
+int tf_server_wait(tf_server s, int64_t req, double* x, int* iters,
+                   double* true_rel_res, int* status, double* latency_ms,
+                   double* queue_ms);
+int tf_server_stats(tf_server s, long long* admitted, long long* completed,
+                    int* peak_running, int* sweeps);
+int tf_server_destroy(tf_server s);
+
+/* ---------------------------------------------------------------------------
  *  Building blocks exposed for testing and for callers that keep their own
  *  Krylov loop.  All pointers are device pointers; vectors have n_cells
  *  entries; val has nnz entries.  Each call is asynchronous on ctx's stream;

@@ -1,0 +1,1087 @@
+// tf_batch.cu -- many independent systems solved together.
+//
+// Design
+// ------
+// Every system keeps its own CSR (0-based, tile table) and Krylov state in
+// one contiguous segment of a device arena.  A work list names (system,
+// row tile) items; persistent CTAs walk it, so all active systems advance
+// one Jacobi-CG iteration per kernel sequence, each with its own alpha and
+// beta.  The Cg/Bicg recurrence is the reference's (Bicg.f90's shadow
+// sequence equals the primary one, see tf_fp64.cu).
+//
+// Precision: the Krylov vectors (x correction, r, p, q, z, 1/diag) are
+// stored in V = float ("mixed") or double; the matrix values are FP64 by
+// default (optionally FP32); every SpMV row is accumulated in FP64; all dot
+// products, alpha, beta and norms are FP64.  Iterative refinement runs as
+// reliable updates: when the recursive residual has fallen by `ru_delta`
+// since the last update (or reaches tol, or maxit), the FP32 correction is
+// folded into the FP64 solution, and the residual is recomputed in FP64 as
+// b - A x with FP64 values, which also decides convergence:
+// ||b - A x||_2 <= tol ||b||_2.  Measured on stretched Poisson matrices,
+// FP32 iterates with FP64 values need ~1.03x the FP64 iteration count,
+// while FP32 values need 1.3-1.75x (the perturbed operator breaks the
+// recurrence), so FP64 values are the default.
+//
+// Per-system reductions: each tile writes its partial sums; the CTA that
+// finishes a system's last tile sums that system's partials in tile order.
+// A system's arithmetic therefore never depends on which other systems
+// share the batch: results are bit-identical alone and in any mix.
+//
+// Kernels of one iteration (all skip systems with nothing to do):
+//   kb_pupdate  z = dinv r, p = z + beta p
+//   kb_spmv     q = A p (tile streamer), p.q, alpha
+//   kb_update   xlo += alpha p, r -= alpha q, rho, |r|^2, beta, RU trigger
+//   kb_ru_fold  x += xlo, xlo = 0                        (systems due an RU)
+//   kb_ru_res   r = b - A x in FP64 (tile streamer), |r|^2, rho, test;
+//               on a new system also forms dinv and |b|^2
+// A sweep of S iterations is captured once as a CUDA graph; the host only
+// looks at the state array between sweeps (retire, admit, rebuild the list).
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "tf_internal.h"
+#include "tf_tile.cuh"
+
+namespace tfb {
+
+using namespace tf;
+
+enum SysStatus : int {
+  kFree = 0, kInit = 1, kActive = 2, kConverged = 3, kMaxIter = 4, kBreakdown = 5
+};
+
+constexpr int kRows = 256;       // rows per tile = threads per CTA
+constexpr int kNnzCap = 4096;    // entries per tile stage
+constexpr int kStages = 2;
+constexpr int kPartQ = 4;        // partial sums kept per tile
+
+template <typename V>
+struct SysDev {
+  const int* row;       // n+1, 0-based
+  const int* col;       // nnz, 0-based local
+  const double* val;    // FP64 values
+  const float* val32;   // FP32 copy (use_val32)
+  const int* tiles;     // ntiles+1 row boundaries
+  const int* dia;       // n, 0-based
+  const double* b;
+  double* x;
+  V* xlo;
+  V* r;
+  V* p;
+  V* q;
+  V* dinv;
+  double* part;         // ntiles * kPartQ
+  int n, ntiles;
+  int maxit, use_val32;
+  double tol;
+};
+
+struct SysState {
+  double rho, rho_old, beta, alpha;
+  double rr, rr_ru, bnorm2, res_true;
+  int status, iter, first, need_ru;
+  int n_ru, pad;
+  unsigned cnt_spmv, cnt_upd, cnt_res, cnt_pad;
+};
+
+struct Work {
+  int sys;
+  int tile;
+};
+
+struct BatchArgs {
+  const void* desc;       // SysDev<V>*
+  SysState* st;
+  const Work* work;
+  const int* nwork;
+  double ru_delta2;
+};
+
+__device__ __forceinline__ bool active(const SysState& s) { return s.status == kActive; }
+
+// ---------------------------------------------------------------------------
+template <typename V>
+__global__ void __launch_bounds__(kRows) kb_pupdate(BatchArgs a) {
+  const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
+  const int nw = *a.nwork;
+  for (int k = blockIdx.x; k < nw; k += gridDim.x) {
+    const Work w = a.work[k];
+    const SysState& s = a.st[w.sys];
+    if (!active(s)) continue;
+    const SysDev<V>& d = D[w.sys];
+    const int i = d.tiles[w.tile] + threadIdx.x;
+    if (i >= d.tiles[w.tile + 1]) continue;
+    const V z = d.r[i] * d.dinv[i];
+    d.p[i] = s.first ? z : (V)((double)z + s.beta * (double)d.p[i]);
+  }
+}
+
+// Per-system "last CTA" reduction over the system's tile partials.
+// Called CTA-wide; returns true in the CTA that completed the system, with
+// the sums in out[0..nq).
+template <int NQ>
+__device__ bool sys_reduce(unsigned* cnt, const double* part, int ntiles,
+                           const double (&mine)[NQ], double* tile_slot, double (&out)[NQ],
+                           double* scratch) {
+  __shared__ int s_last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) tile_slot[q] = mine[q];
+    __threadfence();
+    s_last = (atomicAdd(cnt, 1u) == (unsigned)ntiles - 1);
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double acc = 0.0;
+    for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
+      acc = __dadd_rn(acc, __ldcg(part + (size_t)t * kPartQ + q));
+    out[q] = block_red<kSum>(acc, scratch);
+  }
+  if (threadIdx.x == 0) *cnt = 0u;
+  return true;
+}
+
+// q = A p with FP64 row sums, p.q per tile, alpha per system.
+template <typename V, typename VT>
+struct SpmvWork {
+  const SysDev<V>* D;
+  SysState* st;
+  const Work* work;
+  int nw;
+  double acc;     // this thread's p_i q_i in the current tile
+  double* scratch;
+  __device__ int count() const { return nw; }
+  __device__ bool skip(int k) const { return !active(st[work[k].sys]); }
+  __device__ void tile(int k, const int*& row, const int*& col, const VT*& val, int& r0,
+                       int& r1) const {
+    const Work w = work[k];
+    const SysDev<V>& d = D[w.sys];
+    row = d.row;
+    col = d.col;
+    if constexpr (sizeof(VT) == 4) val = d.val32;
+    else val = d.val;
+    r0 = d.tiles[w.tile];
+    r1 = d.tiles[w.tile + 1];
+  }
+  __device__ void row(int k, int i, const VT* v, const int* c, int len) {
+    const SysDev<V>& d = D[work[k].sys];
+    double s = 0.0;
+#pragma unroll 1
+    for (int j0 = 0; j0 < len; j0 += 8) {
+      double pv[8], vv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (j0 + u < len) {
+          vv[u] = (double)v[j0 + u];
+          pv[u] = (double)d.p[c[j0 + u]];
+        }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (j0 + u < len) s = __dadd_rn(s, __dmul_rn(vv[u], pv[u]));
+    }
+    const V qi = (V)s;
+    d.q[i] = qi;
+    acc = __dadd_rn(acc, __dmul_rn((double)d.p[i], (double)qi));
+  }
+  __device__ void tile_end(int k) {
+    const Work w = work[k];
+    const SysDev<V>& d = D[w.sys];
+    double mine[1] = {block_red<kSum>(acc, scratch)};
+    acc = 0.0;
+    double out[1];
+    if (sys_reduce<1>(&st[w.sys].cnt_spmv, d.part, d.ntiles, mine,
+                      d.part + (size_t)w.tile * kPartQ, out, scratch) &&
+        threadIdx.x == 0) {
+      SysState& s = st[w.sys];
+      if (!(out[0] > 0.0)) s.status = kBreakdown;   // p.q <= 0 or NaN
+      else s.alpha = __ddiv_rn(s.rho, out[0]);
+    }
+  }
+};
+
+template <typename V, typename VT>
+__global__ void __launch_bounds__(kRows) kb_spmv(BatchArgs a) {
+  __shared__ double scratch[32];
+  SpmvWork<V, VT> w{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, *a.nwork, 0.0,
+                    scratch};
+  stream_work<kRows, kNnzCap, VT, kStages>(w);
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kRows) kb_update(BatchArgs a) {
+  __shared__ double scratch[32];
+  const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
+  const int nw = *a.nwork;
+  for (int k = blockIdx.x; k < nw; k += gridDim.x) {
+    const Work w = a.work[k];
+    SysState& s = a.st[w.sys];
+    if (!active(s)) continue;   // CTA-uniform
+    const SysDev<V>& d = D[w.sys];
+    const int i = d.tiles[w.tile] + threadIdx.x;
+    double rho = 0.0, rr = 0.0;
+    if (i < d.tiles[w.tile + 1]) {
+      const double al = s.alpha;
+      const V xl = (V)((double)d.xlo[i] + al * (double)d.p[i]);
+      const V ri = (V)((double)d.r[i] - al * (double)d.q[i]);
+      d.xlo[i] = xl;
+      d.r[i] = ri;
+      const V zi = ri * d.dinv[i];
+      rho = __dmul_rn((double)zi, (double)ri);
+      rr = __dmul_rn((double)ri, (double)ri);
+    }
+    double mine[2] = {block_red<kSum>(rho, scratch), block_red<kSum>(rr, scratch)};
+    double out[2];
+    if (sys_reduce<2>(&s.cnt_upd, d.part, d.ntiles, mine, d.part + (size_t)w.tile * kPartQ,
+                      out, scratch) &&
+        threadIdx.x == 0) {
+      s.rho_old = s.rho;
+      s.rho = out[0];
+      s.beta = __ddiv_rn(s.rho, s.rho_old);
+      s.rr = out[1];
+      s.iter += 1;
+      s.first = 0;
+      const double tb = d.tol * d.tol * s.bnorm2;
+      if (s.rr < a.ru_delta2 * s.rr_ru || s.rr <= tb || s.iter >= d.maxit || !(s.rr == s.rr))
+        s.need_ru = 1;
+    }
+  }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kRows) kb_ru_fold(BatchArgs a) {
+  const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
+  const int nw = *a.nwork;
+  for (int k = blockIdx.x; k < nw; k += gridDim.x) {
+    const Work w = a.work[k];
+    const SysState& s = a.st[w.sys];
+    if (!(s.status == kActive && s.need_ru)) continue;
+    const SysDev<V>& d = D[w.sys];
+    const int i = d.tiles[w.tile] + threadIdx.x;
+    if (i >= d.tiles[w.tile + 1]) continue;
+    d.x[i] = __dadd_rn(d.x[i], (double)d.xlo[i]);
+    d.xlo[i] = (V)0;
+  }
+}
+
+// r = b - A x in FP64; new systems also form dinv and |b|^2.
+template <typename V>
+struct ResWork {
+  const SysDev<V>* D;
+  SysState* st;
+  const Work* work;
+  int nw;
+  double rr, rho, bb;
+  double* scratch;
+  __device__ int count() const { return nw; }
+  __device__ bool skip(int k) const {
+    const SysState& s = st[work[k].sys];
+    return !(s.status == kInit || (s.status == kActive && s.need_ru));
+  }
+  __device__ void tile(int k, const int*& row, const int*& col, const double*& val, int& r0,
+                       int& r1) const {
+    const Work w = work[k];
+    const SysDev<V>& d = D[w.sys];
+    row = d.row;
+    col = d.col;
+    val = d.val;
+    r0 = d.tiles[w.tile];
+    r1 = d.tiles[w.tile + 1];
+  }
+  __device__ void row(int k, int i, const double* v, const int* c, int len) {
+    const Work w = work[k];
+    const SysDev<V>& d = D[w.sys];
+    const bool init = st[w.sys].status == kInit;
+    double s = d.b[i];
+#pragma unroll 1
+    for (int j0 = 0; j0 < len; j0 += 8) {
+      double xv[8], vv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (j0 + u < len) {
+          vv[u] = v[j0 + u];
+          xv[u] = d.x[c[j0 + u]];
+        }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (j0 + u < len) s = __dsub_rn(s, __dmul_rn(vv[u], xv[u]));
+    }
+    if (init) {
+      const double aii = d.val[d.dia[i]];
+      d.dinv[i] = (V)__drcp_rn(aii);
+      bb = __dadd_rn(bb, __dmul_rn(d.b[i], d.b[i]));
+    }
+    const V ri = (V)s;
+    d.r[i] = ri;
+    const V zi = ri * d.dinv[i];
+    rr = __dadd_rn(rr, __dmul_rn(s, s));
+    rho = __dadd_rn(rho, __dmul_rn((double)zi, (double)ri));
+  }
+  __device__ void tile_end(int k) {
+    const Work w = work[k];
+    const SysDev<V>& d = D[w.sys];
+    double mine[3] = {block_red<kSum>(rr, scratch), block_red<kSum>(rho, scratch),
+                      block_red<kSum>(bb, scratch)};
+    rr = rho = bb = 0.0;
+    double out[3];
+    if (sys_reduce<3>(&st[w.sys].cnt_res, d.part, d.ntiles, mine,
+                      d.part + (size_t)w.tile * kPartQ, out, scratch) &&
+        threadIdx.x == 0) {
+      SysState& s = st[w.sys];
+      if (s.status == kInit) {
+        s.bnorm2 = out[2];
+        s.status = kActive;
+        s.first = 1;
+        s.iter = 0;
+      }
+      s.n_ru += 1;
+      const double bn = s.bnorm2 > 0.0 ? __dsqrt_rn(s.bnorm2) : 1.0;
+      s.res_true = __ddiv_rn(__dsqrt_rn(out[0]), bn);
+      s.need_ru = 0;
+      if (s.res_true <= d.tol) {
+        s.status = kConverged;
+      } else if (s.iter >= d.maxit) {
+        s.status = kMaxIter;
+      } else if (!(out[0] == out[0])) {
+        s.status = kBreakdown;
+      } else {
+        s.rr = out[0];
+        s.rr_ru = out[0];
+        s.rho = out[1];
+        if (!s.first) s.beta = __ddiv_rn(s.rho, s.rho_old);
+      }
+    }
+  }
+};
+
+template <typename V>
+__global__ void __launch_bounds__(kRows) kb_ru_res(BatchArgs a) {
+  __shared__ double scratch[32];
+  ResWork<V> w{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, *a.nwork, 0.0, 0.0, 0.0,
+               scratch};
+  stream_work<kRows, kNnzCap, double, kStages>(w);
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+struct Arena {
+  char* base = nullptr;
+  size_t size = 0;
+  std::map<size_t, size_t> free_;   // offset -> length
+  int init(size_t bytes) {
+    size = bytes;
+    TF_CUDA_TRY(cudaMalloc((void**)&base, bytes));
+    free_.clear();
+    free_[0] = bytes;
+    return TF_OK;
+  }
+  static size_t up(size_t v) { return (v + 255) & ~size_t(255); }
+  bool alloc(size_t bytes, size_t* off) {
+    bytes = up(bytes);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= bytes) {
+        *off = it->first;
+        const size_t rest = it->second - bytes;
+        const size_t o = it->first + bytes;
+        free_.erase(it);
+        if (rest) free_[o] = rest;
+        return true;
+      }
+    }
+    return false;
+  }
+  void release(size_t off, size_t bytes) {
+    bytes = up(bytes);
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  size_t free_bytes() const {
+    size_t s = 0;
+    for (auto& kv : free_) s += kv.second;
+    return s;
+  }
+};
+
+// Host copy of one system, converted and tiled, ready to upload.
+struct HostSys {
+  int n = 0;
+  long long nnz = 0;
+  std::vector<int> row, col, dia, tiles;
+  std::vector<double> val, b, x0;
+  std::vector<float> val32;
+  double tol = 1e-10;
+  int maxit = 10000;
+};
+
+int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* col,
+                 const int* dia, const double* val, const double* b, const double* x0,
+                 double tol, int maxit, int use_val32) {
+  if (n < 1 || nnz < n || !row || !col || !dia || !val || !b) return TF_ERR_ARG;
+  if (row[0] != 1 || (long long)row[n] - 1 != nnz) return TF_ERR_LAYOUT;
+  h.n = n;
+  h.nnz = nnz;
+  h.tol = tol;
+  h.maxit = maxit;
+  h.row.resize((size_t)n + 1 + 8);
+  h.col.resize((size_t)nnz + 8);
+  h.dia.resize((size_t)n + 8);
+  for (int i = 0; i <= n; ++i) h.row[i] = row[i] - 1;
+  for (size_t i = n + 1; i < h.row.size(); ++i) h.row[i] = h.row[n];
+  for (long long j = 0; j < nnz; ++j) {
+    if (col[j] < 1 || col[j] > n) return TF_ERR_LAYOUT;
+    h.col[j] = col[j] - 1;
+  }
+  for (int i = 0; i < n; ++i) {
+    if (h.row[i + 1] < h.row[i]) return TF_ERR_LAYOUT;
+    const int d = dia[i] - 1;
+    if (d < h.row[i] || d >= h.row[i + 1] || h.col[d] != i) return TF_ERR_LAYOUT;
+    h.dia[i] = d;
+  }
+  // tiles: <= kRows rows and <= kNnzCap entries each
+  h.tiles.clear();
+  h.tiles.push_back(0);
+  int r0 = 0;
+  while (r0 < n) {
+    int r1 = r0;
+    while (r1 < n && r1 - r0 < kRows && h.row[r1 + 1] - h.row[r0] <= kNnzCap) ++r1;
+    if (r1 == r0) return TF_ERR_LAYOUT;   // one row longer than a tile stage
+    h.tiles.push_back(r1);
+    r0 = r1;
+  }
+  h.val.assign(val, val + nnz);
+  h.val.resize((size_t)nnz + 8, 0.0);
+  if (use_val32) {
+    h.val32.resize((size_t)nnz + 8);
+    for (long long j = 0; j < nnz + 8; ++j) h.val32[j] = (float)h.val[j];
+  }
+  h.b.assign(b, b + n);
+  if (x0) h.x0.assign(x0, x0 + n);
+  else h.x0.assign(n, 0.0);
+  return TF_OK;
+}
+
+// Byte layout of one system's segment.
+struct Layout {
+  size_t row, col, dia, tiles, val, val32, b, x, xlo, r, p, q, dinv, part, total;
+};
+
+Layout layout_for(const HostSys& h, size_t vsz, int use_val32) {
+  Layout L{};
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t r = o; o = Arena::up(o + bytes); return r; };
+  const size_t n8 = (size_t)h.n + 8;
+  const int ntiles = (int)h.tiles.size() - 1;
+  L.row = take(h.row.size() * 4);
+  L.col = take(h.col.size() * 4);
+  L.dia = take(h.dia.size() * 4);
+  L.tiles = take(h.tiles.size() * 4);
+  L.val = take(h.val.size() * 8);
+  L.val32 = use_val32 ? take(h.val32.size() * 4) : 0;
+  L.b = take(n8 * 8);
+  L.x = take(n8 * 8);
+  L.xlo = take(n8 * vsz);
+  L.r = take(n8 * vsz);
+  L.p = take(n8 * vsz);
+  L.q = take(n8 * vsz);
+  L.dinv = take(n8 * vsz);
+  L.part = take((size_t)ntiles * kPartQ * 8);
+  L.total = o;
+  return L;
+}
+
+struct Slot {
+  int used = 0;
+  size_t off = 0, bytes = 0;
+  int n = 0, ntiles = 0;
+  Layout L{};
+};
+
+}  // namespace tfb
+
+using namespace tfb;
+
+// ---------------------------------------------------------------------------
+// The engine (one per tf_batch / tf_server)
+// ---------------------------------------------------------------------------
+struct tf_batch_s {
+  tf_ctx_s* ctx = nullptr;
+  tf_batch_opts opts{};
+  size_t vsz = 4;
+  Arena arena;
+  int max_sys = 0;
+  std::vector<Slot> slots;
+  void* d_desc = nullptr;           // SysDev<V>[max_sys]
+  SysState* d_state = nullptr;
+  SysState* h_state = nullptr;      // pinned mirror
+  Work* d_work = nullptr;
+  int* d_nwork = nullptr;
+  int work_cap = 0;
+  std::vector<Work> h_work;
+  int nwork = 0;
+  cudaGraphExec_t sweep = nullptr;
+  int grid_plain = 1, grid_tile = 1;
+  int sweeps = 0;
+  long long total_iters = 0;
+
+  ~tf_batch_s() {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (sweep) cudaGraphExecDestroy(sweep);
+    if (arena.base) cudaFree(arena.base);
+    for (void* p : {d_desc, (void*)d_state, (void*)d_work, (void*)d_nwork})
+      if (p) cudaFree(p);
+    if (h_state) cudaFreeHost(h_state);
+  }
+
+  template <typename V>
+  void launch_iteration(cudaStream_t s, const BatchArgs& a) {
+    const size_t sm = TileLayout<kRows, kNnzCap, double, kStages>::kSmemBytes;
+    const size_t sm32 = TileLayout<kRows, kNnzCap, float, kStages>::kSmemBytes;
+    kb_pupdate<V><<<grid_plain, kRows, 0, s>>>(a);
+    if (opts.val_fp32) kb_spmv<V, float><<<grid_tile, kRows, sm32, s>>>(a);
+    else kb_spmv<V, double><<<grid_tile, kRows, sm, s>>>(a);
+    kb_update<V><<<grid_plain, kRows, 0, s>>>(a);
+    kb_ru_fold<V><<<grid_plain, kRows, 0, s>>>(a);
+    kb_ru_res<V><<<grid_tile, kRows, sm, s>>>(a);
+  }
+
+  template <typename V>
+  int setup_kernels() {
+    const size_t sm = TileLayout<kRows, kNnzCap, double, kStages>::kSmemBytes;
+    const size_t sm32 = TileLayout<kRows, kNnzCap, float, kStages>::kSmemBytes;
+    TF_CUDA_TRY(cudaFuncSetAttribute(kb_spmv<V, double>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    TF_CUDA_TRY(cudaFuncSetAttribute(kb_spmv<V, float>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm32));
+    TF_CUDA_TRY(cudaFuncSetAttribute(kb_ru_res<V>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int per_sm = 1;
+    TF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_spmv<V, double>,
+                                                              kRows, sm));
+    grid_tile = std::max(1, per_sm) * ctx->sm_count;
+    grid_plain = ctx->sm_count * 8;
+    return TF_OK;
+  }
+
+  int build_sweep() {
+    if (sweep) {
+      cudaGraphExecDestroy(sweep);
+      sweep = nullptr;
+    }
+    cudaStream_t s = ctx->stream;
+    BatchArgs a{d_desc, d_state, d_work, d_nwork, opts.ru_delta * opts.ru_delta};
+    cudaGraph_t g = nullptr;
+    TF_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int it = 0; it < opts.sweep_iters; ++it) {
+      if (vsz == 4) launch_iteration<float>(s, a);
+      else launch_iteration<double>(s, a);
+    }
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    TF_CUDA_TRY(e);
+    e = cudaGraphInstantiate(&sweep, g, 0);
+    cudaGraphDestroy(g);
+    TF_CUDA_TRY(e);
+    return TF_OK;
+  }
+
+  int init(tf_ctx_s* c, const tf_batch_opts* o) {
+    ctx = c;
+    opts.vec_fp32 = 1;
+    opts.val_fp32 = 0;
+    opts.sweep_iters = 8;
+    opts.ru_delta = 0.1;
+    opts.mem_budget = (size_t)4 << 30;
+    opts.max_systems = 1024;
+    if (o) {
+      opts = *o;
+      if (opts.sweep_iters < 1) opts.sweep_iters = 8;
+      if (!(opts.ru_delta > 0.0 && opts.ru_delta < 1.0)) opts.ru_delta = 0.1;
+      if (opts.max_systems < 1) opts.max_systems = 1024;
+      if (opts.mem_budget < ((size_t)1 << 20)) opts.mem_budget = (size_t)1 << 20;
+    }
+    vsz = opts.vec_fp32 ? 4 : 8;
+    max_sys = opts.max_systems;
+    TF_CUDA_TRY(cudaSetDevice(ctx->device));
+    int st = arena.init(opts.mem_budget);
+    if (st != TF_OK) return st;
+    slots.assign(max_sys, Slot{});
+    const size_t desc_bytes = (size_t)max_sys * std::max(sizeof(SysDev<float>),
+                                                         sizeof(SysDev<double>));
+    TF_CUDA_TRY(cudaMalloc(&d_desc, desc_bytes));
+    TF_CUDA_TRY(cudaMemset(d_desc, 0, desc_bytes));
+    TF_CUDA_TRY(cudaMalloc((void**)&d_state, (size_t)max_sys * sizeof(SysState)));
+    TF_CUDA_TRY(cudaMemset(d_state, 0, (size_t)max_sys * sizeof(SysState)));
+    TF_CUDA_TRY(cudaMallocHost((void**)&h_state, (size_t)max_sys * sizeof(SysState)));
+    memset(h_state, 0, (size_t)max_sys * sizeof(SysState));
+    TF_CUDA_TRY(cudaMalloc((void**)&d_nwork, sizeof(int)));
+    TF_CUDA_TRY(cudaMemset(d_nwork, 0, sizeof(int)));
+    st = (vsz == 4) ? setup_kernels<float>() : setup_kernels<double>();
+    if (st != TF_OK) return st;
+    return build_sweep();
+  }
+
+  // Upload a prepared system into a free slot; TF_ERR_BUSY if no slot or
+  // no arena space (the caller may retry after other systems retire).
+  int admit(const HostSys& h, int* out_slot) {
+    int slot = -1;
+    for (int i = 0; i < max_sys; ++i)
+      if (!slots[i].used) { slot = i; break; }
+    if (slot < 0) return TF_ERR_BUSY;
+    const Layout L = layout_for(h, vsz, opts.val_fp32);
+    size_t off = 0;
+    if (!arena.alloc(L.total, &off)) return TF_ERR_BUSY;
+    cudaStream_t s = ctx->stream;
+    char* base = arena.base + off;
+    auto up = [&](size_t o, const void* src, size_t bytes) {
+      return cudaMemcpyAsync(base + o, src, bytes, cudaMemcpyHostToDevice, s);
+    };
+    const size_t n8 = (size_t)h.n + 8;
+    cudaError_t e = up(L.row, h.row.data(), h.row.size() * 4);
+    if (e == cudaSuccess) e = up(L.col, h.col.data(), h.col.size() * 4);
+    if (e == cudaSuccess) e = up(L.dia, h.dia.data(), h.dia.size() * 4);
+    if (e == cudaSuccess) e = up(L.tiles, h.tiles.data(), h.tiles.size() * 4);
+    if (e == cudaSuccess) e = up(L.val, h.val.data(), h.val.size() * 8);
+    if (e == cudaSuccess && opts.val_fp32) e = up(L.val32, h.val32.data(), h.val32.size() * 4);
+    if (e == cudaSuccess) e = up(L.b, h.b.data(), (size_t)h.n * 8);
+    if (e == cudaSuccess) e = up(L.x, h.x0.data(), (size_t)h.n * 8);
+    if (e == cudaSuccess) e = cudaMemsetAsync(base + L.xlo, 0, n8 * vsz, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(base + L.p, 0, n8 * vsz, s);
+    if (e != cudaSuccess) {
+      arena.release(off, L.total);
+      tf_set_last_cuda_error(e, "batch admit copies", __FILE__, __LINE__);
+      return TF_ERR_CUDA;
+    }
+    const int ntiles = (int)h.tiles.size() - 1;
+    auto fill = [&](auto& d) {
+      using VV = std::remove_pointer_t<decltype(d.xlo)>;
+      d.row = (const int*)(base + L.row);
+      d.col = (const int*)(base + L.col);
+      d.dia = (const int*)(base + L.dia);
+      d.tiles = (const int*)(base + L.tiles);
+      d.val = (const double*)(base + L.val);
+      d.val32 = opts.val_fp32 ? (const float*)(base + L.val32) : nullptr;
+      d.b = (const double*)(base + L.b);
+      d.x = (double*)(base + L.x);
+      d.xlo = (VV*)(base + L.xlo);
+      d.r = (VV*)(base + L.r);
+      d.p = (VV*)(base + L.p);
+      d.q = (VV*)(base + L.q);
+      d.dinv = (VV*)(base + L.dinv);
+      d.part = (double*)(base + L.part);
+      d.n = h.n;
+      d.ntiles = ntiles;
+      d.maxit = h.maxit;
+      d.use_val32 = opts.val_fp32;
+      d.tol = h.tol;
+    };
+    SysState ss{};
+    ss.status = kInit;
+    if (vsz == 4) {
+      SysDev<float> d{};
+      fill(d);
+      e = cudaMemcpyAsync((SysDev<float>*)d_desc + slot, &d, sizeof d, cudaMemcpyHostToDevice, s);
+    } else {
+      SysDev<double> d{};
+      fill(d);
+      e = cudaMemcpyAsync((SysDev<double>*)d_desc + slot, &d, sizeof d, cudaMemcpyHostToDevice, s);
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_state + slot, &ss, sizeof ss, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // host buffers may go away
+    if (e != cudaSuccess) {
+      arena.release(off, L.total);
+      tf_set_last_cuda_error(e, "batch admit descriptors", __FILE__, __LINE__);
+      return TF_ERR_CUDA;
+    }
+    Slot& sl = slots[slot];
+    sl.used = 1;
+    sl.off = off;
+    sl.bytes = L.total;
+    sl.n = h.n;
+    sl.ntiles = ntiles;
+    sl.L = L;
+    h_state[slot] = ss;
+    *out_slot = slot;
+    return TF_OK;
+  }
+
+  // Work list = every tile of every system that still iterates.
+  int rebuild_work() {
+    h_work.clear();
+    for (int i = 0; i < max_sys; ++i) {
+      if (!slots[i].used) continue;
+      const int stt = h_state[i].status;
+      if (stt != kInit && stt != kActive) continue;
+      for (int t = 0; t < slots[i].ntiles; ++t) h_work.push_back(Work{i, t});
+    }
+    nwork = (int)h_work.size();
+    if (nwork > work_cap) {
+      if (d_work) cudaFree(d_work);
+      d_work = nullptr;
+      work_cap = std::max(nwork, 2 * work_cap);
+      TF_CUDA_TRY(cudaMalloc((void**)&d_work, (size_t)work_cap * sizeof(Work)));
+      int st = build_sweep();   // the graph holds the work-list pointer
+      if (st != TF_OK) return st;
+    }
+    cudaStream_t s = ctx->stream;
+    if (nwork)
+      TF_CUDA_TRY(cudaMemcpyAsync(d_work, h_work.data(), (size_t)nwork * sizeof(Work),
+                                  cudaMemcpyHostToDevice, s));
+    TF_CUDA_TRY(cudaMemcpyAsync(d_nwork, &nwork, sizeof(int), cudaMemcpyHostToDevice, s));
+    TF_CUDA_TRY(cudaStreamSynchronize(s));
+    return TF_OK;
+  }
+
+  // One sweep (sweep_iters iterations), then refresh the host state mirror.
+  int run_sweep() {
+    cudaStream_t s = ctx->stream;
+    TF_CUDA_TRY(cudaGraphLaunch(sweep, s));
+    TF_CUDA_TRY(cudaMemcpyAsync(h_state, d_state, (size_t)max_sys * sizeof(SysState),
+                                cudaMemcpyDeviceToHost, s));
+    TF_CUDA_TRY(cudaStreamSynchronize(s));
+    ++sweeps;
+    return TF_OK;
+  }
+
+  int n_running() const {
+    int c = 0;
+    for (int i = 0; i < max_sys; ++i)
+      if (slots[i].used && (h_state[i].status == kInit || h_state[i].status == kActive)) ++c;
+    return c;
+  }
+
+  int run_all() {
+    int st = rebuild_work();
+    if (st != TF_OK) return st;
+    int running = n_running();
+    while (running > 0) {
+      st = run_sweep();
+      if (st != TF_OK) return st;
+      const int now = n_running();
+      if (now != running) {
+        st = rebuild_work();
+        if (st != TF_OK) return st;
+      }
+      running = now;
+    }
+    return TF_OK;
+  }
+
+  int fetch_x(int slot, double* x) {
+    const Slot& sl = slots[slot];
+    TF_CUDA_TRY(cudaMemcpyAsync(x, arena.base + sl.off + sl.L.x, (size_t)sl.n * 8,
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    TF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return TF_OK;
+  }
+
+  void retire(int slot) {
+    Slot& sl = slots[slot];
+    if (!sl.used) return;
+    arena.release(sl.off, sl.bytes);
+    sl = Slot{};
+    h_state[slot].status = kFree;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// C ABI: batches
+// ---------------------------------------------------------------------------
+extern "C" int tf_batch_create(tf_ctx ctx, const tf_batch_opts* opts, tf_batch* out) {
+  if (!ctx || !out) return TF_ERR_ARG;
+  *out = nullptr;
+  auto* b = new tf_batch_s();
+  const int st = b->init(ctx, opts);
+  if (st != TF_OK) {
+    delete b;
+    return st;
+  }
+  *out = b;
+  return TF_OK;
+}
+
+extern "C" int tf_batch_destroy(tf_batch b) {
+  if (!b) return TF_ERR_ARG;
+  delete b;
+  return TF_OK;
+}
+
+extern "C" int tf_batch_add(tf_batch bt, int n, int64_t nnz, const int* row, const int* col,
+                            const int* dia, const double* val, const double* b,
+                            const double* x0, double tol, int maxit, int* sys) {
+  if (!bt || !sys) return TF_ERR_ARG;
+  HostSys h;
+  int st = prepare_host(h, n, nnz, row, col, dia, val, b, x0, tol, maxit, bt->opts.val_fp32);
+  if (st != TF_OK) return st;
+  TF_CUDA_TRY(cudaSetDevice(bt->ctx->device));
+  return bt->admit(h, sys);
+}
+
+extern "C" int tf_batch_run(tf_batch bt) {
+  if (!bt) return TF_ERR_ARG;
+  TF_CUDA_TRY(cudaSetDevice(bt->ctx->device));
+  return bt->run_all();
+}
+
+extern "C" int tf_batch_result(tf_batch bt, int sys, double* x, int* iters,
+                               double* true_rel_res, int* status, int* n_updates) {
+  if (!bt || sys < 0 || sys >= bt->max_sys || !bt->slots[sys].used) return TF_ERR_ARG;
+  const SysState& s = bt->h_state[sys];
+  if (iters) *iters = s.iter;
+  if (true_rel_res) *true_rel_res = s.res_true;
+  if (status) *status = s.status;
+  if (n_updates) *n_updates = s.n_ru;
+  if (x) return bt->fetch_x(sys, x);
+  return TF_OK;
+}
+
+extern "C" int tf_batch_remove(tf_batch bt, int sys) {
+  if (!bt || sys < 0 || sys >= bt->max_sys || !bt->slots[sys].used) return TF_ERR_ARG;
+  bt->retire(sys);
+  return TF_OK;
+}
+
+extern "C" int tf_batch_info(tf_batch bt, int* sweeps, int* work_items, size_t* free_bytes) {
+  if (!bt) return TF_ERR_ARG;
+  if (sweeps) *sweeps = bt->sweeps;
+  if (work_items) *work_items = bt->nwork;
+  if (free_bytes) *free_bytes = bt->arena.free_bytes();
+  return TF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI: the serving loop (continuous batching)
+// ---------------------------------------------------------------------------
+namespace {
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  int64_t id = 0;
+  HostSys h;
+  Clock::time_point t_submit, t_admit, t_done;
+  int slot = -1;
+  int status = 0;       // SysStatus at completion, or an error code (< 0)
+  int iters = 0, n_ru = 0;
+  double res = 0.0;
+  std::vector<double> x;
+  bool done = false;
+};
+}  // namespace
+
+struct tf_server_s {
+  tf_batch_s eng;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<std::shared_ptr<Request>> queue;
+  std::map<int64_t, std::shared_ptr<Request>> live;     // submitted, not yet collected
+  std::map<int, std::shared_ptr<Request>> by_slot;      // admitted, running
+  int64_t next_id = 1;
+  bool stop = false;
+  int error = TF_OK;
+  std::thread worker;
+  // stats
+  long long admitted = 0, completed = 0, rejected = 0;
+  int peak_running = 0;
+
+  void loop() {
+    cudaSetDevice(eng.ctx->device);
+    for (;;) {
+      std::vector<std::shared_ptr<Request>> incoming;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_work.wait(lk, [&] { return stop || !queue.empty() || !by_slot.empty(); });
+        if (stop) return;
+      }
+      // Admit from the queue in arrival order while memory and slots allow.
+      bool changed = false;
+      for (;;) {
+        std::shared_ptr<Request> r;
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          if (queue.empty()) break;
+          r = queue.front();
+        }
+        int slot = -1;
+        const int st = eng.admit(r->h, &slot);
+        if (st == TF_ERR_BUSY) {
+          if (by_slot.empty()) {   // cannot ever fit: fail the request
+            std::lock_guard<std::mutex> lk(mu);
+            queue.pop_front();
+            r->status = -TF_ERR_OOM;
+            r->done = true;
+            r->t_done = Clock::now();
+            ++rejected;
+            cv_done.notify_all();
+            continue;
+          }
+          break;
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        queue.pop_front();
+        if (st != TF_OK) {
+          r->status = -st;
+          r->done = true;
+          r->t_done = Clock::now();
+          cv_done.notify_all();
+          continue;
+        }
+        r->slot = slot;
+        r->t_admit = Clock::now();
+        by_slot[slot] = r;
+        ++admitted;
+        changed = true;
+      }
+      if (by_slot.empty()) continue;
+      peak_running = std::max(peak_running, (int)by_slot.size());
+      int st = TF_OK;
+      if (changed) st = eng.rebuild_work();
+      if (st == TF_OK) st = eng.run_sweep();
+      if (st != TF_OK) {
+        std::lock_guard<std::mutex> lk(mu);
+        error = st;
+        for (auto& kv : by_slot) {
+          kv.second->status = -st;
+          kv.second->done = true;
+        }
+        by_slot.clear();
+        cv_done.notify_all();
+        continue;
+      }
+      // Retire finished systems.
+      std::vector<int> fin;
+      for (auto& kv : by_slot) {
+        const int s = eng.h_state[kv.first].status;
+        if (s != kInit && s != kActive) fin.push_back(kv.first);
+      }
+      for (int slot : fin) {
+        auto r = by_slot[slot];
+        const SysState& ss = eng.h_state[slot];
+        r->x.resize(r->h.n);
+        eng.fetch_x(slot, r->x.data());
+        std::lock_guard<std::mutex> lk(mu);
+        r->status = ss.status;
+        r->iters = ss.iter;
+        r->n_ru = ss.n_ru;
+        r->res = ss.res_true;
+        r->t_done = Clock::now();
+        r->done = true;
+        eng.retire(slot);
+        by_slot.erase(slot);
+        ++completed;
+        cv_done.notify_all();
+      }
+      if (!fin.empty()) eng.rebuild_work();
+    }
+  }
+};
+
+extern "C" int tf_server_create(tf_ctx ctx, const tf_batch_opts* opts, tf_server* out) {
+  if (!ctx || !out) return TF_ERR_ARG;
+  *out = nullptr;
+  auto* s = new tf_server_s();
+  const int st = s->eng.init(ctx, opts);
+  if (st != TF_OK) {
+    delete s;
+    return st;
+  }
+  s->worker = std::thread([s] { s->loop(); });
+  *out = s;
+  return TF_OK;
+}
+
+extern "C" int tf_server_submit(tf_server sv, int n, int64_t nnz, const int* row,
+                                const int* col, const int* dia, const double* val,
+                                const double* b, const double* x0, double tol, int maxit,
+                                int64_t* req) {
+  if (!sv || !req) return TF_ERR_ARG;
+  auto r = std::make_shared<Request>();
+  const int st = prepare_host(r->h, n, nnz, row, col, dia, val, b, x0, tol, maxit,
+                              sv->eng.opts.val_fp32);
+  if (st != TF_OK) return st;
+  std::lock_guard<std::mutex> lk(sv->mu);
+  if (sv->stop) return TF_ERR_CANCELLED;
+  r->id = sv->next_id++;
+  r->t_submit = Clock::now();
+  sv->queue.push_back(r);
+  sv->live[r->id] = r;
+  *req = r->id;
+  sv->cv_work.notify_one();
+  return TF_OK;
+}
+
+extern "C" int tf_server_wait(tf_server sv, int64_t req, double* x, int* iters,
+                              double* true_rel_res, int* status, double* latency_ms,
+                              double* queue_ms) {
+  if (!sv) return TF_ERR_ARG;
+  std::unique_lock<std::mutex> lk(sv->mu);
+  auto it = sv->live.find(req);
+  if (it == sv->live.end()) return TF_ERR_ARG;
+  auto r = it->second;
+  sv->cv_done.wait(lk, [&] { return r->done; });
+  sv->live.erase(req);
+  if (status) *status = r->status;
+  if (iters) *iters = r->iters;
+  if (true_rel_res) *true_rel_res = r->res;
+  using ms = std::chrono::duration<double, std::milli>;
+  if (latency_ms) *latency_ms = ms(r->t_done - r->t_submit).count();
+  if (queue_ms)
+    *queue_ms = r->slot >= 0 ? ms(r->t_admit - r->t_submit).count()
+                             : ms(r->t_done - r->t_submit).count();
+  if (r->status < 0) return -r->status;
+  if (x && !r->x.empty()) memcpy(x, r->x.data(), r->x.size() * sizeof(double));
+  return TF_OK;
+}
+
+extern "C" int tf_server_stats(tf_server sv, long long* admitted, long long* completed,
+                               int* peak_running, int* sweeps) {
+  if (!sv) return TF_ERR_ARG;
+  std::lock_guard<std::mutex> lk(sv->mu);
+  if (admitted) *admitted = sv->admitted;
+  if (completed) *completed = sv->completed;
+  if (peak_running) *peak_running = sv->peak_running;
+  if (sweeps) *sweeps = sv->eng.sweeps;
+  return sv->error;
+}
+
+extern "C" int tf_server_destroy(tf_server sv) {
+  if (!sv) return TF_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->stop = true;
+    for (auto& kv : sv->live)
+      if (!kv.second->done) {
+        kv.second->status = -TF_ERR_CANCELLED;
+        kv.second->done = true;
+      }
+    sv->cv_work.notify_all();
+    sv->cv_done.notify_all();
+  }
+  if (sv->worker.joinable()) sv->worker.join();
+  delete sv;
+  return TF_OK;
+}

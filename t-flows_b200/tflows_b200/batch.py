@@ -1,0 +1,150 @@
+"""ctypes binding of the batched / served solver API (tf_batch_*, tf_server_*)."""
+import ctypes
+
+import numpy as np
+
+from . import native
+
+_vp = ctypes.c_void_p
+STATUS = {0: "free", 1: "init", 2: "active", 3: "converged", 4: "maxiter", 5: "breakdown"}
+
+
+class BatchOpts(ctypes.Structure):
+    _fields_ = [("vec_fp32", ctypes.c_int), ("val_fp32", ctypes.c_int),
+                ("sweep_iters", ctypes.c_int), ("max_systems", ctypes.c_int),
+                ("ru_delta", ctypes.c_double), ("mem_budget", ctypes.c_size_t)]
+
+
+def _lib():
+    L = native.load()
+    if getattr(L, "_tf_batch_bound", False):
+        return L
+    ip, dp = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    L.tf_batch_create.argtypes = [_vp, ctypes.POINTER(BatchOpts), ctypes.POINTER(_vp)]
+    L.tf_batch_destroy.argtypes = [_vp]
+    L.tf_batch_add.argtypes = [_vp, ctypes.c_int, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp,
+                               _vp, ctypes.c_double, ctypes.c_int, ip]
+    L.tf_batch_run.argtypes = [_vp]
+    L.tf_batch_result.argtypes = [_vp, ctypes.c_int, _vp, ip, dp, ip, ip]
+    L.tf_batch_remove.argtypes = [_vp, ctypes.c_int]
+    L.tf_batch_info.argtypes = [_vp, ip, ip, ctypes.POINTER(ctypes.c_size_t)]
+    L.tf_server_create.argtypes = [_vp, ctypes.POINTER(BatchOpts), ctypes.POINTER(_vp)]
+    L.tf_server_submit.argtypes = [_vp, ctypes.c_int, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp,
+                                   _vp, ctypes.c_double, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_int64)]
+    L.tf_server_wait.argtypes = [_vp, ctypes.c_int64, _vp, ip, dp, ip, dp, dp]
+    L.tf_server_stats.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong),
+                                  ctypes.POINTER(ctypes.c_longlong), ip, ip]
+    L.tf_server_destroy.argtypes = [_vp]
+    L._tf_batch_bound = True
+    return L
+
+
+def _opts(vec_fp32=True, val_fp32=False, sweep_iters=8, max_systems=1024, ru_delta=0.1,
+          mem_budget=4 << 30):
+    return BatchOpts(int(vec_fp32), int(val_fp32), int(sweep_iters), int(max_systems),
+                     float(ru_delta), int(mem_budget))
+
+
+def _sys_args(s):
+    row = np.ascontiguousarray(s.csr.row, np.int32)
+    col = np.ascontiguousarray(s.csr.col, np.int32)
+    dia = np.ascontiguousarray(s.csr.dia, np.int32)
+    val = np.ascontiguousarray(s.val, np.float64)
+    b = np.ascontiguousarray(s.b, np.float64)
+    x0 = np.ascontiguousarray(s.x0, np.float64)
+    keep = (row, col, dia, val, b, x0)
+    p = lambda a: a.ctypes.data_as(_vp)  # noqa: E731
+    return keep, (s.n, s.nnz, p(row), p(col), p(dia), p(val), p(b), p(x0))
+
+
+class Batch:
+    def __init__(self, ctx, **opts):
+        self.L = _lib()
+        self.opts = _opts(**opts)
+        h = _vp()
+        native._check(self.L.tf_batch_create(ctx.h, ctypes.byref(self.opts), ctypes.byref(h)),
+                      "tf_batch_create")
+        self.h = h
+        self.n = {}
+
+    def add(self, s, tol=1e-10, maxit=20000):
+        keep, args = _sys_args(s)
+        sid = ctypes.c_int(-1)
+        native._check(self.L.tf_batch_add(self.h, *args, float(tol), int(maxit),
+                                          ctypes.byref(sid)), "tf_batch_add")
+        self.n[sid.value] = s.n
+        return sid.value
+
+    def run(self):
+        native._check(self.L.tf_batch_run(self.h), "tf_batch_run")
+
+    def result(self, sid, want_x=True):
+        x = np.empty(self.n[sid]) if want_x else None
+        it, st, nru = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        res = ctypes.c_double()
+        native._check(self.L.tf_batch_result(self.h, sid, x.ctypes.data_as(_vp) if want_x else None,
+                                             ctypes.byref(it), ctypes.byref(res),
+                                             ctypes.byref(st), ctypes.byref(nru)),
+                      "tf_batch_result")
+        return dict(x=x, iters=it.value, res=res.value, status=STATUS[st.value],
+                    n_updates=nru.value)
+
+    def remove(self, sid):
+        native._check(self.L.tf_batch_remove(self.h, sid), "tf_batch_remove")
+        self.n.pop(sid, None)
+
+    def info(self):
+        sw, wi = ctypes.c_int(), ctypes.c_int()
+        fb = ctypes.c_size_t()
+        native._check(self.L.tf_batch_info(self.h, ctypes.byref(sw), ctypes.byref(wi),
+                                           ctypes.byref(fb)), "tf_batch_info")
+        return dict(sweeps=sw.value, work_items=wi.value, free_bytes=fb.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.tf_batch_destroy(self.h)
+            self.h = None
+
+
+class Server:
+    def __init__(self, ctx, **opts):
+        self.L = _lib()
+        self.opts = _opts(**opts)
+        h = _vp()
+        native._check(self.L.tf_server_create(ctx.h, ctypes.byref(self.opts), ctypes.byref(h)),
+                      "tf_server_create")
+        self.h = h
+        self.n = {}
+
+    def submit(self, s, tol=1e-10, maxit=20000):
+        keep, args = _sys_args(s)
+        rid = ctypes.c_int64()
+        native._check(self.L.tf_server_submit(self.h, *args, float(tol), int(maxit),
+                                              ctypes.byref(rid)), "tf_server_submit")
+        self.n[rid.value] = s.n
+        return rid.value
+
+    def wait(self, rid):
+        x = np.empty(self.n.pop(rid))
+        it, st = ctypes.c_int(), ctypes.c_int()
+        res, lat, qms = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        rc = self.L.tf_server_wait(self.h, rid, x.ctypes.data_as(_vp), ctypes.byref(it),
+                                   ctypes.byref(res), ctypes.byref(st), ctypes.byref(lat),
+                                   ctypes.byref(qms))
+        native._check(rc, "tf_server_wait")
+        return dict(x=x, iters=it.value, res=res.value, status=STATUS.get(st.value, st.value),
+                    latency_ms=lat.value, queue_ms=qms.value)
+
+    def stats(self):
+        a, c = ctypes.c_longlong(), ctypes.c_longlong()
+        pk, sw = ctypes.c_int(), ctypes.c_int()
+        err = self.L.tf_server_stats(self.h, ctypes.byref(a), ctypes.byref(c), ctypes.byref(pk),
+                                     ctypes.byref(sw))
+        return dict(admitted=a.value, completed=c.value, peak_running=pk.value,
+                    sweeps=sw.value, error=err)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.tf_server_destroy(self.h)
+            self.h = None

@@ -1,0 +1,151 @@
+"""GPU tests of the batched and served mixed-precision solver.
+
+Accuracy bar: every system reaches ||b - A x||_2 / ||b||_2 <= 1e-10 in FP64
+(recomputed here with scipy), and x agrees with a direct FP64 solve to
+rel-L2 1e-6 (the condition numbers here are <= ~1e4).  Determinism bar: a
+system's x and iteration count are bit-identical alone and in any mix.
+"""
+import threading
+import time
+
+import numpy as np
+import pytest
+import scipy.sparse as sps
+import scipy.sparse.linalg as spla
+
+from tflows_b200 import batch, systems
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def _A(s):
+    return sps.csr_matrix((s.val, s.csr.col - 1, s.csr.row - 1), shape=(s.n, s.n))
+
+
+def _true_rel(s, x):
+    return np.linalg.norm(s.b - _A(s) @ x) / np.linalg.norm(s.b)
+
+
+def _direct(s):
+    return spla.spsolve(_A(s).tocsc(), s.b)
+
+
+def mixed_systems():
+    return [
+        systems.small_hex(12, seed=1, kind="pressure", ratio=1.02),
+        systems.small_hex(20, seed=2, kind="pressure", ratio=1.02),
+        systems.small_hex(10, seed=3, kind="momentum", peclet=1.0),
+        systems.poly_system(3000, seed=4, kind="pressure"),
+        systems.poly_system(2500, seed=5, kind="momentum", peclet=10.0),
+        systems.small_hex(3, seed=6, kind="pressure"),
+    ]
+
+
+@pytest.mark.parametrize("mode", [dict(vec_fp32=True), dict(vec_fp32=False),
+                                  dict(vec_fp32=True, val_fp32=True)],
+                         ids=["fp32vec", "fp64vec", "fp32vec_fp32val"])
+def test_batch_converges_to_true_tolerance(gpu_ctx, mode):
+    sysl = mixed_systems()
+    b = batch.Batch(gpu_ctx, mem_budget=1 << 30, **mode)
+    try:
+        ids = [b.add(s, tol=TOL, maxit=20000) for s in sysl]
+        b.run()
+        for s, i in zip(sysl, ids):
+            r = b.result(i)
+            assert r["status"] == "converged", (s.name, r["status"], r["res"])
+            assert r["res"] <= TOL
+            assert _true_rel(s, r["x"]) <= 1.01 * TOL
+            xd = _direct(s)
+            assert np.linalg.norm(r["x"] - xd) / np.linalg.norm(xd) < 1e-6
+    finally:
+        b.close()
+
+
+def test_batch_alone_equals_in_mix(gpu_ctx):
+    sysl = mixed_systems()
+    alone = []
+    for s in sysl[:3]:
+        b = batch.Batch(gpu_ctx, mem_budget=1 << 28)
+        try:
+            i = b.add(s)
+            b.run()
+            alone.append(b.result(i))
+        finally:
+            b.close()
+    b = batch.Batch(gpu_ctx, mem_budget=1 << 30, sweep_iters=5)
+    try:
+        ids = [b.add(s) for s in reversed(sysl)]
+        b.run()
+        mix = {len(sysl) - 1 - k: b.result(i) for k, i in enumerate(ids)}
+    finally:
+        b.close()
+    for k in range(3):
+        assert mix[k]["iters"] == alone[k]["iters"]
+        assert np.array_equal(mix[k]["x"], alone[k]["x"])
+
+
+def test_batch_memory_budget(gpu_ctx):
+    big = systems.small_hex(40, seed=1, kind="pressure")
+    b = batch.Batch(gpu_ctx, mem_budget=1 << 20)
+    try:
+        from tflows_b200 import native
+        with pytest.raises(native.TFError) as e:
+            b.add(big)
+        assert e.value.status == 7     # TF_ERR_BUSY
+        small = systems.small_hex(4, seed=1, kind="pressure")
+        i = b.add(small)
+        b.run()
+        assert b.result(i)["status"] == "converged"
+    finally:
+        b.close()
+
+
+def test_batch_maxiter_reported(gpu_ctx):
+    s = systems.small_hex(16, seed=1, kind="pressure", ratio=1.02)
+    b = batch.Batch(gpu_ctx, mem_budget=1 << 28)
+    try:
+        i = b.add(s, tol=TOL, maxit=5)
+        b.run()
+        r = b.result(i)
+        assert r["status"] == "maxiter" and r["iters"] == 5 and r["res"] > TOL
+    finally:
+        b.close()
+
+
+def test_server_continuous_batching(gpu_ctx):
+    """Requests arriving while others run join at the next sweep; each result
+    equals the same system solved alone."""
+    sysl = mixed_systems()
+    ref = {}
+    b = batch.Batch(gpu_ctx, mem_budget=1 << 30)
+    try:
+        ids = [b.add(s) for s in sysl]
+        b.run()
+        ref = {k: b.result(i) for k, i in enumerate(ids)}
+    finally:
+        b.close()
+    srv = batch.Server(gpu_ctx, mem_budget=1 << 30, sweep_iters=4)
+    try:
+        rids = {}
+
+        def producer():
+            for k, s in enumerate(sysl * 2):
+                rids[k] = srv.submit(s)
+                time.sleep(0.002 * (k % 3))
+
+        t = threading.Thread(target=producer)
+        t.start()
+        t.join()
+        for k in range(len(sysl) * 2):
+            r = srv.wait(rids[k])
+            want = ref[k % len(sysl)]
+            assert r["status"] == "converged"
+            assert r["iters"] == want["iters"]
+            assert np.array_equal(r["x"], want["x"])
+            assert r["latency_ms"] >= r["queue_ms"] >= 0.0
+        st = srv.stats()
+        assert st["completed"] == len(sysl) * 2 and st["error"] == 0
+    finally:
+        srv.close()
