@@ -165,9 +165,12 @@ int tf_batch_add(tf_batch b, int n, int64_t nnz, const int* row, const int* col,
 /* Iterate until every system has converged or stopped. */
 int tf_batch_run(tf_batch b);
 /* x (host, n doubles) may be NULL; true_rel_res = ||b-Ax||_2/||b||_2 in FP64;
- * n_updates counts FP64 residual evaluations (initial one included). */
+ * n_updates counts FP64 residual evaluations (initial one included);
+ * done_ms = wall time from the start of tf_batch_run to the sweep in which
+ * the system finished (-1 if it has not). */
 int tf_batch_result(tf_batch b, int sys, double* x, int* iters,
-                    double* true_rel_res, int* status, int* n_updates);
+                    double* true_rel_res, int* status, int* n_updates,
+                    double* done_ms);
 int tf_batch_remove(tf_batch b, int sys);
 int tf_batch_info(tf_batch b, int* sweeps, int* work_items, size_t* free_bytes);
 

@@ -518,6 +518,7 @@ struct Slot {
   int used = 0;
   size_t off = 0, bytes = 0;
   int n = 0, ntiles = 0;
+  double done_ms = -1.0;   // wall time from tf_batch_run's start to completion
   Layout L{};
 };
 
@@ -776,12 +777,20 @@ struct tf_batch_s {
   }
 
   int run_all() {
+    const auto t0 = std::chrono::steady_clock::now();
     int st = rebuild_work();
     if (st != TF_OK) return st;
     int running = n_running();
     while (running > 0) {
       st = run_sweep();
       if (st != TF_OK) return st;
+      const double ms =
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+              .count();
+      for (int i = 0; i < max_sys; ++i)
+        if (slots[i].used && slots[i].done_ms < 0.0 && h_state[i].status != kInit &&
+            h_state[i].status != kActive)
+          slots[i].done_ms = ms;
       const int now = n_running();
       if (now != running) {
         st = rebuild_work();
@@ -849,9 +858,11 @@ extern "C" int tf_batch_run(tf_batch bt) {
 }
 
 extern "C" int tf_batch_result(tf_batch bt, int sys, double* x, int* iters,
-                               double* true_rel_res, int* status, int* n_updates) {
+                               double* true_rel_res, int* status, int* n_updates,
+                               double* done_ms) {
   if (!bt || sys < 0 || sys >= bt->max_sys || !bt->slots[sys].used) return TF_ERR_ARG;
   const SysState& s = bt->h_state[sys];
+  if (done_ms) *done_ms = bt->slots[sys].done_ms;
   if (iters) *iters = s.iter;
   if (true_rel_res) *true_rel_res = s.res_true;
   if (status) *status = s.status;

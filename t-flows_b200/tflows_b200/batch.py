@@ -25,7 +25,7 @@ def _lib():
     L.tf_batch_add.argtypes = [_vp, ctypes.c_int, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp,
                                _vp, ctypes.c_double, ctypes.c_int, ip]
     L.tf_batch_run.argtypes = [_vp]
-    L.tf_batch_result.argtypes = [_vp, ctypes.c_int, _vp, ip, dp, ip, ip]
+    L.tf_batch_result.argtypes = [_vp, ctypes.c_int, _vp, ip, dp, ip, ip, dp]
     L.tf_batch_remove.argtypes = [_vp, ctypes.c_int]
     L.tf_batch_info.argtypes = [_vp, ip, ip, ctypes.POINTER(ctypes.c_size_t)]
     L.tf_server_create.argtypes = [_vp, ctypes.POINTER(BatchOpts), ctypes.POINTER(_vp)]
@@ -82,13 +82,14 @@ class Batch:
     def result(self, sid, want_x=True):
         x = np.empty(self.n[sid]) if want_x else None
         it, st, nru = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        res = ctypes.c_double()
+        res, dms = ctypes.c_double(), ctypes.c_double()
         native._check(self.L.tf_batch_result(self.h, sid, x.ctypes.data_as(_vp) if want_x else None,
                                              ctypes.byref(it), ctypes.byref(res),
-                                             ctypes.byref(st), ctypes.byref(nru)),
+                                             ctypes.byref(st), ctypes.byref(nru),
+                                             ctypes.byref(dms)),
                       "tf_batch_result")
         return dict(x=x, iters=it.value, res=res.value, status=STATUS[st.value],
-                    n_updates=nru.value)
+                    n_updates=nru.value, done_ms=dms.value)
 
     def remove(self, sid):
         native._check(self.L.tf_batch_remove(self.h, sid), "tf_batch_remove")

@@ -160,6 +160,100 @@ def hex_grid(nx, ny, nz, stretch_y=1.0):
                 kind="hex", meta=dict(nx=nx, ny=ny, nz=nz, stretch_y=stretch_y))
 
 
+def poly_lattice_grid(n_target, seed, jitter=0.25):
+    """Median dual of a jittered Freudenthal (Kuhn) tetrahedralisation.
+
+    Lattice vertices (nx*ny*nz ~ n_target, spacing h) are moved by
+    U[-jitter, jitter]*h in each direction; every lattice cube is split into
+    the 6 tetrahedra along its main diagonal.  Each vertex becomes one
+    polyhedral cell whose faces are the median-dual faces of its 14 edges
+    (directions (1,0,0), (0,1,0), (0,0,1), (1,1,0), (1,0,1), (0,1,1),
+    (1,1,1) and their opposites): interior cells have 14 faces, the face
+    normal is not parallel to the centre-to-centre vector (non-orthogonal
+    mesh), and the whole construction is O(n) and vectorised, unlike a
+    Delaunay dual.  Face area vector of edge (a, b) = sum over its
+    tetrahedra of 1/2 (c_T - m_ab) x (c_f1 - c_f2) with m the edge midpoint,
+    c_T the tet centroid and c_f the centroids of the tet's two faces that
+    contain the edge, oriented along b - a.  Cell volume = 1/4 of every
+    incident tet.  No boundary faces (zero-gradient walls).
+    """
+    m = max(2, int(round(n_target ** (1.0 / 3.0))))
+    nx = ny = m
+    nz = max(2, int(round(n_target / (m * m))))
+    h = 1.0 / max(nx - 1, ny - 1, nz - 1)
+    rng = np.random.default_rng(seed)
+    I, J, K = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    pts = np.stack([I.ravel(), J.ravel(), K.ravel()], axis=1).astype(np.float64) * h
+    pts += rng.uniform(-jitter, jitter, pts.shape) * h
+    vid = lambda i, j, k: (i * ny + j) * nz + k  # noqa: E731
+    # the 6 tetrahedra of every cube: paths (0,0,0) -> (1,1,1) along axes
+    ci, cj, ck = np.meshgrid(np.arange(nx - 1), np.arange(ny - 1), np.arange(nz - 1),
+                             indexing="ij")
+    ci, cj, ck = ci.ravel(), cj.ravel(), ck.ravel()
+    perms = [(0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)]
+    tets = []
+    for pm in perms:
+        o = np.zeros((len(ci), 3), dtype=np.int64)
+        v = [vid(ci, cj, ck)]
+        for ax in pm:
+            o[:, ax] += 1
+            v.append(vid(ci + o[:, 0], cj + o[:, 1], ck + o[:, 2]))
+        tets.append(np.stack(v, axis=1))
+    tets = np.concatenate(tets)
+    P = pts[tets]
+    cT = P.mean(axis=1)
+    n = nx * ny * nz
+    vol_t = np.abs(np.einsum("ij,ij->i", P[:, 1] - P[:, 0],
+                             np.cross(P[:, 2] - P[:, 0], P[:, 3] - P[:, 0]))) / 6.0
+    vol = np.bincount(tets.ravel(), weights=np.repeat(vol_t / 4.0, 4), minlength=n)
+    # Every tet edge joins a vertex to one of its 7 forward lattice neighbours
+    # (the path is monotone), so edge id = vertex * 8 + direction code.
+    stride = np.array([ny * nz, nz, 1])
+    code_off = np.array([[i >> 2 & 1, i >> 1 & 1, i & 1] for i in range(8)])
+    acc = np.zeros((8 * n, 3))
+    for (u, w) in ((0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)):
+        o1, o2 = [k for k in range(4) if k not in (u, w)]
+        mab = 0.5 * (P[:, u] + P[:, w])
+        cf1 = (P[:, u] + P[:, w] + P[:, o1]) / 3.0
+        cf2 = (P[:, u] + P[:, w] + P[:, o2]) / 3.0
+        sv = 0.5 * np.cross(cT - mab, cf1 - cf2)
+        a, b = tets[:, u], tets[:, w]            # a precedes b on the path
+        e = pts[b] - pts[a]
+        sgn = np.sign(np.einsum("ij,ij->i", sv, e))
+        sgn[sgn == 0] = 1.0
+        sv = sv * sgn[:, None]
+        d = b - a
+        code = ((d // stride[0]) % 2) * 4 + ((d % stride[0]) // stride[1] % 2) * 2 + (d % nz)
+        eid = a * 8 + code
+        for c in range(3):
+            acc[:, c] += np.bincount(eid, weights=sv[:, c], minlength=8 * n)
+    present = np.nonzero(np.any(acc != 0.0, axis=1))[0]
+    S = acc[present]
+    c1 = present // 8
+    off = code_off[present % 8]
+    c2 = c1 + off @ stride
+    # renumber cells by (x, y, z) like Sort_Cells_By_Coordinates.f90
+    order = np.lexsort((pts[:, 2], pts[:, 1], pts[:, 0]))
+    new = np.empty(n, dtype=np.int64)
+    new[order] = np.arange(n)
+    pts, vol = pts[order], vol[order]
+    c1, c2 = new[c1], new[c2]
+    flip = c1 > c2
+    c1, c2 = np.where(flip, c2, c1), np.where(flip, c1, c2)
+    S[flip] = -S[flip]
+    dvec = pts[c2] - pts[c1]
+    faces_c = np.stack([c1 + 1, c2 + 1], axis=1).astype(np.int32)
+    deg = np.bincount(c1, minlength=n) + np.bincount(c2, minlength=n)
+    dist = np.linalg.norm(dvec, axis=1)
+    return Grid(n_cells=n, faces_c=faces_c, sx=S[:, 0].copy(), sy=S[:, 1].copy(),
+                sz=S[:, 2].copy(), dx=dvec[:, 0].copy(), dy=dvec[:, 1].copy(),
+                dz=dvec[:, 2].copy(), fw=np.full(len(c1), 0.5), vol=vol,
+                h_min=float(dist.min()), h_mean=float(np.cbrt(vol).mean()), kind="poly-lattice",
+                meta=dict(seed=seed, dims=(nx, ny, nz), jitter=jitter,
+                          faces_per_cell_mean=float(deg.mean()),
+                          faces_per_cell_max=int(deg.max())))
+
+
 def poly_dual_grid(n_points, seed):
     """Voronoi dual of a seeded random Delaunay tetrahedralisation of [0,1]^3.
 
