@@ -92,6 +92,49 @@ def _drop_in_solve_times(ctx, sysl, rel):
     return out
 
 
+def _drop_in_stream_pool(sysl, workers, rel):
+    """The FP64 drop-in run from `workers` host threads, each owning a context
+    (one CUDA stream), so independent solves overlap on the GPU.  Systems are
+    dealt to the workers in decreasing size order; matrices are registered
+    and inputs uploaded before timing.  Returns wall seconds and
+    per-system (ms, iterations)."""
+    import torch
+    from tflows_b200 import native, workloads
+    ctxs = [native.Context(0) for _ in range(workers)]
+    order = sorted(range(len(sysl)), key=lambda k: -sysl[k].n)
+    jobs = [[] for _ in range(workers)]
+    for r, k in enumerate(order):
+        w = r % workers
+        s = sysl[k]
+        m = native.Matrix(ctxs[w], s.csr.row, s.csr.col, s.csr.dia)
+        jobs[w].append((k, s, m, torch.from_numpy(s.val).cuda(), torch.from_numpy(s.b).cuda(),
+                        torch.zeros(s.n, dtype=torch.float64, device="cuda"),
+                        rel * workloads.nrms_b(s)))
+    torch.cuda.synchronize()
+    out = [None] * len(sysl)
+
+    def worker(w):
+        for k, s, m, dval, db, dx, tol in jobs[w]:
+            t0 = time.perf_counter()
+            it, _ = native.solve_device(ctxs[w], m, s.solver, "jacobi", dval.data_ptr(),
+                                        dx.data_ptr(), db.data_ptr(), 100000, tol, 1.0)
+            out[k] = ((time.perf_counter() - t0) * 1e3, it)
+
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=worker, args=(w,)) for w in range(workers)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    wall = time.perf_counter() - t0
+    for jl in jobs:
+        for j in jl:
+            j[2].close()
+    for c in ctxs:
+        c.close()
+    return wall, out
+
+
 def _batch_solve(ctx, sysl, **opts):
     import scipy.sparse as sps
     from tflows_b200 import batch
@@ -132,8 +175,9 @@ def run_batched(args):
            "workload": f"{len(sysl)} systems, n log-uniform [1e3,1e6]: hex Poisson (Cg) and "
                        "polyhedral upwind convection-diffusion (Bicg, Pe U[1,50], CFL 0.1); "
                        "Jacobi; target ||b-Ax||/||b|| <= 1e-10"}
+    smallest = sorted(sysl, key=lambda s: s.n)[:4]
     for label, opts in (("mixed", dict(vec_fp32=True)), ("fp64_batched", dict(vec_fp32=False))):
-        _drop = _batch_solve(ctx, sysl[:4], **opts)   # warm-up (module load, graphs)
+        _drop = _batch_solve(ctx, smallest, **opts)   # warm-up (module load, graphs)
         t_add, t_run, res, info = _batch_solve(ctx, sysl, **opts)
         ok = sum(r["status"] == "converged" and r["rel"] <= 1.01e-10 for r in res)
         done = np.array([r["done_ms"] for r in res])
@@ -146,7 +190,7 @@ def run_batched(args):
                       "done_ms_p99": float(np.percentile(done, 99)),
                       "sweeps": info["sweeps"],
                       "iters_total": int(sum(r["iters"] for r in res))}
-    _drop_in_solve_times(ctx, sysl[:2], 1e-10)   # warm-up
+    _drop_in_solve_times(ctx, smallest[:2], 1e-10)   # warm-up
     t = _drop_in_solve_times(ctx, sysl, 1e-10)
     ms = np.array([a for a, _, _ in t])
     out["fp64_drop_in"] = {"run_s": float(ms.sum() / 1e3),
@@ -158,6 +202,13 @@ def run_batched(args):
                            "solve_ms_p50": float(np.percentile(ms, 50)),
                            "solve_ms_p99": float(np.percentile(ms, 99)),
                            "iters_total": int(sum(it for _, it, _ in t))}
+    for workers in (8, 32):
+        _drop_in_stream_pool(smallest, workers, 1e-10)   # warm-up
+        wall, res = _drop_in_stream_pool(sysl, workers, 1e-10)
+        out[f"fp64_drop_in_{workers}streams"] = {
+            "run_s": wall, "solves_per_s": len(sysl) / wall,
+            "mcell_iters_per_s": sum(s.n * it for s, (_, it) in zip(sysl, res)) / wall / 1e6,
+            "iters_total": int(sum(it for _, it in res))}
     out["speedup_mixed_vs_drop_in"] = out["mixed"]["solves_per_s"] / out["fp64_drop_in"]["solves_per_s"]
     out["speedup_mixed_vs_fp64_batched"] = (out["mixed"]["solves_per_s"]
                                             / out["fp64_batched"]["solves_per_s"])

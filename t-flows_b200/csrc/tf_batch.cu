@@ -22,10 +22,15 @@
 // while FP32 values need 1.3-1.75x (the perturbed operator breaks the
 // recurrence), so FP64 values are the default.
 //
-// Per-system reductions: each tile writes its partial sums; the CTA that
-// finishes a system's last tile sums that system's partials in tile order.
-// A system's arithmetic therefore never depends on which other systems
-// share the batch: results are bit-identical alone and in any mix.
+// Per-system reductions are warp-level, with no CTA-wide barrier: in the
+// elementwise kernels one warp owns a tile; in the tile-streaming kernels
+// each warp reports a partial, the tile's last warp sums them in warp order.
+// The warp that reports a system's last tile sums the tile totals in tile
+// order and finalises the system's scalars.  A system's arithmetic never
+// depends on which other systems share the batch: results are
+// bit-identical alone and in any mix.  The refinement kernels walk a compact
+// list of the tiles of the systems due an update, appended by the warp that
+// decides it.
 //
 // Kernels of one iteration (all skip systems with nothing to do):
 //   kb_pupdate  z = dinv r, p = z + beta p
@@ -61,10 +66,11 @@ enum SysStatus : int {
   kFree = 0, kInit = 1, kActive = 2, kConverged = 3, kMaxIter = 4, kBreakdown = 5
 };
 
-constexpr int kRows = 256;       // rows per tile = threads per CTA
+constexpr int kRows = 512;       // rows per tile (max) = threads per tile CTA
+constexpr int kWarps = kRows / 32;
 constexpr int kNnzCap = 4096;    // entries per tile stage
 constexpr int kStages = 2;
-constexpr int kPartQ = 4;        // partial sums kept per tile
+constexpr int kPartQ = 4;        // partial sums kept per tile / warp
 
 template <typename V>
 struct SysDev {
@@ -81,7 +87,9 @@ struct SysDev {
   V* p;
   V* q;
   V* dinv;
-  double* part;         // ntiles * kPartQ
+  double* tile_tot;     // ntiles * kPartQ: per-tile totals
+  double* warp_part;    // ntiles * kWarps * kPartQ: per-warp partials (tile kernels)
+  unsigned* tile_cnt;   // ntiles: warps of a tile that have reported
   int n, ntiles;
   int maxit, use_val32;
   double tol;
@@ -98,6 +106,18 @@ struct SysState {
 struct Work {
   int sys;
   int tile;
+  int r0, r1;             // the tile's rows
+  int j0, j1;             // its entries (row[r0], row[r1])
+};
+
+// Refinement (reliable-update) work list: the warp that finishes a system in
+// kb_update appends that system's tiles when an update is due; the host
+// pre-fills it with the tiles of newly admitted systems; the last CTA of
+// kb_ru_res empties it.  The refinement kernels touch only these tiles.
+struct RuList {
+  Work* items;
+  int* count;
+  unsigned* exit_cnt;
 };
 
 struct BatchArgs {
@@ -106,79 +126,207 @@ struct BatchArgs {
   const Work* work;
   const int* nwork;
   double ru_delta2;
+  RuList ru;
 };
 
 __device__ __forceinline__ bool active(const SysState& s) { return s.status == kActive; }
 
 // ---------------------------------------------------------------------------
-template <typename V>
-__global__ void __launch_bounds__(kRows) kb_pupdate(BatchArgs a) {
-  const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
-  const int nw = *a.nwork;
-  for (int k = blockIdx.x; k < nw; k += gridDim.x) {
-    const Work w = a.work[k];
-    const SysState& s = a.st[w.sys];
-    if (!active(s)) continue;
-    const SysDev<V>& d = D[w.sys];
-    const int i = d.tiles[w.tile] + threadIdx.x;
-    if (i >= d.tiles[w.tile + 1]) continue;
-    const V z = d.r[i] * d.dinv[i];
-    d.p[i] = s.first ? z : (V)((double)z + s.beta * (double)d.p[i]);
+// Warp-level per-system reductions (no CTA barriers).
+// ---------------------------------------------------------------------------
+// One whole warp reports the total of tile `tile` (v, lane-independent).
+// Returns true in the warp that reports the system's last tile, with v =
+// the system totals summed over the tile totals in tile order.
+template <int NQ>
+__device__ bool warp_tile_done(unsigned* sys_cnt, double* tile_tot, int ntiles, int tile,
+                               double (&v)[NQ]) {
+  const int lane = threadIdx.x & 31;
+  unsigned last = 0;
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) tile_tot[(size_t)tile * kPartQ + q] = v[q];
+    __threadfence();
+    last = (atomicAdd(sys_cnt, 1u) == (unsigned)ntiles - 1);
   }
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (!last) return false;
+  __threadfence();
+  double acc[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
+  for (int t = lane; t < ntiles; t += 32)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+      acc[q] = __dadd_rn(acc[q], __ldcg(tile_tot + (size_t)t * kPartQ + q));
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) v[q] = warp_sum(acc[q]);
+  if (lane == 0) *sys_cnt = 0u;
+  return true;
 }
 
-// Per-system "last CTA" reduction over the system's tile partials.
-// Called CTA-wide; returns true in the CTA that completed the system, with
-// the sums in out[0..nq).
+// Tile kernels (one CTA of kWarps warps per tile): every warp reports its
+// partial; the tile's last warp sums the kWarps partials in warp order and
+// reports the tile through warp_tile_done.  v: this thread's values.
 template <int NQ>
-__device__ bool sys_reduce(unsigned* cnt, const double* part, int ntiles,
-                           const double (&mine)[NQ], double* tile_slot, double (&out)[NQ],
-                           double* scratch) {
-  __shared__ int s_last;
-  if (threadIdx.x == 0) {
+__device__ bool cta_tile_done(unsigned* sys_cnt, double* tile_tot, double* warp_part,
+                              unsigned* tile_cnt, int ntiles, int tile, double (&v)[NQ]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) tile_slot[q] = mine[q];
+  for (int q = 0; q < NQ; ++q) v[q] = warp_sum(v[q]);
+  unsigned last = 0;
+  if (lane == 0) {
+    double* wp = warp_part + ((size_t)tile * kWarps + warp) * kPartQ;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) wp[q] = v[q];
     __threadfence();
-    s_last = (atomicAdd(cnt, 1u) == (unsigned)ntiles - 1);
+    last = (atomicAdd(tile_cnt + tile, 1u) == (unsigned)kWarps - 1);
   }
-  __syncthreads();
-  if (!s_last) return false;
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (!last) return false;
   __threadfence();
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
-    double acc = 0.0;
-    for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
-      acc = __dadd_rn(acc, __ldcg(part + (size_t)t * kPartQ + q));
-    out[q] = block_red<kSum>(acc, scratch);
+    const double w = lane < kWarps
+                         ? __ldcg(warp_part + ((size_t)tile * kWarps + lane) * kPartQ + q)
+                         : 0.0;
+    v[q] = warp_sum(w);
   }
-  if (threadIdx.x == 0) *cnt = 0u;
-  return true;
+  if (lane == 0) tile_cnt[tile] = 0u;
+  return warp_tile_done<NQ>(sys_cnt, tile_tot, ntiles, tile, v);
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise kernels: one warp per tile.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int warp_global() {
+  return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+}
+__device__ __forceinline__ int warps_total() { return (int)((gridDim.x * blockDim.x) >> 5); }
+
+template <typename V>
+__global__ void __launch_bounds__(256) kb_pupdate(BatchArgs a) {
+  const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
+  const int nw = *a.nwork;
+  const int lane = threadIdx.x & 31;
+  for (int k = warp_global(); k < nw; k += warps_total()) {
+    const Work w = a.work[k];
+    const SysState& s = a.st[w.sys];
+    if (!active(s)) continue;
+    const V* __restrict__ r = D[w.sys].r;
+    const V* __restrict__ dinv = D[w.sys].dinv;
+    V* __restrict__ p = D[w.sys].p;
+    const int first = s.first;
+    const double beta = s.beta;
+#pragma unroll 4
+    for (int i = w.r0 + lane; i < w.r1; i += 32) {
+      const V z = r[i] * dinv[i];
+      p[i] = first ? z : (V)((double)z + beta * (double)p[i]);
+    }
+  }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(256) kb_update(BatchArgs a) {
+  const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
+  const int nw = *a.nwork;
+  const int lane = threadIdx.x & 31;
+  for (int k = warp_global(); k < nw; k += warps_total()) {
+    const Work w = a.work[k];
+    SysState& s = a.st[w.sys];
+    if (!active(s)) continue;   // warp-uniform
+    const SysDev<V>& d = D[w.sys];
+    V* __restrict__ xlo = d.xlo;
+    V* __restrict__ r = d.r;
+    const V* __restrict__ p = d.p;
+    const V* __restrict__ q = d.q;
+    const V* __restrict__ dinv = d.dinv;
+    const double al = s.alpha;
+    double v[2] = {0.0, 0.0};   // rho, |r|^2
+#pragma unroll 4
+    for (int i = w.r0 + lane; i < w.r1; i += 32) {
+      const V xl = (V)((double)xlo[i] + al * (double)p[i]);
+      const V ri = (V)((double)r[i] - al * (double)q[i]);
+      xlo[i] = xl;
+      r[i] = ri;
+      const V zi = ri * dinv[i];
+      v[0] = __dadd_rn(v[0], __dmul_rn((double)zi, (double)ri));
+      v[1] = __dadd_rn(v[1], __dmul_rn((double)ri, (double)ri));
+    }
+    v[0] = warp_sum(v[0]);
+    v[1] = warp_sum(v[1]);
+    if (!warp_tile_done<2>(&s.cnt_upd, d.tile_tot, d.ntiles, w.tile, v)) continue;
+    int base = -1;
+    if (lane == 0) {
+      s.rho_old = s.rho;
+      s.rho = v[0];
+      s.beta = __ddiv_rn(s.rho, s.rho_old);
+      s.rr = v[1];
+      s.iter += 1;
+      s.first = 0;
+      const double tb = d.tol * d.tol * s.bnorm2;
+      if (s.rr < a.ru_delta2 * s.rr_ru || s.rr <= tb || s.iter >= d.maxit ||
+          !(s.rr == s.rr)) {
+        s.need_ru = 1;
+        base = atomicAdd(a.ru.count, d.ntiles);
+      }
+    }
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= 0)   // list this system's tiles for the refinement kernels
+      for (int t = lane; t < d.ntiles; t += 32)
+        a.ru.items[base + t] = Work{w.sys, t, d.tiles[t], d.tiles[t + 1],
+                                    d.row[d.tiles[t]], d.row[d.tiles[t + 1]]};
+  }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(256) kb_ru_fold(BatchArgs a) {
+  const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
+  const int nw = *a.ru.count;
+  const int lane = threadIdx.x & 31;
+  for (int k = warp_global(); k < nw; k += warps_total()) {
+    const Work w = a.ru.items[k];
+    const SysState& s = a.st[w.sys];
+    if (!(s.status == kActive && s.need_ru)) continue;
+    double* __restrict__ x = D[w.sys].x;
+    V* __restrict__ xlo = D[w.sys].xlo;
+#pragma unroll 4
+    for (int i = w.r0 + lane; i < w.r1; i += 32) {
+      x[i] = __dadd_rn(x[i], (double)xlo[i]);
+      xlo[i] = (V)0;
+    }
+  }
 }
 
 // q = A p with FP64 row sums, p.q per tile, alpha per system.
 template <typename V, typename VT>
 struct SpmvWork {
+  using Item = Work;
   const SysDev<V>* D;
   SysState* st;
   const Work* work;
   int nw;
   double acc;     // this thread's p_i q_i in the current tile
-  double* scratch;
+  int ck;         // item whose pointers are cached below
+  const V* cp;
+  V* cq;
   __device__ int count() const { return nw; }
-  __device__ bool skip(int k) const { return !active(st[work[k].sys]); }
-  __device__ void tile(int k, const int*& row, const int*& col, const VT*& val, int& r0,
-                       int& r1) const {
-    const Work w = work[k];
+  __device__ Work item(int k) const { return work[k]; }
+  __device__ void resolve(const Work& w, TileRes<VT>& rs) const {
     const SysDev<V>& d = D[w.sys];
-    row = d.row;
-    col = d.col;
-    if constexpr (sizeof(VT) == 4) val = d.val32;
-    else val = d.val;
-    r0 = d.tiles[w.tile];
-    r1 = d.tiles[w.tile + 1];
+    rs.row = d.row;
+    rs.col = d.col;
+    if constexpr (sizeof(VT) == 4) rs.val = d.val32;
+    else rs.val = d.val;
+    rs.skip = !active(st[w.sys]);
   }
   __device__ void row(int k, int i, const VT* v, const int* c, int len) {
-    const SysDev<V>& d = D[work[k].sys];
+    if (k != ck) {
+      ck = k;
+      const SysDev<V>& d = D[work[k].sys];
+      cp = d.p;
+      cq = d.q;
+    }
+    const V* __restrict__ p = cp;
     double s = 0.0;
 #pragma unroll 1
     for (int j0 = 0; j0 < len; j0 += 8) {
@@ -187,119 +335,56 @@ struct SpmvWork {
       for (int u = 0; u < 8; ++u)
         if (j0 + u < len) {
           vv[u] = (double)v[j0 + u];
-          pv[u] = (double)d.p[c[j0 + u]];
+          pv[u] = (double)__ldg(p + c[j0 + u]);
         }
 #pragma unroll
       for (int u = 0; u < 8; ++u)
         if (j0 + u < len) s = __dadd_rn(s, __dmul_rn(vv[u], pv[u]));
     }
     const V qi = (V)s;
-    d.q[i] = qi;
-    acc = __dadd_rn(acc, __dmul_rn((double)d.p[i], (double)qi));
+    cq[i] = qi;
+    acc = __dadd_rn(acc, __dmul_rn((double)__ldg(p + i), (double)qi));
   }
   __device__ void tile_end(int k) {
     const Work w = work[k];
     const SysDev<V>& d = D[w.sys];
-    double mine[1] = {block_red<kSum>(acc, scratch)};
+    double v[1] = {acc};
     acc = 0.0;
-    double out[1];
-    if (sys_reduce<1>(&st[w.sys].cnt_spmv, d.part, d.ntiles, mine,
-                      d.part + (size_t)w.tile * kPartQ, out, scratch) &&
-        threadIdx.x == 0) {
+    if (cta_tile_done<1>(&st[w.sys].cnt_spmv, d.tile_tot, d.warp_part, d.tile_cnt, d.ntiles,
+                         w.tile, v) &&
+        (threadIdx.x & 31) == 0) {
       SysState& s = st[w.sys];
-      if (!(out[0] > 0.0)) s.status = kBreakdown;   // p.q <= 0 or NaN
-      else s.alpha = __ddiv_rn(s.rho, out[0]);
+      if (!(v[0] > 0.0)) s.status = kBreakdown;   // p.q <= 0 or NaN
+      else s.alpha = __ddiv_rn(s.rho, v[0]);
     }
   }
 };
 
 template <typename V, typename VT>
-__global__ void __launch_bounds__(kRows) kb_spmv(BatchArgs a) {
-  __shared__ double scratch[32];
-  SpmvWork<V, VT> w{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, *a.nwork, 0.0,
-                    scratch};
-  stream_work<kRows, kNnzCap, VT, kStages>(w);
-}
-
-template <typename V>
-__global__ void __launch_bounds__(kRows) kb_update(BatchArgs a) {
-  __shared__ double scratch[32];
-  const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
-  const int nw = *a.nwork;
-  for (int k = blockIdx.x; k < nw; k += gridDim.x) {
-    const Work w = a.work[k];
-    SysState& s = a.st[w.sys];
-    if (!active(s)) continue;   // CTA-uniform
-    const SysDev<V>& d = D[w.sys];
-    const int i = d.tiles[w.tile] + threadIdx.x;
-    double rho = 0.0, rr = 0.0;
-    if (i < d.tiles[w.tile + 1]) {
-      const double al = s.alpha;
-      const V xl = (V)((double)d.xlo[i] + al * (double)d.p[i]);
-      const V ri = (V)((double)d.r[i] - al * (double)d.q[i]);
-      d.xlo[i] = xl;
-      d.r[i] = ri;
-      const V zi = ri * d.dinv[i];
-      rho = __dmul_rn((double)zi, (double)ri);
-      rr = __dmul_rn((double)ri, (double)ri);
-    }
-    double mine[2] = {block_red<kSum>(rho, scratch), block_red<kSum>(rr, scratch)};
-    double out[2];
-    if (sys_reduce<2>(&s.cnt_upd, d.part, d.ntiles, mine, d.part + (size_t)w.tile * kPartQ,
-                      out, scratch) &&
-        threadIdx.x == 0) {
-      s.rho_old = s.rho;
-      s.rho = out[0];
-      s.beta = __ddiv_rn(s.rho, s.rho_old);
-      s.rr = out[1];
-      s.iter += 1;
-      s.first = 0;
-      const double tb = d.tol * d.tol * s.bnorm2;
-      if (s.rr < a.ru_delta2 * s.rr_ru || s.rr <= tb || s.iter >= d.maxit || !(s.rr == s.rr))
-        s.need_ru = 1;
-    }
-  }
-}
-
-template <typename V>
-__global__ void __launch_bounds__(kRows) kb_ru_fold(BatchArgs a) {
-  const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
-  const int nw = *a.nwork;
-  for (int k = blockIdx.x; k < nw; k += gridDim.x) {
-    const Work w = a.work[k];
-    const SysState& s = a.st[w.sys];
-    if (!(s.status == kActive && s.need_ru)) continue;
-    const SysDev<V>& d = D[w.sys];
-    const int i = d.tiles[w.tile] + threadIdx.x;
-    if (i >= d.tiles[w.tile + 1]) continue;
-    d.x[i] = __dadd_rn(d.x[i], (double)d.xlo[i]);
-    d.xlo[i] = (V)0;
-  }
+__global__ void __launch_bounds__(kRows, 2) kb_spmv(BatchArgs a) {
+  SpmvWork<V, VT> w{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, *a.nwork, 0.0, -1,
+                    nullptr, nullptr};
+  stream_items<kRows, kNnzCap, VT, kStages>(w);
 }
 
 // r = b - A x in FP64; new systems also form dinv and |b|^2.
 template <typename V>
 struct ResWork {
+  using Item = Work;
   const SysDev<V>* D;
   SysState* st;
   const Work* work;
   int nw;
   double rr, rho, bb;
-  double* scratch;
   __device__ int count() const { return nw; }
-  __device__ bool skip(int k) const {
-    const SysState& s = st[work[k].sys];
-    return !(s.status == kInit || (s.status == kActive && s.need_ru));
-  }
-  __device__ void tile(int k, const int*& row, const int*& col, const double*& val, int& r0,
-                       int& r1) const {
-    const Work w = work[k];
+  __device__ Work item(int k) const { return work[k]; }
+  __device__ void resolve(const Work& w, TileRes<double>& rs) const {
     const SysDev<V>& d = D[w.sys];
-    row = d.row;
-    col = d.col;
-    val = d.val;
-    r0 = d.tiles[w.tile];
-    r1 = d.tiles[w.tile + 1];
+    rs.row = d.row;
+    rs.col = d.col;
+    rs.val = d.val;
+    const SysState& s = st[w.sys];
+    rs.skip = !(s.status == kInit || (s.status == kActive && s.need_ru));
   }
   __device__ void row(int k, int i, const double* v, const int* c, int len) {
     const Work w = work[k];
@@ -333,34 +418,32 @@ struct ResWork {
   __device__ void tile_end(int k) {
     const Work w = work[k];
     const SysDev<V>& d = D[w.sys];
-    double mine[3] = {block_red<kSum>(rr, scratch), block_red<kSum>(rho, scratch),
-                      block_red<kSum>(bb, scratch)};
+    double v[3] = {rr, rho, bb};
     rr = rho = bb = 0.0;
-    double out[3];
-    if (sys_reduce<3>(&st[w.sys].cnt_res, d.part, d.ntiles, mine,
-                      d.part + (size_t)w.tile * kPartQ, out, scratch) &&
-        threadIdx.x == 0) {
+    if (cta_tile_done<3>(&st[w.sys].cnt_res, d.tile_tot, d.warp_part, d.tile_cnt, d.ntiles,
+                         w.tile, v) &&
+        (threadIdx.x & 31) == 0) {
       SysState& s = st[w.sys];
       if (s.status == kInit) {
-        s.bnorm2 = out[2];
+        s.bnorm2 = v[2];
         s.status = kActive;
         s.first = 1;
         s.iter = 0;
       }
       s.n_ru += 1;
       const double bn = s.bnorm2 > 0.0 ? __dsqrt_rn(s.bnorm2) : 1.0;
-      s.res_true = __ddiv_rn(__dsqrt_rn(out[0]), bn);
+      s.res_true = __ddiv_rn(__dsqrt_rn(v[0]), bn);
       s.need_ru = 0;
       if (s.res_true <= d.tol) {
         s.status = kConverged;
       } else if (s.iter >= d.maxit) {
         s.status = kMaxIter;
-      } else if (!(out[0] == out[0])) {
+      } else if (!(v[0] == v[0])) {
         s.status = kBreakdown;
       } else {
-        s.rr = out[0];
-        s.rr_ru = out[0];
-        s.rho = out[1];
+        s.rr = v[0];
+        s.rr_ru = v[0];
+        s.rho = v[1];
         if (!s.first) s.beta = __ddiv_rn(s.rho, s.rho_old);
       }
     }
@@ -368,11 +451,18 @@ struct ResWork {
 };
 
 template <typename V>
-__global__ void __launch_bounds__(kRows) kb_ru_res(BatchArgs a) {
-  __shared__ double scratch[32];
-  ResWork<V> w{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, *a.nwork, 0.0, 0.0, 0.0,
-               scratch};
-  stream_work<kRows, kNnzCap, double, kStages>(w);
+__global__ void __launch_bounds__(kRows, 2) kb_ru_res(BatchArgs a) {
+  ResWork<V> w{static_cast<const SysDev<V>*>(a.desc), a.st, a.ru.items, *a.ru.count, 0.0,
+               0.0, 0.0};
+  stream_items<kRows, kNnzCap, double, kStages>(w);
+  // The last CTA to leave empties the refinement list for the next iteration.
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(a.ru.exit_cnt, 1u) == gridDim.x - 1) {
+      *a.ru.count = 0;
+      *a.ru.exit_cnt = 0u;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -487,7 +577,8 @@ int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* co
 
 // Byte layout of one system's segment.
 struct Layout {
-  size_t row, col, dia, tiles, val, val32, b, x, xlo, r, p, q, dinv, part, total;
+  size_t row, col, dia, tiles, val, val32, b, x, xlo, r, p, q, dinv, tile_tot, warp_part,
+      tile_cnt, total;
 };
 
 Layout layout_for(const HostSys& h, size_t vsz, int use_val32) {
@@ -509,7 +600,9 @@ Layout layout_for(const HostSys& h, size_t vsz, int use_val32) {
   L.p = take(n8 * vsz);
   L.q = take(n8 * vsz);
   L.dinv = take(n8 * vsz);
-  L.part = take((size_t)ntiles * kPartQ * 8);
+  L.tile_tot = take((size_t)ntiles * kPartQ * 8);
+  L.warp_part = take((size_t)ntiles * kWarps * kPartQ * 8);
+  L.tile_cnt = take((size_t)ntiles * 4);
   L.total = o;
   return L;
 }
@@ -520,6 +613,8 @@ struct Slot {
   int n = 0, ntiles = 0;
   double done_ms = -1.0;   // wall time from tf_batch_run's start to completion
   Layout L{};
+  std::vector<int> tiles;  // row boundaries of the tiles (host copy)
+  std::vector<int> tile_j; // entry boundaries of the tiles (row[tiles[t]])
 };
 
 }  // namespace tfb
@@ -541,8 +636,11 @@ struct tf_batch_s {
   SysState* h_state = nullptr;      // pinned mirror
   Work* d_work = nullptr;
   int* d_nwork = nullptr;
+  Work* d_ru = nullptr;          // refinement work list (same capacity)
+  int* d_ru_count = nullptr;
+  unsigned* d_ru_exit = nullptr;
   int work_cap = 0;
-  std::vector<Work> h_work;
+  std::vector<Work> h_work, h_ru;
   int nwork = 0;
   cudaGraphExec_t sweep = nullptr;
   int grid_plain = 1, grid_tile = 1;
@@ -554,7 +652,8 @@ struct tf_batch_s {
     cudaStreamSynchronize(ctx->stream);
     if (sweep) cudaGraphExecDestroy(sweep);
     if (arena.base) cudaFree(arena.base);
-    for (void* p : {d_desc, (void*)d_state, (void*)d_work, (void*)d_nwork})
+    for (void* p : {d_desc, (void*)d_state, (void*)d_work, (void*)d_nwork, (void*)d_ru,
+                    (void*)d_ru_count, (void*)d_ru_exit})
       if (p) cudaFree(p);
     if (h_state) cudaFreeHost(h_state);
   }
@@ -563,11 +662,11 @@ struct tf_batch_s {
   void launch_iteration(cudaStream_t s, const BatchArgs& a) {
     const size_t sm = TileLayout<kRows, kNnzCap, double, kStages>::kSmemBytes;
     const size_t sm32 = TileLayout<kRows, kNnzCap, float, kStages>::kSmemBytes;
-    kb_pupdate<V><<<grid_plain, kRows, 0, s>>>(a);
+    kb_pupdate<V><<<grid_plain, 256, 0, s>>>(a);
     if (opts.val_fp32) kb_spmv<V, float><<<grid_tile, kRows, sm32, s>>>(a);
     else kb_spmv<V, double><<<grid_tile, kRows, sm, s>>>(a);
-    kb_update<V><<<grid_plain, kRows, 0, s>>>(a);
-    kb_ru_fold<V><<<grid_plain, kRows, 0, s>>>(a);
+    kb_update<V><<<grid_plain, 256, 0, s>>>(a);
+    kb_ru_fold<V><<<grid_plain, 256, 0, s>>>(a);
     kb_ru_res<V><<<grid_tile, kRows, sm, s>>>(a);
   }
 
@@ -595,7 +694,8 @@ struct tf_batch_s {
       sweep = nullptr;
     }
     cudaStream_t s = ctx->stream;
-    BatchArgs a{d_desc, d_state, d_work, d_nwork, opts.ru_delta * opts.ru_delta};
+    BatchArgs a{d_desc, d_state, d_work, d_nwork, opts.ru_delta * opts.ru_delta,
+                RuList{d_ru, d_ru_count, d_ru_exit}};
     cudaGraph_t g = nullptr;
     TF_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int it = 0; it < opts.sweep_iters; ++it) {
@@ -641,6 +741,10 @@ struct tf_batch_s {
     memset(h_state, 0, (size_t)max_sys * sizeof(SysState));
     TF_CUDA_TRY(cudaMalloc((void**)&d_nwork, sizeof(int)));
     TF_CUDA_TRY(cudaMemset(d_nwork, 0, sizeof(int)));
+    TF_CUDA_TRY(cudaMalloc((void**)&d_ru_count, sizeof(int)));
+    TF_CUDA_TRY(cudaMemset(d_ru_count, 0, sizeof(int)));
+    TF_CUDA_TRY(cudaMalloc((void**)&d_ru_exit, sizeof(unsigned)));
+    TF_CUDA_TRY(cudaMemset(d_ru_exit, 0, sizeof(unsigned)));
     st = (vsz == 4) ? setup_kernels<float>() : setup_kernels<double>();
     if (st != TF_OK) return st;
     return build_sweep();
@@ -672,6 +776,8 @@ struct tf_batch_s {
     if (e == cudaSuccess) e = up(L.x, h.x0.data(), (size_t)h.n * 8);
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.xlo, 0, n8 * vsz, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.p, 0, n8 * vsz, s);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(base + L.tile_cnt, 0, (h.tiles.size() - 1) * 4, s);
     if (e != cudaSuccess) {
       arena.release(off, L.total);
       tf_set_last_cuda_error(e, "batch admit copies", __FILE__, __LINE__);
@@ -693,7 +799,9 @@ struct tf_batch_s {
       d.p = (VV*)(base + L.p);
       d.q = (VV*)(base + L.q);
       d.dinv = (VV*)(base + L.dinv);
-      d.part = (double*)(base + L.part);
+      d.tile_tot = (double*)(base + L.tile_tot);
+      d.warp_part = (double*)(base + L.warp_part);
+      d.tile_cnt = (unsigned*)(base + L.tile_cnt);
       d.n = h.n;
       d.ntiles = ntiles;
       d.maxit = h.maxit;
@@ -726,34 +834,53 @@ struct tf_batch_s {
     sl.n = h.n;
     sl.ntiles = ntiles;
     sl.L = L;
+    sl.tiles = h.tiles;
+    sl.tile_j.resize(h.tiles.size());
+    for (size_t t = 0; t < h.tiles.size(); ++t) sl.tile_j[t] = h.row[h.tiles[t]];
     h_state[slot] = ss;
     *out_slot = slot;
     return TF_OK;
   }
 
-  // Work list = every tile of every system that still iterates.
+  // Work list = every tile of every system that still iterates; the
+  // refinement list starts with the tiles of systems not yet initialised.
   int rebuild_work() {
     h_work.clear();
+    h_ru.clear();
     for (int i = 0; i < max_sys; ++i) {
       if (!slots[i].used) continue;
       const int stt = h_state[i].status;
       if (stt != kInit && stt != kActive) continue;
-      for (int t = 0; t < slots[i].ntiles; ++t) h_work.push_back(Work{i, t});
+      const std::vector<int>& tl = slots[i].tiles;
+      const std::vector<int>& tj = slots[i].tile_j;
+      for (int t = 0; t < slots[i].ntiles; ++t) {
+        const Work wk{i, t, tl[t], tl[t + 1], tj[t], tj[t + 1]};
+        h_work.push_back(wk);
+        if (stt == kInit) h_ru.push_back(wk);
+      }
     }
     nwork = (int)h_work.size();
     if (nwork > work_cap) {
       if (d_work) cudaFree(d_work);
+      if (d_ru) cudaFree(d_ru);
       d_work = nullptr;
+      d_ru = nullptr;
       work_cap = std::max(nwork, 2 * work_cap);
       TF_CUDA_TRY(cudaMalloc((void**)&d_work, (size_t)work_cap * sizeof(Work)));
-      int st = build_sweep();   // the graph holds the work-list pointer
+      TF_CUDA_TRY(cudaMalloc((void**)&d_ru, (size_t)work_cap * sizeof(Work)));
+      int st = build_sweep();   // the graph holds the work-list pointers
       if (st != TF_OK) return st;
     }
     cudaStream_t s = ctx->stream;
+    const int nru = (int)h_ru.size();
     if (nwork)
       TF_CUDA_TRY(cudaMemcpyAsync(d_work, h_work.data(), (size_t)nwork * sizeof(Work),
                                   cudaMemcpyHostToDevice, s));
+    if (nru)
+      TF_CUDA_TRY(cudaMemcpyAsync(d_ru, h_ru.data(), (size_t)nru * sizeof(Work),
+                                  cudaMemcpyHostToDevice, s));
     TF_CUDA_TRY(cudaMemcpyAsync(d_nwork, &nwork, sizeof(int), cudaMemcpyHostToDevice, s));
+    TF_CUDA_TRY(cudaMemcpyAsync(d_ru_count, &nru, sizeof(int), cudaMemcpyHostToDevice, s));
     TF_CUDA_TRY(cudaStreamSynchronize(s));
     return TF_OK;
   }

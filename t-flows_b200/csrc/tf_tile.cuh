@@ -251,6 +251,136 @@ __device__ bool stream_work(W& w) {
   return ok;
 }
 
+// ---------------------------------------------------------------------------
+// Work-list streamer with descriptor prefetch.  Items carry their row range
+// and entry range (r0, r1, j0, j1) so issuing a tile needs only the owning
+// matrix's base pointers.  Thread 0 runs a two-deep prefetch ring: while
+// item k is computed, the item that will refill its stage (k + STAGES*G)
+// is already resolved (base pointers and skip flag loaded before the wait)
+// and the following one (k + G + STAGES*G) is being fetched, so the bulk
+// copies of a freed stage go out with no dependent global load on the
+// critical path.
+//   W::Item, W::count(), W::item(k) -> Item (has r0, r1, j0, j1)
+//   W::resolve(const Item&, TileRes<VT>&)   base pointers + skip flag
+//   W::row(k, i, vals, cols, len)            one thread per row
+//   W::tile_end(k)                           all threads, after the rows
+// ---------------------------------------------------------------------------
+template <typename VT>
+struct TileRes {
+  const int* row;
+  const int* col;
+  const VT* val;
+  int skip;
+};
+
+template <int ROWS, int NNZCAP, typename VT, int STAGES, class W>
+__device__ bool stream_items(W& w) {
+  using L = TileLayout<ROWS, NNZCAP, VT, STAGES>;
+  using It = typename W::Item;
+  constexpr int kEv = L::kEv;
+  extern __shared__ __align__(128) unsigned char tf_smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tf_smem + L::kBarOffset);
+  int* meta = reinterpret_cast<int*>(tf_smem + L::kMetaOffset);
+  auto sval = [&](int s) { return reinterpret_cast<VT*>(tf_smem + s * L::kStageBytes); };
+  auto scol = [&](int s) {
+    return reinterpret_cast<int*>(tf_smem + s * L::kStageBytes + L::kValBytes);
+  };
+  auto srow = [&](int s) {
+    return reinterpret_cast<int*>(tf_smem + s * L::kStageBytes + L::kValBytes + L::kColBytes);
+  };
+  const int count = w.count();
+  const int G = gridDim.x;
+  if ((int)blockIdx.x >= count) return true;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  // Copies of a resolved item into stage s (thread 0).
+  auto issue = [&](const It& it, const TileRes<VT>& rs, int s) {
+    int* m = meta + 8 * s;
+    if (rs.skip) {   // nothing to copy: complete the phase at once
+      m[5] = 1;
+      mbar_arrive_expect_tx(&bars[s], 0);
+      return;
+    }
+    const int r0 = it.r0, r1 = it.r1, j0 = it.j0, j1 = it.j1;
+    const int a0 = j0 & ~(kEv - 1), a1 = (j1 + kEv - 1) & ~(kEv - 1);
+    const int c0 = j0 & ~3, c1 = (j1 + 3) & ~3;
+    const int p0 = r0 & ~3, p1 = (r1 + 1 + 3) & ~3;
+    m[0] = a0; m[1] = c0; m[2] = p0; m[3] = r0; m[4] = r1; m[5] = 0;
+    const unsigned bv = (unsigned)(a1 - a0) * (unsigned)sizeof(VT);
+    const unsigned bc = (unsigned)(c1 - c0) * 4u;
+    const unsigned br = (unsigned)(p1 - p0) * 4u;
+    mbar_arrive_expect_tx(&bars[s], bv + bc + br);
+    if (bv) bulk_g2s(sval(s), rs.val + a0, bv, &bars[s]);
+    if (bc) bulk_g2s(scol(s), rs.col + c0, bc, &bars[s]);
+    bulk_g2s(srow(s), rs.row + p0, br, &bars[s]);
+  };
+
+  // At the iteration of item k: nxt = item k + STAGES*G (refills this
+  // stage at the end of the iteration), nxt2 = item k + G + STAGES*G.
+  It nxt{}, nxt2{};
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < STAGES; ++s) {
+      const int k = blockIdx.x + s * G;
+      if (k < count) {
+        const It it = w.item(k);
+        TileRes<VT> rs;
+        w.resolve(it, rs);
+        issue(it, rs, s);
+      }
+    }
+    const int k1 = blockIdx.x + STAGES * G;
+    if (k1 < count) nxt = w.item(k1);
+    if (k1 + G < count) nxt2 = w.item(k1 + G);
+  }
+
+  bool ok = true;
+  int it_no = 0;
+  for (int k = blockIdx.x; k < count; k += G, ++it_no) {
+    const int s = it_no % STAGES;
+    const unsigned par = (unsigned)(it_no / STAGES) & 1u;
+    const int nk = k + STAGES * G;
+    TileRes<VT> nres{};
+    if (threadIdx.x == 0 && nk < count) w.resolve(nxt, nres);   // loads in flight
+    const bool mine = mbar_wait_bounded(&bars[s], par);
+    if (__syncthreads_or(!mine)) { ok = false; break; }
+    const int* m = meta + 8 * s;
+    if (!m[5]) {
+      const int a0 = m[0], c0 = m[1], p0 = m[2], r0 = m[3], r1 = m[4];
+      const VT* sv = sval(s);
+      const int* sc = scol(s);
+      const int* sr = srow(s);
+      for (int r = r0 + (int)threadIdx.x; r < r1; r += ROWS) {
+        const int js = sr[r - p0], je = sr[r + 1 - p0];
+        w.row(k, r, sv + (js - a0), sc + (js - c0), je - js);
+      }
+      w.tile_end(k);
+    }
+    __syncthreads();   // stage s fully consumed
+    if (threadIdx.x == 0 && nk < count) {
+      fence_proxy_async_smem();
+      issue(nxt, nres, s);
+      nxt = nxt2;                        // item nk + G
+      if (nk + 2 * G < count) nxt2 = w.item(nk + 2 * G);
+    }
+  }
+  if (!ok && threadIdx.x == 0) {
+    for (int d = 0; d < STAGES; ++d) {
+      const int itk = it_no + d;
+      const int k = blockIdx.x + itk * G;
+      if (k >= count) break;
+      mbar_wait_bounded(&bars[itk % STAGES], (unsigned)(itk / STAGES) & 1u);
+    }
+  }
+  __syncthreads();
+  return ok;
+}
+
 // Tile configurations the host may pick (rows per tile = threads per CTA).
 enum TileCfgId { kTile512 = 0, kTile256 = 1, kTile128 = 2, kTileNone = 3 };
 constexpr int kTileRows[3] = {512, 256, 128};
