@@ -209,6 +209,25 @@ def run_batched(args):
             "run_s": wall, "solves_per_s": len(sysl) / wall,
             "mcell_iters_per_s": sum(s.n * it for s, (_, it) in zip(sysl, res)) / wall / 1e6,
             "iters_total": int(sum(it for _, it in res))}
+    from tflows_b200 import pool as tpool
+    for workers in (8, 16):
+        for rep in range(2):             # first pass warms the memory pool and graphs
+            pl = tpool.Pool(workers=workers, mem_budget=40 << 30)
+            t0 = time.perf_counter()
+            rids = [pl.submit(s, miter=100000, tol=1e-10 * workloads.nrms_b(s), norm=1.0)
+                    for s in sysl]
+            got = [pl.wait(r) for r in rids]
+            wall = time.perf_counter() - t0
+            pl.close()
+        lat = np.array([g["latency_ms"] for g in got])
+        out[f"fp64_pool_{workers}"] = {
+            "run_s_incl_upload_and_registration": wall, "solves_per_s": len(sysl) / wall,
+            "mcell_iters_per_s": sum(s.n * g["niter"] for s, g in zip(sysl, got)) / wall / 1e6,
+            "latency_ms_p50": float(np.percentile(lat, 50)),
+            "latency_ms_p99": float(np.percentile(lat, 99)),
+            "iters_total": int(sum(g["niter"] for g in got))}
+    out["speedup_pool16_vs_drop_in"] = (out["fp64_pool_16"]["solves_per_s"]
+                                        / out["fp64_drop_in"]["solves_per_s"])
     out["speedup_mixed_vs_drop_in"] = out["mixed"]["solves_per_s"] / out["fp64_drop_in"]["solves_per_s"]
     out["speedup_mixed_vs_fp64_batched"] = (out["mixed"]["solves_per_s"]
                                             / out["fp64_batched"]["solves_per_s"])

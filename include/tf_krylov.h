@@ -192,6 +192,34 @@ int tf_server_stats(tf_server s, long long* admitted, long long* completed,
 int tf_server_destroy(tf_server s);
 
 /* ---------------------------------------------------------------------------
+ *  Request pool: concurrent Solve_Native calls on a pool of CUDA streams.
+ *
+ *  Each request is exactly one Solve_Native call (Solve_Native.f90:33-44,
+ *  same arguments and results as tf_solve; x is the initial guess on entry
+ *  and receives the solution; val and b are read, not modified).  The
+ *  caller's arrays are used in place and must stay valid until tf_pool_wait
+ *  returns.  `workers` threads each own a context (stream); a request is
+ *  registered with stream-ordered allocation, solved by the FP64 drop-in
+ *  and released, so independent solves overlap on the GPU.  Requests are
+ *  admitted in arrival order while the device bytes in flight stay within
+ *  mem_budget (0: 20 GiB); one larger than the budget fails with
+ *  TF_ERR_OOM.  Submit returns at once; wait blocks
+ *  until the request finished and reports end-to-end and queueing latency
+ *  in milliseconds.  All pool functions are thread-safe.
+ * ------------------------------------------------------------------------- */
+typedef struct tf_pool_s* tf_pool;
+int tf_pool_create(int device, int workers, size_t mem_budget, tf_pool* out);
+int tf_pool_submit(tf_pool p, int solver, int prec, int n, int64_t nnz,
+                   const int* row, const int* col, const int* dia,
+                   const double* val, const double* rhs, double* x,
+                   int miter, double tol, const double* norm, int64_t* req);
+int tf_pool_wait(tf_pool p, int64_t req, int* niter, double* fin_res,
+                 double* latency_ms, double* queue_ms);
+int tf_pool_stats(tf_pool p, long long* submitted, long long* completed,
+                  long long* rejected, size_t* peak_bytes);
+int tf_pool_destroy(tf_pool p);
+
+/* ---------------------------------------------------------------------------
  *  Building blocks exposed for testing and for callers that keep their own
  *  Krylov loop.  All pointers are device pointers; vectors have n_cells
  *  entries; val has nnz entries.  Each call is asynchronous on ctx's stream;

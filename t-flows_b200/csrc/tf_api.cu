@@ -135,14 +135,30 @@ extern "C" int tf_host_unpin(void* ptr) {
 namespace {
 
 template <class T>
-int dev_alloc(T** p, size_t count) {
+int dev_alloc(tf_ctx_s* ctx, T** p, size_t count) {
+  void* v = nullptr;
+  const int st = tf_dev_alloc_bytes(ctx, &v, std::max<size_t>(count, 1) * sizeof(T));
+  *p = static_cast<T*>(v);
+  return st;
+}
+
+}  // namespace
+
+// Zeroed device memory; stream-ordered on the context's stream when the
+// context asks for it (no device-wide synchronisation).
+int tf_dev_alloc_bytes(tf_ctx_s* ctx, void** p, size_t bytes) {
   *p = nullptr;
-  TF_CUDA_TRY(cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T)));
-  TF_CUDA_TRY(cudaMemset(*p, 0, std::max<size_t>(count, 1) * sizeof(T)));
+  if (ctx->async_alloc) {
+    TF_CUDA_TRY(cudaMallocAsync(p, bytes, ctx->stream));
+    TF_CUDA_TRY(cudaMemsetAsync(*p, 0, bytes, ctx->stream));
+  } else {
+    TF_CUDA_TRY(cudaMalloc(p, bytes));
+    TF_CUDA_TRY(cudaMemset(*p, 0, bytes));
+  }
   return TF_OK;
 }
 
-void free_matrix(tf_matrix_s* m) {
+void tf_matrix_free(tf_matrix_s* m) {
   if (!m) return;
   cudaSetDevice(m->ctx->device);
   for (auto& g : m->graph)
@@ -152,11 +168,25 @@ void free_matrix(tf_matrix_s* m) {
                   m->d_hist, m->d_state, m->d_params, m->d_levf_rows, m->d_levb_rows,
                   m->d_icc_d, m->d_icc_dinv};
   for (void* p : ptrs)
-    if (p) cudaFree(p);
-  if (m->h_state) cudaFreeHost(m->h_state);
-  if (m->h_params) cudaFreeHost(m->h_params);
+    if (p) {
+      if (m->async_alloc) cudaFreeAsync(p, m->ctx->stream);
+      else cudaFree(p);
+    }
+  if (!m->host_lent) {
+    if (m->h_state) cudaFreeHost(m->h_state);
+    if (m->h_params) cudaFreeHost(m->h_params);
+  }
   delete m;
 }
+
+size_t tf_matrix_bytes(int n_cells, int64_t nnz) {
+  auto up = [](size_t b) { return (b + 511) & ~size_t(511); };
+  const size_t nv = (size_t)n_cells + 8, nz = (size_t)nnz + 8;
+  return up(((size_t)n_cells + 9) * 4) + up(nz * 4) + up(nv * 4) + up(nz * 8) +
+         6 * up(nv * 8) + up(((size_t)8 * tf::kMaxBlocks + 16) * 8) + 2048;
+}
+
+namespace {
 
 // Largest nnz of any tile of `rows` consecutive rows among the first ni.
 int64_t max_tile_nnz(const std::vector<int>& row0, int ni, int rows) {
@@ -173,6 +203,12 @@ int64_t max_tile_nnz(const std::vector<int>& row0, int ni, int rows) {
 extern "C" int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own,
                                   int64_t nnz, const int* row, const int* col,
                                   const int* dia, tf_matrix* out) {
+  if (!ctx || !out) return TF_ERR_ARG;
+  return tf_matrix_create(ctx, n_cells, n_own, nnz, row, col, dia, 1, out);
+}
+
+int tf_matrix_create(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const int* row,
+                     const int* col, const int* dia, int want_icc, tf_matrix_s** out) {
   if (!ctx || !out) return TF_ERR_ARG;
   *out = nullptr;
   if (n_cells < 0 || n_own < 0 || n_own > n_cells || nnz < 0) return TF_ERR_ARG;
@@ -202,6 +238,8 @@ extern "C" int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own,
   m->nnz = nnz;
   m->max_row_len = max_len;
   m->diag_first = diag_first;
+  m->async_alloc = ctx->async_alloc;
+  m->dev_bytes = tf_matrix_bytes(n_cells, nnz);
 
   std::vector<int> row0((size_t)n_cells + 1 + 8, 0), col0((size_t)nnz + 8, 0),
       dia0((size_t)n_cells + 8, 0);
@@ -215,7 +253,7 @@ extern "C" int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own,
   const size_t nv = (size_t)n_cells + 8, nz = (size_t)nnz + 8;
   int st = TF_OK;
 #define TRY_ALLOC(p, n)                          \
-  if (st == TF_OK) st = dev_alloc(&(p), (n));
+  if (st == TF_OK) st = dev_alloc(ctx, &(p), (n));
   TRY_ALLOC(m->d_row, row0.size());
   TRY_ALLOC(m->d_col, nz);
   TRY_ALLOC(m->d_dia, nv);
@@ -230,7 +268,11 @@ extern "C" int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own,
   TRY_ALLOC(m->d_state, 1);
   TRY_ALLOC(m->d_params, 1);
 #undef TRY_ALLOC
-  if (st == TF_OK) {
+  if (st == TF_OK && ctx->async_alloc && ctx->h_state) {   // lent by the context
+    m->h_state = ctx->h_state;
+    m->h_params = ctx->h_params;
+    m->host_lent = 1;
+  } else if (st == TF_OK) {
     cudaError_t e = cudaMallocHost((void**)&m->h_state, sizeof(tf::SolveState));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&m->h_params, sizeof(tf::SolveParams));
     if (e != cudaSuccess) {
@@ -239,12 +281,17 @@ extern "C" int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own,
     }
   }
   if (st == TF_OK) {
-    cudaError_t e = cudaMemcpy(m->d_row, row0.data(), row0.size() * sizeof(int),
-                               cudaMemcpyHostToDevice);
+    // From pageable memory these return once the source has been staged.
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(m->d_row, row0.data(), row0.size() * sizeof(int),
+                                    cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
-      e = cudaMemcpy(m->d_col, col0.data(), col0.size() * sizeof(int), cudaMemcpyHostToDevice);
+      e = cudaMemcpyAsync(m->d_col, col0.data(), col0.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
-      e = cudaMemcpy(m->d_dia, dia0.data(), dia0.size() * sizeof(int), cudaMemcpyHostToDevice);
+      e = cudaMemcpyAsync(m->d_dia, dia0.data(), dia0.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && !ctx->async_alloc) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
       tf_set_last_cuda_error(e, "cudaMemcpy(structure)", __FILE__, __LINE__);
       st = TF_ERR_CUDA;
@@ -267,9 +314,10 @@ extern "C" int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own,
     }
     if (n_cells > 0) st = tf_fp64_prepare(m);
   }
-  if (st == TF_OK && n_cells > 0 && diag_first) st = tf_icc_build(m, row0.data(), col0.data());
+  if (st == TF_OK && n_cells > 0 && diag_first && want_icc)
+    st = tf_icc_build(m, row0.data(), col0.data());
   if (st != TF_OK) {
-    free_matrix(m);
+    tf_matrix_free(m);
     return st;
   }
   *out = m;
@@ -280,7 +328,7 @@ extern "C" int tf_matrix_release(tf_matrix m) {
   if (!m) return TF_ERR_ARG;
   cudaSetDevice(m->ctx->device);
   cudaStreamSynchronize(m->ctx->stream);
-  free_matrix(m);
+  tf_matrix_free(m);
   return TF_OK;
 }
 
@@ -355,6 +403,20 @@ int finish_solve(tf_matrix_s* m, int* niter, double* fin_res) {
   }
   return TF_OK;
 }
+
+}  // namespace
+
+int tf_solve_resident(tf_matrix_s* m, int prec, int miter, double tol, const double* norm,
+                      int* niter, double* fin_res) {
+  const int st = run_solve_core(m, prec, miter, tol, norm);
+  if (st != TF_OK) {
+    cudaStreamSynchronize(m->ctx->stream);
+    return st;
+  }
+  return finish_solve(m, niter, fin_res);
+}
+
+namespace {
 
 int check_solve_args(tf_ctx ctx, tf_matrix m, int solver, int prec, int* niter,
                      double* fin_res) {

@@ -53,16 +53,23 @@ int tf_icc_build(tf_matrix_s* m, const int* row0, const int* col0) {
   bucket(levf, nf, m->h_levf_ptr, rf);
   bucket(levb, nb, m->h_levb_ptr, rb);
   const size_t nv = (size_t)m->nt + 8;
-  TF_CUDA_TRY(cudaMalloc((void**)&m->d_levf_rows, std::max<size_t>(rf.size(), 1) * sizeof(int)));
-  TF_CUDA_TRY(cudaMalloc((void**)&m->d_levb_rows, std::max<size_t>(rb.size(), 1) * sizeof(int)));
-  TF_CUDA_TRY(cudaMemcpy(m->d_levf_rows, rf.data(), rf.size() * sizeof(int),
-                         cudaMemcpyHostToDevice));
-  TF_CUDA_TRY(cudaMemcpy(m->d_levb_rows, rb.data(), rb.size() * sizeof(int),
-                         cudaMemcpyHostToDevice));
-  TF_CUDA_TRY(cudaMalloc((void**)&m->d_z, nv * sizeof(double)));
-  TF_CUDA_TRY(cudaMalloc((void**)&m->d_icc_d, nv * sizeof(double)));
-  TF_CUDA_TRY(cudaMalloc((void**)&m->d_icc_dinv, nv * sizeof(double)));
-  TF_CUDA_TRY(cudaMemset(m->d_z, 0, nv * sizeof(double)));
+  void* p = nullptr;
+  int st = tf_dev_alloc_bytes(m->ctx, &p, std::max<size_t>(rf.size(), 1) * sizeof(int));
+  m->d_levf_rows = (int*)p;
+  if (st == TF_OK) st = tf_dev_alloc_bytes(m->ctx, &p, std::max<size_t>(rb.size(), 1) * sizeof(int));
+  m->d_levb_rows = (int*)p;
+  if (st == TF_OK) st = tf_dev_alloc_bytes(m->ctx, &p, nv * sizeof(double));
+  m->d_z = (double*)p;
+  if (st == TF_OK) st = tf_dev_alloc_bytes(m->ctx, &p, nv * sizeof(double));
+  m->d_icc_d = (double*)p;
+  if (st == TF_OK) st = tf_dev_alloc_bytes(m->ctx, &p, nv * sizeof(double));
+  m->d_icc_dinv = (double*)p;
+  if (st != TF_OK) return st;
+  // From pageable memory these return once the source has been staged.
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_levf_rows, rf.data(), rf.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, m->ctx->stream));
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_levb_rows, rb.data(), rb.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, m->ctx->stream));
   m->icc_ready = 1;
   return TF_OK;
 }

@@ -32,6 +32,12 @@ struct tf_ctx_s {
   int history = 0;
   std::vector<double> last_hist;
   int last_count = 0;
+  // Stream-ordered allocation (cudaMallocAsync / cudaFreeAsync on `stream`)
+  // for matrices registered on this context: set by the request pool so a
+  // worker never synchronises the device when it registers or releases.
+  int async_alloc = 0;
+  tf::SolveState* h_state = nullptr;    // pinned, lent to async matrices
+  tf::SolveParams* h_params = nullptr;
 };
 
 // Device mirror of one Matrix_Type plus the Krylov workspace of its solves.
@@ -75,6 +81,9 @@ struct tf_matrix_s {
   // cached graphs, one per preconditioner
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   std::mutex mu;
+  int async_alloc = 0;   // device arrays from cudaMallocAsync on ctx->stream
+  int host_lent = 0;     // h_state / h_params belong to the context
+  size_t dev_bytes = 0;  // device bytes this matrix holds
 };
 
 // FP64 drop-in entry points implemented in tf_fp64.cu
@@ -87,4 +96,14 @@ int tf_fp64_residual(tf_matrix_s* m, const double* val, const double* b,
 int tf_fp64_nrms(tf_matrix_s* m, const double* val, const double* r,
                  const double* x, int has_norm, double norm, double* out);
 int tf_icc_build(tf_matrix_s* m, const int* h_row0, const int* h_col0);
+// Registration behind tf_matrix_register; want_icc = 0 skips the ICC level
+// schedule.  Device bytes the matrix will hold, for budgeting.
+int tf_matrix_create(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const int* row,
+                     const int* col, const int* dia, int want_icc, tf_matrix_s** out);
+void tf_matrix_free(tf_matrix_s* m);
+size_t tf_matrix_bytes(int n_cells, int64_t nnz);
+// Solve on a registered matrix with val/x/b already in its device buffers.
+int tf_solve_resident(tf_matrix_s* m, int prec, int miter, double tol, const double* norm,
+                      int* niter, double* fin_res);
+int tf_dev_alloc_bytes(tf_ctx_s* ctx, void** p, size_t bytes);
 

@@ -1,0 +1,268 @@
+// tf_pool.cu -- a pool of CUDA streams that serves Solve_Native requests.
+//
+// Independent solves are overlapped rather than fused: each worker thread
+// owns a context (one CUDA stream) and runs whole requests through the FP64
+// drop-in (one graph launch per solve, convergence decided on the device).
+// A request is exactly a Solve_Native call (Solve_Native.f90:33-44) on a
+// system the caller hands over: the pool copies it, registers it on the
+// worker's stream with stream-ordered allocation (cudaMallocAsync, so no
+// registration or release ever synchronises the device or another worker),
+// uploads the values, solves, writes x back and releases the memory.  The
+// caller's arrays are used in place (no copy on submission), so they must
+// stay valid until tf_pool_wait returns; conversion and upload run on the
+// workers, in parallel.
+//
+// Admission: requests are taken in arrival order while the device bytes of
+// the requests in flight plus the next one's stay within the memory budget;
+// a request larger than the whole budget is rejected (TF_ERR_OOM).  Small
+// systems, which a single stream leaves launch-latency bound, thus run many
+// at a time, and a large one shares the GPU with whatever fits beside it.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "tf_internal.h"
+
+namespace {
+using Clock = std::chrono::steady_clock;
+
+struct PoolReq {
+  int64_t id = 0;
+  int solver = 0, prec = 1;
+  int n = 0;
+  int64_t nnz = 0;
+  const int* row = nullptr;   // caller's arrays, valid until tf_pool_wait
+  const int* col = nullptr;
+  const int* dia = nullptr;
+  const double* val = nullptr;
+  const double* b = nullptr;
+  double* x = nullptr;        // initial guess in, solution out
+  int miter = 0;
+  double tol = 0.0;
+  int has_norm = 0;
+  double norm = 0.0;
+  size_t bytes = 0;
+  Clock::time_point t_submit, t_start, t_done;
+  int status = TF_OK;
+  int niter = 0;
+  double fin_res = 0.0;
+  bool done = false;
+};
+}  // namespace
+
+struct tf_pool_s {
+  int device = 0;
+  size_t budget = 0, used = 0, peak = 0;
+  std::vector<tf_ctx_s*> ctxs;
+  std::vector<std::thread> workers;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<std::shared_ptr<PoolReq>> queue;
+  std::map<int64_t, std::shared_ptr<PoolReq>> live;
+  int64_t next_id = 1;
+  bool stop = false;
+  long long submitted = 0, completed = 0, rejected = 0;
+
+  // Run one request on worker w's context.
+  int run(tf_ctx_s* ctx, PoolReq& r) {
+    tf_matrix_s* m = nullptr;
+    int st = tf_matrix_create(ctx, r.n, r.n, r.nnz, r.row, r.col, r.dia,
+                              r.prec == tf::kPrecIcc, &m);
+    if (st != TF_OK) return st;
+    cudaStream_t s = ctx->stream;
+    const size_t vb = (size_t)r.nnz * 8, nb = (size_t)r.n * 8;
+    cudaError_t e = cudaMemcpyAsync(m->d_val, r.val, vb, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->d_x, r.x, nb, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->d_b, r.b, nb, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+      tf_set_last_cuda_error(e, "pool upload", __FILE__, __LINE__);
+      st = TF_ERR_CUDA;
+    }
+    if (st == TF_OK)
+      st = tf_solve_resident(m, r.prec, r.miter, r.tol, r.has_norm ? &r.norm : nullptr,
+                             &r.niter, &r.fin_res);
+    if (st == TF_OK) {
+      e = cudaMemcpyAsync(r.x, m->d_x, nb, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) {
+        tf_set_last_cuda_error(e, "pool download", __FILE__, __LINE__);
+        st = TF_ERR_CUDA;
+      }
+    }
+    tf_matrix_free(m);
+    return st;
+  }
+
+  void loop(int w) {
+    tf_ctx_s* ctx = ctxs[w];
+    cudaSetDevice(device);
+    for (;;) {
+      std::shared_ptr<PoolReq> r;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_work.wait(lk, [&] {
+          return stop || (!queue.empty() && used + queue.front()->bytes <= budget);
+        });
+        if (stop) return;
+        r = queue.front();
+        queue.pop_front();
+        used += r->bytes;
+        peak = std::max(peak, used);
+        r->t_start = Clock::now();
+      }
+      const int st = run(ctx, *r);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        used -= r->bytes;
+        r->status = st;
+        r->t_done = Clock::now();
+        r->done = true;
+        ++completed;
+        cv_done.notify_all();
+        cv_work.notify_all();
+      }
+    }
+  }
+};
+
+extern "C" int tf_pool_create(int device, int workers, size_t mem_budget, tf_pool* out) {
+  if (!out || workers < 1 || workers > 256) return TF_ERR_ARG;
+  *out = nullptr;
+  auto* p = new tf_pool_s();
+  p->budget = mem_budget ? mem_budget : ((size_t)20 << 30);
+  for (int w = 0; w < workers; ++w) {
+    tf_ctx c = nullptr;
+    int st = tf_ctx_create(device, &c);
+    if (st == TF_OK) {
+      c->async_alloc = 1;
+      cudaError_t e = cudaMallocHost((void**)&c->h_state, sizeof(tf::SolveState));
+      if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_params, sizeof(tf::SolveParams));
+      if (e != cudaSuccess) st = TF_ERR_OOM;
+    }
+    if (st != TF_OK) {
+      if (c) tf_ctx_destroy(c);
+      for (tf_ctx_s* x : p->ctxs) tf_ctx_destroy(x);
+      delete p;
+      return st;
+    }
+    p->ctxs.push_back(c);
+  }
+  p->device = p->ctxs[0]->device;
+  // Keep freed stream-ordered memory in the device's pool for reuse.
+  cudaMemPool_t mp;
+  if (cudaDeviceGetDefaultMemPool(&mp, p->device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  for (int w = 0; w < workers; ++w) p->workers.emplace_back([p, w] { p->loop(w); });
+  *out = p;
+  return TF_OK;
+}
+
+extern "C" int tf_pool_submit(tf_pool p, int solver, int prec, int n, int64_t nnz,
+                              const int* row, const int* col, const int* dia,
+                              const double* val, const double* b, double* x,
+                              int miter, double tol, const double* norm, int64_t* req) {
+  if (!p || !req || n < 1 || nnz < n || !row || !col || !dia || !val || !b || !x)
+    return TF_ERR_ARG;
+  if (solver != TF_SOLVER_CG && solver != TF_SOLVER_BICG) return TF_ERR_UNKNOWN_SOLVER;
+  if (prec < TF_PREC_NONE || prec > TF_PREC_ICC) return TF_ERR_UNKNOWN_PREC;
+  auto r = std::make_shared<PoolReq>();
+  r->solver = solver;
+  r->prec = prec;
+  r->n = n;
+  r->nnz = nnz;
+  r->row = row;
+  r->col = col;
+  r->dia = dia;
+  r->val = val;
+  r->b = b;
+  r->x = x;
+  r->miter = miter;
+  r->tol = tol;
+  r->has_norm = norm ? 1 : 0;
+  r->norm = norm ? *norm : 0.0;
+  r->bytes = tf_matrix_bytes(n, nnz) +
+             (prec == TF_PREC_ICC ? (size_t)n * 40 + 4096 : 0);
+  std::lock_guard<std::mutex> lk(p->mu);
+  if (p->stop) return TF_ERR_CANCELLED;
+  r->id = p->next_id++;
+  r->t_submit = Clock::now();
+  p->live[r->id] = r;
+  ++p->submitted;
+  if (r->bytes > p->budget) {      // can never be admitted
+    r->status = TF_ERR_OOM;
+    r->done = true;
+    r->t_start = r->t_done = r->t_submit;
+    ++p->rejected;
+  } else {
+    p->queue.push_back(r);
+    p->cv_work.notify_all();
+  }
+  *req = r->id;
+  return TF_OK;
+}
+
+extern "C" int tf_pool_wait(tf_pool p, int64_t req, int* niter, double* fin_res,
+                            double* latency_ms, double* queue_ms) {
+  if (!p) return TF_ERR_ARG;
+  std::unique_lock<std::mutex> lk(p->mu);
+  auto it = p->live.find(req);
+  if (it == p->live.end()) return TF_ERR_ARG;
+  auto r = it->second;
+  p->cv_done.wait(lk, [&] { return r->done; });
+  p->live.erase(it);
+  using ms = std::chrono::duration<double, std::milli>;
+  if (latency_ms) *latency_ms = ms(r->t_done - r->t_submit).count();
+  if (queue_ms) *queue_ms = ms(r->t_start - r->t_submit).count();
+  if (r->status != TF_OK) return r->status;
+  if (niter) *niter = r->niter;
+  if (fin_res) *fin_res = r->fin_res;
+  return TF_OK;
+}
+
+extern "C" int tf_pool_stats(tf_pool p, long long* submitted, long long* completed,
+                             long long* rejected, size_t* peak_bytes) {
+  if (!p) return TF_ERR_ARG;
+  std::lock_guard<std::mutex> lk(p->mu);
+  if (submitted) *submitted = p->submitted;
+  if (completed) *completed = p->completed;
+  if (rejected) *rejected = p->rejected;
+  if (peak_bytes) *peak_bytes = p->peak;
+  return TF_OK;
+}
+
+extern "C" int tf_pool_destroy(tf_pool p) {
+  if (!p) return TF_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lk(p->mu);
+    p->stop = true;
+    for (auto& kv : p->live)
+      if (!kv.second->done) {
+        kv.second->status = TF_ERR_CANCELLED;
+        kv.second->done = true;
+      }
+    p->cv_work.notify_all();
+    p->cv_done.notify_all();
+  }
+  for (auto& t : p->workers) t.join();
+  for (tf_ctx_s* c : p->ctxs) {
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    if (c->h_state) cudaFreeHost(c->h_state);
+    if (c->h_params) cudaFreeHost(c->h_params);
+    c->h_state = nullptr;
+    c->h_params = nullptr;
+    tf_ctx_destroy(c);
+  }
+  delete p;
+  return TF_OK;
+}

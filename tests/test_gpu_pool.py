@@ -1,0 +1,74 @@
+"""GPU tests of the request pool: concurrent Solve_Native calls on several
+streams give exactly the results of tf_solve on the same inputs (the pool
+runs the same deterministic drop-in), under a device-memory budget."""
+import threading
+
+import numpy as np
+import pytest
+
+from tflows_b200 import native, pool, systems
+
+pytestmark = pytest.mark.gpu
+
+
+def _systems():
+    return [systems.small_hex(12, seed=1, kind="pressure", ratio=1.02),
+            systems.small_hex(24, seed=2, kind="pressure", ratio=1.02),
+            systems.small_hex(10, seed=3, kind="momentum", peclet=1.0),
+            systems.poly_system(2000, seed=4, kind="pressure"),
+            systems.small_hex(8, seed=5, kind="pressure", tol=1e-9, miter=300, prec="icc")]
+
+
+def _reference(ctx, s):
+    m = native.Matrix(ctx, s.csr.row, s.csr.col, s.csr.dia)
+    try:
+        v, x, b = s.val.copy(), s.x0.copy(), s.b.copy()
+        it, res = native.solve(ctx, m, s.solver, s.prec, v, x, b, s.miter, s.tol, s.norm)
+        return x, it, res
+    finally:
+        m.close()
+
+
+def test_pool_matches_single_solves(gpu_ctx):
+    sysl = _systems()
+    ref = [_reference(gpu_ctx, s) for s in sysl]
+    p = pool.Pool(workers=4, mem_budget=1 << 30)
+    try:
+        rids = {}
+
+        def submitter(offset):
+            for k in range(offset, 3 * len(sysl), 2):
+                rids[k] = p.submit(sysl[k % len(sysl)])
+
+        th = [threading.Thread(target=submitter, args=(o,)) for o in (0, 1)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        for k in sorted(rids):
+            r = p.wait(rids[k])
+            x, it, res = ref[k % len(sysl)]
+            assert r["niter"] == it and r["fin_res"] == res
+            assert np.array_equal(r["x"], x)
+            assert r["latency_ms"] >= r["queue_ms"] >= 0.0
+        st = p.stats()
+        assert st["completed"] == 3 * len(sysl) and st["rejected"] == 0
+        assert 0 < st["peak_bytes"] <= 1 << 30
+    finally:
+        p.close()
+
+
+def test_pool_budget(gpu_ctx):
+    small = systems.small_hex(6, seed=1, kind="pressure")
+    big = systems.small_hex(40, seed=1, kind="pressure")
+    p = pool.Pool(workers=2, mem_budget=4 << 20)
+    try:
+        r_big = p.submit(big)
+        r_small = p.submit(small)
+        with pytest.raises(native.TFError) as e:
+            p.wait(r_big)
+        assert e.value.status == 2          # TF_ERR_OOM: larger than the budget
+        assert p.wait(r_small)["niter"] > 0
+        assert p.stats()["rejected"] == 1
+    finally:
+        p.close()
