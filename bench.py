@@ -54,7 +54,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--count", type=int, default=512)
-    ap.add_argument("--mode", default="solve", choices=["solve", "spmv", "batched"],
+    ap.add_argument("--rate", type=float, default=200.0, help="served: arrivals per second")
+    ap.add_argument("--seconds", type=float, default=60.0, help="served: window length")
+    ap.add_argument("--mode", default="solve", choices=["solve", "spmv", "batched", "served"],
                     help="spmv: only the pressure matrix and `--steps` SpMV launches "
                          "(the small case profiled with ncu)")
     return ap.parse_args()
@@ -235,6 +237,125 @@ def run_batched(args):
     ctx.close()
 
 
+def _serve_stream(req_sys, rhs, rate, seconds, workers, budget, seed, max_outstanding=256):
+    """Poisson arrivals at `rate`/s for `seconds` into a request pool of
+    `workers` streams.  A request that arrives while `max_outstanding` are
+    queued or running is shed at the front door (counted, not submitted).
+    Completion times come from the library's own latency (submit to x copied
+    back); a request counts toward throughput when it completed inside the
+    window.  Everything still outstanding at the end is drained before the
+    pool closes."""
+    import math
+    from tflows_b200 import pool as tpool
+    rng = np.random.default_rng(seed)
+    sizes = np.array([s.n for s in req_sys])
+    kinds = np.array([s.solver for s in req_sys])
+    pl = tpool.Pool(workers=workers, mem_budget=budget)
+    pending, results = [], []
+    cv = threading.Condition()
+    state = {"submitting": True, "outstanding": 0}
+
+    def waiter():
+        while True:
+            with cv:
+                while not pending and state["submitting"]:
+                    cv.wait(0.05)
+                if not pending:
+                    return
+                rid, t_sub, idx = pending.pop(0)
+            r = pl.wait(rid)
+            with cv:
+                state["outstanding"] -= 1
+            results.append((t_sub, r["latency_ms"], r["queue_ms"], req_sys[idx].n * r["niter"]))
+
+    wt = threading.Thread(target=waiter)
+    wt.start()
+    t_start = time.perf_counter()
+    stop_at = t_start + seconds
+    t_next, offered, shed = t_start, 0, 0
+    while True:
+        t_next += rng.exponential(1.0 / rate)
+        if t_next > stop_at:
+            break
+        delay = t_next - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        kind = "cg" if rng.random() < 0.5 else "bicg"
+        n = math.exp(rng.uniform(math.log(1e4), math.log(4e6)))
+        cand = np.nonzero(kinds == kind)[0]
+        idx = int(cand[np.argmin(np.abs(np.log(sizes[cand]) - math.log(n)))])
+        offered += 1
+        with cv:
+            if state["outstanding"] >= max_outstanding:
+                shed += 1
+                continue
+            state["outstanding"] += 1
+        v = offered % len(rhs[idx])
+        s = req_sys[idx]
+        t_sub = time.perf_counter()
+        rid = pl.submit(s, b=rhs[idx][v][0], x0=np.zeros(s.n), miter=100000,
+                        tol=1e-10 * rhs[idx][v][1], norm=1.0)
+        with cv:
+            pending.append((rid, t_sub, idx))
+            cv.notify()
+    with cv:
+        state["submitting"] = False
+        cv.notify()
+    wt.join()
+    stats = pl.stats()
+    pl.close()
+    inwin = [r for r in results if r[0] + r[1] * 1e-3 <= stop_at]
+    lat = np.array([r[1] for r in inwin]) if inwin else np.zeros(1)
+    qms = np.array([r[2] for r in inwin]) if inwin else np.zeros(1)
+    return {"rate_per_s": rate, "seconds": seconds, "workers": workers,
+            "offered": offered, "shed": shed, "admitted": offered - shed,
+            "completed_in_window": len(inwin),
+            "solves_per_s": len(inwin) / seconds,
+            "mcell_iters_per_s": sum(r[3] for r in inwin) / seconds / 1e6,
+            "latency_ms_p50": float(np.percentile(lat, 50)),
+            "latency_ms_p99": float(np.percentile(lat, 99)),
+            "queue_ms_p50": float(np.percentile(qms, 50)),
+            "peak_device_bytes": stats["peak_bytes"]}
+
+
+def run_served(args):
+    """Served stream through the request pool (each request one Solve_Native
+    on the FP64 drop-in): Poisson arrivals at `--rate`/s of hex Poisson (Cg)
+    and polyhedral convection-diffusion (Bicg) systems, n log-uniform in
+    [1e4, 4e6], 20 GB device budget.  Compared with the same stream served
+    one request at a time (one stream), and with the pool at half its
+    measured saturation throughput for latency under a sustainable load."""
+    from tflows_b200 import systems, workloads
+    t0 = time.perf_counter()
+    req_sys = workloads.served_pool(seed=5, per_kind=8)
+    rhs = {}
+    for k, s in enumerate(req_sys):
+        a = s.val[s.csr.dia - 1]
+        rhs[k] = []
+        for v in range(3):
+            b = systems.uniform_rhs(s.n, 7000 + 10 * k + v, zero_mean=(s.solver == "cg"))
+            rhs[k].append((b, float(np.sqrt(np.sum((b / a) ** 2)))))
+    out = {"mode": "served", "gen_s": time.perf_counter() - t0,
+           "request_systems": [(s.name, s.n) for s in req_sys],
+           "workload": "Poisson arrivals; each request a hex Poisson (Cg) or polyhedral "
+                       "convection-diffusion (Bicg) system, n log-uniform [1e4, 4e6] "
+                       "(nearest of 16 pre-generated systems), seeded RHS, x0 = 0, "
+                       "tol 1e-10 x NRMS(b); FP64 Jacobi drop-in per request; 20 GB budget; "
+                       "at most 256 requests outstanding (the rest shed)"}
+    budget = 20 << 30
+    _serve_stream(req_sys, rhs, 5.0, 3.0, 8, budget, 1)          # warm-up
+    sat = _serve_stream(req_sys, rhs, args.rate, args.seconds, 8, budget, 2)
+    out["pool_8_streams"] = sat
+    out["one_at_a_time"] = _serve_stream(req_sys, rhs, args.rate, args.seconds / 2, 1,
+                                         budget, 2)
+    light = max(1.0, 0.5 * sat["solves_per_s"])
+    out["pool_8_streams_half_load"] = _serve_stream(req_sys, rhs, light, args.seconds / 2, 8,
+                                                    budget, 3)
+    out["throughput_ratio_pool_vs_one_at_a_time"] = (
+        sat["solves_per_s"] / max(out["one_at_a_time"]["solves_per_s"], 1e-9))
+    print(json.dumps(out), flush=True)
+
+
 def run_spmv_only(args):
     """Register the pressure matrix and launch the tiled SpMV --steps times."""
     import torch
@@ -266,10 +387,8 @@ def run_spmv_only(args):
 
 
 def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    from tflows_b200.replicas import dist_env as env
+    return env()
 
 
 def make_workload(size, peclet):
@@ -439,35 +558,16 @@ def main():
     if args.mode == "batched":
         run_batched(args)
         return
+    if args.mode == "served":
+        run_served(args)
+        return
 
     import torch
-    from tflows_b200 import native
+    from tflows_b200 import native, replicas
 
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def allmax(v):
-        if not dist:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def allsum(v):
-        if not dist:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    rep = replicas.Replicas("nccl")
+    barrier, allmax, allsum = rep.barrier, rep.max, rep.sum
 
     sysl = make_workload(args.size, args.peclet)
     ctx = native.Context(local)
@@ -619,8 +719,7 @@ def main():
     for m in mats:
         m.close()
     ctx.close()
-    if dist:
-        dist.destroy_process_group()
+    rep.close()
 
 
 if __name__ == "__main__":
