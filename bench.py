@@ -40,7 +40,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "t-flows_b200"))
 
-SPMV_BYTES = lambda n, nnz: 12 * nnz + 4 * (n + 1) + 16 * n  # noqa: E731
+def SPMV_BYTES(n, nnz, row_patterns=False):
+    """Bytes one SpMV launch must move: values, row pointers, column data,
+    p once and q once.  CSR columns: 4 bytes per entry; row-pattern layout:
+    one pattern byte per row."""
+    cols = n if row_patterns else 4 * nnz
+    return 8 * nnz + cols + 4 * (n + 1) + 16 * n
 
 
 def parse():
@@ -378,9 +383,10 @@ def run_spmv_only(args):
     e1.record(stream)
     e1.synchronize()
     t = e0.elapsed_time(e1) / 1e3 / max(args.steps, 1)
-    by = SPMV_BYTES(s.n, s.nnz)
+    by = SPMV_BYTES(s.n, s.nnz, m.row_patterns > 0)
     print(json.dumps({"mode": "spmv", "n": s.n, "nnz": s.nnz, "tile_cfg": m.tile_config,
-                      "launch_ms": t * 1e3, "bytes_per_launch": by,
+                      "row_patterns": m.row_patterns, "launch_ms": t * 1e3,
+                      "bytes_per_launch": by, "csr_bytes_per_launch": SPMV_BYTES(s.n, s.nnz),
                       "achieved_gbs": by / t / 1e9}), flush=True)
     m.close()
     ctx.close()
@@ -585,14 +591,23 @@ def main():
 
     results = {}
 
-    def device_step():
+    sys_ev = [[] for _ in sysl]   # per-system (start, end) events of the timed steps
+
+    def device_step(record=False):
         cells, its = 0, []
         with torch.cuda.stream(stream):
-            for s, m, d in zip(sysl, mats, dev):
+            for k, (s, m, d) in enumerate(zip(sysl, mats, dev)):
                 d["x"].copy_(d["x0"])
+                if record:
+                    ea = torch.cuda.Event(enable_timing=True)
+                    ea.record(stream)
                 it, res = native.solve_device(ctx, m, s.solver, s.prec, d["val"].data_ptr(),
                                               d["x"].data_ptr(), d["b"].data_ptr(), s.miter,
                                               s.tol, s.norm)
+                if record:
+                    eb = torch.cuda.Event(enable_timing=True)
+                    eb.record(stream)
+                    sys_ev[k].append((ea, eb))
                 cells += s.n * it
                 its.append((it, res))
         return cells, its
@@ -610,7 +625,7 @@ def main():
     for _ in range(args.steps):
         e_a = torch.cuda.Event(enable_timing=True)
         e_a.record(stream)
-        c, its = device_step()
+        c, its = device_step(record=True)
         e_b = torch.cuda.Event(enable_timing=True)
         e_b.record(stream)
         per_solve.append((e_a, e_b))
@@ -623,6 +638,7 @@ def main():
     t_dev_max = allmax(t_dev)
     cells_all = allsum(cells)
     step_ms = [a.elapsed_time(b) for a, b in per_solve]
+    per_system_ms = [sum(a.elapsed_time(b) for a, b in evs) for evs in sys_ev]
 
     # End-to-end through tf_solve with pinned host buffers.
     host = []
@@ -680,8 +696,14 @@ def main():
     r1.synchronize()
     t_spmv = r0.elapsed_time(r1) / 1e3 / nrep
     peak, peak_kind = measured_peak()
-    bytes_spmv = SPMV_BYTES(s0.n, s0.nnz)
+    pat = m0.row_patterns > 0
+    bytes_spmv = SPMV_BYTES(s0.n, s0.nnz, pat)
     achieved = bytes_spmv / t_spmv / 1e9
+    # Whole Cg iteration (pressure solve): the SpMV, k_update (read r, q,
+    # diag; write r) and k_pupdate (read r, diag, p, x; write p, x).
+    it_p = iters[0][0] * args.steps
+    t_iter = per_system_ms[0] / 1e3 / max(it_p, 1) if per_system_ms else None
+    bytes_iter = bytes_spmv + 32 * s0.n + 48 * s0.n
 
     launches = sum(args.steps * (4 + 3 * it) for it, _ in iters)
 
@@ -705,11 +727,19 @@ def main():
             "accuracy": acc,
             "e2e": {"value": e2e_all / t_e2e_max / 1e6, "unit": "Mcell-iters/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "hbm", "kernel": "k_spmv_alpha (tiled CSR SpMV + p.q)",
+            "roofline": {"bound": "hbm",
+                         "kernel": "k_spmv_alpha (tiled SpMV + p.q, "
+                                   + ("row-pattern columns)" if pat else "CSR columns)"),
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "bytes_per_launch": bytes_spmv, "launch_ms": t_spmv * 1e3,
-                         "traffic": ncu_traffic(args.size)},
+                         "bytes_per_launch": bytes_spmv,
+                         "csr_bytes_per_launch": SPMV_BYTES(s0.n, s0.nnz),
+                         "launch_ms": t_spmv * 1e3,
+                         "traffic": ncu_traffic(args.size),
+                         "cg_iteration": None if not t_iter else {
+                             "bytes": bytes_iter, "us": t_iter * 1e6,
+                             "achieved": bytes_iter / t_iter / 1e9,
+                             "frac": bytes_iter / t_iter / 1e9 / peak}},
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": launches,

@@ -82,6 +82,12 @@ int tf_matrix_info(tf_matrix m, int* n_cells, int* n_own, int64_t* nnz,
 /* SpMV tile configuration chosen at registration: 0/1/2 = 512/256/128-row
  * shared-memory tiles, 3 = rows read straight from global memory. */
 int tf_matrix_tile_config(tf_matrix m);
+/* Number of row patterns of the compressed column layout chosen at
+ * registration (rows whose column offsets relative to the row index repeat,
+ * as on structured hex blocks: one byte per row instead of four per entry;
+ * same entries, same order, same sums), 0 when the CSR columns are used.
+ * No reference counterpart: a property of this library's device layout. */
+int tf_matrix_row_patterns(tf_matrix m);
 
 /* Solve A x = b.  Replaces Native_Type % Solve_Native (Solve_Native.f90:2-46)
  * and so Cg.f90:2-257 / Bicg.f90:2-269.  val, x and b are host arrays of

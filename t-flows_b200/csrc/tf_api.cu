@@ -166,7 +166,7 @@ void tf_matrix_free(tf_matrix_s* m) {
   void* ptrs[] = {m->d_row, m->d_col, m->d_dia, m->d_val, m->d_x, m->d_b,
                   m->d_r, m->d_p, m->d_q, m->d_z, m->d_adiag, m->d_part,
                   m->d_hist, m->d_state, m->d_params, m->d_levf_rows, m->d_levb_rows,
-                  m->d_icc_d, m->d_icc_dinv};
+                  m->d_icc_d, m->d_icc_dinv, m->d_pat, m->d_pat_tab};
   for (void* p : ptrs)
     if (p) {
       if (m->async_alloc) cudaFreeAsync(p, m->ctx->stream);
@@ -183,10 +183,56 @@ size_t tf_matrix_bytes(int n_cells, int64_t nnz) {
   auto up = [](size_t b) { return (b + 511) & ~size_t(511); };
   const size_t nv = (size_t)n_cells + 8, nz = (size_t)nnz + 8;
   return up(((size_t)n_cells + 9) * 4) + up(nz * 4) + up(nv * 4) + up(nz * 8) +
-         6 * up(nv * 8) + up(((size_t)8 * tf::kMaxBlocks + 16) * 8) + 2048;
+         6 * up(nv * 8) + up(((size_t)8 * tf::kMaxBlocks + 16) * 8) + up((size_t)n_cells + 32) +
+         up((size_t)tf::kPatMax * (tf::kPatMaxLen + 1) * 4) + 2048;
 }
 
 namespace {
+
+// Row patterns of the first ni rows: pat[i] names the offset sequence
+// (col_j - i over the row's entries, in storage order).  Returns the number
+// of patterns, or 0 when there are more than kPatMax of them or a row is
+// longer than kPatMaxLen (then the CSR columns are used).
+int find_row_patterns(const std::vector<int>& row0, const std::vector<int>& col0, int ni,
+                      std::vector<unsigned char>& pat, std::vector<int>& tab) {
+  using tf::kPatMax;
+  using tf::kPatMaxLen;
+  std::vector<int> offs((size_t)kPatMax * kPatMaxLen, 0), lens;
+  std::vector<uint64_t> keys;
+  pat.assign((size_t)ni + 32, 0);
+  int last = -1;
+  for (int i = 0; i < ni; ++i) {
+    const int js = row0[i], len = row0[i + 1] - js;
+    if (len > kPatMaxLen) return 0;
+    uint64_t h = 1469598103934665603ull ^ (uint64_t)len;
+    for (int k = 0; k < len; ++k)
+      h = (h ^ (uint64_t)(uint32_t)(col0[js + k] - i)) * 1099511628211ull;
+    auto same = [&](int p) {
+      if (keys[p] != h || lens[p] != len) return false;
+      for (int k = 0; k < len; ++k)
+        if (offs[(size_t)p * kPatMaxLen + k] != col0[js + k] - i) return false;
+      return true;
+    };
+    int id = -1;
+    if (last >= 0 && same(last)) id = last;   // runs of equal rows are the norm
+    for (int p = 0; id < 0 && p < (int)keys.size(); ++p)
+      if (same(p)) id = p;
+    if (id < 0) {
+      if ((int)keys.size() == kPatMax) return 0;
+      id = (int)keys.size();
+      keys.push_back(h);
+      lens.push_back(len);
+      for (int k = 0; k < len; ++k) offs[(size_t)id * kPatMaxLen + k] = col0[js + k] - i;
+    }
+    pat[i] = (unsigned char)id;
+    last = id;
+  }
+  const int np = (int)keys.size();
+  tab.assign((size_t)np * (kPatMaxLen + 1), 0);
+  std::copy(offs.begin(), offs.begin() + (size_t)np * kPatMaxLen, tab.begin());
+  std::copy(lens.begin(), lens.end(), tab.begin() + (size_t)np * kPatMaxLen);
+  return np;
+}
 
 // Largest nnz of any tile of `rows` consecutive rows among the first ni.
 int64_t max_tile_nnz(const std::vector<int>& row0, int ni, int rows) {
@@ -312,7 +358,30 @@ int tf_matrix_create(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const i
           (c == 3 || max_tile_nnz(row0, n_own, tf::kTileRows[c]) <= tf::kTileNnzCap[c]))
         m->tile_cfg = c;
     }
-    if (n_cells > 0) st = tf_fp64_prepare(m);
+    // Row-pattern columns for tiled matrices (TF_NO_ROW_PATTERNS keeps CSR).
+    if (n_cells > 0 && m->tile_cfg != tf::kTileNone && !getenv("TF_NO_ROW_PATTERNS")) {
+      std::vector<unsigned char> pat;
+      std::vector<int> tab;
+      const int np = find_row_patterns(row0, col0, n_own, pat, tab);
+      if (np > 0) {
+        st = dev_alloc(ctx, &m->d_pat, pat.size());
+        if (st == TF_OK) st = dev_alloc(ctx, &m->d_pat_tab, tab.size());
+        if (st == TF_OK) {
+          cudaError_t e = cudaMemcpyAsync(m->d_pat, pat.data(), pat.size(),
+                                          cudaMemcpyHostToDevice, ctx->stream);
+          if (e == cudaSuccess)
+            e = cudaMemcpyAsync(m->d_pat_tab, tab.data(), tab.size() * sizeof(int),
+                                cudaMemcpyHostToDevice, ctx->stream);
+          if (e == cudaSuccess && !ctx->async_alloc) e = cudaStreamSynchronize(ctx->stream);
+          if (e != cudaSuccess) {
+            tf_set_last_cuda_error(e, "cudaMemcpy(row patterns)", __FILE__, __LINE__);
+            st = TF_ERR_CUDA;
+          }
+        }
+        if (st == TF_OK) m->npat = np;
+      }
+    }
+    if (st == TF_OK && n_cells > 0) st = tf_fp64_prepare(m);
   }
   if (st == TF_OK && n_cells > 0 && diag_first && want_icc)
     st = tf_icc_build(m, row0.data(), col0.data());
@@ -330,6 +399,10 @@ extern "C" int tf_matrix_release(tf_matrix m) {
   cudaStreamSynchronize(m->ctx->stream);
   tf_matrix_free(m);
   return TF_OK;
+}
+
+extern "C" int tf_matrix_row_patterns(tf_matrix m) {
+  return m ? m->npat : TF_ERR_ARG;
 }
 
 extern "C" int tf_matrix_info(tf_matrix m, int* n_cells, int* n_own,

@@ -45,6 +45,8 @@ struct SolveState {
   int niter;
   int done;
   int status;         // TF_OK or TF_ERR_TIMEOUT
+  int x_pend;         // x still lacks the last alpha * p (deferred update)
+  int pad;
   unsigned counter[8];  // last-block-done counters, one per kernel kind
 };
 
@@ -113,6 +115,42 @@ __device__ double block_red(double v, double* scratch) {
   return r;
 }
 
+// Block reduction of NQ values at once (two __syncthreads instead of two
+// per value); every thread gets the results.  `scratch` needs
+// NQ * blockDim/32 doubles.  Warp partials are combined in warp order, as
+// block_red does, so the result is the same as NQ separate block_red calls.
+template <int NQ>
+__device__ void block_red_n(double (&v)[NQ], const int (&ops)[NQ], double* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    if (ops[q] == kSum) v[q] = warp_red<kSum>(v[q]);
+    else if (ops[q] == kMin) v[q] = warp_red<kMin>(v[q]);
+    else v[q] = warp_red<kMax>(v[q]);
+  }
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) scratch[q * 32 + warp] = v[q];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double r;
+    if (ops[q] == kSum) r = red_identity<kSum>();
+    else if (ops[q] == kMin) r = red_identity<kMin>();
+    else r = red_identity<kMax>();
+    for (int w = 0; w < nw; ++w) {
+      const double s = scratch[q * 32 + w];
+      if (ops[q] == kSum) r = red2<kSum>(r, s);
+      else if (ops[q] == kMin) r = red2<kMin>(r, s);
+      else r = red2<kMax>(r, s);
+    }
+    v[q] = r;
+  }
+}
+
 // Grid-level "last block done" reduction of NQ values with ops OPS.
 // Every block calls it once with its block-reduced values (valid in all
 // threads).  Returns true in all threads of the last block, whose `vals`
@@ -151,6 +189,43 @@ __device__ bool grid_reduce_last(double (&vals)[NQ], const int (&ops)[NQ],
     else acc = block_red<kMax>(acc, scratch);
     vals[q] = acc;
   }
+  if (threadIdx.x == 0) *counter = 0u;  // ready for the next launch
+  return true;
+}
+
+// grid_reduce_last with one block_red_n for all NQ values in the last
+// block; scratch needs NQ * 32 doubles.  Same combination order, so the
+// same results as grid_reduce_last.
+template <int NQ>
+__device__ bool grid_reduce_last_n(double (&vals)[NQ], const int (&ops)[NQ],
+                                   double* part, unsigned* counter, double* scratch) {
+  __shared__ int s_last;
+  const unsigned G = gridDim.x;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) part[q * G + blockIdx.x] = vals[q];
+    __threadfence();
+    unsigned prev = atomicAdd(counter, 1u);
+    s_last = (prev == G - 1);
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double acc;
+    if (ops[q] == kSum) acc = 0.0;
+    else if (ops[q] == kMin) acc = red_identity<kMin>();
+    else acc = red_identity<kMax>();
+    for (unsigned b = threadIdx.x; b < G; b += blockDim.x) {
+      double v = __ldcg(part + q * G + b);
+      if (ops[q] == kSum) acc = __dadd_rn(acc, v);
+      else if (ops[q] == kMin) acc = fmin(acc, v);
+      else acc = fmax(acc, v);
+    }
+    vals[q] = acc;
+  }
+  block_red_n<NQ>(vals, ops, scratch);
   if (threadIdx.x == 0) *counter = 0u;  // ready for the next launch
   return true;
 }
@@ -197,6 +272,10 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar,
           smem_u32(bar)),
       "r"(bytes)
       : "memory");
+}
+// Plain arrival (one of the barrier's expected count), release semantics.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   unsigned ok;

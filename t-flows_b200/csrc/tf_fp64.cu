@@ -104,6 +104,7 @@ __global__ void __launch_bounds__(256) k_diag(VecArgs a) {
     st->rho = 0.0;
     st->rho_old = 0.0;
     st->alpha = 0.0;
+    st->x_pend = 0;
   }
 }
 
@@ -152,7 +153,8 @@ __global__ void __launch_bounds__(256) k_scale(VecArgs a) {
   }
 }
 
-// val /= fn, b /= fn (Cg.f90:245-250)
+// val /= fn, b /= fn (Cg.f90:245-250); the last x += alfa p when the
+// update was deferred (k_update with XDEF).
 __global__ void __launch_bounds__(256) k_unscale(VecArgs a) {
   const double fn = a.st->fn;
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -160,18 +162,27 @@ __global__ void __launch_bounds__(256) k_unscale(VecArgs a) {
 #pragma unroll 4
   for (long long j = tid; j < a.nnz; j += stride) a.val[j] = __ddiv_rn(a.val[j], fn);
   for (long long i = tid; i < a.nt; i += stride) a.b[i] = __ddiv_rn(a.b[i], fn);
+  if (a.st->x_pend) {
+    const double alpha = a.st->alpha;
+    for (long long i = tid; i < a.ni; i += stride)
+      a.x[i] = __dadd_rn(a.x[i], __dmul_rn(alpha, a.p[i]));
+  }
 }
 
 // ---------------------------------------------------------------------------
 // Per-row operators for the tile streamer
 // ---------------------------------------------------------------------------
+// Row sums visit the row's entries in storage order.  COL(k) gives the
+// column of entry k: the staged column index (CSR tiles) or i + offset
+// (row-pattern tiles); either way the same operands in the same order.
+
 // q_i = sum_j a_ij p_j (Cg.f90:179-183), accumulates p_i q_i (:190-195)
 struct OpSpmvDot {
   const double* __restrict__ p;
   double* __restrict__ q;
   double pq;
-  __device__ __forceinline__ void operator()(int i, const double* v,
-                                             const int* c, int len) {
+  template <class COL>
+  __device__ __forceinline__ void body(int i, const double* v, COL col, int len) {
     double acc = 0.0;
 #pragma unroll 1
     for (int k0 = 0; k0 < len; k0 += 8) {
@@ -180,7 +191,7 @@ struct OpSpmvDot {
       for (int u = 0; u < 8; ++u)
         if (k0 + u < len) {
           vv[u] = v[k0 + u];
-          pv[u] = __ldg(p + c[k0 + u]);
+          pv[u] = __ldg(p + col(k0 + u));
         }
 #pragma unroll
       for (int u = 0; u < 8; ++u)
@@ -188,6 +199,12 @@ struct OpSpmvDot {
     }
     q[i] = acc;
     pq = __dadd_rn(pq, __dmul_rn(__ldg(p + i), acc));
+  }
+  __device__ __forceinline__ void operator()(int i, const double* v, const int* c, int len) {
+    body(i, v, [c](int k) { return c[k]; }, len);
+  }
+  __device__ __forceinline__ void pat(int i, const double* v, const int* o, int len) {
+    body(i, v, [i, o](int k) { return i + o[k]; }, len);
   }
 };
 
@@ -200,8 +217,8 @@ struct OpResidual {
   double* __restrict__ r;
   const double* __restrict__ adiag;
   double s, rho;
-  __device__ __forceinline__ void operator()(int i, const double* v,
-                                             const int* c, int len) {
+  template <class COL>
+  __device__ __forceinline__ void body(int i, const double* v, COL col, int len) {
     double acc = b[i];
 #pragma unroll 1
     for (int k0 = 0; k0 < len; k0 += 8) {
@@ -210,7 +227,7 @@ struct OpResidual {
       for (int u = 0; u < 8; ++u)
         if (k0 + u < len) {
           vv[u] = v[k0 + u];
-          xv[u] = __ldg(x + c[k0 + u]);
+          xv[u] = __ldg(x + col(k0 + u));
         }
 #pragma unroll
       for (int u = 0; u < 8; ++u)
@@ -226,22 +243,33 @@ struct OpResidual {
       rho = __dadd_rn(rho, __dmul_rn(acc, acc));
     }
   }
+  __device__ __forceinline__ void operator()(int i, const double* v, const int* c, int len) {
+    body(i, v, [c](int k) { return c[k]; }, len);
+  }
+  __device__ __forceinline__ void pat(int i, const double* v, const int* o, int len) {
+    body(i, v, [i, o](int k) { return i + o[k]; }, len);
+  }
 };
 
 struct SpArgs {
   const int* row;
   const int* col;
   const double* val;
+  PatTable pt;       // row patterns (pt.npat > 0 when the PAT kernels run)
   int nrows;
   VecArgs v;
   double* out_scalar;  // building-block mode: receives the dot product
 };
 
-// Rows through shared-memory tiles (CFG < kTileNone) or straight from
-// global memory (kTileNone: rows too long for any tile).
-template <int CFG, class Op>
+// Rows through shared-memory tiles (CFG < kTileNone; PAT: row-pattern
+// columns) or straight from global memory (kTileNone: rows too long for
+// any tile).
+template <int CFG, int PAT, class Op>
 __device__ __forceinline__ bool run_rows(const SpArgs& a, Op& op) {
-  if constexpr (CFG == kTileNone) {
+  if constexpr (CFG != kTileNone && PAT) {
+    return stream_tiles_pat<kTileRows[CFG], kTileNnzCap[CFG], kPatStages>(a.row, a.pt, a.val,
+                                                                          a.nrows, op);
+  } else if constexpr (CFG == kTileNone) {
     const int stride = gridDim.x * blockDim.x;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nrows; i += stride) {
       const int js = a.row[i], je = a.row[i + 1];
@@ -254,21 +282,30 @@ __device__ __forceinline__ bool run_rows(const SpArgs& a, Op& op) {
   }
 }
 
-template <int CFG>
-constexpr int cfg_threads() { return CFG == kTileNone ? 256 : kTileRows[CFG]; }
+template <int CFG, int PAT = 0>
+constexpr int cfg_threads() {
+  if constexpr (CFG == kTileNone) return 256;
+  else if constexpr (PAT != 0) return pat_threads<kTileRows[CFG]>();
+  else return kTileRows[CFG];
+}
+// Two CTAs per SM: caps the row-pattern kernels (ROWS + 32 threads) at the
+// registers that two of them can hold.
+template <int CFG, int PAT>
+constexpr int cfg_min_blocks() { return (CFG != kTileNone && PAT) ? 2 : 1; }
 
 __device__ __forceinline__ void flag_timeout(SolveState* st) {
   if (st) atomicExch(&st->status, (int)TF_ERR_TIMEOUT);
 }
 
 // r = b - A x, NRMS(r) (Cg.f90:109-123), rho of iteration 1.
-template <int CFG, int PREC>
-__global__ void __launch_bounds__(cfg_threads<CFG>()) k_residual(SpArgs a) {
+template <int CFG, int PREC, int PAT>
+__global__ void __launch_bounds__(cfg_threads<CFG, PAT>(), cfg_min_blocks<CFG, PAT>())
+    k_residual(SpArgs a) {
   __shared__ double scratch[32];
   SolveState* st = a.v.st;
   if (st && st->done) return;
   OpResidual<PREC> op{a.v.x, a.v.b, a.v.r, a.v.adiag, 0.0, 0.0};
-  if (!run_rows<CFG>(a, op) && threadIdx.x == 0) flag_timeout(st);
+  if (!run_rows<CFG, PAT>(a, op) && threadIdx.x == 0) flag_timeout(st);
   double v[2] = {block_red<kSum>(op.s, scratch), block_red<kSum>(op.rho, scratch)};
   const int ops[2] = {kSum, kSum};
   unsigned* cnt = st ? &st->counter[kCntResid] : reinterpret_cast<unsigned*>(a.out_scalar + 1);
@@ -290,33 +327,93 @@ __global__ void __launch_bounds__(cfg_threads<CFG>()) k_residual(SpArgs a) {
   }
 }
 
+// Vector kernels walk the rows in pairs (16-byte loads) and, per step,
+// load kBatch pairs into registers before computing any of them, so each
+// thread keeps kBatch x (arrays read) x 16 bytes in flight.  Pair j of
+// step t is base + u * stride for u < kBatch (coalesced across a warp).
+// DESC walks pairs from the top down: the rows a kernel touches last are
+// still in L2 when the next kernel, walking the other way, starts on them.
+constexpr int kBatch = 2;
+
+__device__ __forceinline__ int pair_index(int j, int np, bool desc) {
+  return desc ? np - 1 - j : j;
+}
+
 // z = M^-1 r (Prec_Solve.f90:44-49 / :97-102) and p = z + beta p
-// (Cg.f90:158-171).  ICC reads z from the triangular solves.
-template <int PREC>
+// (Cg.f90:158-171).  ICC reads z from the triangular solves.  XDEF: the
+// previous iteration's x += alfa p (Cg.f90:204-206) is applied here, just
+// before p is overwritten, instead of in k_update -- same operands, same
+// rounding, one pass over p fewer.
+template <int PREC, int XDEF, int DESC>
 __global__ void __launch_bounds__(256) k_pupdate(VecArgs a) {
   const SolveState* st = a.st;
   if (st->done) return;
   const int k = st->iter;
-  const double beta = (k == 1) ? 0.0 : __ddiv_rn(st->rho, st->rho_old);
+  const bool first = (k == 1);
+  const double beta = first ? 0.0 : __ddiv_rn(st->rho, st->rho_old);
+  const double alpha = st->alpha;   // alfa of iteration k-1
+  const double2* __restrict__ r2 = reinterpret_cast<const double2*>(PREC == kPrecIcc ? a.z : a.r);
+  const double2* __restrict__ a2 = reinterpret_cast<const double2*>(a.adiag);
+  double2* __restrict__ p2 = reinterpret_cast<double2*>(a.p);
+  double2* __restrict__ x2 = reinterpret_cast<double2*>(a.x);
+  const int np = a.ni >> 1;
   const int stride = gridDim.x * blockDim.x;
-#pragma unroll 4
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.ni; i += stride) {
-    double zi;
-    if (PREC == kPrecJacobi) zi = __dmul_rn(a.r[i], __drcp_rn(a.adiag[i]));
-    else if (PREC == kPrecNone) zi = a.r[i];
-    else zi = a.z[i];
-    a.p[i] = (k == 1) ? zi : __dadd_rn(zi, __dmul_rn(beta, a.p[i]));
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  auto zval = [&](double ri, double ai) {
+    if (PREC == kPrecJacobi) return __dmul_rn(ri, __drcp_rn(ai));
+    return ri;
+  };
+  auto pval = [&](double zi, double pi) {
+    return first ? zi : __dadd_rn(zi, __dmul_rn(beta, pi));
+  };
+  for (int base = tid; base < np; base += kBatch * stride) {
+    double2 rv[kBatch], av[kBatch], pv[kBatch], xv[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int j = base + u * stride;
+      if (j < np) {
+        const int jj = pair_index(j, np, DESC);
+        rv[u] = r2[jj];
+        if (PREC == kPrecJacobi) av[u] = a2[jj];
+        if (!first) pv[u] = p2[jj];
+        if (XDEF && !first) xv[u] = x2[jj];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int j = base + u * stride;
+      if (j < np) {
+        const int jj = pair_index(j, np, DESC);
+        if (XDEF && !first) {
+          xv[u].x = __dadd_rn(xv[u].x, __dmul_rn(alpha, pv[u].x));
+          xv[u].y = __dadd_rn(xv[u].y, __dmul_rn(alpha, pv[u].y));
+          x2[jj] = xv[u];
+        }
+        double2 o;
+        o.x = pval(zval(rv[u].x, PREC == kPrecJacobi ? av[u].x : 1.0), pv[u].x);
+        o.y = pval(zval(rv[u].y, PREC == kPrecJacobi ? av[u].y : 1.0), pv[u].y);
+        p2[jj] = o;
+      }
+    }
+  }
+  if ((a.ni & 1) && tid == 0) {   // the odd last row
+    const int i = a.ni - 1;
+    const double ri = (PREC == kPrecIcc) ? a.z[i] : a.r[i];
+    const double pi = first ? 0.0 : a.p[i];
+    if (XDEF && !first) a.x[i] = __dadd_rn(a.x[i], __dmul_rn(alpha, pi));
+    a.p[i] = pval(zval(ri, PREC == kPrecJacobi ? a.adiag[i] : 1.0), pi);
   }
 }
 
 // q = A p, p.q, alfa = rho / p.q (Cg.f90:176-198)
-template <int CFG>
-__global__ void __launch_bounds__(cfg_threads<CFG>()) k_spmv_alpha(SpArgs a) {
+template <int CFG, int PAT>
+__global__ void __launch_bounds__(cfg_threads<CFG, PAT>(), cfg_min_blocks<CFG, PAT>())
+    k_spmv_alpha(SpArgs a) {
   __shared__ double scratch[32];
   SolveState* st = a.v.st;
   if (st && st->done) return;
   OpSpmvDot op{a.v.p, a.v.q, 0.0};
-  if (!run_rows<CFG>(a, op) && threadIdx.x == 0) flag_timeout(st);
+  if (!run_rows<CFG, PAT>(a, op) && threadIdx.x == 0) flag_timeout(st);
   double v[1] = {block_red<kSum>(op.pq, scratch)};
   const int ops[1] = {kSum};
   unsigned* cnt = st ? &st->counter[kCntSpmv] : reinterpret_cast<unsigned*>(a.out_scalar + 1);
@@ -329,11 +426,13 @@ __global__ void __launch_bounds__(cfg_threads<CFG>()) k_spmv_alpha(SpArgs a) {
   }
 }
 
-// x += alfa p; r -= alfa q (Cg.f90:204-209); NRMS(r, x) and the test
-// (:214-222); rho for the next iteration (Jacobi / none).
-template <int PREC>
-__global__ void __launch_bounds__(256) k_update(VecArgs a) {
-  __shared__ double scratch[32];
+// r -= alfa q (Cg.f90:207-209) and, unless deferred to the next k_pupdate
+// (XDEF), x += alfa p (:204-206); NRMS(r, x) and the test (:214-222); rho
+// for the next iteration (Jacobi / none).  XDEF requires norm present (the
+// NRMS then does not look at x).
+template <int PREC, int XDEF, int DESC>
+__global__ void __launch_bounds__(256, 3) k_update(VecArgs a) {
+  __shared__ double scratch[4 * 32];
   SolveState* st = a.st;
   if (st->done) {
     if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(a, 0);
@@ -343,14 +442,17 @@ __global__ void __launch_bounds__(256) k_update(VecArgs a) {
   const SolveParams* prm = a.prm;
   const int has_norm = prm->has_norm;
   double s = 0.0, rho = 0.0, mn = kHuge, mx = -kHuge;
+  double2* __restrict__ r2 = reinterpret_cast<double2*>(a.r);
+  const double2* __restrict__ q2 = reinterpret_cast<const double2*>(a.q);
+  const double2* __restrict__ a2 = reinterpret_cast<const double2*>(a.adiag);
+  const double2* __restrict__ p2 = reinterpret_cast<const double2*>(a.p);
+  double2* __restrict__ x2 = reinterpret_cast<double2*>(a.x);
+  const int np = a.ni >> 1;
   const int stride = gridDim.x * blockDim.x;
-#pragma unroll 2
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.ni; i += stride) {
-    const double xi = __dadd_rn(a.x[i], __dmul_rn(alpha, a.p[i]));
-    const double ri = __dsub_rn(a.r[i], __dmul_rn(alpha, a.q[i]));
-    a.x[i] = xi;
-    a.r[i] = ri;
-    const double ai = a.adiag[i];
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  // one row: returns the new r; accumulates the NRMS term, rho, x range
+  auto row = [&](double ri, double qi, double ai) {
+    ri = __dsub_rn(ri, __dmul_rn(alpha, qi));
     s = __dadd_rn(s, nrms_term(ri, ai));
     if (PREC == kPrecJacobi) {
       const double zi = __dmul_rn(ri, __drcp_rn(ai));
@@ -358,15 +460,58 @@ __global__ void __launch_bounds__(256) k_update(VecArgs a) {
     } else if (PREC == kPrecNone) {
       rho = __dadd_rn(rho, __dmul_rn(ri, ri));
     }
+    return ri;
+  };
+  auto xrow = [&](double xi, double pi) {
+    xi = __dadd_rn(xi, __dmul_rn(alpha, pi));
     if (!has_norm) {
       mn = fmin_ref(mn, xi);
       mx = fmax_ref(mx, xi);
     }
+    return xi;
+  };
+  for (int base = tid; base < np; base += kBatch * stride) {
+    double2 rv[kBatch], qv[kBatch], av[kBatch], pv[kBatch], xv[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int j = base + u * stride;
+      if (j < np) {
+        const int jj = pair_index(j, np, DESC);
+        rv[u] = r2[jj];
+        qv[u] = q2[jj];
+        av[u] = a2[jj];
+        if (!XDEF) {
+          pv[u] = p2[jj];
+          xv[u] = x2[jj];
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int j = base + u * stride;
+      if (j < np) {
+        const int jj = pair_index(j, np, DESC);
+        if (!XDEF) {   // the reference's order: x first (:204-206), then r
+          xv[u].x = xrow(xv[u].x, pv[u].x);
+          xv[u].y = xrow(xv[u].y, pv[u].y);
+          x2[jj] = xv[u];
+        }
+        double2 o;
+        o.x = row(rv[u].x, qv[u].x, av[u].x);
+        o.y = row(rv[u].y, qv[u].y, av[u].y);
+        r2[jj] = o;
+      }
+    }
   }
-  double v[4] = {block_red<kSum>(s, scratch), block_red<kSum>(rho, scratch),
-                 block_red<kMin>(mn, scratch), block_red<kMax>(mx, scratch)};
+  if ((a.ni & 1) && tid == 0) {   // the odd last row
+    const int i = a.ni - 1;
+    if (!XDEF) a.x[i] = xrow(a.x[i], a.p[i]);
+    a.r[i] = row(a.r[i], a.q[i], a.adiag[i]);
+  }
+  double v[4] = {s, rho, mn, mx};
   const int ops[4] = {kSum, kSum, kMin, kMax};
-  if (grid_reduce_last<4>(v, ops, a.part, &st->counter[kCntUpdate], scratch) &&
+  block_red_n<4>(v, ops, scratch);
+  if (grid_reduce_last_n<4>(v, ops, a.part, &st->counter[kCntUpdate], scratch) &&
       threadIdx.x == 0) {
     const double res = nrms_finish(v[0], has_norm, prm->norm, v[2], v[3]);
     st->res = res;
@@ -388,6 +533,7 @@ __global__ void __launch_bounds__(256) k_update(VecArgs a) {
       }
       st->iter = k + 1;
     }
+    if (XDEF && st->done) st->x_pend = 1;   // k_unscale applies the last alfa p
     set_cond(a, st->done ? 0 : 1);
   }
 }
@@ -401,19 +547,21 @@ using namespace tf;
 // ---------------------------------------------------------------------------
 namespace {
 
-template <int CFG>
+template <int CFG, int PAT>
 size_t cfg_smem() {
   if constexpr (CFG == kTileNone) return 0;
+  else if constexpr (PAT)
+    return PatLayout<kTileRows[CFG], kTileNnzCap[CFG], kPatStages>::kSmemBytes;
   else return TileLayout<kTileRows[CFG], kTileNnzCap[CFG], double, 2>::kSmemBytes;
 }
 
-template <int CFG, int PREC>
+template <int CFG, int PREC, int PAT>
 int set_attrs_cfg() {
-  const size_t sm = cfg_smem<CFG>();
+  const size_t sm = cfg_smem<CFG, PAT>();
   if (sm > 48 * 1024) {
-    TF_CUDA_TRY(cudaFuncSetAttribute(k_residual<CFG, PREC>,
+    TF_CUDA_TRY(cudaFuncSetAttribute(k_residual<CFG, PREC, PAT>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    TF_CUDA_TRY(cudaFuncSetAttribute(k_spmv_alpha<CFG>,
+    TF_CUDA_TRY(cudaFuncSetAttribute(k_spmv_alpha<CFG, PAT>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   }
   return TF_OK;
@@ -446,6 +594,9 @@ SpArgs make_sp_args(tf_matrix_s* m, const VecArgs& v) {
   s.row = m->d_row;
   s.col = m->d_col;
   s.val = m->d_val;
+  s.pt.pat = m->d_pat;
+  s.pt.tab = m->d_pat_tab;
+  s.pt.npat = m->npat;
   s.nrows = m->ni;
   s.v = v;
   s.out_scalar = nullptr;
@@ -523,9 +674,27 @@ struct RhoArgs {
   SolveState* st;
 };
 
-template <int CFG, int PREC>
-int build_graph_t(tf_matrix_s* m, cudaGraphExec_t* out) {
-  int st = set_attrs_cfg<CFG, PREC>();
+// The iteration's vector kernels for this solve: xdef defers x += alfa p
+// to the next k_pupdate (norm present; Jacobi / none only).  vec_dir 0
+// walks k_update up and k_pupdate down, 1 the reverse.
+struct IterFns {
+  const void* pupdate;
+  const void* update;
+};
+template <int PREC>
+IterFns iter_fns(int xdef, int dir) {
+  if (PREC == kPrecIcc) xdef = 0;
+  if (xdef) {
+    if (dir) return {(const void*)k_pupdate<PREC, 1, 0>, (const void*)k_update<PREC, 1, 1>};
+    return {(const void*)k_pupdate<PREC, 1, 1>, (const void*)k_update<PREC, 1, 0>};
+  }
+  if (dir) return {(const void*)k_pupdate<PREC, 0, 0>, (const void*)k_update<PREC, 0, 1>};
+  return {(const void*)k_pupdate<PREC, 0, 1>, (const void*)k_update<PREC, 0, 0>};
+}
+
+template <int CFG, int PREC, int PAT>
+int build_graph_t(tf_matrix_s* m, int xdef, cudaGraphExec_t* out) {
+  int st = set_attrs_cfg<CFG, PREC, PAT>();
   if (st != TF_OK) return st;
   cudaGraph_t g = nullptr;
   TF_CUDA_TRY(cudaGraphCreate(&g, 0));
@@ -540,8 +709,8 @@ int build_graph_t(tf_matrix_s* m, cudaGraphExec_t* out) {
   va.use_cond = 1;
   SpArgs sa = make_sp_args(m, va);
   const dim3 vb(256), vg(m->vec_grid);
-  const dim3 sb(cfg_threads<CFG>()), sg(m->spmv_grid);
-  const size_t ssm = cfg_smem<CFG>();
+  const dim3 sb(cfg_threads<CFG, PAT>()), sg(m->spmv_grid);
+  const size_t ssm = cfg_smem<CFG, PAT>();
 
   NodeBuilder nb{g};
   void* vargs[] = {&va};
@@ -573,7 +742,7 @@ int build_graph_t(tf_matrix_s* m, cudaGraphExec_t* out) {
     for (size_t l = 0; l < lv.form.size(); ++l)
       n2 = nb.add((const void*)k_icc_form_level, lgrid(lv.form[l].count), dim3(256), 0,
                   &form_args[l], n2);
-  cudaGraphNode_t n3 = nb.add((const void*)k_residual<CFG, PREC>, sg, sb, ssm, sargs, n2);
+  cudaGraphNode_t n3 = nb.add((const void*)k_residual<CFG, PREC, PAT>, sg, sb, ssm, sargs, n2);
   cudaGraphNode_t last = n3;
   if (PREC == kPrecIcc) last = add_icc_apply(nb, last);
   cudaGraphNode_t cnode = nullptr;
@@ -589,9 +758,10 @@ int build_graph_t(tf_matrix_s* m, cudaGraphExec_t* out) {
       nb.status = TF_ERR_CUDA;
     } else {
       NodeBuilder body{cp.conditional.phGraph_out[0]};
-      cudaGraphNode_t b1 = body.add((const void*)k_pupdate<PREC>, vg, vb, 0, vargs, nullptr);
-      cudaGraphNode_t b2 = body.add((const void*)k_spmv_alpha<CFG>, sg, sb, ssm, sargs, b1);
-      cudaGraphNode_t b3 = body.add((const void*)k_update<PREC>, vg, vb, 0, vargs, b2);
+      const IterFns fns = iter_fns<PREC>(xdef, m->vec_dir);
+      cudaGraphNode_t b1 = body.add(fns.pupdate, vg, vb, 0, vargs, nullptr);
+      cudaGraphNode_t b2 = body.add((const void*)k_spmv_alpha<CFG, PAT>, sg, sb, ssm, sargs, b1);
+      cudaGraphNode_t b3 = body.add(fns.update, vg, vb, 0, vargs, b2);
       if (PREC == kPrecIcc) add_icc_apply(body, b3);
       if (body.status != TF_OK) nb.status = body.status;
     }
@@ -608,12 +778,19 @@ int build_graph_t(tf_matrix_s* m, cudaGraphExec_t* out) {
 }
 
 template <int PREC>
-int build_graph_p(tf_matrix_s* m, cudaGraphExec_t* out) {
+int build_graph_p(tf_matrix_s* m, int xdef, cudaGraphExec_t* out) {
+  const bool pat = m->npat > 0;
   switch (m->tile_cfg) {
-    case kTile512: return build_graph_t<kTile512, PREC>(m, out);
-    case kTile256: return build_graph_t<kTile256, PREC>(m, out);
-    case kTile128: return build_graph_t<kTile128, PREC>(m, out);
-    default: return build_graph_t<kTileNone, PREC>(m, out);
+    case kTile512:
+      return pat ? build_graph_t<kTile512, PREC, 1>(m, xdef, out)
+                 : build_graph_t<kTile512, PREC, 0>(m, xdef, out);
+    case kTile256:
+      return pat ? build_graph_t<kTile256, PREC, 1>(m, xdef, out)
+                 : build_graph_t<kTile256, PREC, 0>(m, xdef, out);
+    case kTile128:
+      return pat ? build_graph_t<kTile128, PREC, 1>(m, xdef, out)
+                 : build_graph_t<kTile128, PREC, 0>(m, xdef, out);
+    default: return build_graph_t<kTileNone, PREC, 0>(m, xdef, out);
   }
 }
 
@@ -631,28 +808,35 @@ int occupancy_grid(tf_matrix_s* m, const void* fn, int threads, size_t smem,
   return TF_OK;
 }
 
-template <int CFG>
+template <int CFG, int PAT>
 int prepare_cfg(tf_matrix_s* m) {
-  int st = set_attrs_cfg<CFG, kPrecJacobi>();
+  int st = set_attrs_cfg<CFG, kPrecJacobi, PAT>();
   if (st != TF_OK) return st;
-  st = set_attrs_cfg<CFG, kPrecNone>();
+  st = set_attrs_cfg<CFG, kPrecNone, PAT>();
   if (st != TF_OK) return st;
-  st = set_attrs_cfg<CFG, kPrecIcc>();
+  st = set_attrs_cfg<CFG, kPrecIcc, PAT>();
   if (st != TF_OK) return st;
-  return occupancy_grid<CFG>(m, (const void*)k_spmv_alpha<CFG>, cfg_threads<CFG>(),
-                             cfg_smem<CFG>(), m->ni, &m->spmv_grid);
+  return occupancy_grid<CFG>(m, (const void*)k_spmv_alpha<CFG, PAT>, cfg_threads<CFG, PAT>(),
+                             cfg_smem<CFG, PAT>(), m->ni, &m->spmv_grid);
 }
 
 }  // namespace
 
 int tf_fp64_prepare(tf_matrix_s* m) {
   const int n = std::max(m->nt, 1);
-  m->vec_grid = std::max(1, std::min({(n + 1023) / 1024, m->ctx->sm_count * 4, kMaxBlocks}));
+  int per_sm = 0;
+  TF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, (const void*)k_update<kPrecJacobi, 1, 0>, 256, 0));
+  per_sm = std::max(1, per_sm);
+  m->vec_grid = std::max(1, std::min({(n + 511) / 512, m->ctx->sm_count * per_sm, kMaxBlocks}));
+  if (const char* e = getenv("TF_VEC_DIR")) m->vec_dir = atoi(e) ? 1 : 0;
+  if (m->tile_cfg == kTileNone) m->npat = 0;
+  const bool pat = m->npat > 0;
   switch (m->tile_cfg) {
-    case kTile512: return prepare_cfg<kTile512>(m);
-    case kTile256: return prepare_cfg<kTile256>(m);
-    case kTile128: return prepare_cfg<kTile128>(m);
-    default: return prepare_cfg<kTileNone>(m);
+    case kTile512: return pat ? prepare_cfg<kTile512, 1>(m) : prepare_cfg<kTile512, 0>(m);
+    case kTile256: return pat ? prepare_cfg<kTile256, 1>(m) : prepare_cfg<kTile256, 0>(m);
+    case kTile128: return pat ? prepare_cfg<kTile128, 1>(m) : prepare_cfg<kTile128, 0>(m);
+    default: return prepare_cfg<kTileNone, 0>(m);
   }
 }
 
@@ -660,15 +844,17 @@ namespace {
 // Host-driven loop: the same kernels launched directly, the loop condition
 // read back every kChunk iterations (kernels after convergence return at
 // once).  Used when TF_NO_GRAPH is set.
-template <int CFG, int PREC>
-int run_host_loop_t(tf_matrix_s* m) {
-  int st = set_attrs_cfg<CFG, PREC>();
+template <int CFG, int PREC, int PAT>
+int run_host_loop_t(tf_matrix_s* m, int xdef) {
+  int st = set_attrs_cfg<CFG, PREC, PAT>();
   if (st != TF_OK) return st;
   cudaStream_t s = m->ctx->stream;
   VecArgs va = make_vec_args(m);
   SpArgs sa = make_sp_args(m, va);
   const int vg = m->vec_grid, sg = m->spmv_grid;
-  const size_t ssm = cfg_smem<CFG>();
+  const size_t ssm = cfg_smem<CFG, PAT>();
+  const IterFns fns = iter_fns<PREC>(xdef, m->vec_dir);
+  void* vargs[] = {&va};
   IccLevelArgs lv;
   if (PREC == kPrecIcc) lv = icc_level_args(m);
   auto lgrid = [](int count) { return std::max(1, (count + 255) / 256); };
@@ -681,7 +867,7 @@ int run_host_loop_t(tf_matrix_s* m) {
   k_scale<<<vg, 256, 0, s>>>(va);
   if (PREC == kPrecIcc)
     for (auto& a : lv.form) k_icc_form_level<<<lgrid(a.count), 256, 0, s>>>(a);
-  k_residual<CFG, PREC><<<sg, cfg_threads<CFG>(), ssm, s>>>(sa);
+  k_residual<CFG, PREC, PAT><<<sg, cfg_threads<CFG, PAT>(), ssm, s>>>(sa);
   if (PREC == kPrecIcc) icc_apply();
   TF_CUDA_TRY(cudaGetLastError());
   constexpr int kChunk = 16;
@@ -691,9 +877,9 @@ int run_host_loop_t(tf_matrix_s* m) {
     TF_CUDA_TRY(cudaStreamSynchronize(s));
     if (m->h_state->done) break;
     for (int k = 0; k < kChunk; ++k) {
-      k_pupdate<PREC><<<vg, 256, 0, s>>>(va);
-      k_spmv_alpha<CFG><<<sg, cfg_threads<CFG>(), ssm, s>>>(sa);
-      k_update<PREC><<<vg, 256, 0, s>>>(va);
+      TF_CUDA_TRY(cudaLaunchKernel(fns.pupdate, dim3(vg), dim3(256), vargs, 0, s));
+      k_spmv_alpha<CFG, PAT><<<sg, cfg_threads<CFG, PAT>(), ssm, s>>>(sa);
+      TF_CUDA_TRY(cudaLaunchKernel(fns.update, dim3(vg), dim3(256), vargs, 0, s));
       if (PREC == kPrecIcc) icc_apply();
     }
     TF_CUDA_TRY(cudaGetLastError());
@@ -704,38 +890,49 @@ int run_host_loop_t(tf_matrix_s* m) {
 }
 
 template <int PREC>
-int run_host_loop_p(tf_matrix_s* m) {
+int run_host_loop_p(tf_matrix_s* m, int xdef) {
+  const bool pat = m->npat > 0;
   switch (m->tile_cfg) {
-    case kTile512: return run_host_loop_t<kTile512, PREC>(m);
-    case kTile256: return run_host_loop_t<kTile256, PREC>(m);
-    case kTile128: return run_host_loop_t<kTile128, PREC>(m);
-    default: return run_host_loop_t<kTileNone, PREC>(m);
+    case kTile512:
+      return pat ? run_host_loop_t<kTile512, PREC, 1>(m, xdef)
+                 : run_host_loop_t<kTile512, PREC, 0>(m, xdef);
+    case kTile256:
+      return pat ? run_host_loop_t<kTile256, PREC, 1>(m, xdef)
+                 : run_host_loop_t<kTile256, PREC, 0>(m, xdef);
+    case kTile128:
+      return pat ? run_host_loop_t<kTile128, PREC, 1>(m, xdef)
+                 : run_host_loop_t<kTile128, PREC, 0>(m, xdef);
+    default: return run_host_loop_t<kTileNone, PREC, 0>(m, xdef);
   }
 }
 }  // namespace
 
 int tf_fp64_run(tf_matrix_s* m, int prec) {
   if (prec < 0 || prec > 2) return TF_ERR_ARG;
+  // x += alfa p can wait for the next k_pupdate when the NRMS does not
+  // need the range of x (norm present); ICC keeps it in k_update.
+  const int xdef = (prec != kPrecIcc && m->h_params->has_norm) ? 1 : 0;
   static const bool no_graph = getenv("TF_NO_GRAPH") != nullptr;
   if (no_graph) {
-    if (prec == kPrecJacobi) return run_host_loop_p<kPrecJacobi>(m);
-    if (prec == kPrecNone) return run_host_loop_p<kPrecNone>(m);
-    return run_host_loop_p<kPrecIcc>(m);
+    if (prec == kPrecJacobi) return run_host_loop_p<kPrecJacobi>(m, xdef);
+    if (prec == kPrecNone) return run_host_loop_p<kPrecNone>(m, xdef);
+    return run_host_loop_p<kPrecIcc>(m, 0);
   }
-  if (!m->graph[prec]) {
+  cudaGraphExec_t& g = m->graph[2 * prec + xdef];
+  if (!g) {
     int st;
-    if (prec == kPrecJacobi) st = build_graph_p<kPrecJacobi>(m, &m->graph[prec]);
-    else if (prec == kPrecNone) st = build_graph_p<kPrecNone>(m, &m->graph[prec]);
-    else st = build_graph_p<kPrecIcc>(m, &m->graph[prec]);
+    if (prec == kPrecJacobi) st = build_graph_p<kPrecJacobi>(m, xdef, &g);
+    else if (prec == kPrecNone) st = build_graph_p<kPrecNone>(m, xdef, &g);
+    else st = build_graph_p<kPrecIcc>(m, 0, &g);
     if (st != TF_OK) return st;
   }
-  TF_CUDA_TRY(cudaGraphLaunch(m->graph[prec], m->ctx->stream));
+  TF_CUDA_TRY(cudaGraphLaunch(g, m->ctx->stream));
   return TF_OK;
 }
 
 // ---- building blocks (direct launches, no solve state) --------------------
 namespace {
-template <int CFG>
+template <int CFG, int PAT>
 int launch_spmv(tf_matrix_s* m, const double* val, const double* p, double* q,
                 double* scal) {
   VecArgs va = make_vec_args(m);
@@ -745,11 +942,12 @@ int launch_spmv(tf_matrix_s* m, const double* val, const double* p, double* q,
   SpArgs sa = make_sp_args(m, va);
   sa.val = val;
   sa.out_scalar = scal;
-  k_spmv_alpha<CFG><<<m->spmv_grid, cfg_threads<CFG>(), cfg_smem<CFG>(), m->ctx->stream>>>(sa);
+  k_spmv_alpha<CFG, PAT><<<m->spmv_grid, cfg_threads<CFG, PAT>(), cfg_smem<CFG, PAT>(),
+                          m->ctx->stream>>>(sa);
   TF_CUDA_TRY(cudaGetLastError());
   return TF_OK;
 }
-template <int CFG>
+template <int CFG, int PAT>
 int launch_resid(tf_matrix_s* m, const double* val, const double* b,
                  const double* x, double* r, double* scal) {
   VecArgs va = make_vec_args(m);
@@ -760,7 +958,8 @@ int launch_resid(tf_matrix_s* m, const double* val, const double* b,
   SpArgs sa = make_sp_args(m, va);
   sa.val = val;
   sa.out_scalar = scal;
-  k_residual<CFG, kPrecNone><<<m->spmv_grid, cfg_threads<CFG>(), cfg_smem<CFG>(), m->ctx->stream>>>(sa);
+  k_residual<CFG, kPrecNone, PAT><<<m->spmv_grid, cfg_threads<CFG, PAT>(), cfg_smem<CFG, PAT>(),
+                                   m->ctx->stream>>>(sa);
   TF_CUDA_TRY(cudaGetLastError());
   return TF_OK;
 }
@@ -774,11 +973,21 @@ int tf_fp64_spmv(tf_matrix_s* m, const double* val, const double* p, double* q,
                  double* pq) {
   double* scal = bb_scalar(m);
   int st;
+  const bool pat = m->npat > 0;
   switch (m->tile_cfg) {
-    case kTile512: st = launch_spmv<kTile512>(m, val, p, q, scal); break;
-    case kTile256: st = launch_spmv<kTile256>(m, val, p, q, scal); break;
-    case kTile128: st = launch_spmv<kTile128>(m, val, p, q, scal); break;
-    default: st = launch_spmv<kTileNone>(m, val, p, q, scal); break;
+    case kTile512:
+      st = pat ? launch_spmv<kTile512, 1>(m, val, p, q, scal)
+               : launch_spmv<kTile512, 0>(m, val, p, q, scal);
+      break;
+    case kTile256:
+      st = pat ? launch_spmv<kTile256, 1>(m, val, p, q, scal)
+               : launch_spmv<kTile256, 0>(m, val, p, q, scal);
+      break;
+    case kTile128:
+      st = pat ? launch_spmv<kTile128, 1>(m, val, p, q, scal)
+               : launch_spmv<kTile128, 0>(m, val, p, q, scal);
+      break;
+    default: st = launch_spmv<kTileNone, 0>(m, val, p, q, scal); break;
   }
   if (st == TF_OK && pq)
     TF_CUDA_TRY(cudaMemcpyAsync(pq, scal, sizeof(double), cudaMemcpyDeviceToDevice,
@@ -789,11 +998,18 @@ int tf_fp64_spmv(tf_matrix_s* m, const double* val, const double* p, double* q,
 int tf_fp64_residual(tf_matrix_s* m, const double* val, const double* b,
                      const double* x, double* r) {
   double* scal = bb_scalar(m);
+  const bool pat = m->npat > 0;
   switch (m->tile_cfg) {
-    case kTile512: return launch_resid<kTile512>(m, val, b, x, r, scal);
-    case kTile256: return launch_resid<kTile256>(m, val, b, x, r, scal);
-    case kTile128: return launch_resid<kTile128>(m, val, b, x, r, scal);
-    default: return launch_resid<kTileNone>(m, val, b, x, r, scal);
+    case kTile512:
+      return pat ? launch_resid<kTile512, 1>(m, val, b, x, r, scal)
+                 : launch_resid<kTile512, 0>(m, val, b, x, r, scal);
+    case kTile256:
+      return pat ? launch_resid<kTile256, 1>(m, val, b, x, r, scal)
+                 : launch_resid<kTile256, 0>(m, val, b, x, r, scal);
+    case kTile128:
+      return pat ? launch_resid<kTile128, 1>(m, val, b, x, r, scal)
+                 : launch_resid<kTile128, 0>(m, val, b, x, r, scal);
+    default: return launch_resid<kTileNone, 0>(m, val, b, x, r, scal);
   }
 }
 

@@ -67,10 +67,16 @@ struct tf_matrix_s {
   tf::SolveParams* d_params = nullptr;
   tf::SolveState* h_state = nullptr;    // pinned
   tf::SolveParams* h_params = nullptr;  // pinned
+  // Row-pattern column layout (structured meshes): one pattern byte per
+  // own row and the pattern table; npat = 0 when the rows do not fit it.
+  unsigned char* d_pat = nullptr;
+  int* d_pat_tab = nullptr;
+  int npat = 0;
   // SpMV tiling picked at registration
   int tile_cfg = tf::kTileNone;
   int spmv_grid = 1;
   int vec_grid = 1;
+  int vec_dir = 0;       // walking direction of the vector kernels (see tf_fp64.cu)
   // ICC level schedule (built at registration for diagonal-first matrices)
   int icc_ready = 0;
   int* d_levf_rows = nullptr;  // forward-sweep rows grouped by level
@@ -78,8 +84,8 @@ struct tf_matrix_s {
   std::vector<int> h_levf_ptr, h_levb_ptr;
   double* d_icc_d = nullptr;     // Prec_Form's d
   double* d_icc_dinv = nullptr;  // Prec_Form's d_inv
-  // cached graphs, one per preconditioner
-  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  // cached graphs, one per (preconditioner, x update deferred or not)
+  cudaGraphExec_t graph[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   std::mutex mu;
   int async_alloc = 0;   // device arrays from cudaMallocAsync on ctx->stream
   int host_lent = 0;     // h_state / h_params belong to the context

@@ -381,6 +381,164 @@ __device__ bool stream_items(W& w) {
   return ok;
 }
 
+// ---------------------------------------------------------------------------
+// Row-pattern variant.  On structured parts of a mesh most rows have the
+// same column offsets relative to their own index (a hex cell's diagonal
+// then its six neighbours at -nx*ny, -nx, -1, +1, +nx, +nx*ny), so the
+// column array can be replaced by one byte per row naming the row's offset
+// pattern, col_j = i + off[pattern(i)][j - row_i].  The values, the order
+// of the entries and hence every row sum are those of the CSR arrays; only
+// the column bytes (4 per entry) shrink to 1 per row.  A tile stage holds
+// the values, the row pointers and the pattern bytes; the pattern table
+// (at most kPatMax patterns of at most kPatMaxLen entries) sits in shared
+// memory for the whole kernel.
+// ---------------------------------------------------------------------------
+constexpr int kPatMax = 64;
+constexpr int kPatMaxLen = 16;
+// Stages of the row-pattern ring.  Two: a third (2 x 109 KB of shared
+// memory per SM) measured slower, the smaller L1 left for the x-gather
+// costing more than the deeper copy pipeline gains.
+constexpr int kPatStages = 2;
+
+template <int ROWS, int NNZCAP, int STAGES>
+struct PatLayout {
+  static constexpr size_t kValBytes = (((NNZCAP + 4) * 8 + 127) / 128) * 128;
+  static constexpr size_t kRowBytes = (((ROWS + 8) * 4 + 127) / 128) * 128;
+  static constexpr size_t kPatBytes = ((ROWS + 32 + 127) / 128) * 128;
+  static constexpr size_t kStageBytes = kValBytes + kRowBytes + kPatBytes;
+  static constexpr size_t kTabOffset = STAGES * kStageBytes;
+  static constexpr size_t kTabBytes = (size_t)kPatMax * (kPatMaxLen + 1) * 4;
+  static constexpr size_t kBarOffset = kTabOffset + kTabBytes;      // full[S], empty[S]
+  static constexpr size_t kMetaOffset = kBarOffset + 16 * STAGES;
+  static constexpr size_t kSmemBytes = kMetaOffset + 32 * STAGES + 16;
+};
+
+// Pattern table in global memory: npat rows of kPatMaxLen offsets, then
+// npat lengths.
+struct PatTable {
+  const unsigned char* pat;  // one byte per row
+  const int* tab;            // [npat][kPatMaxLen] offsets, then [npat] lengths
+  int npat;
+};
+
+// Threads of a row-pattern CTA: ROWS consumer threads (one row each) and
+// one producer warp.
+template <int ROWS>
+constexpr int pat_threads() { return ROWS + 32; }
+
+// Warp-specialised streamer over row-pattern tiles.  The last warp is the
+// producer: lane 0 issues the bulk copies of tile k into stage k % STAGES
+// once every consumer warp has released that stage (empty[s], one arrival
+// per consumer warp) and arms full[s] with the byte count.  Consumer warps
+// wait on full[s], run op.pat(i, vals, offs, len) for their rows (thread t
+// of the CTA takes row r0 + t; offs are the row pattern's offsets in
+// shared memory, col = i + offs[k]) and release the stage -- no CTA-wide
+// barrier per tile, so a warp whose rows are done moves on to the next
+// staged tile while slower warps finish theirs.
+//
+// Every wait is bounded.  A consumer that times out raises a shared abort
+// flag; the others stop at their next tile, the producer stops issuing, and
+// before returning the producer waits (bounded) for the copies of every
+// stage it armed.  Returns false on a timeout (the caller records it).
+template <int ROWS, int NNZCAP, int STAGES, class Op>
+__device__ bool stream_tiles_pat(const int* __restrict__ row, const PatTable& pt,
+                                 const double* __restrict__ val, int nrows, Op& op) {
+  using L = PatLayout<ROWS, NNZCAP, STAGES>;
+  constexpr int kConsumerWarps = ROWS / 32;
+  extern __shared__ __align__(128) unsigned char tf_smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(tf_smem + L::kBarOffset);
+  uint64_t* empty = full + STAGES;
+  int* meta = reinterpret_cast<int*>(tf_smem + L::kMetaOffset);
+  volatile int* abort_flag = meta + 8 * STAGES;
+  int* tab = reinterpret_cast<int*>(tf_smem + L::kTabOffset);
+  auto sval = [&](int s) { return reinterpret_cast<double*>(tf_smem + s * L::kStageBytes); };
+  auto srow = [&](int s) {
+    return reinterpret_cast<int*>(tf_smem + s * L::kStageBytes + L::kValBytes);
+  };
+  auto spat = [&](int s) {
+    return tf_smem + s * L::kStageBytes + L::kValBytes + L::kRowBytes;
+  };
+
+  const int ntiles = (nrows + ROWS - 1) / ROWS;
+  if ((int)blockIdx.x >= ntiles) return true;
+  const int ntab = pt.npat * (kPatMaxLen + 1);
+  for (int k = threadIdx.x; k < ntab; k += blockDim.x) tab[k] = __ldg(pt.tab + k);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    *abort_flag = 0;
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int* tab_len = tab + pt.npat * kPatMaxLen;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  bool ok = true;
+
+  if (warp == kConsumerWarps) {
+    // ---- producer warp ----
+    if (lane == 0) {
+      int issued = 0;
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++issued) {
+        const int s = issued % STAGES;
+        if (issued >= STAGES) {
+          if (!mbar_wait_bounded(&empty[s], (unsigned)(issued / STAGES - 1) & 1u)) {
+            ok = false;
+            *abort_flag = 1;
+            break;
+          }
+          fence_proxy_async_smem();   // consumers' reads before the async overwrite
+        }
+        if (*abort_flag) break;
+        const int r0 = tile * ROWS;
+        const int r1 = min(r0 + ROWS, nrows);
+        const int j0 = __ldg(row + r0), j1 = __ldg(row + r1);
+        const int a0 = j0 & ~1, a1 = (j1 + 1) & ~1;
+        const int p0 = r0 & ~3, p1 = (r1 + 1 + 3) & ~3;
+        const int b0 = r0 & ~15, b1 = (r1 + 15) & ~15;
+        int* m = meta + 8 * s;
+        m[0] = a0; m[1] = b0; m[2] = p0; m[3] = r0; m[4] = r1;
+        const unsigned bv = (unsigned)(a1 - a0) * 8u;
+        const unsigned br = (unsigned)(p1 - p0) * 4u;
+        const unsigned bp = (unsigned)(b1 - b0);
+        mbar_arrive_expect_tx(&full[s], bv + br + bp);
+        if (bv) bulk_g2s(sval(s), val + a0, bv, &full[s]);
+        bulk_g2s(srow(s), row + p0, br, &full[s]);
+        bulk_g2s(spat(s), pt.pat + b0, bp, &full[s]);
+      }
+      // Drain: the copies of the last armed phase of every stage.
+      for (int k = (issued > STAGES ? issued - STAGES : 0); k < issued; ++k)
+        mbar_wait_bounded(&full[k % STAGES], (unsigned)(k / STAGES) & 1u);
+    }
+  } else {
+    // ---- consumer warps ----
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+      const int s = it % STAGES;
+      if (!mbar_wait_bounded(&full[s], (unsigned)(it / STAGES) & 1u)) {
+        ok = false;
+        *abort_flag = 1;
+        break;
+      }
+      const int* m = meta + 8 * s;
+      const int a0 = m[0], b0 = m[1], p0 = m[2], r0 = m[3], r1 = m[4];
+      const int r = r0 + (int)threadIdx.x;
+      if (r < r1) {
+        const int js = srow(s)[r - p0];
+        const int pid = spat(s)[r - b0];
+        op.pat(r, sval(s) + (js - a0), tab + pid * kPatMaxLen, tab_len[pid]);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+      if (*abort_flag) { ok = false; break; }
+    }
+  }
+  __syncthreads();
+  return !__syncthreads_or(!ok);
+}
+
 // Tile configurations the host may pick (rows per tile = threads per CTA).
 enum TileCfgId { kTile512 = 0, kTile256 = 1, kTile128 = 2, kTileNone = 3 };
 constexpr int kTileRows[3] = {512, 256, 128};

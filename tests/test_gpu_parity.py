@@ -47,6 +47,27 @@ def oracle_solve(row, col, dia, val, b, x0, solver, prec, miter, tol, norm, thre
     return x, v, bb, r["niter"], r["fin_res"]
 
 
+def check_fin_res(row, col, dia, val, b, g, norm):
+    """The reported fin_res is the NRMS (Normalized_Root_Mean_Square.f90) of
+    the returned x: checks the device reductions (sum of r^2/a^2 and, with
+    norm absent, the range of x) independently of the iteration history.
+    The solver's r is the recursively updated residual, which drifts from
+    b - A x by rounding (0.2 % after ten orders of magnitude of reduction
+    on a 30^3 Poisson system), hence the loose bound; a wrong reduction is
+    off by factors."""
+    x, res = g[0], g[4]
+    r = O.residual(row, col, dia, val, b, x)
+    want = O.nrms(row, col, dia, val, r, x, norm=norm)
+    assert res == pytest.approx(want, rel=2e-2, abs=1e-14), (res, want)
+
+
+def iters_near_tol(hist, k, tol, factor=1.25):
+    """True when the oracle's residual after iteration k lies within `factor`
+    of tol: the stopping decision there is within reach of a different
+    summation order of the dot products."""
+    return k < len(hist) and tol / factor <= hist[k] <= tol * factor
+
+
 def check_parity(g, o, tol, exact_iters=False):
     x, v, b, it, res = g
     ox, ov, ob, oit, ores = o
@@ -73,7 +94,17 @@ def test_golden_fixture_parity(gpu_ctx, case):
         assert g[3] == case["niter"] == case["miter"]
         assert g[4] == pytest.approx(case["fin_res"], rel=1e-3)
         return
-    check_parity(g, o, case["tol"], exact_iters=True)
+    check_fin_res(case["row"], case["col"], case["dia"], case["val"], case["b"], g,
+                  case["norm"])
+    # Exact iteration counts, except where the oracle's own residual at the
+    # deciding iteration is within 25 % of tol (one such fixture: the
+    # unpreconditioned, norm-absent Poisson case, whose residual after 42
+    # iterations moves by ~20 % with the summation order of its dots).
+    k = min(g[3], case["niter"])
+    exact = not iters_near_tol(case["hist"], k, case["tol"])
+    if not exact:
+        assert abs(g[3] - case["niter"]) <= 1, (g[3], case["niter"])
+    check_parity(g, o, case["tol"], exact_iters=exact)
 
 
 def _dev_arrays(torch, *arrs):
@@ -82,8 +113,14 @@ def _dev_arrays(torch, *arrs):
 
 @pytest.mark.parametrize("kind,n,ratio", [("hex", 13, 1.0), ("hex", 40, 1.02),
                                           ("poly", 3000, None)])
-def test_spmv_and_residual_bitwise(gpu_ctx, kind, n, ratio):
+@pytest.mark.parametrize("patterns", [True, False])
+def test_spmv_and_residual_bitwise(gpu_ctx, kind, n, ratio, patterns, monkeypatch):
+    """Both column layouts (row patterns, CSR columns) give the oracle's q and
+    r bit for bit; hex matrices take the row-pattern layout, a random
+    polyhedral mesh (more than 64 distinct rows) keeps the CSR columns."""
     torch = torch_dev()
+    if not patterns:
+        monkeypatch.setenv("TF_NO_ROW_PATTERNS", "1")
     if kind == "hex":
         s = systems.small_hex(n, seed=3, kind="momentum", ratio=ratio)
     else:
@@ -93,6 +130,10 @@ def test_spmv_and_residual_bitwise(gpu_ctx, kind, n, ratio):
     xx = rng.standard_normal(s.n)
     m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia)
     try:
+        if patterns and kind == "hex":
+            assert 1 <= m.row_patterns <= 27   # interior, faces, edges, corners
+        else:
+            assert m.row_patterns == 0
         dval, dp, dq, db, dx, dr = _dev_arrays(torch, s.val, p, np.zeros(s.n), s.b, xx,
                                                np.zeros(s.n))
         dpq = torch.zeros(1, dtype=torch.float64, device="cuda")
@@ -111,14 +152,19 @@ def test_spmv_and_residual_bitwise(gpu_ctx, kind, n, ratio):
 
 
 @pytest.mark.parametrize("cfg", [0, 1, 2, 3])
-def test_every_tile_configuration(gpu_ctx, cfg, monkeypatch):
-    """Tile widths 512/256/128 and the direct-from-global path agree."""
+@pytest.mark.parametrize("patterns", [True, False])
+def test_every_tile_configuration(gpu_ctx, cfg, patterns, monkeypatch):
+    """Tile widths 512/256/128 (row-pattern or CSR columns) and the
+    direct-from-global path agree."""
     torch = torch_dev()
     monkeypatch.setenv("TF_TILE_CFG", str(cfg))
+    if not patterns:
+        monkeypatch.setenv("TF_NO_ROW_PATTERNS", "1")
     s = systems.small_hex(17, seed=5, kind="pressure", ratio=1.05)
     m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia)
     try:
         assert m.tile_config == cfg
+        assert (m.row_patterns > 0) == (patterns and cfg != 3)
         p = np.random.default_rng(1).standard_normal(s.n)
         dval, dp, dq = _dev_arrays(torch, s.val, p, np.zeros(s.n))
         torch.cuda.synchronize()
@@ -128,6 +174,20 @@ def test_every_tile_configuration(gpu_ctx, cfg, monkeypatch):
                                                         s.val, p))
     finally:
         m.close()
+
+
+@pytest.mark.parametrize("prec,norm", [("jacobi", 1.0), ("jacobi", None), ("icc", 1.0)])
+def test_row_patterns_do_not_change_the_solve(gpu_ctx, prec, norm, monkeypatch):
+    """The row-pattern layout feeds the same operands in the same order to
+    every row sum, so a whole solve is bit-identical with the CSR columns."""
+    s = systems.small_hex(23, seed=9, kind="pressure", ratio=1.04)
+    args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, "cg", prec, 3000, 1e-10, norm)
+    g1 = gpu_solve(gpu_ctx, *args)
+    monkeypatch.setenv("TF_NO_ROW_PATTERNS", "1")
+    g2 = gpu_solve(gpu_ctx, *args)
+    assert g1[3] == g2[3] and g1[4] == g2[4]
+    for u, w in zip(g1[:3], g2[:3]):
+        assert np.array_equal(u, w)
 
 
 def test_long_rows_fall_back_to_global_path(gpu_ctx):
@@ -158,11 +218,36 @@ def test_long_rows_fall_back_to_global_path(gpu_ctx):
 @pytest.mark.parametrize("solver", ["cg", "bicg"])
 @pytest.mark.parametrize("prec", ["jacobi", "none"])
 @pytest.mark.parametrize("norm", [None, 1.0])
-def test_solve_variants_small(gpu_ctx, solver, prec, norm):
-    s = systems.small_hex(12, seed=6, kind="pressure", ratio=1.03)
+@pytest.mark.parametrize("m", [11, 12])   # odd and even cell counts
+def test_solve_variants_small(gpu_ctx, solver, prec, norm, m):
+    s = systems.small_hex(m, seed=6, kind="pressure", ratio=1.03)
     x0 = np.random.default_rng(4).uniform(-0.5, 0.5, s.n)
     args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, x0, solver, prec, 2000, 1e-10, norm)
     check_parity(gpu_solve(gpu_ctx, *args), oracle_solve(*args), 1e-10)
+
+
+@pytest.mark.parametrize("prec", ["jacobi", "none"])
+@pytest.mark.parametrize("norm", [None, 1.0])
+@pytest.mark.parametrize("kind,m", [("hex", 11), ("hex", 64), ("poly", 3001)])
+@pytest.mark.parametrize("miter", [1, 2, 7])
+def test_fin_res_is_nrms_of_returned_x(gpu_ctx, prec, norm, kind, m, miter):
+    """After a few iterations (no drift between the updated and the true
+    residual yet) fin_res equals NRMS(b - A x) of the returned x to rounding:
+    checks the device reductions and that x holds every update, including
+    the last one when the x update is deferred."""
+    if kind == "hex":
+        s = systems.small_hex(m, seed=6, kind="pressure", ratio=1.03)
+    else:
+        s = systems.poly_system(m, seed=2, kind="pressure", tol=1e-10, miter=10, norm=1.0)
+    x0 = np.random.default_rng(5).uniform(-0.5, 0.5, s.n)
+    args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, x0, "cg", prec, miter, 1e-300, norm)
+    g = gpu_solve(gpu_ctx, *args)
+    assert g[3] == miter
+    r = O.residual(s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, g[0])
+    want = O.nrms(s.csr.row, s.csr.col, s.csr.dia, s.val, r, g[0], norm=norm)
+    assert g[4] == pytest.approx(want, rel=1e-9), (g[4], want)
+    o = oracle_solve(*args)
+    assert rel_l2(g[0], o[0]) <= 1e-12 and g[4] == pytest.approx(o[4], rel=1e-11)
 
 
 def test_bicg_equals_cg_on_gpu(gpu_ctx):
