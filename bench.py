@@ -61,9 +61,18 @@ def parse():
     ap.add_argument("--count", type=int, default=512)
     ap.add_argument("--rate", type=float, default=200.0, help="served: arrivals per second")
     ap.add_argument("--seconds", type=float, default=60.0, help="served: window length")
-    ap.add_argument("--mode", default="solve", choices=["solve", "spmv", "batched", "served"],
+    ap.add_argument("--iters", type=int, default=30, help="iters: Cg iterations per solve")
+    ap.add_argument("--mesh", default="hex", choices=["hex", "poly-lattice", "poly-delaunay"],
+                    help="spmv: hex (--size^3 cells) or a polyhedral mesh of --cells cells")
+    ap.add_argument("--cells", type=int, default=2000000)
+    ap.add_argument("--rcm", action="store_true",
+                    help="spmv: renumber the cells by reverse Cuthill-McKee first")
+    ap.add_argument("--mode", default="solve",
+                    choices=["solve", "spmv", "iters", "batched", "served"],
                     help="spmv: only the pressure matrix and `--steps` SpMV launches "
-                         "(the small case profiled with ncu)")
+                         "(the small case profiled with ncu); iters: `--steps` Cg solves "
+                         "of exactly `--iters` iterations on the pressure matrix (launch "
+                         "lists: run with TF_NO_GRAPH=1)")
     return ap.parse_args()
 
 
@@ -365,9 +374,16 @@ def run_spmv_only(args):
     """Register the pressure matrix and launch the tiled SpMV --steps times."""
     import torch
     from tflows_b200 import native, systems
-    from tflows_b200.grids import hex_grid
-    g = hex_grid(args.size, args.size, args.size, stretch_y=1.02)
+    from tflows_b200.grids import hex_grid, poly_dual_grid, poly_lattice_grid
+    if args.mesh == "hex":
+        g = hex_grid(args.size, args.size, args.size, stretch_y=1.02)
+    elif args.mesh == "poly-lattice":
+        g = poly_lattice_grid(args.cells, 3)
+    else:
+        g = poly_dual_grid(args.cells, 3)
     s = systems.pressure_system(g, 2, tol=1e-10, miter=1, singular="pin", norm=1.0)
+    if args.rcm:
+        s = systems.renumber_rcm(s)
     ctx = native.Context(0)
     m = native.Matrix(ctx, s.csr.row, s.csr.col, s.csr.dia)
     val = torch.from_numpy(s.val).cuda()
@@ -384,10 +400,50 @@ def run_spmv_only(args):
     e1.synchronize()
     t = e0.elapsed_time(e1) / 1e3 / max(args.steps, 1)
     by = SPMV_BYTES(s.n, s.nnz, m.row_patterns > 0)
-    print(json.dumps({"mode": "spmv", "n": s.n, "nnz": s.nnz, "tile_cfg": m.tile_config,
+    print(json.dumps({"mode": "spmv", "mesh": args.mesh, "n": s.n, "nnz": s.nnz,
+                      "tile_cfg": m.tile_config,
                       "row_patterns": m.row_patterns, "launch_ms": t * 1e3,
                       "bytes_per_launch": by, "csr_bytes_per_launch": SPMV_BYTES(s.n, s.nnz),
                       "achieved_gbs": by / t / 1e9}), flush=True)
+    m.close()
+    ctx.close()
+
+
+def run_fixed_iterations(args):
+    """`--steps` Cg + Jacobi solves of exactly `--iters` iterations (tol 0)
+    on the bench's pressure matrix: per-iteration time with CUDA events."""
+    import torch
+    from tflows_b200 import native, systems
+    from tflows_b200.grids import poly_dual_grid, poly_lattice_grid
+    if args.mesh == "hex":
+        p = make_workload(args.size, args.peclet)[0]
+    else:
+        g = (poly_lattice_grid(args.cells, 3) if args.mesh == "poly-lattice"
+             else poly_dual_grid(args.cells, 3))
+        p = systems.pressure_system(g, 2, tol=1e-10, miter=1, singular="pin", norm=1.0)
+    ctx = native.Context(0)
+    m = native.Matrix(ctx, p.csr.row, p.csr.col, p.csr.dia)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    val0, b0 = torch.from_numpy(p.val).cuda(), torch.from_numpy(p.b).cuda()
+    val, b = val0.clone(), b0.clone()
+    x = torch.zeros(p.n, dtype=torch.float64, device="cuda")
+    out = []
+    for _ in range(args.steps):
+        val.copy_(val0)
+        b.copy_(b0)
+        x.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        it, _ = native.solve_device(ctx, m, "cg", "jacobi", val.data_ptr(), x.data_ptr(),
+                                    b.data_ptr(), args.iters, 0.0, 1.0)
+        e1.record(stream)
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1) / it * 1e3)
+    print(json.dumps({"mode": "iters", "mesh": args.mesh, "n": p.n, "nnz": p.nnz,
+                      "iters": args.iters, "row_patterns": m.row_patterns,
+                      "renumbered": m.renumbered, "us_per_iteration": out,
+                      "mcell_iters_per_s": p.n / min(out)}), flush=True)
     m.close()
     ctx.close()
 
@@ -560,6 +616,9 @@ def main():
         return
     if args.mode == "spmv":
         run_spmv_only(args)
+        return
+    if args.mode == "iters":
+        run_fixed_iterations(args)
         return
     if args.mode == "batched":
         run_batched(args)

@@ -88,6 +88,13 @@ int tf_matrix_tile_config(tf_matrix m);
  * same entries, same order, same sums), 0 when the CSR columns are used.
  * No reference counterpart: a property of this library's device layout. */
 int tf_matrix_row_patterns(tf_matrix m);
+/* 1 when registration also built a renumbered copy of the matrix (reverse
+ * Cuthill-McKee, applied symmetrically) because the given cell numbering
+ * scatters the SpMV's gathers; Jacobi / none solves then run on that copy
+ * (inputs permuted in and results back on the device; every row keeps its
+ * entries in storage order, so row sums are unchanged).  0 otherwise.
+ * No reference counterpart: a property of this library's device layout. */
+int tf_matrix_renumbered(tf_matrix m);
 
 /* Solve A x = b.  Replaces Native_Type % Solve_Native (Solve_Native.f90:2-46)
  * and so Cg.f90:2-257 / Bicg.f90:2-269.  val, x and b are host arrays of

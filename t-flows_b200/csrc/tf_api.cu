@@ -161,12 +161,13 @@ int tf_dev_alloc_bytes(tf_ctx_s* ctx, void** p, size_t bytes) {
 void tf_matrix_free(tf_matrix_s* m) {
   if (!m) return;
   cudaSetDevice(m->ctx->device);
+  tf_matrix_free(m->ren);
   for (auto& g : m->graph)
     if (g) cudaGraphExecDestroy(g);
   void* ptrs[] = {m->d_row, m->d_col, m->d_dia, m->d_val, m->d_x, m->d_b,
                   m->d_r, m->d_p, m->d_q, m->d_z, m->d_adiag, m->d_part,
                   m->d_hist, m->d_state, m->d_params, m->d_levf_rows, m->d_levb_rows,
-                  m->d_icc_d, m->d_icc_dinv, m->d_pat, m->d_pat_tab};
+                  m->d_icc_d, m->d_icc_dinv, m->d_pat, m->d_pat_tab, m->d_perm, m->d_src};
   for (void* p : ptrs)
     if (p) {
       if (m->async_alloc) cudaFreeAsync(p, m->ctx->stream);
@@ -177,6 +178,14 @@ void tf_matrix_free(tf_matrix_s* m) {
     if (m->h_params) cudaFreeHost(m->h_params);
   }
   delete m;
+}
+
+size_t tf_matrix_bytes_for(int n_cells, int64_t nnz, const int* row, const int* col) {
+  size_t b = tf_matrix_bytes(n_cells, nnz);
+  if (n_cells >= kRenumberMinRows && row && col && !getenv("TF_NO_RENUMBER") &&
+      tf_gather_lines_per_warp(row, col, n_cells, 1) > kRenumberLines)
+    b += tf_matrix_bytes(n_cells, nnz) + 4 * ((size_t)n_cells + (size_t)nnz) + 1024;
+  return b;
 }
 
 size_t tf_matrix_bytes(int n_cells, int64_t nnz) {
@@ -253,8 +262,73 @@ extern "C" int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own,
   return tf_matrix_create(ctx, n_cells, n_own, nnz, row, col, dia, 1, out);
 }
 
+namespace {
+int matrix_create_impl(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const int* row,
+                       const int* col, const int* dia, int want_icc, int allow_renumber,
+                       tf_matrix_s** out);
+
+// Renumbered copy of m for the Jacobi / none solves, when the gathers of the
+// given numbering are scattered and reverse Cuthill-McKee gathers better.
+int attach_renumbered(tf_matrix_s* m, const std::vector<int>& row0,
+                      const std::vector<int>& col0, const std::vector<int>& dia0) {
+  const int n = m->nt;
+  if (n < kRenumberMinRows || m->ni != n || getenv("TF_NO_RENUMBER")) return TF_OK;
+  const double before = tf_gather_lines_per_warp(row0.data(), col0.data(), n, 0);
+  if (before <= kRenumberLines) return TF_OK;
+  std::vector<int> order;
+  tf_rcm_order(row0, col0, n, order);
+  std::vector<int> inv(n);
+  for (int i = 0; i < n; ++i) inv[order[i]] = i;
+  const int64_t nnz = m->nnz;
+  std::vector<int> row_r((size_t)n + 1), col_r((size_t)nnz), dia_r(n), src((size_t)nnz),
+      row_r0((size_t)n + 1), col_r0((size_t)nnz);
+  row_r[0] = 1;
+  for (int i = 0; i < n; ++i) {
+    const int o = order[i], js = row0[o], len = row0[o + 1] - js;
+    const int base = row_r[i] - 1;
+    for (int k = 0; k < len; ++k) {
+      src[base + k] = js + k;
+      col_r0[base + k] = inv[col0[js + k]];
+      col_r[base + k] = col_r0[base + k] + 1;
+    }
+    row_r[i + 1] = row_r[i] + len;
+    dia_r[i] = row_r[i] + (dia0[o] - js);
+  }
+  for (int i = 0; i <= n; ++i) row_r0[i] = row_r[i] - 1;
+  const double after = tf_gather_lines_per_warp(row_r0.data(), col_r0.data(), n, 0);
+  if (after > 0.8 * before) return TF_OK;
+  tf_matrix_s* r = nullptr;
+  int st = matrix_create_impl(m->ctx, n, n, nnz, row_r.data(), col_r.data(), dia_r.data(), 0,
+                              0, &r);
+  if (st != TF_OK) return st;
+  m->ren = r;
+  st = tf_dev_alloc_bytes(m->ctx, (void**)&m->d_perm, (size_t)n * sizeof(int));
+  if (st == TF_OK) st = tf_dev_alloc_bytes(m->ctx, (void**)&m->d_src, (size_t)nnz * sizeof(int));
+  if (st != TF_OK) return st;
+  cudaError_t e = cudaMemcpyAsync(m->d_perm, order.data(), (size_t)n * sizeof(int),
+                                  cudaMemcpyHostToDevice, m->ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m->d_src, src.data(), (size_t)nnz * sizeof(int),
+                        cudaMemcpyHostToDevice, m->ctx->stream);
+  if (e == cudaSuccess && !m->ctx->async_alloc) e = cudaStreamSynchronize(m->ctx->stream);
+  if (e != cudaSuccess) {
+    tf_set_last_cuda_error(e, "cudaMemcpy(renumbering)", __FILE__, __LINE__);
+    return TF_ERR_CUDA;
+  }
+  m->dev_bytes += r->dev_bytes + 4 * ((size_t)n + (size_t)nnz);
+  return TF_OK;
+}
+}  // namespace
+
 int tf_matrix_create(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const int* row,
                      const int* col, const int* dia, int want_icc, tf_matrix_s** out) {
+  return matrix_create_impl(ctx, n_cells, n_own, nnz, row, col, dia, want_icc, 1, out);
+}
+
+namespace {
+int matrix_create_impl(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const int* row,
+                       const int* col, const int* dia, int want_icc, int allow_renumber,
+                       tf_matrix_s** out) {
   if (!ctx || !out) return TF_ERR_ARG;
   *out = nullptr;
   if (n_cells < 0 || n_own < 0 || n_own > n_cells || nnz < 0) return TF_ERR_ARG;
@@ -385,6 +459,7 @@ int tf_matrix_create(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const i
   }
   if (st == TF_OK && n_cells > 0 && diag_first && want_icc)
     st = tf_icc_build(m, row0.data(), col0.data());
+  if (st == TF_OK && allow_renumber) st = attach_renumbered(m, row0, col0, dia0);
   if (st != TF_OK) {
     tf_matrix_free(m);
     return st;
@@ -392,6 +467,7 @@ int tf_matrix_create(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const i
   *out = m;
   return TF_OK;
 }
+}  // namespace
 
 extern "C" int tf_matrix_release(tf_matrix m) {
   if (!m) return TF_ERR_ARG;
@@ -403,6 +479,10 @@ extern "C" int tf_matrix_release(tf_matrix m) {
 
 extern "C" int tf_matrix_row_patterns(tf_matrix m) {
   return m ? m->npat : TF_ERR_ARG;
+}
+
+extern "C" int tf_matrix_renumbered(tf_matrix m) {
+  return m ? (m->ren != nullptr) : TF_ERR_ARG;
 }
 
 extern "C" int tf_matrix_info(tf_matrix m, int* n_cells, int* n_own,
@@ -435,7 +515,10 @@ int ensure_hist(tf_matrix_s* m, int need) {
 int run_solve_core(tf_matrix_s* m, int prec, int miter, double tol,
                    const double* norm) {
   tf_ctx_s* c = m->ctx;
-  tf::SolveParams* hp = m->h_params;
+  // Jacobi / none run on the renumbered copy when there is one.
+  tf_matrix_s* a = (m->ren && prec != tf::kPrecIcc) ? m->ren : m;
+  m->active = a;
+  tf::SolveParams* hp = a->h_params;
   hp->tol = tol;
   hp->norm = norm ? *norm : 0.0;
   hp->has_norm = norm ? 1 : 0;
@@ -443,16 +526,19 @@ int run_solve_core(tf_matrix_s* m, int prec, int miter, double tol,
   hp->hist = nullptr;
   hp->hist_cap = 0;
   if (c->history && miter >= 0) {
-    int st = ensure_hist(m, miter + 1);
+    int st = ensure_hist(a, miter + 1);
     if (st != TF_OK) return st;
-    hp->hist = m->d_hist;
+    hp->hist = a->d_hist;
     hp->hist_cap = miter + 1;
   }
-  TF_CUDA_TRY(cudaMemcpyAsync(m->d_params, hp, sizeof(*hp), cudaMemcpyHostToDevice, c->stream));
+  TF_CUDA_TRY(cudaMemcpyAsync(a->d_params, hp, sizeof(*hp), cudaMemcpyHostToDevice, c->stream));
   if (prec == tf::kPrecIcc && !m->icc_ready) return TF_ERR_LAYOUT;  // needs diagonal first
-  int st = tf_fp64_run(m, prec);
+  int st = TF_OK;
+  if (a != m) st = tf_renumber_in(m);
+  if (st == TF_OK) st = tf_fp64_run(a, prec);
+  if (st == TF_OK && a != m) st = tf_renumber_out(m);
   if (st != TF_OK) return st;
-  TF_CUDA_TRY(cudaMemcpyAsync(m->h_state, m->d_state, sizeof(tf::SolveState),
+  TF_CUDA_TRY(cudaMemcpyAsync(m->h_state, a->d_state, sizeof(tf::SolveState),
                               cudaMemcpyDeviceToHost, c->stream));
   return TF_OK;
 }
@@ -465,12 +551,13 @@ int finish_solve(tf_matrix_s* m, int* niter, double* fin_res) {
   *niter = s.niter;
   *fin_res = s.res;
   c->last_count = 0;
-  if (c->history && m->hist_cap > 0) {
-    const bool early_b = s.bnrm2 < m->h_params->tol;
-    const int cnt = early_b ? 0 : std::min(s.niter + 1, m->hist_cap);
+  const tf_matrix_s* a = m->active ? m->active : m;
+  if (c->history && a->hist_cap > 0) {
+    const bool early_b = s.bnrm2 < a->h_params->tol;
+    const int cnt = early_b ? 0 : std::min(s.niter + 1, a->hist_cap);
     c->last_hist.resize(std::max(cnt, 1));
     if (cnt > 0)
-      TF_CUDA_TRY(cudaMemcpy(c->last_hist.data(), m->d_hist, cnt * sizeof(double),
+      TF_CUDA_TRY(cudaMemcpy(c->last_hist.data(), a->d_hist, cnt * sizeof(double),
                              cudaMemcpyDeviceToHost));
     c->last_count = cnt;
   }

@@ -41,6 +41,7 @@
 #include "tf_icc.cuh"
 #include "tf_internal.h"
 #include "tf_tile.cuh"
+#include "tf_tile2.cuh"
 
 namespace tf {
 
@@ -206,6 +207,18 @@ struct OpSpmvDot {
   __device__ __forceinline__ void pat(int i, const double* v, const int* o, int len) {
     body(i, v, [i, o](int k) { return i + o[k]; }, len);
   }
+  // two-phase streamer
+  __device__ __forceinline__ void begin(int) {}
+  __device__ __forceinline__ double gather(int c) const { return __ldg(p + c); }
+  __device__ __forceinline__ double row_init(int) const { return 0.0; }
+  __device__ __forceinline__ double combine(double acc, double prod) const {
+    return __dadd_rn(acc, prod);
+  }
+  __device__ __forceinline__ void row_done(int i, double acc) {
+    q[i] = acc;
+    pq = __dadd_rn(pq, __dmul_rn(__ldg(p + i), acc));
+  }
+  __device__ __forceinline__ void tile_end(int) {}
 };
 
 // r_i = b_i - sum_j a_ij x_j (Residual_Vector.f90:35-41), accumulates the
@@ -249,6 +262,47 @@ struct OpResidual {
   __device__ __forceinline__ void pat(int i, const double* v, const int* o, int len) {
     body(i, v, [i, o](int k) { return i + o[k]; }, len);
   }
+  // two-phase streamer
+  __device__ __forceinline__ void begin(int) {}
+  __device__ __forceinline__ double gather(int c) const { return __ldg(x + c); }
+  __device__ __forceinline__ double row_init(int i) const { return b[i]; }
+  __device__ __forceinline__ double combine(double acc, double prod) const {
+    return __dsub_rn(acc, prod);
+  }
+  __device__ __forceinline__ void row_done(int i, double acc) {
+    r[i] = acc;
+    const double ai = adiag[i];
+    s = __dadd_rn(s, nrms_term(acc, ai));
+    if (PREC == kPrecJacobi) {
+      const double zi = __dmul_rn(acc, __drcp_rn(ai));
+      rho = __dadd_rn(rho, __dmul_rn(zi, acc));
+    } else if (PREC == kPrecNone) {
+      rho = __dadd_rn(rho, __dmul_rn(acc, acc));
+    }
+  }
+  __device__ __forceinline__ void tile_end(int) {}
+};
+
+// Fixed tiles of ROWS rows over one matrix (the drop-in's tile source).
+template <int ROWS>
+struct FixedTiles {
+  const int* row;
+  const int* col;
+  const double* val;
+  int nrows;
+  __device__ int count() const { return (nrows + ROWS - 1) / ROWS; }
+  __device__ TileDesc desc(int k) const {
+    TileDesc d;
+    d.row = row;
+    d.col = col;
+    d.val = val;
+    d.r0 = k * ROWS;
+    d.r1 = min(d.r0 + ROWS, nrows);
+    d.j0 = __ldg(row + d.r0);
+    d.j1 = __ldg(row + d.r1);
+    d.skip = 0;
+    return d;
+  }
 };
 
 struct SpArgs {
@@ -277,8 +331,8 @@ __device__ __forceinline__ bool run_rows(const SpArgs& a, Op& op) {
     }
     return true;
   } else {
-    return stream_tiles<kTileRows[CFG], kTileNnzCap[CFG], double, 2>(
-        a.row, a.col, a.val, a.nrows, op);
+    FixedTiles<kTileRows[CFG]> src{a.row, a.col, a.val, a.nrows};
+    return stream_csr2<kTileRows[CFG], kTileNnzCap[CFG], 2>(src, op);
   }
 }
 
@@ -286,12 +340,12 @@ template <int CFG, int PAT = 0>
 constexpr int cfg_threads() {
   if constexpr (CFG == kTileNone) return 256;
   else if constexpr (PAT != 0) return pat_threads<kTileRows[CFG]>();
-  else return kTileRows[CFG];
+  else return kCsr2Threads;
 }
-// Two CTAs per SM: caps the row-pattern kernels (ROWS + 32 threads) at the
-// registers that two of them can hold.
+// Two CTAs per SM: caps the tiled kernels (consumers + a producer warp) at
+// the registers that two of them can hold.
 template <int CFG, int PAT>
-constexpr int cfg_min_blocks() { return (CFG != kTileNone && PAT) ? 2 : 1; }
+constexpr int cfg_min_blocks() { return CFG != kTileNone ? 2 : 1; }
 
 __device__ __forceinline__ void flag_timeout(SolveState* st) {
   if (st) atomicExch(&st->status, (int)TF_ERR_TIMEOUT);
@@ -552,7 +606,7 @@ size_t cfg_smem() {
   if constexpr (CFG == kTileNone) return 0;
   else if constexpr (PAT)
     return PatLayout<kTileRows[CFG], kTileNnzCap[CFG], kPatStages>::kSmemBytes;
-  else return TileLayout<kTileRows[CFG], kTileNnzCap[CFG], double, 2>::kSmemBytes;
+  else return Csr2Layout<kTileRows[CFG], kTileNnzCap[CFG], 2>::kSmemBytes;
 }
 
 template <int CFG, int PREC, int PAT>

@@ -89,7 +89,13 @@ struct tf_matrix_s {
   std::mutex mu;
   int async_alloc = 0;   // device arrays from cudaMallocAsync on ctx->stream
   int host_lent = 0;     // h_state / h_params belong to the context
-  size_t dev_bytes = 0;  // device bytes this matrix holds
+  size_t dev_bytes = 0;  // device bytes this matrix holds (with `ren`)
+  // Renumbered copy for the Jacobi / none solves (tf_renumber.cu): row i'
+  // of `ren` is row perm[i'] here, entry j' of `ren` is entry src[j'].
+  tf_matrix_s* ren = nullptr;
+  int* d_perm = nullptr;
+  int* d_src = nullptr;
+  tf_matrix_s* active = nullptr;  // the matrix the last solve ran on
 };
 
 // FP64 drop-in entry points implemented in tf_fp64.cu
@@ -112,4 +118,17 @@ size_t tf_matrix_bytes(int n_cells, int64_t nnz);
 int tf_solve_resident(tf_matrix_s* m, int prec, int miter, double tol, const double* norm,
                       int* niter, double* fin_res);
 int tf_dev_alloc_bytes(tf_ctx_s* ctx, void** p, size_t bytes);
+// Renumbering (tf_renumber.cu)
+double tf_gather_lines_per_warp(const int* row, const int* col, int n, int base);
+void tf_rcm_order(const std::vector<int>& row0, const std::vector<int>& col0, int n,
+                  std::vector<int>& order);
+int tf_renumber_in(tf_matrix_s* m);
+int tf_renumber_out(tf_matrix_s* m);
+// Matrices of at least this many rows whose sampled warp gathers touch more
+// than kRenumberLines lines get a renumbered copy when RCM cuts that by 20 %.
+constexpr int kRenumberMinRows = 10000;
+constexpr double kRenumberLines = 6.0;
+// Device bytes registration may take, renumbered copy included, for
+// budgeting before the matrix exists (Matrix_Type 1-based row/col).
+size_t tf_matrix_bytes_for(int n_cells, int64_t nnz, const int* row, const int* col);
 

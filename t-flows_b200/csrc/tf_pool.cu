@@ -190,7 +190,7 @@ extern "C" int tf_pool_submit(tf_pool p, int solver, int prec, int n, int64_t nn
   r->tol = tol;
   r->has_norm = norm ? 1 : 0;
   r->norm = norm ? *norm : 0.0;
-  r->bytes = tf_matrix_bytes(n, nnz) +
+  r->bytes = tf_matrix_bytes_for(n, nnz, row, col) +
              (prec == TF_PREC_ICC ? (size_t)n * 40 + 4096 : 0);
   std::lock_guard<std::mutex> lk(p->mu);
   if (p->stop) return TF_ERR_CANCELLED;

@@ -1,0 +1,246 @@
+// tf_tile2.cuh -- two-phase CSR tile streamer with a producer warp.
+//
+// A tile holds at most kCons rows and NNZCAP entries.  Tiles of more than
+// kCons/2 rows are summed one thread per row.  Shorter tiles (long rows:
+// polyhedral cells have 10-18 entries, so a 4096-entry tile has ~270 rows)
+// would leave half the threads idle, so they are consumed in two phases:
+//
+//   A  tpr = 2 or 4 threads per row: thread t forms the products
+//      a_j * x(col_j) of every tpr-th entry of row r0 + (t mod kCons/tpr)
+//      (a warp gathers for 32 consecutive rows, coalesced when neighbours
+//      have nearby indices) and stores them over the staged values;
+//   B  one thread per row sums the row's products in storage order,
+//      starting from op.row_init (0 for A p, b_i for b - A x).
+//
+// Every product is rounded once (__dmul_rn) and the row's sum adds them one
+// by one in the order of the entries (__dadd_rn / __dsub_rn), exactly the
+// sequence of the reference's loop (Native_Mod/Cg.f90:180-183,
+// Residual_Vector.f90:35-41), so results are bit-identical to one thread
+// walking the row.
+//
+// Pipeline: the last warp is the producer; its lane 0 issues three 1D bulk
+// copies (values, columns, row pointers) per tile into a ring of STAGES
+// stages, arming full[s] with the byte count once every consumer warp has
+// released the stage (empty[s]).  Consumers meet at a named barrier before
+// each tile (to agree on stopping) and between the two phases (the
+// products of a row come from other threads) -- the producer never waits
+// there.  All waits are bounded; on a
+// timeout the CTA stops, the producer drains its armed copies and the
+// streamer returns false.
+//
+// The tile source `S` provides (producer lane only):
+//   int count()                    -- tiles (items) to walk
+//   TileDesc desc(int k)           -- arrays and row/entry range of item k
+// and the operator `Op` (consumer threads):
+//   void begin(int k)              -- item k starts (cache pointers)
+//   double gather(int c)           -- the vector entry multiplied by column c
+//   double row_init(int i)         -- 0.0 or b_i
+//   double combine(double acc, double prod)  -- acc + prod or acc - prod
+//   void row_done(int i, double acc)
+//   void tile_end(int k)           -- consumer warps, after the rows (may be
+//                                     empty; must not use CTA barriers)
+#pragma once
+#include "tf_common.cuh"
+
+namespace tf {
+
+constexpr int kCons = 512;               // consumer threads per CTA
+constexpr int kCsr2Threads = kCons + 32;  // + the producer warp
+
+struct TileDesc {
+  const int* row;
+  const int* col;
+  const double* val;
+  int r0, r1, j0, j1;
+  int skip;
+};
+
+template <int ROWCAP, int NNZCAP, int STAGES>
+struct Csr2Layout {
+  static constexpr size_t kValBytes = (((NNZCAP + 4) * 8 + 127) / 128) * 128;
+  static constexpr size_t kColBytes = (((NNZCAP + 8) * 4 + 127) / 128) * 128;
+  static constexpr size_t kRowBytes = (((ROWCAP + 8) * 4 + 127) / 128) * 128;
+  static constexpr size_t kStageBytes = kValBytes + kColBytes + kRowBytes;
+  static constexpr size_t kBarOffset = STAGES * kStageBytes;   // full[S], empty[S]
+  static constexpr size_t kMetaOffset = kBarOffset + 16 * STAGES;
+  static constexpr int kMetaInts = 12;
+  static constexpr size_t kSmemBytes = kMetaOffset + 4 * kMetaInts * STAGES + 16;
+};
+
+// Named barrier 1 over the consumer threads only (the producer warp never
+// joins it).
+__device__ __forceinline__ void consumer_bar() {
+  asm volatile("bar.sync 1, %0;" ::"r"(kCons) : "memory");
+}
+// The same barrier with an OR-reduction: every consumer gets the same
+// answer, so all of them leave a loop at the same tile.
+__device__ __forceinline__ bool consumer_bar_or(bool v) {
+  unsigned r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((unsigned)v), "r"(kCons)
+      : "memory");
+  return r != 0;
+}
+
+template <int ROWCAP, int NNZCAP, int STAGES, class S, class Op>
+__device__ bool stream_csr2(S& src, Op& op) {
+  using L = Csr2Layout<ROWCAP, NNZCAP, STAGES>;
+  constexpr int kConsWarps = kCons / 32;
+  extern __shared__ __align__(128) unsigned char tf_smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(tf_smem + L::kBarOffset);
+  uint64_t* empty = full + STAGES;
+  int* meta = reinterpret_cast<int*>(tf_smem + L::kMetaOffset);
+  volatile int* abort_flag = meta + L::kMetaInts * STAGES;
+  auto sval = [&](int s) { return reinterpret_cast<double*>(tf_smem + s * L::kStageBytes); };
+  auto scol = [&](int s) {
+    return reinterpret_cast<int*>(tf_smem + s * L::kStageBytes + L::kValBytes);
+  };
+  auto srow = [&](int s) {
+    return reinterpret_cast<int*>(tf_smem + s * L::kStageBytes + L::kValBytes + L::kColBytes);
+  };
+
+  const int count = src.count();
+  if ((int)blockIdx.x >= count) return true;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsWarps);
+    }
+    *abort_flag = 0;
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  bool ok = true;
+
+  if (warp == kConsWarps) {
+    // ---- producer warp ----
+    if (lane == 0) {
+      int issued = 0;
+      for (int k = blockIdx.x; k < count; k += gridDim.x, ++issued) {
+        const int s = issued % STAGES;
+        if (issued >= STAGES) {
+          if (!mbar_wait_bounded(&empty[s], (unsigned)(issued / STAGES - 1) & 1u)) {
+            ok = false;
+            *abort_flag = 1;
+            break;
+          }
+          fence_proxy_async_smem();
+        }
+        if (*abort_flag) break;
+        const TileDesc d = src.desc(k);
+        int* m = meta + L::kMetaInts * s;
+        m[7] = d.skip;
+        m[8] = k;
+        if (d.skip) {
+          mbar_arrive_expect_tx(&full[s], 0);
+          continue;
+        }
+        const int a0 = d.j0 & ~1, a1 = (d.j1 + 1) & ~1;
+        const int c0 = d.j0 & ~3, c1 = (d.j1 + 3) & ~3;
+        const int p0 = d.r0 & ~3, p1 = (d.r1 + 1 + 3) & ~3;
+        m[0] = a0; m[1] = c0; m[2] = p0; m[3] = d.r0; m[4] = d.r1; m[5] = d.j0; m[6] = d.j1;
+        const unsigned bv = (unsigned)(a1 - a0) * 8u;
+        const unsigned bc = (unsigned)(c1 - c0) * 4u;
+        const unsigned br = (unsigned)(p1 - p0) * 4u;
+        mbar_arrive_expect_tx(&full[s], bv + bc + br);
+        if (bv) bulk_g2s(sval(s), d.val + a0, bv, &full[s]);
+        if (bc) bulk_g2s(scol(s), d.col + c0, bc, &full[s]);
+        bulk_g2s(srow(s), d.row + p0, br, &full[s]);
+      }
+      for (int k = (issued > STAGES ? issued - STAGES : 0); k < issued; ++k)
+        mbar_wait_bounded(&full[k % STAGES], (unsigned)(k / STAGES) & 1u);
+    }
+  } else {
+    // ---- consumer warps ----
+    const int t = threadIdx.x;
+    int it = 0;
+    for (int k = blockIdx.x; k < count; k += gridDim.x, ++it) {
+      const int s = it % STAGES;
+      bool stop = !mbar_wait_bounded(&full[s], (unsigned)(it / STAGES) & 1u);
+      stop = stop || *abort_flag;
+      // Consumers must pass the named barrier equally often: they decide
+      // together whether to stop here.
+      if (consumer_bar_or(stop)) {
+        ok = false;
+        *abort_flag = 1;
+        break;
+      }
+      const int* m = meta + L::kMetaInts * s;
+      if (!m[7]) {
+        const int a0 = m[0], c0 = m[1], p0 = m[2], r0 = m[3], r1 = m[4], j0 = m[5];
+        double* prod = sval(s) + (j0 - a0);
+        const int* cc = scol(s) + (j0 - c0);
+        op.begin(k);
+        const int* sr = srow(s);
+        const int nr = r1 - r0;
+        if (nr > kCons / 2) {
+          // One thread per row: the row's gathers are in flight together
+          // and its products are summed as they arrive.
+          const int i = r0 + t;
+          if (i < r1) {
+            const int js = sr[i - p0] - j0, je = sr[i + 1 - p0] - j0;
+            double acc = op.row_init(i);
+            for (int q0 = js; q0 < je; q0 += 8) {
+              double g[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u)
+                if (q0 + u < je) g[u] = op.gather(cc[q0 + u]);
+#pragma unroll
+              for (int u = 0; u < 8; ++u)
+                if (q0 + u < je) acc = op.combine(acc, __dmul_rn(prod[q0 + u], g[u]));
+            }
+            op.row_done(i, acc);
+          }
+        } else {
+          // tpr = 2 or 4 threads per row: thread t takes row r0 + (t mod R)
+          // and every tpr-th entry of it from slot t / R, so a warp's
+          // gathers are those of 32 consecutive rows (coalesced for
+          // structured column offsets).  Products go over the staged
+          // values; then one thread per row sums them in storage order.
+          const int lg = (nr > kCons / 4) ? 1 : 2;      // log2(tpr)
+          const int tpr = 1 << lg, R = kCons >> lg;
+          const int i = r0 + (t & (R - 1)), sl = t >> (__ffs(R) - 1);
+          int js = 0, je = 0;
+          if (i < r1) {
+            js = sr[i - p0] - j0;
+            je = sr[i + 1 - p0] - j0;
+          }
+          for (int q0 = js + sl; q0 < je; q0 += 8 * tpr) {
+            double g[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const int q = q0 + u * tpr;
+              if (q < je) g[u] = op.gather(cc[q]);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const int q = q0 + u * tpr;
+              if (q < je) prod[q] = __dmul_rn(prod[q], g[u]);
+            }
+          }
+          consumer_bar();
+          if (sl == 0 && i < r1) {
+            double acc = op.row_init(i);
+            for (int q = js; q < je; ++q) acc = op.combine(acc, prod[q]);
+            op.row_done(i, acc);
+          }
+        }
+        op.tile_end(k);
+      }
+      fence_proxy_async_smem();   // product writes before the next bulk copy
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+  }
+  __syncthreads();
+  return !__syncthreads_or(!ok);
+}
+
+}  // namespace tf

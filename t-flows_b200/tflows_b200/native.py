@@ -31,7 +31,7 @@ EXPORTS = [
     "tf_solve_native", "tf_solve_device", "tf_ctx_set_history", "tf_last_history",
     "tf_host_pin", "tf_host_unpin", "tf_spmv", "tf_residual", "tf_nrms",
     "tf_ctx_sync", "tf_ctx_stream", "tf_last_error_message", "tf_matrix_tile_config",
-    "tf_matrix_row_patterns",
+    "tf_matrix_row_patterns", "tf_matrix_renumbered",
 ]
 
 
@@ -82,6 +82,7 @@ def load(path=LIB_PATH):
                                  ctypes.POINTER(ctypes.c_int64), _c_int_p]
     L.tf_matrix_tile_config.argtypes = [_vp]
     L.tf_matrix_row_patterns.argtypes = [_vp]
+    L.tf_matrix_renumbered.argtypes = [_vp]
     solve_args = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int,
                   _c_int_p, ctypes.c_double, _c_dbl_p, _c_dbl_p]
     L.tf_solve.argtypes = solve_args
@@ -172,6 +173,11 @@ class Matrix:
     @property
     def tile_config(self):
         return load().tf_matrix_tile_config(self.h)
+
+    @property
+    def renumbered(self):
+        """True when Jacobi / none solves run on a renumbered copy."""
+        return bool(load().tf_matrix_renumbered(self.h))
 
     @property
     def row_patterns(self):

@@ -255,3 +255,43 @@ def poly_system(n_points, seed, kind="pressure", tol=1e-10, miter=20000, **kw):
     if kind == "pressure":
         return pressure_system(g, seed, tol=tol, miter=miter, singular="pin", **kw)
     return momentum_system(g, seed, tol=tol, miter=miter, **kw)
+
+
+def renumber_rcm(s: System) -> System:
+    """The same system with cells renumbered by reverse Cuthill-McKee (a
+    symmetric permutation P A P^T): row i' = perm[i] keeps its entries in
+    their original storage order with relabelled columns, so every row sum
+    is the original row's sum.  `pos` is not carried over."""
+    import copy
+    import scipy.sparse as sps
+    from scipy.sparse.csgraph import reverse_cuthill_mckee
+    c = s.csr
+    n = c.n
+    A = sps.csr_matrix((np.ones(c.nnz), c.col - 1, c.row - 1), shape=(n, n))
+    order = reverse_cuthill_mckee(A, symmetric_mode=True)     # new -> old
+    inv = np.empty(n, np.int64)
+    inv[order] = np.arange(n)                                  # old -> new
+    lens = np.diff(c.row)[order]
+    row = np.concatenate([[1], 1 + np.cumsum(lens)]).astype(np.int32)
+    src = np.concatenate([np.arange(c.row[o] - 1, c.row[o + 1] - 1) for o in order]) \
+        if n < 50000 else _gather_rows(c.row, order)
+    col = (inv[c.col[src] - 1] + 1).astype(np.int32)
+    dia_old = c.dia[order] - 1                                  # entry index in old arrays
+    # position of the diagonal within each new row = its offset in the old row
+    dia = (row[:-1] + (dia_old - (c.row[order] - 1))).astype(np.int32)
+    t = copy.copy(s)
+    t.csr = Csr(n=n, row=row, col=col, dia=dia, pos=np.zeros((0, 2), np.int32))
+    t.val = s.val[src]
+    t.b = s.b[order]
+    t.x0 = s.x0[order]
+    t.meta = dict(s.meta, renumbered="rcm")
+    return t
+
+
+def _gather_rows(row, order):
+    """Entry indices (0-based) of the rows `order`, row after row."""
+    starts = row[order].astype(np.int64) - 1
+    lens = (row[order + 1] - row[order]).astype(np.int64)
+    out_start = np.concatenate([[0], np.cumsum(lens)[:-1]])
+    idx = np.arange(lens.sum(), dtype=np.int64)
+    return starts.repeat(lens) + (idx - out_start.repeat(lens))

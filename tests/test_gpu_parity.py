@@ -190,6 +190,71 @@ def test_row_patterns_do_not_change_the_solve(gpu_ctx, prec, norm, monkeypatch):
         assert np.array_equal(u, w)
 
 
+def _lattice_poly(n, seed):
+    """Polyhedral Poisson system numbered by sorted cell centres (as
+    Sort_Cells_By_Coordinates.f90 numbers Generate/Convert meshes)."""
+    from tflows_b200.grids import poly_lattice_grid
+    return systems.pressure_system(poly_lattice_grid(n, seed), seed, tol=1e-10, miter=4000,
+                                   singular="pin", norm=1.0)
+
+
+def test_renumbering_is_chosen_for_scattered_numberings(gpu_ctx, monkeypatch):
+    """A polyhedral mesh numbered like T-Flows' coordinate sort (scattered
+    gathers) gets the renumbered copy; a hex lattice does not; the switch
+    turns it off."""
+    poly = _lattice_poly(20000, 5)
+    hexs = systems.small_hex(30, seed=1, kind="pressure")
+    for s, want in ((poly, True), (hexs, False)):
+        m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia)
+        try:
+            assert m.renumbered == want
+        finally:
+            m.close()
+    monkeypatch.setenv("TF_NO_RENUMBER", "1")
+    m = native.Matrix(gpu_ctx, poly.csr.row, poly.csr.col, poly.csr.dia)
+    try:
+        assert not m.renumbered
+    finally:
+        m.close()
+
+
+@pytest.mark.parametrize("prec,norm", [("jacobi", 1.0), ("jacobi", None), ("none", 1.0)])
+def test_renumbered_solve_parity(gpu_ctx, prec, norm, monkeypatch):
+    """Solves on the renumbered copy agree with the oracle (original order)
+    and with the solve on the given numbering: same rows, same sums; only
+    the dot products are summed in another order."""
+    s = _lattice_poly(20000, 6)
+    x0 = np.random.default_rng(2).uniform(-0.5, 0.5, s.n)
+    args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, x0, "cg", prec, 4000, 1e-10, norm)
+    g = gpu_solve(gpu_ctx, *args)
+    check_parity(g, oracle_solve(*args), 1e-10)
+    monkeypatch.setenv("TF_NO_RENUMBER", "1")
+    g2 = gpu_solve(gpu_ctx, *args)
+    assert abs(g[3] - g2[3]) <= max(1, 0.02 * g2[3])
+    assert rel_l2(g[0], g2[0]) <= 1e-9
+    # val and b come back exactly as on the given numbering: (v*fn)/fn
+    # elementwise, with the same fn up to the order of the diagonal sum
+    assert np.allclose(g[1], g2[1], rtol=4e-16, atol=0)
+    assert np.allclose(g[2], g2[2], rtol=4e-16, atol=0)
+
+
+@pytest.mark.parametrize("miter", [1, 5])
+def test_renumbered_fin_res_is_nrms_of_returned_x(gpu_ctx, miter):
+    s = _lattice_poly(20000, 7)
+    x0 = np.random.default_rng(8).uniform(-0.5, 0.5, s.n)
+    m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia)
+    try:
+        assert m.renumbered
+        v, x, b = s.val.copy(), x0.copy(), s.b.copy()
+        it, res = native.solve(gpu_ctx, m, "cg", "jacobi", v, x, b, miter, 1e-300, None)
+    finally:
+        m.close()
+    assert it == miter
+    r = O.residual(s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, x)
+    assert res == pytest.approx(O.nrms(s.csr.row, s.csr.col, s.csr.dia, s.val, r, x),
+                                rel=1e-9)
+
+
 def test_long_rows_fall_back_to_global_path(gpu_ctx):
     """A row longer than any tile stage (a dense coupling row) still works."""
     n = 6000
