@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--count", type=int, default=512)
+    ap.add_argument("--parts", default="all",
+                    help="batched: comma list of mixed, fp64_batched, drop_in, streams, pool "
+                         "(default all)")
     ap.add_argument("--rate", type=float, default=200.0, help="served: arrivals per second")
     ap.add_argument("--seconds", type=float, default=60.0, help="served: window length")
     ap.add_argument("--iters", type=int, default=30, help="iters: Cg iterations per solve")
@@ -192,7 +195,11 @@ def run_batched(args):
                        "polyhedral upwind convection-diffusion (Bicg, Pe U[1,50], CFL 0.1); "
                        "Jacobi; target ||b-Ax||/||b|| <= 1e-10"}
     smallest = sorted(sysl, key=lambda s: s.n)[:4]
+    parts = set(("mixed,fp64_batched,drop_in,streams,pool" if args.parts == "all"
+                 else args.parts).split(","))
     for label, opts in (("mixed", dict(vec_fp32=True)), ("fp64_batched", dict(vec_fp32=False))):
+        if label not in parts:
+            continue
         _drop = _batch_solve(ctx, smallest, **opts)   # warm-up (module load, graphs)
         t_add, t_run, res, info = _batch_solve(ctx, sysl, **opts)
         ok = sum(r["status"] == "converged" and r["rel"] <= 1.01e-10 for r in res)
@@ -206,19 +213,20 @@ def run_batched(args):
                       "done_ms_p99": float(np.percentile(done, 99)),
                       "sweeps": info["sweeps"],
                       "iters_total": int(sum(r["iters"] for r in res))}
-    _drop_in_solve_times(ctx, smallest[:2], 1e-10)   # warm-up
-    t = _drop_in_solve_times(ctx, sysl, 1e-10)
-    ms = np.array([a for a, _, _ in t])
-    out["fp64_drop_in"] = {"run_s": float(ms.sum() / 1e3),
-                           "solves_per_s": len(sysl) / float(ms.sum() / 1e3),
-                           "mcell_iters_per_s": sum(s.n * it for s, (_, it, _) in zip(sysl, t))
-                           / float(ms.sum() / 1e3) / 1e6,
-                           "tol": "1e-10 x NRMS(b) (reference normalisation, norm=1)",
-                           "max_true_rel": max(r for _, _, r in t),
-                           "solve_ms_p50": float(np.percentile(ms, 50)),
-                           "solve_ms_p99": float(np.percentile(ms, 99)),
-                           "iters_total": int(sum(it for _, it, _ in t))}
-    for workers in (8, 32):
+    if "drop_in" in parts:
+        _drop_in_solve_times(ctx, smallest[:2], 1e-10)   # warm-up
+        t = _drop_in_solve_times(ctx, sysl, 1e-10)
+        ms = np.array([a for a, _, _ in t])
+        out["fp64_drop_in"] = {"run_s": float(ms.sum() / 1e3),
+            "solves_per_s": len(sysl) / float(ms.sum() / 1e3),
+            "mcell_iters_per_s": sum(s.n * it for s, (_, it, _) in zip(sysl, t))
+            / float(ms.sum() / 1e3) / 1e6,
+            "tol": "1e-10 x NRMS(b) (reference normalisation, norm=1)",
+            "max_true_rel": max(r for _, _, r in t),
+            "solve_ms_p50": float(np.percentile(ms, 50)),
+            "solve_ms_p99": float(np.percentile(ms, 99)),
+            "iters_total": int(sum(it for _, it, _ in t))}
+    for workers in ((8, 32) if "streams" in parts else ()):
         _drop_in_stream_pool(smallest, workers, 1e-10)   # warm-up
         wall, res = _drop_in_stream_pool(sysl, workers, 1e-10)
         out[f"fp64_drop_in_{workers}streams"] = {
@@ -226,7 +234,7 @@ def run_batched(args):
             "mcell_iters_per_s": sum(s.n * it for s, (_, it) in zip(sysl, res)) / wall / 1e6,
             "iters_total": int(sum(it for _, it in res))}
     from tflows_b200 import pool as tpool
-    for workers in (8, 16):
+    for workers in ((8, 16) if "pool" in parts else ()):
         for rep in range(2):             # first pass warms the memory pool and graphs
             pl = tpool.Pool(workers=workers, mem_budget=40 << 30)
             t0 = time.perf_counter()
@@ -242,11 +250,13 @@ def run_batched(args):
             "latency_ms_p50": float(np.percentile(lat, 50)),
             "latency_ms_p99": float(np.percentile(lat, 99)),
             "iters_total": int(sum(g["niter"] for g in got))}
-    out["speedup_pool16_vs_drop_in"] = (out["fp64_pool_16"]["solves_per_s"]
-                                        / out["fp64_drop_in"]["solves_per_s"])
-    out["speedup_mixed_vs_drop_in"] = out["mixed"]["solves_per_s"] / out["fp64_drop_in"]["solves_per_s"]
-    out["speedup_mixed_vs_fp64_batched"] = (out["mixed"]["solves_per_s"]
-                                            / out["fp64_batched"]["solves_per_s"])
+    def ratio(a, b):
+        if a in out and b in out:
+            out[f"speedup_{a}_vs_{b}"] = out[a]["solves_per_s"] / out[b]["solves_per_s"]
+    ratio("fp64_pool_16", "fp64_drop_in")
+    ratio("fp64_drop_in_8streams", "fp64_drop_in")
+    ratio("mixed", "fp64_drop_in")
+    ratio("mixed", "fp64_batched")
     print(json.dumps(out), flush=True)
     ctx.close()
 

@@ -230,6 +230,12 @@ int tf_pool_wait(tf_pool p, int64_t req, int* niter, double* fin_res,
                  double* latency_ms, double* queue_ms);
 int tf_pool_stats(tf_pool p, long long* submitted, long long* completed,
                   long long* rejected, size_t* peak_bytes);
+/* Resident structures: requests reusing a held registration (`reused`),
+ * registrations currently held and their budgeted bytes.  A request whose
+ * row/col/dia arrays (same addresses, same sampled contents, same sizes)
+ * were registered by an earlier request runs on that registration when the
+ * worker holding it takes it.  No reference counterpart. */
+int tf_pool_resident(tf_pool p, long long* reused, int* held, size_t* held_bytes);
 int tf_pool_destroy(tf_pool p);
 
 /* ---------------------------------------------------------------------------

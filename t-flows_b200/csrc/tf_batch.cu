@@ -57,6 +57,7 @@
 
 #include "tf_internal.h"
 #include "tf_tile.cuh"
+#include "tf_tile2.cuh"
 
 namespace tfb {
 
@@ -360,11 +361,82 @@ struct SpmvWork {
   }
 };
 
+// Work-list items as tiles of the producer-warp streamer; SKIP decides
+// which items have nothing to do in this launch.
+template <typename V, int KIND>
+struct BatchTiles {
+  const SysDev<V>* D;
+  const SysState* st;
+  const Work* work;
+  int nw;
+  __device__ int count() const { return nw; }
+  __device__ TileDesc desc(int k) const {
+    const Work w = work[k];
+    const SysDev<V>& d = D[w.sys];
+    TileDesc t;
+    t.row = d.row;
+    t.col = d.col;
+    t.val = d.val;
+    t.r0 = w.r0;
+    t.r1 = w.r1;
+    t.j0 = w.j0;
+    t.j1 = w.j1;
+    const SysState& s = st[w.sys];
+    t.skip = KIND == 0 ? !active(s) : !(s.status == kInit || (s.status == kActive && s.need_ru));
+    return t;
+  }
+};
+
+// q = A p (FP64 values, FP64 row sums), p.q per tile, alpha per system.
+template <typename V>
+struct SpmvOp2 {
+  const SysDev<V>* D;
+  SysState* st;
+  const Work* work;
+  double acc;
+  Work w;
+  const V* p;
+  V* q;
+  __device__ void begin(int k) {
+    w = work[k];
+    p = D[w.sys].p;
+    q = D[w.sys].q;
+  }
+  __device__ double gather(int c) const { return (double)__ldg(p + c); }
+  __device__ double row_init(int) const { return 0.0; }
+  __device__ double combine(double a, double prod) const { return __dadd_rn(a, prod); }
+  __device__ void row_done(int i, double sum) {
+    const V qi = (V)sum;
+    q[i] = qi;
+    acc = __dadd_rn(acc, __dmul_rn((double)__ldg(p + i), (double)qi));
+  }
+  __device__ void tile_end(int) {
+    const SysDev<V>& d = D[w.sys];
+    double v[1] = {acc};
+    acc = 0.0;
+    if (cta_tile_done<1>(&st[w.sys].cnt_spmv, d.tile_tot, d.warp_part, d.tile_cnt, d.ntiles,
+                         w.tile, v) &&
+        (threadIdx.x & 31) == 0) {
+      SysState& s = st[w.sys];
+      if (!(v[0] > 0.0)) s.status = kBreakdown;   // p.q <= 0 or NaN
+      else s.alpha = __ddiv_rn(s.rho, v[0]);
+    }
+  }
+};
+
 template <typename V, typename VT>
-__global__ void __launch_bounds__(kRows, 2) kb_spmv(BatchArgs a) {
-  SpmvWork<V, VT> w{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, *a.nwork, 0.0, -1,
-                    nullptr, nullptr};
-  stream_items<kRows, kNnzCap, VT, kStages>(w);
+__global__ void __launch_bounds__(kCsr2Threads, 2) kb_spmv(BatchArgs a) {
+  if constexpr (sizeof(VT) == 8) {
+    BatchTiles<V, 0> src{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, *a.nwork};
+    SpmvOp2<V> op{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, 0.0};
+    stream_csr2<kRows, kNnzCap, kStages>(src, op);
+  } else {
+    // FP32 values: the one-thread-per-row streamer (kRows threads do the
+    // work; the extra warp only joins the CTA-wide barriers).
+    SpmvWork<V, VT> w{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, *a.nwork, 0.0, -1,
+                      nullptr, nullptr};
+    stream_items<kRows, kNnzCap, VT, kStages>(w);
+  }
 }
 
 // r = b - A x in FP64; new systems also form dinv and |b|^2.
@@ -450,11 +522,48 @@ struct ResWork {
   }
 };
 
+// r = b - A x in FP64 for the producer-warp streamer (see ResWork).
 template <typename V>
-__global__ void __launch_bounds__(kRows, 2) kb_ru_res(BatchArgs a) {
-  ResWork<V> w{static_cast<const SysDev<V>*>(a.desc), a.st, a.ru.items, *a.ru.count, 0.0,
-               0.0, 0.0};
-  stream_items<kRows, kNnzCap, double, kStages>(w);
+struct ResOp2 {
+  const SysDev<V>* D;
+  SysState* st;
+  const Work* work;
+  double rr, rho, bb;
+  Work w;
+  const SysDev<V>* d;
+  bool init;
+  __device__ void begin(int k) {
+    w = work[k];
+    d = &D[w.sys];
+    init = st[w.sys].status == kInit;
+  }
+  __device__ double gather(int c) const { return d->x[c]; }
+  __device__ double row_init(int i) const { return d->b[i]; }
+  __device__ double combine(double a, double prod) const { return __dsub_rn(a, prod); }
+  __device__ void row_done(int i, double s) {
+    if (init) {
+      const double aii = d->val[d->dia[i]];
+      d->dinv[i] = (V)__drcp_rn(aii);
+      bb = __dadd_rn(bb, __dmul_rn(d->b[i], d->b[i]));
+    }
+    const V ri = (V)s;
+    d->r[i] = ri;
+    const V zi = ri * d->dinv[i];
+    rr = __dadd_rn(rr, __dmul_rn(s, s));
+    rho = __dadd_rn(rho, __dmul_rn((double)zi, (double)ri));
+  }
+  __device__ void tile_end(int k) {
+    ResWork<V> rw{D, st, work, 0, rr, rho, bb};
+    rr = rho = bb = 0.0;
+    rw.tile_end(k);
+  }
+};
+
+template <typename V>
+__global__ void __launch_bounds__(kCsr2Threads, 2) kb_ru_res(BatchArgs a) {
+  BatchTiles<V, 1> src{static_cast<const SysDev<V>*>(a.desc), a.st, a.ru.items, *a.ru.count};
+  ResOp2<V> op{static_cast<const SysDev<V>*>(a.desc), a.st, a.ru.items, 0.0, 0.0, 0.0};
+  stream_csr2<kRows, kNnzCap, kStages>(src, op);
   // The last CTA to leave empties the refinement list for the next iteration.
   if (threadIdx.x == 0) {
     __threadfence();
@@ -524,6 +633,7 @@ struct HostSys {
   std::vector<int> row, col, dia, tiles;
   std::vector<double> val, b, x0;
   std::vector<float> val32;
+  std::vector<int> perm;   // renumbered: row i here is row perm[i] of the caller's
   double tol = 1e-10;
   int maxit = 10000;
 };
@@ -552,6 +662,38 @@ int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* co
     if (d < h.row[i] || d >= h.row[i + 1] || h.col[d] != i) return TF_ERR_LAYOUT;
     h.dia[i] = d;
   }
+  // Scattered numbering: renumber by reverse Cuthill-McKee, each row keeping
+  // its entries in storage order (the same row sums; see tf_renumber.cu).
+  std::vector<long long> src;   // entry j here is entry src[j] of the caller's
+  h.perm.clear();
+  if (n >= kRenumberMinRows && !getenv("TF_NO_RENUMBER")) {
+    const double before = tf_gather_lines_per_warp(h.row.data(), h.col.data(), n, 0);
+    if (before > kRenumberLines) {
+      std::vector<int> order, inv(n);
+      tf_rcm_order(h.row, h.col, n, order);
+      for (int i = 0; i < n; ++i) inv[order[i]] = i;
+      std::vector<int> row2(h.row.size()), col2(h.col.size(), 0), dia2(h.dia.size(), 0);
+      std::vector<long long> src2((size_t)nnz);
+      row2[0] = 0;
+      for (int i = 0; i < n; ++i) {
+        const int o = order[i], js = h.row[o], len = h.row[o + 1] - js;
+        for (int k = 0; k < len; ++k) {
+          src2[row2[i] + k] = js + k;
+          col2[row2[i] + k] = inv[h.col[js + k]];
+        }
+        dia2[i] = row2[i] + (h.dia[o] - js);
+        row2[i + 1] = row2[i] + len;
+      }
+      for (size_t i = n + 1; i < row2.size(); ++i) row2[i] = row2[n];
+      if (tf_gather_lines_per_warp(row2.data(), col2.data(), n, 0) <= 0.8 * before) {
+        h.row.swap(row2);
+        h.col.swap(col2);
+        h.dia.swap(dia2);
+        h.perm.swap(order);
+        src.swap(src2);
+      }
+    }
+  }
   // tiles: <= kRows rows and <= kNnzCap entries each
   h.tiles.clear();
   h.tiles.push_back(0);
@@ -560,18 +702,38 @@ int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* co
     int r1 = r0;
     while (r1 < n && r1 - r0 < kRows && h.row[r1 + 1] - h.row[r0] <= kNnzCap) ++r1;
     if (r1 == r0) return TF_ERR_LAYOUT;   // one row longer than a tile stage
+    // A tile cut short by its entry cap is trimmed to kRows/2 or kRows/4
+    // rows, so the streamer can give each row 2 or 4 threads.
+    if (r1 < n) {
+      if (r1 - r0 > kRows / 2 && r1 - r0 < kRows) r1 = r0 + kRows / 2;
+      else if (r1 - r0 > kRows / 4 && r1 - r0 < kRows / 2) r1 = r0 + kRows / 4;
+    }
     h.tiles.push_back(r1);
     r0 = r1;
   }
-  h.val.assign(val, val + nnz);
+  if (src.empty()) {
+    h.val.assign(val, val + nnz);
+  } else {
+    h.val.resize((size_t)nnz);
+    for (long long j = 0; j < nnz; ++j) h.val[j] = val[src[j]];
+  }
   h.val.resize((size_t)nnz + 8, 0.0);
   if (use_val32) {
     h.val32.resize((size_t)nnz + 8);
     for (long long j = 0; j < nnz + 8; ++j) h.val32[j] = (float)h.val[j];
   }
-  h.b.assign(b, b + n);
-  if (x0) h.x0.assign(x0, x0 + n);
-  else h.x0.assign(n, 0.0);
+  if (h.perm.empty()) {
+    h.b.assign(b, b + n);
+    if (x0) h.x0.assign(x0, x0 + n);
+    else h.x0.assign(n, 0.0);
+  } else {
+    h.b.resize(n);
+    h.x0.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+      h.b[i] = b[h.perm[i]];
+      if (x0) h.x0[i] = x0[h.perm[i]];
+    }
+  }
   return TF_OK;
 }
 
@@ -615,6 +777,7 @@ struct Slot {
   Layout L{};
   std::vector<int> tiles;  // row boundaries of the tiles (host copy)
   std::vector<int> tile_j; // entry boundaries of the tiles (row[tiles[t]])
+  std::vector<int> perm;   // renumbered system: device row i is caller row perm[i]
 };
 
 }  // namespace tfb
@@ -658,31 +821,35 @@ struct tf_batch_s {
     if (h_state) cudaFreeHost(h_state);
   }
 
+  // Shared memory of the tile kernels: the producer-warp streamer (FP64
+  // values) and the one-thread-per-row streamer (FP32 values).
+  static size_t smem_csr2() { return Csr2Layout<kRows, kNnzCap, kStages>::kSmemBytes; }
+  static size_t smem_rows32() { return TileLayout<kRows, kNnzCap, float, kStages>::kSmemBytes; }
+
   template <typename V>
   void launch_iteration(cudaStream_t s, const BatchArgs& a) {
-    const size_t sm = TileLayout<kRows, kNnzCap, double, kStages>::kSmemBytes;
-    const size_t sm32 = TileLayout<kRows, kNnzCap, float, kStages>::kSmemBytes;
     kb_pupdate<V><<<grid_plain, 256, 0, s>>>(a);
-    if (opts.val_fp32) kb_spmv<V, float><<<grid_tile, kRows, sm32, s>>>(a);
-    else kb_spmv<V, double><<<grid_tile, kRows, sm, s>>>(a);
+    if (opts.val_fp32) kb_spmv<V, float><<<grid_tile, kRows, smem_rows32(), s>>>(a);
+    else kb_spmv<V, double><<<grid_tile, kCsr2Threads, smem_csr2(), s>>>(a);
     kb_update<V><<<grid_plain, 256, 0, s>>>(a);
     kb_ru_fold<V><<<grid_plain, 256, 0, s>>>(a);
-    kb_ru_res<V><<<grid_tile, kRows, sm, s>>>(a);
+    kb_ru_res<V><<<grid_tile, kCsr2Threads, smem_csr2(), s>>>(a);
   }
 
   template <typename V>
   int setup_kernels() {
-    const size_t sm = TileLayout<kRows, kNnzCap, double, kStages>::kSmemBytes;
-    const size_t sm32 = TileLayout<kRows, kNnzCap, float, kStages>::kSmemBytes;
     TF_CUDA_TRY(cudaFuncSetAttribute(kb_spmv<V, double>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_csr2()));
     TF_CUDA_TRY(cudaFuncSetAttribute(kb_spmv<V, float>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm32));
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_rows32()));
     TF_CUDA_TRY(cudaFuncSetAttribute(kb_ru_res<V>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_csr2()));
     int per_sm = 1;
     TF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_spmv<V, double>,
-                                                              kRows, sm));
+                                                              kCsr2Threads, smem_csr2()));
     grid_tile = std::max(1, per_sm) * ctx->sm_count;
     grid_plain = ctx->sm_count * 8;
     return TF_OK;
@@ -835,6 +1002,7 @@ struct tf_batch_s {
     sl.ntiles = ntiles;
     sl.L = L;
     sl.tiles = h.tiles;
+    sl.perm = h.perm;
     sl.tile_j.resize(h.tiles.size());
     for (size_t t = 0; t < h.tiles.size(); ++t) sl.tile_j[t] = h.row[h.tiles[t]];
     h_state[slot] = ss;
@@ -930,9 +1098,17 @@ struct tf_batch_s {
 
   int fetch_x(int slot, double* x) {
     const Slot& sl = slots[slot];
-    TF_CUDA_TRY(cudaMemcpyAsync(x, arena.base + sl.off + sl.L.x, (size_t)sl.n * 8,
+    if (sl.perm.empty()) {
+      TF_CUDA_TRY(cudaMemcpyAsync(x, arena.base + sl.off + sl.L.x, (size_t)sl.n * 8,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+      TF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+      return TF_OK;
+    }
+    std::vector<double> tmp((size_t)sl.n);
+    TF_CUDA_TRY(cudaMemcpyAsync(tmp.data(), arena.base + sl.off + sl.L.x, (size_t)sl.n * 8,
                                 cudaMemcpyDeviceToHost, ctx->stream));
     TF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < sl.n; ++i) x[sl.perm[i]] = tmp[i];
     return TF_OK;
   }
 

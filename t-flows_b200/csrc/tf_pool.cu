@@ -17,6 +17,17 @@
 // a request larger than the whole budget is rejected (TF_ERR_OOM).  Small
 // systems, which a single stream leaves launch-latency bound, thus run many
 // at a time, and a large one shares the GPU with whatever fits beside it.
+//
+// Resident structures: a Process solves the same Matrix_Type over and over
+// (Create_Native.f90 builds it once; every outer iteration only refills
+// val and b).  A registered matrix therefore stays on the device after its
+// request, keyed by the caller's row/col/dia pointers, sizes and a sampled
+// fingerprint of their contents; a later request with the same key, taken
+// by the worker that holds it, skips validation, tiling, renumbering and
+// the structure upload.  Held structures count toward the budget and are
+// released, least recently used first, when a new request needs the room.
+// A worker looks a few requests down the queue for one whose structure it
+// holds before taking the head.
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -50,12 +61,32 @@ struct PoolReq {
   int has_norm = 0;
   double norm = 0.0;
   size_t bytes = 0;
+  uint64_t key = 0;           // structure key (pointers, sizes, sampled contents)
   Clock::time_point t_submit, t_start, t_done;
   int status = TF_OK;
   int niter = 0;
   double fin_res = 0.0;
   bool done = false;
 };
+// Sampled fingerprint of a Matrix_Type structure plus the caller's array
+// addresses: equal keys mean "the same arrays, unchanged where sampled".
+uint64_t structure_key(int n, int64_t nnz, const int* row, const int* col, const int* dia,
+                       int icc) {
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&](uint64_t v) { h = (h ^ v) * 1099511628211ull; };
+  mix((uint64_t)n);
+  mix((uint64_t)nnz);
+  mix((uint64_t)(uintptr_t)row);
+  mix((uint64_t)(uintptr_t)col);
+  mix((uint64_t)(uintptr_t)dia);
+  mix((uint64_t)icc);
+  for (int k = 0; k <= 64; ++k) mix((uint64_t)(uint32_t)row[(int64_t)n * k / 64]);
+  for (int k = 0; k < 256; ++k) mix((uint64_t)(uint32_t)col[nnz * k / 256]);
+  for (int k = 0; k < 64; ++k) mix((uint64_t)(uint32_t)dia[(int64_t)(n - 1) * k / 63]);
+  return h;
+}
+
+constexpr int kLookahead = 16;   // queued requests a worker scans for its own structures
 }  // namespace
 
 struct tf_pool_s {
@@ -69,14 +100,69 @@ struct tf_pool_s {
   std::map<int64_t, std::shared_ptr<PoolReq>> live;
   int64_t next_id = 1;
   bool stop = false;
-  long long submitted = 0, completed = 0, rejected = 0;
+  long long submitted = 0, completed = 0, rejected = 0, reused = 0;
 
-  // Run one request on worker w's context.
-  int run(tf_ctx_s* ctx, PoolReq& r) {
+  // Resident structures (see the header comment).
+  struct Held {
+    uint64_t key = 0;
     tf_matrix_s* m = nullptr;
-    int st = tf_matrix_create(ctx, r.n, r.n, r.nnz, r.row, r.col, r.dia,
-                              r.prec == tf::kPrecIcc, &m);
-    if (st != TF_OK) return st;
+    int owner = 0;
+    bool in_use = false;
+    size_t bytes = 0;
+    uint64_t last = 0;
+  };
+  std::vector<Held> held;
+  uint64_t tick = 0;
+
+  int find_held(uint64_t key, int w) const {
+    for (size_t i = 0; i < held.size(); ++i)
+      if (held[i].key == key && held[i].owner == w && !held[i].in_use) return (int)i;
+    return -1;
+  }
+  // Release idle held structures, least recently used first, until `need`
+  // more bytes fit in the budget.  Caller holds mu.
+  bool make_room(size_t need) {
+    while (used + need > budget) {
+      int victim = -1;
+      for (size_t i = 0; i < held.size(); ++i)
+        if (!held[i].in_use && (victim < 0 || held[i].last < held[victim].last)) victim = (int)i;
+      if (victim < 0) return false;
+      tf_matrix_free(held[victim].m);   // stream-ordered on its owner's stream
+      used -= held[victim].bytes;
+      held.erase(held.begin() + victim);
+    }
+    return true;
+  }
+  // Pick worker w's next request: one whose structure it holds among the
+  // first kLookahead, else the head if it fits.  Caller holds mu.
+  std::shared_ptr<PoolReq> pick(int w, int* slot) {
+    *slot = -1;
+    const int look = std::min<int>((int)queue.size(), kLookahead);
+    for (int q = 0; q < look; ++q) {
+      const int h = find_held(queue[q]->key, w);
+      if (h >= 0) {
+        auto r = queue[q];
+        queue.erase(queue.begin() + q);
+        *slot = h;
+        return r;
+      }
+    }
+    if (queue.empty() || !make_room(queue.front()->bytes)) return nullptr;
+    auto r = queue.front();
+    queue.pop_front();
+    return r;
+  }
+
+  // Run one request on worker w's context, on matrix m when it is held.
+  int run(tf_ctx_s* ctx, PoolReq& r, tf_matrix_s** pm) {
+    tf_matrix_s* m = *pm;
+    int st = TF_OK;
+    if (!m) {
+      st = tf_matrix_create(ctx, r.n, r.n, r.nnz, r.row, r.col, r.dia, r.prec == tf::kPrecIcc,
+                            &m);
+      if (st != TF_OK) return st;
+      *pm = m;
+    }
     cudaStream_t s = ctx->stream;
     const size_t vb = (size_t)r.nnz * 8, nb = (size_t)r.n * 8;
     cudaError_t e = cudaMemcpyAsync(m->d_val, r.val, vb, cudaMemcpyHostToDevice, s);
@@ -97,7 +183,6 @@ struct tf_pool_s {
         st = TF_ERR_CUDA;
       }
     }
-    tf_matrix_free(m);
     return st;
   }
 
@@ -106,22 +191,48 @@ struct tf_pool_s {
     cudaSetDevice(device);
     for (;;) {
       std::shared_ptr<PoolReq> r;
+      int h = -1;
+      tf_matrix_s* m = nullptr;
       {
         std::unique_lock<std::mutex> lk(mu);
         cv_work.wait(lk, [&] {
-          return stop || (!queue.empty() && used + queue.front()->bytes <= budget);
+          if (stop) return true;
+          r = pick(w, &h);
+          return r != nullptr;
         });
         if (stop) return;
-        r = queue.front();
-        queue.pop_front();
-        used += r->bytes;
-        peak = std::max(peak, used);
+        if (h >= 0) {
+          held[h].in_use = true;
+          m = held[h].m;
+          ++reused;
+        } else {
+          used += r->bytes;
+          peak = std::max(peak, used);
+        }
         r->t_start = Clock::now();
       }
-      const int st = run(ctx, *r);
+      const int st = run(ctx, *r, &m);
       {
         std::lock_guard<std::mutex> lk(mu);
-        used -= r->bytes;
+        if (h >= 0) {
+          // the held entry may have moved in the vector: find it again
+          for (auto& e : held)
+            if (e.m == m) {
+              e.in_use = false;
+              e.last = ++tick;
+            }
+        } else if (m && st == TF_OK) {   // keep the structure resident
+          Held e;
+          e.key = r->key;
+          e.m = m;
+          e.owner = w;
+          e.bytes = r->bytes;
+          e.last = ++tick;
+          held.push_back(e);
+        } else {
+          if (m) tf_matrix_free(m);
+          used -= r->bytes;
+        }
         r->status = st;
         r->t_done = Clock::now();
         r->done = true;
@@ -192,6 +303,7 @@ extern "C" int tf_pool_submit(tf_pool p, int solver, int prec, int n, int64_t nn
   r->norm = norm ? *norm : 0.0;
   r->bytes = tf_matrix_bytes_for(n, nnz, row, col) +
              (prec == TF_PREC_ICC ? (size_t)n * 40 + 4096 : 0);
+  r->key = structure_key(n, nnz, row, col, dia, prec == TF_PREC_ICC);
   std::lock_guard<std::mutex> lk(p->mu);
   if (p->stop) return TF_ERR_CANCELLED;
   r->id = p->next_id++;
@@ -240,6 +352,19 @@ extern "C" int tf_pool_stats(tf_pool p, long long* submitted, long long* complet
   return TF_OK;
 }
 
+extern "C" int tf_pool_resident(tf_pool p, long long* reused, int* held, size_t* held_bytes) {
+  if (!p) return TF_ERR_ARG;
+  std::lock_guard<std::mutex> lk(p->mu);
+  if (reused) *reused = p->reused;
+  if (held) *held = (int)p->held.size();
+  if (held_bytes) {
+    size_t b = 0;
+    for (auto& e : p->held) b += e.bytes;
+    *held_bytes = b;
+  }
+  return TF_OK;
+}
+
 extern "C" int tf_pool_destroy(tf_pool p) {
   if (!p) return TF_ERR_ARG;
   {
@@ -254,6 +379,8 @@ extern "C" int tf_pool_destroy(tf_pool p) {
     p->cv_done.notify_all();
   }
   for (auto& t : p->workers) t.join();
+  for (auto& e : p->held) tf_matrix_free(e.m);
+  p->held.clear();
   for (tf_ctx_s* c : p->ctxs) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);

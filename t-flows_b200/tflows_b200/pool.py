@@ -22,6 +22,8 @@ def _lib():
     L.tf_pool_wait.argtypes = [_vp, ctypes.c_int64, ip, dp, dp, dp]
     L.tf_pool_stats.argtypes = [_vp] + [ctypes.POINTER(ctypes.c_longlong)] * 3 + [
         ctypes.POINTER(ctypes.c_size_t)]
+    L.tf_pool_resident.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong),
+                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_size_t)]
     L.tf_pool_destroy.argtypes = [_vp]
     L._tf_pool_bound = True
     return L
@@ -80,6 +82,14 @@ class Pool:
         native._check(self.L.tf_pool_stats(self.h, ctypes.byref(a), ctypes.byref(c),
                                            ctypes.byref(r), ctypes.byref(pk)), "tf_pool_stats")
         return dict(submitted=a.value, completed=c.value, rejected=r.value, peak_bytes=pk.value)
+
+    def resident(self):
+        """Requests that reused a held registration, registrations held and
+        their bytes."""
+        r, h, b = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_size_t()
+        native._check(self.L.tf_pool_resident(self.h, ctypes.byref(r), ctypes.byref(h),
+                                              ctypes.byref(b)), "tf_pool_resident")
+        return dict(reused=r.value, held=h.value, held_bytes=b.value)
 
     def close(self):
         if getattr(self, "h", None):

@@ -32,6 +32,16 @@ def _direct(s):
     return spla.spsolve(_A(s).tocsc(), s.b)
 
 
+def lattice_poly(n, seed, kind="pressure", **kw):
+    """Polyhedral system numbered by sorted cell centres (scattered gathers:
+    the engine renumbers it)."""
+    from tflows_b200.grids import poly_lattice_grid
+    g = poly_lattice_grid(n, seed)
+    if kind == "pressure":
+        return systems.pressure_system(g, seed, tol=TOL, miter=20000, singular="pin", norm=1.0)
+    return systems.momentum_system(g, seed, tol=TOL, miter=20000, cfl=0.1, **kw)
+
+
 def mixed_systems():
     return [
         systems.small_hex(12, seed=1, kind="pressure", ratio=1.02),
@@ -40,6 +50,8 @@ def mixed_systems():
         systems.poly_system(3000, seed=4, kind="pressure"),
         systems.poly_system(2500, seed=5, kind="momentum", peclet=10.0),
         systems.small_hex(3, seed=6, kind="pressure"),
+        lattice_poly(20000, 7),
+        lattice_poly(15000, 8, kind="momentum", peclet=5.0),
     ]
 
 

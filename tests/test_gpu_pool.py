@@ -1,6 +1,7 @@
 """GPU tests of the request pool: concurrent Solve_Native calls on several
 streams give exactly the results of tf_solve on the same inputs (the pool
 runs the same deterministic drop-in), under a device-memory budget."""
+import copy
 import threading
 
 import numpy as np
@@ -70,5 +71,57 @@ def test_pool_budget(gpu_ctx):
         assert e.value.status == 2          # TF_ERR_OOM: larger than the budget
         assert p.wait(r_small)["niter"] > 0
         assert p.stats()["rejected"] == 1
+    finally:
+        p.close()
+
+
+def test_pool_reuses_resident_structures(gpu_ctx):
+    """Requests on the same Matrix_Type arrays run on the held registration
+    (no re-registration) and give the single-solve results every time, also
+    with fresh right-hand sides."""
+    s = systems.small_hex(20, seed=7, kind="pressure", ratio=1.03)
+    rhs = [systems.uniform_rhs(s.n, 100 + k, zero_mean=True) for k in range(6)]
+    refs = []
+    for b in rhs:
+        t = copy.copy(s)
+        t.b = b
+        refs.append(_reference(gpu_ctx, t))
+    p = pool.Pool(workers=2, mem_budget=1 << 30)
+    try:
+        for rounds in range(2):
+            rids = [p.submit(s, b=b) for b in rhs]
+            for rid, (x, it, res) in zip(rids, refs):
+                r = p.wait(rid)
+                assert r["niter"] == it and r["fin_res"] == res
+                assert np.array_equal(r["x"], x)
+        res_info = p.resident()
+        assert res_info["held"] >= 1 and res_info["reused"] >= 2 * len(rhs) - 2
+        assert res_info["held_bytes"] <= 1 << 30
+    finally:
+        p.close()
+
+
+def test_pool_releases_held_structures_for_new_requests(gpu_ctx):
+    """Held registrations give way (least recently used first) when a new
+    request needs the budget."""
+    sysl = [systems.small_hex(16 + k, seed=k, kind="pressure") for k in range(4)]
+    refs = [_reference(gpu_ctx, s) for s in sysl]
+    # room for about two of these systems at a time
+    probe = pool.Pool(workers=1, mem_budget=1 << 30)
+    try:
+        probe.wait(probe.submit(sysl[-1]))
+        one = probe.stats()["peak_bytes"]
+    finally:
+        probe.close()
+    budget = int(2.5 * one)
+    p = pool.Pool(workers=1, mem_budget=budget)
+    try:
+        for rounds in range(2):
+            for s, (x, it, res) in zip(sysl, refs):
+                r = p.wait(p.submit(s))
+                assert r["niter"] == it and np.array_equal(r["x"], x)
+        info = p.resident()
+        assert info["held_bytes"] <= budget and info["held"] <= 2
+        assert p.stats()["peak_bytes"] <= budget
     finally:
         p.close()
