@@ -80,37 +80,47 @@ int bfs_far(const std::vector<int>& row0, const std::vector<int>& col0, int s,
 
 // Reverse Cuthill-McKee order (new -> old) of the graph of a CSR pattern
 // (0-based), component by component, each started from a pseudo-peripheral
-// node; neighbours are visited in increasing degree.
+// node (the lowest-degree node of the last level of a sweep from the
+// component's first node); neighbours are visited in increasing degree,
+// ties by index.
 void tf_rcm_order(const std::vector<int>& row0, const std::vector<int>& col0, int n,
                   std::vector<int>& order) {
   order.clear();
   order.reserve(n);
-  std::vector<int> stamp(n, -1), queue, nb;
+  std::vector<int> stamp(n, -1), queue;
   std::vector<char> placed(n, 0);
-  auto deg = [&](int u) { return row0[u + 1] - row0[u]; };
   int pass = 0;
   for (int seed = 0; seed < n; ++seed) {
     if (placed[seed]) continue;
-    // pseudo-peripheral start: two sweeps of "farthest, then lowest degree"
-    int d0 = 0, d1 = 0;
-    int s = bfs_far(row0, col0, seed, stamp, pass++, queue, d0);
-    int t = bfs_far(row0, col0, s, stamp, pass++, queue, d1);
-    if (d1 > d0) s = t;
+    int depth = 0;
+    const int s = bfs_far(row0, col0, seed, stamp, pass++, queue, depth);
     const size_t begin = order.size();
     order.push_back(s);
     placed[s] = 1;
     for (size_t head = begin; head < order.size(); ++head) {
       const int u = order[head];
-      nb.clear();
+      const size_t first = order.size();
       for (int j = row0[u]; j < row0[u + 1]; ++j) {
         const int v = col0[j];
         if (!placed[v]) {
           placed[v] = 1;
-          nb.push_back(v);
+          order.push_back(v);
         }
       }
-      std::stable_sort(nb.begin(), nb.end(), [&](int a, int b) { return deg(a) < deg(b); });
-      order.insert(order.end(), nb.begin(), nb.end());
+      // insertion sort of the few new neighbours by (degree, index)
+      for (size_t a = first + 1; a < order.size(); ++a) {
+        const int v = order[a];
+        const int dv = row0[v + 1] - row0[v];
+        size_t b = a;
+        while (b > first) {
+          const int w = order[b - 1];
+          const int dw = row0[w + 1] - row0[w];
+          if (dw < dv || (dw == dv && w < v)) break;
+          order[b] = w;
+          --b;
+        }
+        order[b] = v;
+      }
     }
   }
   std::reverse(order.begin(), order.end());
