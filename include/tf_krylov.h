@@ -244,6 +244,33 @@ int tf_pool_destroy(tf_pool p);
  *  entries; val has nnz entries.  Each call is asynchronous on ctx's stream;
  *  tf_ctx_sync waits for it.
  * ------------------------------------------------------------------------- */
+/* Device-side assembly through Matrix_Type's pos map (no counterpart in the
+ * C ABI of the reference: replaces the host face loops that fill A % val).
+ *
+ * tf_faces_register: the face topology of a registered matrix, once:
+ *   faces_c[2*s], faces_c[2*s+1] = c1, c2 of face s (1-based; c2 <= 0 on a
+ *   boundary face, Grid % faces_c), pos[2*s], pos[2*s+1] = the 1-based
+ *   entries of (c1, c2) and (c2, c1) (Create_Matrix.f90:124-139).
+ * tf_assemble_pressure: d_val (device, nnz) = the pressure-correction
+ *   matrix of Rhie_And_Chow.f90:183-205 (a12 = fc (fs v_m(c1) + (1 - fs)
+ *   v_m(c2)); off-diagonals -a12, diagonals sum a12 in face order) plus
+ *   Compute_Pressure.f90:140-160's boundary faces flagged in d_bnd_open
+ *   (fc v_m(c1) added to the diagonal; may be NULL).  d_fc, d_fw per face,
+ *   d_vm per cell (NULL: 1).
+ * tf_assemble_momentum: d_val = the upwind-blended momentum matrix of
+ *   Compute_Momentum.f90:270-297 (m0 = vis fc, m12 = m0 - min(F,0) rho,
+ *   m21 = m0 + max(F,0) rho; wall faces flagged in d_bnd_wall add m12 to
+ *   the diagonal) plus Inertial_Term.f90's rho vol / dt.
+ * Both zero d_val first and give the reference's face loops' values bit for
+ * bit; they run on the context's stream (d_val is then ready for
+ * tf_solve_device on the same stream). */
+int tf_faces_register(tf_ctx ctx, tf_matrix m, int n_faces, const int* faces_c, const int* pos);
+int tf_assemble_pressure(tf_ctx ctx, tf_matrix m, const double* d_fc, const double* d_fw,
+                         const double* d_vm, const int* d_bnd_open, double* d_val);
+int tf_assemble_momentum(tf_ctx ctx, tf_matrix m, const double* d_fc, const double* d_flux,
+                         const int* d_bnd_wall, double vis, double rho, const double* d_vol,
+                         double dt, double* d_val);
+
 /* q = A p over rows 1..n_own, in the row order and summation order of
  * Cg.f90:177-185.  If pq != NULL, *pq (device) receives sum_i p_i q_i. */
 int tf_spmv(tf_ctx ctx, tf_matrix m, const double* d_val, const double* d_p,

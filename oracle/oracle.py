@@ -156,12 +156,12 @@ def face_coef(grid):
     return out
 
 
-def assemble_pressure(grid, pos, dia, nnz, fc, bnd_open=None):
+def assemble_pressure(grid, pos, dia, nnz, fc, bnd_open=None, v_m=None):
     L = load()
     val = np.zeros(nnz)
     fcs = np.ascontiguousarray(grid.faces_c, dtype=np.int32)
     bo = None if bnd_open is None else _i(bnd_open.astype(np.int32))
-    vm = np.ones(grid.n_cells)
+    vm = np.ones(grid.n_cells) if v_m is None else _d(v_m)
     L.tfo_assemble_pressure(grid.n_faces, ip(fcs), ip(_i(dia)), ip(_i(pos)), dp(_d(fc)),
                             dp(_d(grid.fw)), dp(vm), ip(bo) if bo is not None else None,
                             dp(val))

@@ -96,6 +96,14 @@ struct tf_matrix_s {
   int* d_perm = nullptr;
   int* d_src = nullptr;
   tf_matrix_s* active = nullptr;  // the matrix the last solve ran on
+  // Face topology for device-side assembly (tf_assemble.cu): per face the
+  // two cells (0-based, -1 on a boundary) and pos(1:2) (0-based entries),
+  // per cell its faces in ascending order (bit 0: the cell is the face's c2).
+  int n_faces = 0;
+  int* d_face_cell = nullptr;
+  int* d_face_pos = nullptr;
+  int* d_cf_ptr = nullptr;
+  int* d_cf = nullptr;
 };
 
 // FP64 drop-in entry points implemented in tf_fp64.cu

@@ -32,6 +32,7 @@ EXPORTS = [
     "tf_host_pin", "tf_host_unpin", "tf_spmv", "tf_residual", "tf_nrms",
     "tf_ctx_sync", "tf_ctx_stream", "tf_last_error_message", "tf_matrix_tile_config",
     "tf_matrix_row_patterns", "tf_matrix_renumbered",
+    "tf_faces_register", "tf_assemble_pressure", "tf_assemble_momentum",
 ]
 
 
@@ -93,6 +94,10 @@ def load(path=LIB_PATH):
     L.tf_host_pin.argtypes = [_vp, ctypes.c_size_t]
     L.tf_host_unpin.argtypes = [_vp]
     L.tf_spmv.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
+    L.tf_faces_register.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
+    L.tf_assemble_pressure.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.tf_assemble_momentum.argtypes = [_vp, _vp, _vp, _vp, _vp, ctypes.c_double,
+                                       ctypes.c_double, _vp, ctypes.c_double, _vp]
     L.tf_residual.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
     L.tf_nrms.argtypes = [_vp, _vp, _vp, _vp, _vp, _c_dbl_p, _vp]
     _lib = L
@@ -226,6 +231,27 @@ def solve_device(ctx, mat, solver, prec, d_val, d_x, d_b, miter, tol, norm=None)
                                   int(miter), ctypes.byref(niter), float(tol),
                                   ctypes.byref(res), _norm_arg(norm)), "tf_solve_device")
     return niter.value, res.value
+
+
+def faces_register(ctx, mat, faces_c, pos):
+    """Face topology for device-side assembly: faces_c and pos are
+    (n_faces, 2) 1-based arrays as Grid % faces_c and Matrix_Type % pos."""
+    fcs = np.ascontiguousarray(faces_c, dtype=np.int32)
+    ps = np.ascontiguousarray(pos, dtype=np.int32)
+    _check(load().tf_faces_register(ctx.h, mat.h, len(fcs), fcs.ctypes.data_as(_vp),
+                                    ps.ctypes.data_as(_vp)), "tf_faces_register")
+
+
+def assemble_pressure(ctx, mat, d_fc, d_fw, d_vm, d_bnd_open, d_val):
+    """Device pointers (ints); d_vm / d_bnd_open may be 0 (all ones / none)."""
+    _check(load().tf_assemble_pressure(ctx.h, mat.h, d_fc, d_fw, d_vm or None,
+                                       d_bnd_open or None, d_val), "tf_assemble_pressure")
+
+
+def assemble_momentum(ctx, mat, d_fc, d_flux, d_bnd_wall, vis, rho, d_vol, dt, d_val):
+    _check(load().tf_assemble_momentum(ctx.h, mat.h, d_fc, d_flux, d_bnd_wall or None,
+                                       float(vis), float(rho), d_vol, float(dt), d_val),
+           "tf_assemble_momentum")
 
 
 def spmv(ctx, mat, d_val, d_p, d_q, d_pq=None):
