@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--rcm", action="store_true",
                     help="spmv: renumber the cells by reverse Cuthill-McKee first")
     ap.add_argument("--mode", default="solve",
-                    choices=["solve", "spmv", "iters", "batched", "served"],
+                    choices=["solve", "spmv", "iters", "multi", "batched", "served"],
                     help="spmv: only the pressure matrix and `--steps` SpMV launches "
                          "(the small case profiled with ncu); iters: `--steps` Cg solves "
                          "of exactly `--iters` iterations on the pressure matrix (launch "
@@ -458,6 +458,63 @@ def run_fixed_iterations(args):
     ctx.close()
 
 
+def run_multi_rhs(args):
+    """Three velocity components with one momentum matrix (the bench's
+    200^3 Bicg system, three seeded right-hand sides): one tf_solve_multi
+    against three tf_solve_device calls, CUDA events, inputs in HBM."""
+    import torch
+    from tflows_b200 import native, systems
+    msys = make_workload(args.size, args.peclet)[1]
+    ctx = native.Context(0)
+    m = native.Matrix(ctx, msys.csr.row, msys.csr.col, msys.csr.dia)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    n = msys.n
+    B = np.stack([systems.uniform_rhs(n, 40 + k, zero_mean=False) for k in range(3)])
+    val0 = torch.from_numpy(msys.val).cuda()
+    B0 = torch.from_numpy(np.ascontiguousarray(B)).cuda()
+    val, Bd = val0.clone(), B0.clone()
+    X = torch.zeros((3, n), dtype=torch.float64, device="cuda")
+    tol, miter, norm = msys.tol, msys.miter, msys.norm
+
+    def timed(fn):
+        val.copy_(val0)
+        Bd.copy_(B0)
+        X.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        its = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), its
+
+    def multi():
+        return native.solve_multi_device(ctx, m, "bicg", "jacobi", 3, val.data_ptr(),
+                                         X.data_ptr(), Bd.data_ptr(), miter, tol, norm)[0]
+
+    def singles():
+        its = []
+        for k in range(3):
+            it, _ = native.solve_device(ctx, m, "bicg", "jacobi", val.data_ptr(),
+                                        X[k].data_ptr(), Bd[k].data_ptr(), miter, tol, norm)
+            its.append(it)
+        return its
+
+    for _ in range(2):
+        timed(multi)
+        timed(singles)
+    tm, im = min(timed(multi) for _ in range(args.steps))
+    ts, is_ = min(timed(singles) for _ in range(args.steps))
+    cells = n * sum(im)
+    print(json.dumps({"mode": "multi", "n": n, "nnz": msys.nnz, "rhs": 3,
+                      "iters_multi": im, "iters_single": is_,
+                      "ms_multi": tm, "ms_three_singles": ts, "speedup": ts / tm,
+                      "mcell_iters_per_s_multi": cells / tm / 1e3,
+                      "mcell_iters_per_s_singles": n * sum(is_) / ts / 1e3}), flush=True)
+    m.close()
+    ctx.close()
+
+
 def dist_env():
     from tflows_b200.replicas import dist_env as env
     return env()
@@ -629,6 +686,9 @@ def main():
         return
     if args.mode == "iters":
         run_fixed_iterations(args)
+        return
+    if args.mode == "multi":
+        run_multi_rhs(args)
         return
     if args.mode == "batched":
         run_batched(args)

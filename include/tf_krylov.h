@@ -125,6 +125,23 @@ int tf_solve_device(tf_ctx ctx, tf_matrix m, int solver, int prec,
                     int* niter, double tol, double* fin_res,
                     const double* norm);
 
+/* Several right-hand sides with one matrix: nrhs (1..4) solves of
+ * Solve_Native's kind (Jacobi or none; Bicg = Cg as in tf_solve) on the same
+ * val, x and b holding nrhs vectors of n_cells doubles one after another
+ * (the velocity components of Compute_Momentum.f90:153-399 when their
+ * matrices are equal).  Each right-hand side runs its own recurrence --
+ * niter[i], fin_res[i], x_i and b_i are those of tf_solve on (val, x_i,
+ * b_i), bit for bit on row-pattern matrices (on other matrices to the
+ * rounding of the dot products) -- while one SpMV per iteration reads the
+ * matrix once for all of them.  val is scaled and returned once.  ICC is
+ * not offered here (TF_ERR_ARG).  No reference counterpart. */
+int tf_solve_multi(tf_ctx ctx, tf_matrix m, int solver, int prec, int nrhs,
+                   double* val, double* x, double* b, int miter, int* niter,
+                   double tol, double* fin_res, const double* norm);
+int tf_solve_multi_device(tf_ctx ctx, tf_matrix m, int solver, int prec, int nrhs,
+                          double* d_val, double* d_x, double* d_b, int miter,
+                          int* niter, double tol, double* fin_res, const double* norm);
+
 /* Per-iteration residual history of the last solve on ctx: hist[0] is the
  * residual before the loop, hist[k] after iteration k, for k <= niter.
  * Enabled by tf_ctx_set_history(ctx, 1) (off by default: it costs nothing

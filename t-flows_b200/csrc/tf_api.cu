@@ -164,6 +164,7 @@ void tf_matrix_free(tf_matrix_s* m) {
   tf_matrix_free(m->ren);
   for (auto& g : m->graph)
     if (g) cudaGraphExecDestroy(g);
+  tf_slices_free(m);
   void* ptrs[] = {m->d_row, m->d_col, m->d_dia, m->d_val, m->d_x, m->d_b,
                   m->d_r, m->d_p, m->d_q, m->d_z, m->d_adiag, m->d_part,
                   m->d_hist, m->d_state, m->d_params, m->d_levf_rows, m->d_levb_rows,
@@ -647,6 +648,141 @@ extern "C" int tf_solve_device(tf_ctx ctx, tf_matrix m, int solver, int prec,
   TF_CUDA_TRY(cudaMemcpyAsync(d_x, m->d_x, nb, cudaMemcpyDeviceToDevice, s));
   TF_CUDA_TRY(cudaMemcpyAsync(d_b, m->d_b, nb, cudaMemcpyDeviceToDevice, s));
   return finish_solve(m, niter, fin_res);
+}
+
+// ---------------------------------------------------------------------------
+// Multi-RHS solves
+// ---------------------------------------------------------------------------
+namespace {
+
+// Device pointers of right-hand side i's x and b inside the workspace.
+double* rhs_x(tf_matrix_s* m, int i) { return i == 0 ? m->d_x : m->slices[i - 1]->d_x; }
+double* rhs_b(tf_matrix_s* m, int i) { return i == 0 ? m->d_b : m->slices[i - 1]->d_b; }
+const tf::SolveState* rhs_state(tf_matrix_s* m, int i) {
+  return i == 0 ? m->d_state : m->slices[i - 1]->d_state;
+}
+
+// Runs the multi-RHS graph on the workspace (val, x_i, b_i already there)
+// and fetches the states; the caller copies results and synchronises.
+int run_multi_core(tf_matrix_s* m, int prec, int nrhs, int miter, double tol,
+                   const double* norm) {
+  tf_ctx_s* c = m->ctx;
+  tf::SolveParams* hp = m->h_params;
+  hp->tol = tol;
+  hp->norm = norm ? *norm : 0.0;
+  hp->has_norm = norm ? 1 : 0;
+  hp->miter = miter;
+  hp->hist = nullptr;
+  hp->hist_cap = 0;
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_params, hp, sizeof(*hp), cudaMemcpyHostToDevice, c->stream));
+  int st = tf_fp64_run_multi(m, prec, nrhs);
+  if (st != TF_OK) return st;
+  if (!m->h_mstate) {
+    cudaError_t e = cudaMallocHost((void**)&m->h_mstate, kMaxRhs * sizeof(tf::SolveState));
+    if (e != cudaSuccess) {
+      tf_set_last_cuda_error(e, "cudaMallocHost", __FILE__, __LINE__);
+      return TF_ERR_OOM;
+    }
+  }
+  for (int i = 0; i < nrhs; ++i)
+    TF_CUDA_TRY(cudaMemcpyAsync(m->h_mstate + i, rhs_state(m, i), sizeof(tf::SolveState),
+                                cudaMemcpyDeviceToHost, c->stream));
+  return TF_OK;
+}
+
+int finish_multi(tf_matrix_s* m, int nrhs, int* niter, double* fin_res) {
+  TF_CUDA_TRY(cudaStreamSynchronize(m->ctx->stream));
+  for (int i = 0; i < nrhs; ++i)
+    if (m->h_mstate[i].status != 0) return m->h_mstate[i].status;
+  for (int i = 0; i < nrhs; ++i) {
+    niter[i] = m->h_mstate[i].niter;
+    fin_res[i] = m->h_mstate[i].res;
+  }
+  return TF_OK;
+}
+
+int check_multi_args(tf_ctx ctx, tf_matrix m, int solver, int prec, int nrhs, int* niter,
+                     double* fin_res) {
+  int st = check_solve_args(ctx, m, solver, prec, niter, fin_res);
+  if (st != TF_OK) return st;
+  if (nrhs < 1 || nrhs > kMaxRhs || prec == TF_PREC_ICC) return TF_ERR_ARG;
+  return TF_OK;
+}
+
+}  // namespace
+
+extern "C" int tf_solve_multi(tf_ctx ctx, tf_matrix m, int solver, int prec, int nrhs,
+                              double* val, double* x, double* b, int miter, int* niter,
+                              double tol, double* fin_res, const double* norm) {
+  int st = check_multi_args(ctx, m, solver, prec, nrhs, niter, fin_res);
+  if (st != TF_OK) return st;
+  if (m->nt == 0) {
+    for (int i = 0; i < nrhs; ++i) niter[i] = 0, fin_res[i] = 0.0;
+    return TF_OK;
+  }
+  if (!val || !x || !b) return TF_ERR_ARG;
+  std::lock_guard<std::mutex> lk(m->mu);
+  TF_CUDA_TRY(cudaSetDevice(ctx->device));
+  st = tf_slices_ensure(m, nrhs);
+  if (st != TF_OK) return st;
+  cudaStream_t s = ctx->stream;
+  const size_t vb = (size_t)m->nnz * sizeof(double), nb = (size_t)m->nt * sizeof(double);
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_val, val, vb, cudaMemcpyHostToDevice, s));
+  for (int i = 0; i < nrhs; ++i) {
+    TF_CUDA_TRY(cudaMemcpyAsync(rhs_x(m, i), x + (size_t)i * m->nt, nb,
+                                cudaMemcpyHostToDevice, s));
+    TF_CUDA_TRY(cudaMemcpyAsync(rhs_b(m, i), b + (size_t)i * m->nt, nb,
+                                cudaMemcpyHostToDevice, s));
+  }
+  st = run_multi_core(m, prec, nrhs, miter, tol, norm);
+  if (st != TF_OK) {
+    cudaStreamSynchronize(s);
+    return st;
+  }
+  TF_CUDA_TRY(cudaMemcpyAsync(val, m->d_val, vb, cudaMemcpyDeviceToHost, s));
+  for (int i = 0; i < nrhs; ++i) {
+    TF_CUDA_TRY(cudaMemcpyAsync(x + (size_t)i * m->nt, rhs_x(m, i), nb,
+                                cudaMemcpyDeviceToHost, s));
+    TF_CUDA_TRY(cudaMemcpyAsync(b + (size_t)i * m->nt, rhs_b(m, i), nb,
+                                cudaMemcpyDeviceToHost, s));
+  }
+  return finish_multi(m, nrhs, niter, fin_res);
+}
+
+extern "C" int tf_solve_multi_device(tf_ctx ctx, tf_matrix m, int solver, int prec, int nrhs,
+                                     double* d_val, double* d_x, double* d_b, int miter,
+                                     int* niter, double tol, double* fin_res,
+                                     const double* norm) {
+  int st = check_multi_args(ctx, m, solver, prec, nrhs, niter, fin_res);
+  if (st != TF_OK) return st;
+  if (m->nt == 0) {
+    for (int i = 0; i < nrhs; ++i) niter[i] = 0, fin_res[i] = 0.0;
+    return TF_OK;
+  }
+  if (!d_val || !d_x || !d_b) return TF_ERR_ARG;
+  std::lock_guard<std::mutex> lk(m->mu);
+  TF_CUDA_TRY(cudaSetDevice(ctx->device));
+  st = tf_slices_ensure(m, nrhs);
+  if (st != TF_OK) return st;
+  cudaStream_t s = ctx->stream;
+  const size_t vb = (size_t)m->nnz * sizeof(double), nb = (size_t)m->nt * sizeof(double);
+  const cudaMemcpyKind dd = cudaMemcpyDeviceToDevice;
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_val, d_val, vb, dd, s));
+  for (int i = 0; i < nrhs; ++i) {
+    TF_CUDA_TRY(cudaMemcpyAsync(rhs_x(m, i), d_x + (size_t)i * m->nt, nb, dd, s));
+    TF_CUDA_TRY(cudaMemcpyAsync(rhs_b(m, i), d_b + (size_t)i * m->nt, nb, dd, s));
+  }
+  st = run_multi_core(m, prec, nrhs, miter, tol, norm);
+  if (st != TF_OK) {
+    cudaStreamSynchronize(s);
+    return st;
+  }
+  TF_CUDA_TRY(cudaMemcpyAsync(d_val, m->d_val, vb, dd, s));
+  for (int i = 0; i < nrhs; ++i) {
+    TF_CUDA_TRY(cudaMemcpyAsync(d_x + (size_t)i * m->nt, rhs_x(m, i), nb, dd, s));
+    TF_CUDA_TRY(cudaMemcpyAsync(d_b + (size_t)i * m->nt, rhs_b(m, i), nb, dd, s));
+  }
+  return finish_multi(m, nrhs, niter, fin_res);
 }
 
 namespace {

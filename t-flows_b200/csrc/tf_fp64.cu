@@ -1102,3 +1102,332 @@ int tf_fp64_nrms(tf_matrix_s* m, const double* val, const double* r,
                               m->ctx->stream));
   return TF_OK;
 }
+
+// ===========================================================================
+// Multi-RHS solves: nrhs right-hand sides with one matrix (the three
+// velocity components of Compute_Momentum.f90:153-399 when their matrices
+// are equal).  Right-hand side 0 uses the matrix's own workspace, the others
+// a slice each (tf_slice_s).  Every right-hand side runs its own Cg/Bicg
+// recurrence with the single-RHS kernels -- same arithmetic, same
+// reduction order, so each result is bit-identical to its own solve -- and
+// one SpMV per iteration reads the matrix once for all of them.  The loop
+// ends when every right-hand side is done (k_multi_cond).
+// ===========================================================================
+namespace tf {
+
+struct MultiArgs {
+  SpArgs sa;                   // the matrix (structure, values, patterns)
+  int nr;
+  const double* p[kMaxRhs];
+  double* q[kMaxRhs];
+  SolveState* st[kMaxRhs];
+  double* part[kMaxRhs];
+};
+
+struct MultiCond {
+  SolveState* st[kMaxRhs];
+  int nr;
+  cudaGraphConditionalHandle cond;
+};
+
+// q_r = A p_r for every active right-hand side r < NR; row sums in storage
+// order, entries taken kMultiChunk at a time (the NR gathers of a group in
+// flight together; small enough for two CTAs per SM).
+constexpr int kMultiChunk = 2;
+template <int NR>
+struct OpSpmvMulti {
+  const double* p[NR];
+  double* q[NR];
+  double pq[NR];
+  unsigned act;
+  template <class VAL, class COL>
+  __device__ __forceinline__ void body(int i, VAL v, COL col, int len) {
+    double acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+#pragma unroll 1
+    for (int k0 = 0; k0 < len; k0 += kMultiChunk) {
+      double vv[kMultiChunk];
+      int cc[kMultiChunk];
+#pragma unroll
+      for (int u = 0; u < kMultiChunk; ++u)
+        if (k0 + u < len) {
+          vv[u] = v(k0 + u);
+          cc[u] = col(k0 + u);
+        }
+      double pv[NR][kMultiChunk];
+#pragma unroll
+      for (int r = 0; r < NR; ++r)
+#pragma unroll
+        for (int u = 0; u < kMultiChunk; ++u)
+          if (((act >> r) & 1u) && k0 + u < len) pv[r][u] = __ldg(p[r] + cc[u]);
+#pragma unroll
+      for (int r = 0; r < NR; ++r)
+#pragma unroll
+        for (int u = 0; u < kMultiChunk; ++u)
+          if (((act >> r) & 1u) && k0 + u < len)
+            acc[r] = __dadd_rn(acc[r], __dmul_rn(vv[u], pv[r][u]));
+    }
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      if (!((act >> r) & 1u)) continue;
+      q[r][i] = acc[r];
+      pq[r] = __dadd_rn(pq[r], __dmul_rn(__ldg(p[r] + i), acc[r]));
+    }
+  }
+  __device__ __forceinline__ void operator()(int i, const double* v, const int* c, int len) {
+    body(i, [v](int k) { return v[k]; }, [c](int k) { return c[k]; }, len);
+  }
+  __device__ __forceinline__ void pat(int i, const double* v, const int* o, int len) {
+    body(i, [v](int k) { return v[k]; }, [i, o](int k) { return i + o[k]; }, len);
+  }
+};
+
+// One SpMV for all active right-hand sides: on row-pattern tiles with the
+// single-RHS kernel's tiles and grid (so each p.q is reduced exactly as in
+// its own solve), otherwise one thread per row straight from global memory.
+// Two CTAs per SM, as the single-RHS kernel.
+template <int CFG, int PAT, int NR>
+__global__ void __launch_bounds__(cfg_threads<CFG, PAT>(), 2) k_spmv_multi(MultiArgs a) {
+  __shared__ double scratch[32];
+  unsigned act = 0;
+  for (int r = 0; r < NR; ++r)
+    if (!a.st[r]->done) act |= 1u << r;
+  if (!act) return;
+  OpSpmvMulti<NR> op;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    op.p[r] = a.p[r];
+    op.q[r] = a.q[r];
+    op.pq[r] = 0.0;
+  }
+  op.act = act;
+  bool ok = true;
+  if constexpr (CFG != kTileNone && PAT != 0) {
+    ok = stream_tiles_pat<kTileRows[CFG], kTileNnzCap[CFG], kPatStages>(a.sa.row, a.sa.pt,
+                                                                        a.sa.val, a.sa.nrows, op);
+  } else {
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.sa.nrows; i += stride) {
+      const int js = a.sa.row[i], je = a.sa.row[i + 1];
+      op(i, a.sa.val + js, a.sa.col + js, je - js);
+    }
+  }
+  if (!ok && threadIdx.x == 0)
+    for (int r = 0; r < NR; ++r) flag_timeout(a.st[r]);
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    if (!((act >> r) & 1u)) continue;   // the same for every CTA
+    double v[1] = {block_red<kSum>(op.pq[r], scratch)};
+    const int ops[1] = {kSum};
+    if (grid_reduce_last<1>(v, ops, a.part[r], &a.st[r]->counter[kCntSpmv], scratch) &&
+        threadIdx.x == 0) {
+      a.st[r]->pq = v[0];
+      a.st[r]->alpha = __ddiv_rn(a.st[r]->rho, v[0]);
+    }
+  }
+}
+
+// The loop goes on while any right-hand side is not done.
+__global__ void k_multi_cond(MultiCond c) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  unsigned any = 0;
+  for (int r = 0; r < c.nr; ++r) any |= c.st[r]->done ? 0u : 1u;
+  cudaGraphSetConditional(c.cond, any);
+}
+
+}  // namespace tf
+
+namespace {
+
+VecArgs slice_vec_args(tf_matrix_s* m, int i) {
+  VecArgs a = make_vec_args(m);
+  if (i > 0) {
+    tf_slice_s* s = m->slices[i - 1];
+    a.x = s->d_x;
+    a.b = s->d_b;
+    a.r = s->d_r;
+    a.p = s->d_p;
+    a.q = s->d_q;
+    a.z = nullptr;
+    a.adiag = s->d_adiag;
+    a.part = s->d_part;
+    a.st = s->d_state;
+    a.nnz = 0;   // val is scaled and unscaled once, by right-hand side 0
+  }
+  return a;
+}
+
+template <int CFG, int PAT, int PREC>
+int build_multi_graph_t(tf_matrix_s* m, int nr, int xdef, cudaGraphExec_t* out) {
+  int st = set_attrs_cfg<CFG, PREC, PAT>();
+  if (st != TF_OK) return st;
+  const void* kmulti = nr == 1   ? (const void*)k_spmv_multi<CFG, PAT, 1>
+                       : nr == 2 ? (const void*)k_spmv_multi<CFG, PAT, 2>
+                       : nr == 3 ? (const void*)k_spmv_multi<CFG, PAT, 3>
+                                 : (const void*)k_spmv_multi<CFG, PAT, 4>;
+  if (cfg_smem<CFG, PAT>() > 48 * 1024 && PAT)
+    TF_CUDA_TRY(cudaFuncSetAttribute(kmulti, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)cfg_smem<CFG, PAT>()));
+  cudaGraph_t g = nullptr;
+  TF_CUDA_TRY(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h = 0;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    TF_CUDA_TRY(e);
+  }
+  VecArgs va[kMaxRhs];
+  SpArgs sa[kMaxRhs];
+  MultiArgs ma{};
+  MultiCond mc{};
+  for (int i = 0; i < nr; ++i) {
+    va[i] = slice_vec_args(m, i);
+    sa[i] = make_sp_args(m, va[i]);
+    ma.p[i] = va[i].p;
+    ma.q[i] = va[i].q;
+    ma.st[i] = va[i].st;
+    ma.part[i] = va[i].part;
+    mc.st[i] = va[i].st;
+  }
+  ma.sa = sa[0];
+  ma.nr = nr;
+  mc.nr = nr;
+  mc.cond = h;
+  const dim3 vb(256), vg(m->vec_grid);
+  const dim3 sb(cfg_threads<CFG, PAT>()), sg(m->spmv_grid);
+  const size_t ssm = cfg_smem<CFG, PAT>();
+  const bool tiled_pat = CFG != kTileNone && PAT;
+  const dim3 mb = tiled_pat ? sb : dim3(256), mg = tiled_pat ? sg : vg;
+  const size_t msm = tiled_pat ? ssm : 0;
+  const IterFns fns = iter_fns<PREC>(xdef, m->vec_dir);
+  void* vargs[kMaxRhs][1];
+  void* sargs[kMaxRhs][1];
+  for (int i = 0; i < nr; ++i) {
+    vargs[i][0] = &va[i];
+    sargs[i][0] = &sa[i];
+  }
+  void* margs[] = {&ma};
+  void* cargs[] = {&mc};
+  NodeBuilder nb{g};
+  cudaGraphNode_t prev = nullptr;
+  for (int i = 0; i < nr; ++i) prev = nb.add((const void*)k_diag, vg, vb, 0, vargs[i], prev);
+  for (int i = 0; i < nr; ++i) prev = nb.add((const void*)k_scale, vg, vb, 0, vargs[i], prev);
+  for (int i = 0; i < nr; ++i)
+    prev = nb.add((const void*)k_residual<CFG, PREC, PAT>, sg, sb, ssm, sargs[i], prev);
+  prev = nb.add((const void*)k_multi_cond, dim3(1), dim3(32), 0, cargs, prev);
+  cudaGraphNode_t cnode = nullptr;
+  if (nb.status == TF_OK) {
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&cnode, g, &prev, 1, &cp);
+    if (e != cudaSuccess) {
+      tf_set_last_cuda_error(e, "cudaGraphAddNode(conditional)", __FILE__, __LINE__);
+      nb.status = TF_ERR_CUDA;
+    } else {
+      NodeBuilder body{cp.conditional.phGraph_out[0]};
+      cudaGraphNode_t b = nullptr;
+      for (int i = 0; i < nr; ++i) b = body.add(fns.pupdate, vg, vb, 0, vargs[i], b);
+      b = body.add(kmulti, mg, mb, msm, margs, b);
+      for (int i = 0; i < nr; ++i) b = body.add(fns.update, vg, vb, 0, vargs[i], b);
+      body.add((const void*)k_multi_cond, dim3(1), dim3(32), 0, cargs, b);
+      if (body.status != TF_OK) nb.status = body.status;
+    }
+  }
+  prev = cnode;
+  for (int i = 0; i < nr; ++i) prev = nb.add((const void*)k_unscale, vg, vb, 0, vargs[i], prev);
+  if (nb.status != TF_OK) {
+    cudaGraphDestroy(g);
+    return nb.status;
+  }
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  TF_CUDA_TRY(e);
+  return TF_OK;
+}
+
+template <int PREC>
+int build_multi_graph_p(tf_matrix_s* m, int nr, int xdef, cudaGraphExec_t* out) {
+  const bool pat = m->npat > 0;
+  switch (m->tile_cfg) {
+    case kTile512:
+      return pat ? build_multi_graph_t<kTile512, 1, PREC>(m, nr, xdef, out)
+                 : build_multi_graph_t<kTile512, 0, PREC>(m, nr, xdef, out);
+    case kTile256:
+      return pat ? build_multi_graph_t<kTile256, 1, PREC>(m, nr, xdef, out)
+                 : build_multi_graph_t<kTile256, 0, PREC>(m, nr, xdef, out);
+    case kTile128:
+      return pat ? build_multi_graph_t<kTile128, 1, PREC>(m, nr, xdef, out)
+                 : build_multi_graph_t<kTile128, 0, PREC>(m, nr, xdef, out);
+    default: return build_multi_graph_t<kTileNone, 0, PREC>(m, nr, xdef, out);
+  }
+}
+
+int alloc_slice(tf_matrix_s* m, tf_slice_s** out) {
+  auto* s = new tf_slice_s();
+  const size_t nv = ((size_t)m->nt + 8) * sizeof(double);
+  int st = TF_OK;
+  for (double** p : {&s->d_x, &s->d_b, &s->d_r, &s->d_p, &s->d_q, &s->d_adiag})
+    if (st == TF_OK) st = tf_dev_alloc_bytes(m->ctx, (void**)p, nv);
+  if (st == TF_OK)
+    st = tf_dev_alloc_bytes(m->ctx, (void**)&s->d_part,
+                            ((size_t)8 * kMaxBlocks + 16) * sizeof(double));
+  if (st == TF_OK) st = tf_dev_alloc_bytes(m->ctx, (void**)&s->d_state, sizeof(SolveState));
+  *out = s;
+  return st;
+}
+
+}  // namespace
+
+void tf_slices_free(tf_matrix_s* m) {
+  for (auto& s : m->slices) {
+    if (!s) continue;
+    for (void* p : {(void*)s->d_x, (void*)s->d_b, (void*)s->d_r, (void*)s->d_p, (void*)s->d_q,
+                    (void*)s->d_adiag, (void*)s->d_part, (void*)s->d_state})
+      if (p) {
+        if (m->async_alloc) cudaFreeAsync(p, m->ctx->stream);
+        else cudaFree(p);
+      }
+    delete s;
+    s = nullptr;
+  }
+  for (auto& a : m->mgraph)
+    for (auto& b : a)
+      for (auto& g : b)
+        if (g) {
+          cudaGraphExecDestroy(g);
+          g = nullptr;
+        }
+  if (m->h_mstate) {
+    cudaFreeHost(m->h_mstate);
+    m->h_mstate = nullptr;
+  }
+}
+
+int tf_slices_ensure(tf_matrix_s* m, int nr) {
+  if (nr < 1 || nr > kMaxRhs) return TF_ERR_ARG;
+  for (int i = 0; i + 1 < nr; ++i)
+    if (!m->slices[i]) {
+      const int st = alloc_slice(m, &m->slices[i]);
+      if (st != TF_OK) return st;
+    }
+  return TF_OK;
+}
+
+int tf_fp64_run_multi(tf_matrix_s* m, int prec, int nr) {
+  if (nr < 1 || nr > kMaxRhs || (prec != kPrecJacobi && prec != kPrecNone)) return TF_ERR_ARG;
+  const int st0 = tf_slices_ensure(m, nr);
+  if (st0 != TF_OK) return st0;
+  const int xdef = m->h_params->has_norm ? 1 : 0;
+  cudaGraphExec_t& g = m->mgraph[nr][prec][xdef];
+  if (!g) {
+    const int st = prec == kPrecJacobi ? build_multi_graph_p<kPrecJacobi>(m, nr, xdef, &g)
+                                       : build_multi_graph_p<kPrecNone>(m, nr, xdef, &g);
+    if (st != TF_OK) return st;
+  }
+  TF_CUDA_TRY(cudaGraphLaunch(g, m->ctx->stream));
+  return TF_OK;
+}

@@ -40,6 +40,21 @@ struct tf_ctx_s {
   tf::SolveParams* h_params = nullptr;
 };
 
+// Right-hand sides 2..nrhs of a multi-RHS solve (tf_solve_multi): their own
+// Krylov vectors, reduction partials and solve state over the matrix's
+// structure and values.
+struct tf_slice_s {
+  double* d_x = nullptr;
+  double* d_b = nullptr;
+  double* d_r = nullptr;
+  double* d_p = nullptr;
+  double* d_q = nullptr;
+  double* d_adiag = nullptr;
+  double* d_part = nullptr;
+  tf::SolveState* d_state = nullptr;
+};
+constexpr int kMaxRhs = 4;
+
 // Device mirror of one Matrix_Type plus the Krylov workspace of its solves.
 struct tf_matrix_s {
   tf_ctx_s* ctx = nullptr;
@@ -104,7 +119,18 @@ struct tf_matrix_s {
   int* d_face_pos = nullptr;
   int* d_cf_ptr = nullptr;
   int* d_cf = nullptr;
+  // Multi-RHS solves: slices for right-hand sides 2..kMaxRhs (allocated on
+  // first use), pinned states of all right-hand sides, cached graphs per
+  // (rhs count, preconditioner, x update deferred).
+  tf_slice_s* slices[kMaxRhs - 1] = {nullptr, nullptr, nullptr};
+  tf::SolveState* h_mstate = nullptr;
+  cudaGraphExec_t mgraph[kMaxRhs + 1][2][2] = {};
 };
+// Multi-RHS drop-in (tf_fp64.cu): slice allocation and the solve on
+// device-resident val / x_i / b_i (x and b slices of nt doubles each).
+int tf_fp64_run_multi(tf_matrix_s* m, int prec, int nrhs);
+int tf_slices_ensure(tf_matrix_s* m, int nrhs);   // allocate slices 1..nrhs-1
+void tf_slices_free(tf_matrix_s* m);
 
 // FP64 drop-in entry points implemented in tf_fp64.cu
 int tf_fp64_prepare(tf_matrix_s* m);

@@ -33,6 +33,7 @@ EXPORTS = [
     "tf_ctx_sync", "tf_ctx_stream", "tf_last_error_message", "tf_matrix_tile_config",
     "tf_matrix_row_patterns", "tf_matrix_renumbered",
     "tf_faces_register", "tf_assemble_pressure", "tf_assemble_momentum",
+    "tf_solve_multi", "tf_solve_multi_device",
 ]
 
 
@@ -95,6 +96,9 @@ def load(path=LIB_PATH):
     L.tf_host_unpin.argtypes = [_vp]
     L.tf_spmv.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
     L.tf_faces_register.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
+    L.tf_solve_multi.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp,
+                                 _vp, ctypes.c_int, _vp, ctypes.c_double, _vp, _vp]
+    L.tf_solve_multi_device.argtypes = L.tf_solve_multi.argtypes
     L.tf_assemble_pressure.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.tf_assemble_momentum.argtypes = [_vp, _vp, _vp, _vp, _vp, ctypes.c_double,
                                        ctypes.c_double, _vp, ctypes.c_double, _vp]
@@ -231,6 +235,35 @@ def solve_device(ctx, mat, solver, prec, d_val, d_x, d_b, miter, tol, norm=None)
                                   int(miter), ctypes.byref(niter), float(tol),
                                   ctypes.byref(res), _norm_arg(norm)), "tf_solve_device")
     return niter.value, res.value
+
+
+def solve_multi(ctx, mat, solver, prec, val, X, B, miter, tol, norm=None):
+    """nrhs solves with one matrix: X, B are (nrhs, n_cells) float64 arrays
+    (updated in place like tf_solve's x and b); val is updated once.
+    Returns (niter list, fin_res list)."""
+    L = load()
+    nr = X.shape[0]
+    assert X.flags.c_contiguous and B.flags.c_contiguous and X.shape == B.shape
+    it = np.zeros(nr, np.int32)
+    res = np.zeros(nr)
+    nv = None if norm is None else ctypes.byref(ctypes.c_double(norm))
+    _check(L.tf_solve_multi(ctx.h, mat.h, SOLVERS[solver], PRECS[prec], nr,
+                            val.ctypes.data_as(_vp), X.ctypes.data_as(_vp),
+                            B.ctypes.data_as(_vp), int(miter), it.ctypes.data_as(_vp),
+                            float(tol), res.ctypes.data_as(_vp), nv), "tf_solve_multi")
+    return [int(v) for v in it], [float(v) for v in res]
+
+
+def solve_multi_device(ctx, mat, solver, prec, nrhs, d_val, d_x, d_b, miter, tol, norm=None):
+    """solve_multi on device pointers (d_x, d_b: nrhs * n_cells doubles)."""
+    L = load()
+    it = np.zeros(nrhs, np.int32)
+    res = np.zeros(nrhs)
+    nv = None if norm is None else ctypes.byref(ctypes.c_double(norm))
+    _check(L.tf_solve_multi_device(ctx.h, mat.h, SOLVERS[solver], PRECS[prec], nrhs, d_val,
+                                   d_x, d_b, int(miter), it.ctypes.data_as(_vp), float(tol),
+                                   res.ctypes.data_as(_vp), nv), "tf_solve_multi_device")
+    return [int(v) for v in it], [float(v) for v in res]
 
 
 def faces_register(ctx, mat, faces_c, pos):
