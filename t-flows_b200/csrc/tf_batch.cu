@@ -91,6 +91,8 @@ struct SysDev {
   double* tile_tot;     // ntiles * kPartQ: per-tile totals
   double* warp_part;    // ntiles * kWarps * kPartQ: per-warp partials (tile kernels)
   unsigned* tile_cnt;   // ntiles: warps of a tile that have reported
+  double* chunk_tot;    // n_chunks * kPartQ: per-chunk totals
+  unsigned* chunk_cnt;  // n_chunks: tiles of a chunk that have reported
   int n, ntiles;
   int maxit, use_val32;
   double tol;
@@ -136,18 +138,30 @@ __device__ __forceinline__ bool active(const SysState& s) { return s.status == k
 // Warp-level per-system reductions (no CTA barriers).
 // ---------------------------------------------------------------------------
 // One whole warp reports the total of tile `tile` (v, lane-independent).
-// Returns true in the warp that reports the system's last tile, with v =
-// the system totals summed over the tile totals in tile order.
+// Returns true in the warp that completes the system, with v = the system
+// totals.  Two levels keep the atomics spread: the tiles of a chunk of
+// kChunkTiles report to the chunk's counter, whose last arriver sums the
+// chunk's tile totals in tile order and reports the chunk to the system
+// counter; the system's last chunk sums the chunk totals in chunk order.
+// The order depends only on the system's tiling, never on the mix.
+constexpr int kChunkTiles = 64;
+
+__device__ __forceinline__ int n_chunks(int ntiles) {
+  return (ntiles + kChunkTiles - 1) / kChunkTiles;
+}
+
 template <int NQ>
-__device__ bool warp_tile_done(unsigned* sys_cnt, double* tile_tot, int ntiles, int tile,
-                               double (&v)[NQ]) {
+__device__ bool warp_tile_done(unsigned* sys_cnt, double* tile_tot, double* chunk_tot,
+                               unsigned* chunk_cnt, int ntiles, int tile, double (&v)[NQ]) {
   const int lane = threadIdx.x & 31;
+  const int chunk = tile / kChunkTiles, t0 = chunk * kChunkTiles;
+  const int clen = min(kChunkTiles, ntiles - t0);
   unsigned last = 0;
   if (lane == 0) {
 #pragma unroll
     for (int q = 0; q < NQ; ++q) tile_tot[(size_t)tile * kPartQ + q] = v[q];
     __threadfence();
-    last = (atomicAdd(sys_cnt, 1u) == (unsigned)ntiles - 1);
+    last = (atomicAdd(chunk_cnt + chunk, 1u) == (unsigned)clen - 1);
   }
   last = __shfl_sync(0xffffffffu, last, 0);
   if (!last) return false;
@@ -155,10 +169,30 @@ __device__ bool warp_tile_done(unsigned* sys_cnt, double* tile_tot, int ntiles, 
   double acc[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
-  for (int t = lane; t < ntiles; t += 32)
+  for (int t = lane; t < clen; t += 32)
 #pragma unroll
     for (int q = 0; q < NQ; ++q)
-      acc[q] = __dadd_rn(acc[q], __ldcg(tile_tot + (size_t)t * kPartQ + q));
+      acc[q] = __dadd_rn(acc[q], __ldcg(tile_tot + (size_t)(t0 + t) * kPartQ + q));
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) acc[q] = warp_sum(acc[q]);
+  const int nch = n_chunks(ntiles);
+  last = 0;
+  if (lane == 0) {
+    chunk_cnt[chunk] = 0u;   // ready for the next kernel
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) chunk_tot[(size_t)chunk * kPartQ + q] = acc[q];
+    __threadfence();
+    last = (atomicAdd(sys_cnt, 1u) == (unsigned)nch - 1);
+  }
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (!last) return false;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
+  for (int c = lane; c < nch; c += 32)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+      acc[q] = __dadd_rn(acc[q], __ldcg(chunk_tot + (size_t)c * kPartQ + q));
 #pragma unroll
   for (int q = 0; q < NQ; ++q) v[q] = warp_sum(acc[q]);
   if (lane == 0) *sys_cnt = 0u;
@@ -170,7 +204,8 @@ __device__ bool warp_tile_done(unsigned* sys_cnt, double* tile_tot, int ntiles, 
 // reports the tile through warp_tile_done.  v: this thread's values.
 template <int NQ>
 __device__ bool cta_tile_done(unsigned* sys_cnt, double* tile_tot, double* warp_part,
-                              unsigned* tile_cnt, int ntiles, int tile, double (&v)[NQ]) {
+                              unsigned* tile_cnt, double* chunk_tot, unsigned* chunk_cnt,
+                              int ntiles, int tile, double (&v)[NQ]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < NQ; ++q) v[q] = warp_sum(v[q]);
@@ -193,7 +228,33 @@ __device__ bool cta_tile_done(unsigned* sys_cnt, double* tile_tot, double* warp_
     v[q] = warp_sum(w);
   }
   if (lane == 0) tile_cnt[tile] = 0u;
-  return warp_tile_done<NQ>(sys_cnt, tile_tot, ntiles, tile, v);
+  return warp_tile_done<NQ>(sys_cnt, tile_tot, chunk_tot, chunk_cnt, ntiles, tile, v);
+}
+
+// Tile reduction for the producer-warp streamer (tf_tile2.cuh): every
+// consumer warp's partial goes to shared memory, one barrier among the
+// consumers, then warp 0 sums them in warp order -- the order
+// cta_tile_done uses -- and reports the tile: one fence and one atomic per
+// tile instead of one per warp.  True in warp 0 when the system is complete.
+template <int NQ>
+__device__ bool cons_tile_done(unsigned* sys_cnt, double* tile_tot, double* chunk_tot,
+                               unsigned* chunk_cnt, int ntiles, int tile, double (&v)[NQ]) {
+  __shared__ double sred[kPartQ * kWarps];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) v[q] = warp_sum(v[q]);
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) sred[q * kWarps + warp] = v[q];
+  }
+  consumer_bar();
+  if (warp != 0) return false;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    const double w = lane < kWarps ? sred[q * kWarps + lane] : 0.0;
+    v[q] = warp_sum(w);
+  }
+  return warp_tile_done<NQ>(sys_cnt, tile_tot, chunk_tot, chunk_cnt, ntiles, tile, v);
 }
 
 // ---------------------------------------------------------------------------
@@ -255,7 +316,9 @@ __global__ void __launch_bounds__(256) kb_update(BatchArgs a) {
     }
     v[0] = warp_sum(v[0]);
     v[1] = warp_sum(v[1]);
-    if (!warp_tile_done<2>(&s.cnt_upd, d.tile_tot, d.ntiles, w.tile, v)) continue;
+    if (!warp_tile_done<2>(&s.cnt_upd, d.tile_tot, d.chunk_tot, d.chunk_cnt, d.ntiles, w.tile,
+                           v))
+      continue;
     int base = -1;
     if (lane == 0) {
       s.rho_old = s.rho;
@@ -351,7 +414,8 @@ struct SpmvWork {
     const SysDev<V>& d = D[w.sys];
     double v[1] = {acc};
     acc = 0.0;
-    if (cta_tile_done<1>(&st[w.sys].cnt_spmv, d.tile_tot, d.warp_part, d.tile_cnt, d.ntiles,
+    if (cta_tile_done<1>(&st[w.sys].cnt_spmv, d.tile_tot, d.warp_part, d.tile_cnt, d.chunk_tot,
+                         d.chunk_cnt, d.ntiles,
                          w.tile, v) &&
         (threadIdx.x & 31) == 0) {
       SysState& s = st[w.sys];
@@ -414,8 +478,8 @@ struct SpmvOp2 {
     const SysDev<V>& d = D[w.sys];
     double v[1] = {acc};
     acc = 0.0;
-    if (cta_tile_done<1>(&st[w.sys].cnt_spmv, d.tile_tot, d.warp_part, d.tile_cnt, d.ntiles,
-                         w.tile, v) &&
+    if (cons_tile_done<1>(&st[w.sys].cnt_spmv, d.tile_tot, d.chunk_tot, d.chunk_cnt, d.ntiles,
+                          w.tile, v) &&
         (threadIdx.x & 31) == 0) {
       SysState& s = st[w.sys];
       if (!(v[0] > 0.0)) s.status = kBreakdown;   // p.q <= 0 or NaN
@@ -436,6 +500,34 @@ __global__ void __launch_bounds__(kCsr2Threads, 2) kb_spmv(BatchArgs a) {
     SpmvWork<V, VT> w{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, *a.nwork, 0.0, -1,
                       nullptr, nullptr};
     stream_items<kRows, kNnzCap, VT, kStages>(w);
+  }
+}
+
+// A system's refinement step after its FP64 residual: v = {|r|^2, rho,
+// |b|^2 (first time)}.  Run by one thread.
+template <typename V>
+__device__ void res_finish(SysState& s, const SysDev<V>& d, const double (&v)[3]) {
+  if (s.status == kInit) {
+    s.bnorm2 = v[2];
+    s.status = kActive;
+    s.first = 1;
+    s.iter = 0;
+  }
+  s.n_ru += 1;
+  const double bn = s.bnorm2 > 0.0 ? __dsqrt_rn(s.bnorm2) : 1.0;
+  s.res_true = __ddiv_rn(__dsqrt_rn(v[0]), bn);
+  s.need_ru = 0;
+  if (s.res_true <= d.tol) {
+    s.status = kConverged;
+  } else if (s.iter >= d.maxit) {
+    s.status = kMaxIter;
+  } else if (!(v[0] == v[0])) {
+    s.status = kBreakdown;
+  } else {
+    s.rr = v[0];
+    s.rr_ru = v[0];
+    s.rho = v[1];
+    if (!s.first) s.beta = __ddiv_rn(s.rho, s.rho_old);
   }
 }
 
@@ -492,33 +584,11 @@ struct ResWork {
     const SysDev<V>& d = D[w.sys];
     double v[3] = {rr, rho, bb};
     rr = rho = bb = 0.0;
-    if (cta_tile_done<3>(&st[w.sys].cnt_res, d.tile_tot, d.warp_part, d.tile_cnt, d.ntiles,
+    if (cta_tile_done<3>(&st[w.sys].cnt_res, d.tile_tot, d.warp_part, d.tile_cnt, d.chunk_tot,
+                         d.chunk_cnt, d.ntiles,
                          w.tile, v) &&
-        (threadIdx.x & 31) == 0) {
-      SysState& s = st[w.sys];
-      if (s.status == kInit) {
-        s.bnorm2 = v[2];
-        s.status = kActive;
-        s.first = 1;
-        s.iter = 0;
-      }
-      s.n_ru += 1;
-      const double bn = s.bnorm2 > 0.0 ? __dsqrt_rn(s.bnorm2) : 1.0;
-      s.res_true = __ddiv_rn(__dsqrt_rn(v[0]), bn);
-      s.need_ru = 0;
-      if (s.res_true <= d.tol) {
-        s.status = kConverged;
-      } else if (s.iter >= d.maxit) {
-        s.status = kMaxIter;
-      } else if (!(v[0] == v[0])) {
-        s.status = kBreakdown;
-      } else {
-        s.rr = v[0];
-        s.rr_ru = v[0];
-        s.rho = v[1];
-        if (!s.first) s.beta = __ddiv_rn(s.rho, s.rho_old);
-      }
-    }
+        (threadIdx.x & 31) == 0)
+      res_finish(st[w.sys], d, v);
   }
 };
 
@@ -552,10 +622,13 @@ struct ResOp2 {
     rr = __dadd_rn(rr, __dmul_rn(s, s));
     rho = __dadd_rn(rho, __dmul_rn((double)zi, (double)ri));
   }
-  __device__ void tile_end(int k) {
-    ResWork<V> rw{D, st, work, 0, rr, rho, bb};
+  __device__ void tile_end(int) {
+    double v[3] = {rr, rho, bb};
     rr = rho = bb = 0.0;
-    rw.tile_end(k);
+    if (cons_tile_done<3>(&st[w.sys].cnt_res, d->tile_tot, d->chunk_tot, d->chunk_cnt,
+                          d->ntiles, w.tile, v) &&
+        (threadIdx.x & 31) == 0)
+      res_finish(st[w.sys], *d, v);
   }
 };
 
@@ -740,7 +813,7 @@ int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* co
 // Byte layout of one system's segment.
 struct Layout {
   size_t row, col, dia, tiles, val, val32, b, x, xlo, r, p, q, dinv, tile_tot, warp_part,
-      tile_cnt, total;
+      tile_cnt, chunk_tot, chunk_cnt, total;
 };
 
 Layout layout_for(const HostSys& h, size_t vsz, int use_val32) {
@@ -765,6 +838,9 @@ Layout layout_for(const HostSys& h, size_t vsz, int use_val32) {
   L.tile_tot = take((size_t)ntiles * kPartQ * 8);
   L.warp_part = take((size_t)ntiles * kWarps * kPartQ * 8);
   L.tile_cnt = take((size_t)ntiles * 4);
+  const size_t nch = (size_t)(ntiles + kChunkTiles - 1) / kChunkTiles;
+  L.chunk_tot = take(nch * kPartQ * 8);
+  L.chunk_cnt = take(nch * 4);
   L.total = o;
   return L;
 }
@@ -945,6 +1021,9 @@ struct tf_batch_s {
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.p, 0, n8 * vsz, s);
     if (e == cudaSuccess)
       e = cudaMemsetAsync(base + L.tile_cnt, 0, (h.tiles.size() - 1) * 4, s);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(base + L.chunk_cnt, 0,
+                          ((h.tiles.size() - 1 + kChunkTiles - 1) / kChunkTiles) * 4, s);
     if (e != cudaSuccess) {
       arena.release(off, L.total);
       tf_set_last_cuda_error(e, "batch admit copies", __FILE__, __LINE__);
@@ -969,6 +1048,8 @@ struct tf_batch_s {
       d.tile_tot = (double*)(base + L.tile_tot);
       d.warp_part = (double*)(base + L.warp_part);
       d.tile_cnt = (unsigned*)(base + L.tile_cnt);
+      d.chunk_tot = (double*)(base + L.chunk_tot);
+      d.chunk_cnt = (unsigned*)(base + L.chunk_cnt);
       d.n = h.n;
       d.ntiles = ntiles;
       d.maxit = h.maxit;

@@ -123,8 +123,13 @@ __device__ bool stream_csr2(S& src, Op& op) {
     // ---- producer warp ----
     if (lane == 0) {
       int issued = 0;
+      // The next tile's descriptor is loaded a round early, so its (possibly
+      // dependent) global loads overlap the wait for a free stage.
+      TileDesc nxt = src.desc(blockIdx.x);
       for (int k = blockIdx.x; k < count; k += gridDim.x, ++issued) {
         const int s = issued % STAGES;
+        const TileDesc d = nxt;
+        if (k + (int)gridDim.x < count) nxt = src.desc(k + gridDim.x);
         if (issued >= STAGES) {
           if (!mbar_wait_bounded(&empty[s], (unsigned)(issued / STAGES - 1) & 1u)) {
             ok = false;
@@ -134,7 +139,6 @@ __device__ bool stream_csr2(S& src, Op& op) {
           fence_proxy_async_smem();
         }
         if (*abort_flag) break;
-        const TileDesc d = src.desc(k);
         int* m = meta + L::kMetaInts * s;
         m[7] = d.skip;
         m[8] = k;
