@@ -1,14 +1,17 @@
 // tf_tile.cuh -- row-tile streaming of a CSR matrix through shared memory.
 //
-// A tile is ROWS consecutive rows.  Its row pointers, column indices and
-// values are contiguous in the CSR arrays, so one thread issues three 1D
-// bulk copies (cp.async.bulk, the TMA's linear mode) into a shared-memory
-// stage and arms that stage's mbarrier with the byte count.  Stages form a
-// ring: while the CTA computes tile k from stage s, the copies of the next
-// STAGES-1 tiles are in flight, which keeps ~100 KB per SM in flight with
-// only a few warps resident.  Persistent CTAs walk tiles blockIdx.x,
-// blockIdx.x + gridDim.x, ... so the tile -> CTA map (and hence every
-// partial sum) is fixed for a fixed grid.
+// A tile is a run of consecutive rows.  Its row pointers, column indices
+// (or row-pattern bytes) and values are contiguous in the device arrays, so
+// one thread issues 1D bulk copies (cp.async.bulk, the TMA's linear mode)
+// into a shared-memory stage and arms that stage's mbarrier with the byte
+// count.  Stages form a ring: while tile k is computed from stage s, the
+// copies of the next tiles are in flight.  Persistent CTAs walk tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ... so the tile -> CTA map (and hence
+// every partial sum) is fixed for a fixed grid.
+//
+// Here: the work-list streamer of the batch engine (FP32-value path) and
+// the row-pattern streamer with a producer warp; the CSR streamer with a
+// producer warp is in tf_tile2.cuh.
 //
 // Each row is then handed to a per-row operator with pointers into the
 // stage: one thread per row, entries visited in storage order, so a row sum
@@ -37,219 +40,6 @@ struct TileLayout {
   static constexpr size_t kMetaOffset = kBarOffset + 8 * STAGES;
   static constexpr size_t kSmemBytes = kMetaOffset + 32 * STAGES;
 };
-
-// Tile pointers the per-row operator sees.
-struct TileRow {
-  int i;      // row index (0-based)
-  int len;    // entries in the row
-};
-
-// Streams tiles [0, ntiles) of rows [0, nrows) through shared memory and
-// calls op(i, vals, cols, len) for every row, one thread per row.
-// Returns false if a bounded wait timed out (the caller records the status);
-// in that case every copy this CTA issued has been waited for (boundedly).
-template <int ROWS, int NNZCAP, typename VT, int STAGES, class Op>
-__device__ bool stream_tiles(const int* __restrict__ row,
-                             const int* __restrict__ col,
-                             const VT* __restrict__ val, int nrows, Op& op) {
-  using L = TileLayout<ROWS, NNZCAP, VT, STAGES>;
-  constexpr int kEv = L::kEv;
-  extern __shared__ __align__(128) unsigned char tf_smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(tf_smem + L::kBarOffset);
-  int* meta = reinterpret_cast<int*>(tf_smem + L::kMetaOffset);
-  auto sval = [&](int s) {
-    return reinterpret_cast<VT*>(tf_smem + s * L::kStageBytes);
-  };
-  auto scol = [&](int s) {
-    return reinterpret_cast<int*>(tf_smem + s * L::kStageBytes + L::kValBytes);
-  };
-  auto srow = [&](int s) {
-    return reinterpret_cast<int*>(tf_smem + s * L::kStageBytes + L::kValBytes +
-                                  L::kColBytes);
-  };
-
-  const int ntiles = (nrows + ROWS - 1) / ROWS;
-  if ((int)blockIdx.x >= ntiles) return true;
-
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-
-  // Issue the copies of `tile` into stage s (thread 0 only).
-  auto issue = [&](int tile, int s) {
-    const int r0 = tile * ROWS;
-    const int r1 = min(r0 + ROWS, nrows);
-    const int j0 = __ldg(row + r0), j1 = __ldg(row + r1);
-    const int a0 = j0 & ~(kEv - 1), a1 = (j1 + kEv - 1) & ~(kEv - 1);
-    const int c0 = j0 & ~3, c1 = (j1 + 3) & ~3;
-    const int p0 = r0 & ~3, p1 = (r1 + 1 + 3) & ~3;
-    int* m = meta + 8 * s;
-    m[0] = a0; m[1] = c0; m[2] = p0; m[3] = r0; m[4] = r1;
-    const unsigned bv = (unsigned)(a1 - a0) * (unsigned)sizeof(VT);
-    const unsigned bc = (unsigned)(c1 - c0) * 4u;
-    const unsigned br = (unsigned)(p1 - p0) * 4u;
-    mbar_arrive_expect_tx(&bars[s], bv + bc + br);
-    if (bv) bulk_g2s(sval(s), val + a0, bv, &bars[s]);
-    if (bc) bulk_g2s(scol(s), col + c0, bc, &bars[s]);
-    bulk_g2s(srow(s), row + p0, br, &bars[s]);
-  };
-
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int s = 0; s < STAGES; ++s) {
-      const int t = blockIdx.x + s * gridDim.x;
-      if (t < ntiles) issue(t, s);
-    }
-  }
-
-  bool ok = true;
-  int it = 0;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-    const int s = it % STAGES;
-    const unsigned par = (unsigned)(it / STAGES) & 1u;
-    const bool mine = mbar_wait_bounded(&bars[s], par);
-    if (__syncthreads_or(!mine)) { ok = false; break; }
-
-    const int* m = meta + 8 * s;
-    const int a0 = m[0], c0 = m[1], p0 = m[2], r0 = m[3], r1 = m[4];
-    const VT* sv = sval(s);
-    const int* sc = scol(s);
-    const int* sr = srow(s);
-    for (int r = r0 + (int)threadIdx.x; r < r1; r += ROWS) {
-      const int js = sr[r - p0], je = sr[r + 1 - p0];
-      op(r, sv + (js - a0), sc + (js - c0), je - js);
-    }
-    __syncthreads();  // stage s fully consumed
-    if (threadIdx.x == 0) {
-      const int nt = tile + STAGES * gridDim.x;
-      if (nt < ntiles) {
-        fence_proxy_async_smem();
-        issue(nt, s);
-      }
-    }
-  }
-
-  if (!ok && threadIdx.x == 0) {
-    // Drain: wait (bounded) for every stage that still has copies in flight.
-    for (int k = 0; k < STAGES; ++k) {
-      const int itk = it + k;
-      const int t = blockIdx.x + itk * gridDim.x;
-      if (t >= ntiles) break;
-      mbar_wait_bounded(&bars[itk % STAGES], (unsigned)(itk / STAGES) & 1u);
-    }
-  }
-  __syncthreads();
-  return ok;
-}
-
-// ---------------------------------------------------------------------------
-// Work-list variant: the same pipeline over items that each name a tile of
-// some matrix (used by the batched engine, where every item belongs to one
-// of many independent systems).  `W` provides, for a global item index k:
-//   bool skip(k)                      -- item has nothing to do this launch
-//   void tile(k, row, col, val, r0, r1) -- its CSR arrays and row range
-//   void row(k, i, vals, cols, len)   -- per-row work (one thread per row)
-//   void tile_end(k)                  -- CTA-wide, after all rows of item k
-// Items k = blockIdx.x, blockIdx.x + gridDim.x, ... < W.count().
-// ---------------------------------------------------------------------------
-template <int ROWS, int NNZCAP, typename VT, int STAGES, class W>
-__device__ bool stream_work(W& w) {
-  using L = TileLayout<ROWS, NNZCAP, VT, STAGES>;
-  constexpr int kEv = L::kEv;
-  extern __shared__ __align__(128) unsigned char tf_smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(tf_smem + L::kBarOffset);
-  int* meta = reinterpret_cast<int*>(tf_smem + L::kMetaOffset);
-  auto sval = [&](int s) { return reinterpret_cast<VT*>(tf_smem + s * L::kStageBytes); };
-  auto scol = [&](int s) {
-    return reinterpret_cast<int*>(tf_smem + s * L::kStageBytes + L::kValBytes);
-  };
-  auto srow = [&](int s) {
-    return reinterpret_cast<int*>(tf_smem + s * L::kStageBytes + L::kValBytes + L::kColBytes);
-  };
-  const int count = w.count();
-  if ((int)blockIdx.x >= count) return true;
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-
-  auto issue = [&](int k, int s) {
-    int* m = meta + 8 * s;
-    if (w.skip(k)) {           // nothing to copy: complete the phase at once
-      m[5] = 1;
-      mbar_arrive_expect_tx(&bars[s], 0);
-      return;
-    }
-    const int* row;
-    const int* col;
-    const VT* val;
-    int r0, r1;
-    w.tile(k, row, col, val, r0, r1);
-    const int j0 = __ldg(row + r0), j1 = __ldg(row + r1);
-    const int a0 = j0 & ~(kEv - 1), a1 = (j1 + kEv - 1) & ~(kEv - 1);
-    const int c0 = j0 & ~3, c1 = (j1 + 3) & ~3;
-    const int p0 = r0 & ~3, p1 = (r1 + 1 + 3) & ~3;
-    m[0] = a0; m[1] = c0; m[2] = p0; m[3] = r0; m[4] = r1; m[5] = 0;
-    const unsigned bv = (unsigned)(a1 - a0) * (unsigned)sizeof(VT);
-    const unsigned bc = (unsigned)(c1 - c0) * 4u;
-    const unsigned br = (unsigned)(p1 - p0) * 4u;
-    mbar_arrive_expect_tx(&bars[s], bv + bc + br);
-    if (bv) bulk_g2s(sval(s), val + a0, bv, &bars[s]);
-    if (bc) bulk_g2s(scol(s), col + c0, bc, &bars[s]);
-    bulk_g2s(srow(s), row + p0, br, &bars[s]);
-  };
-
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int s = 0; s < STAGES; ++s) {
-      const int k = blockIdx.x + s * gridDim.x;
-      if (k < count) issue(k, s);
-    }
-  }
-  bool ok = true;
-  int it = 0;
-  for (int k = blockIdx.x; k < count; k += gridDim.x, ++it) {
-    const int s = it % STAGES;
-    const unsigned par = (unsigned)(it / STAGES) & 1u;
-    const bool mine = mbar_wait_bounded(&bars[s], par);
-    if (__syncthreads_or(!mine)) { ok = false; break; }
-    const int* m = meta + 8 * s;
-    if (!m[5]) {
-      const int a0 = m[0], c0 = m[1], p0 = m[2], r0 = m[3], r1 = m[4];
-      const VT* sv = sval(s);
-      const int* sc = scol(s);
-      const int* sr = srow(s);
-      for (int r = r0 + (int)threadIdx.x; r < r1; r += ROWS) {
-        const int js = sr[r - p0], je = sr[r + 1 - p0];
-        w.row(k, r, sv + (js - a0), sc + (js - c0), je - js);
-      }
-      w.tile_end(k);   // CTA-uniform (m[5] is shared)
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int nk = k + STAGES * gridDim.x;
-      if (nk < count) {
-        fence_proxy_async_smem();
-        issue(nk, s);
-      }
-    }
-  }
-  if (!ok && threadIdx.x == 0) {
-    for (int d = 0; d < STAGES; ++d) {
-      const int itk = it + d;
-      const int k = blockIdx.x + itk * gridDim.x;
-      if (k >= count) break;
-      mbar_wait_bounded(&bars[itk % STAGES], (unsigned)(itk / STAGES) & 1u);
-    }
-  }
-  __syncthreads();
-  return ok;
-}
 
 // ---------------------------------------------------------------------------
 // Work-list streamer with descriptor prefetch.  Items carry their row range
