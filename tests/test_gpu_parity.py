@@ -255,6 +255,27 @@ def test_renumbered_fin_res_is_nrms_of_returned_x(gpu_ctx, miter):
                                 rel=1e-9)
 
 
+@pytest.mark.parametrize("prec,norm", [("jacobi", 1.0), ("jacobi", None), ("none", 1.0)])
+def test_buffer_cells(gpu_ctx, prec, norm):
+    """n_own < n_cells, as on an MPI sub-domain (Cg.f90:54, ni = n_cells -
+    n_buff_cells): rows beyond ni are not solved, their x values enter the
+    own rows' sums as fixed halo values."""
+    s = systems.small_hex(13, seed=8, kind="pressure", ratio=1.03)
+    ni = s.n - 150
+    x0 = np.random.default_rng(6).uniform(-0.5, 0.5, s.n)
+    v, x, b = s.val.copy(), x0.copy(), s.b.copy()
+    m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia, n_own=ni)
+    try:
+        it, res = native.solve(gpu_ctx, m, "cg", prec, v, x, b, 3000, 1e-10, norm)
+    finally:
+        m.close()
+    ov, ox, ob = s.val.copy(), x0.copy(), s.b.copy()
+    o = O.solve_native("cg", prec, s.csr.row, s.csr.col, s.csr.dia, ov, ox, ob, 3000, 1e-10,
+                       norm=norm, n_own=ni)
+    check_parity((x, v, b, it, res), (ox, ov, ob, o["niter"], o["fin_res"]), 1e-10)
+    assert np.array_equal(x[ni:], x0[ni:])   # halo values untouched
+
+
 def test_long_rows_fall_back_to_global_path(gpu_ctx):
     """A row longer than any tile stage (a dense coupling row) still works."""
     n = 6000
