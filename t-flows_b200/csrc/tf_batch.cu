@@ -232,32 +232,6 @@ __device__ bool cta_tile_done(unsigned* sys_cnt, double* tile_tot, double* warp_
   return warp_tile_done<NQ>(sys_cnt, tile_tot, chunk_tot, chunk_cnt, ntiles, tile, v);
 }
 
-// Tile reduction for the producer-warp streamer (tf_tile2.cuh): every
-// consumer warp's partial goes to shared memory, one barrier among the
-// consumers, then warp 0 sums them in warp order -- the order
-// cta_tile_done uses -- and reports the tile: one fence and one atomic per
-// tile instead of one per warp.  True in warp 0 when the system is complete.
-template <int NQ>
-__device__ bool cons_tile_done(unsigned* sys_cnt, double* tile_tot, double* chunk_tot,
-                               unsigned* chunk_cnt, int ntiles, int tile, double (&v)[NQ]) {
-  __shared__ double sred[kPartQ * kWarps];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) v[q] = warp_sum(v[q]);
-  if (lane == 0) {
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) sred[q * kWarps + warp] = v[q];
-  }
-  consumer_bar();
-  if (warp != 0) return false;
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-    const double w = lane < kWarps ? sred[q * kWarps + lane] : 0.0;
-    v[q] = warp_sum(w);
-  }
-  return warp_tile_done<NQ>(sys_cnt, tile_tot, chunk_tot, chunk_cnt, ntiles, tile, v);
-}
-
 // ---------------------------------------------------------------------------
 // Elementwise kernels: one warp per tile.
 // ---------------------------------------------------------------------------
@@ -453,9 +427,53 @@ struct BatchTiles {
     t.j1 = w.j1;
     const SysState& s = st[w.sys];
     t.skip = KIND == 0 ? !active(s) : !(s.status == kInit || (s.status == kActive && s.need_ru));
+    t.aux0 = KIND == 0 ? (const void*)d.p : (const void*)&D[w.sys];
+    t.aux1 = KIND == 0 ? (void*)d.q : nullptr;
+    t.aux2 = w.sys;
+    t.aux3 = w.tile;
     return t;
   }
 };
+
+// Per-tile partials of the producer-warp streamer's consumer warps: each
+// warp sums its lanes and parks the result in a double buffer (by consumer
+// iteration parity); flush, after the streamer's next barrier, has warp 0
+// sum the kWarps partials in warp order -- the order cta_tile_done uses --
+// and report the tile, one fence and one atomic per tile.
+// Tile reduction for the producer-warp streamer (tf_tile2.cuh), in two
+// halves.  tile_end: every consumer warp parks its partials in shared
+// memory (slot it & 1).  flush, after the streamer's next consumer barrier:
+// warp 0 sums the kWarps partials in warp order -- the order cta_tile_done
+// uses -- and reports the tile (one fence and one atomic per tile).  The
+// streamer's own per-tile barrier orders the two halves, so the reduction
+// costs no barrier of its own; two slots let tile it+1 park while warp 0
+// still flushes tile it.
+__shared__ double g_tile_part[2][kPartQ][kWarps];
+
+template <int NQ>
+__device__ __forceinline__ void park_partials(double (&v)[NQ], int it) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) v[q] = warp_sum(v[q]);
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) g_tile_part[it & 1][q][warp] = v[q];
+  }
+}
+
+// Warp 0 only; true when the tile completed its system (v = totals).
+template <int NQ>
+__device__ __forceinline__ bool flush_partials(double (&v)[NQ], int it, unsigned* sys_cnt,
+                                               double* tile_tot, double* chunk_tot,
+                                               unsigned* chunk_cnt, int ntiles, int tile) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    const double w = lane < kWarps ? g_tile_part[it & 1][q][lane] : 0.0;
+    v[q] = warp_sum(w);
+  }
+  return warp_tile_done<NQ>(sys_cnt, tile_tot, chunk_tot, chunk_cnt, ntiles, tile, v);
+}
 
 // q = A p (FP64 values, FP64 row sums), p.q per tile, alpha per system.
 template <typename V>
@@ -464,13 +482,14 @@ struct SpmvOp2 {
   SysState* st;
   const Work* work;
   double acc;
-  Work w;
   const V* p;
   V* q;
-  __device__ void begin(int k) {
-    w = work[k];
-    p = D[w.sys].p;
-    q = D[w.sys].q;
+  int sys, tile, prev_sys, prev_tile;
+  __device__ void begin(int, TileAux aux) {
+    p = static_cast<const V*>(aux.a0);
+    q = static_cast<V*>(aux.a1);
+    sys = aux.i2;
+    tile = aux.i3;
   }
   __device__ double gather(int c) const { return (double)__ldg(p + c); }
   __device__ double row_init(int) const { return 0.0; }
@@ -480,14 +499,21 @@ struct SpmvOp2 {
     q[i] = qi;
     acc = __dadd_rn(acc, __dmul_rn((double)__ldg(p + i), (double)qi));
   }
-  __device__ void tile_end(int) {
-    const SysDev<V>& d = D[w.sys];
+  __device__ void tile_end(int it) {
     double v[1] = {acc};
     acc = 0.0;
-    if (cons_tile_done<1>(&st[w.sys].cnt_spmv, d.tile_tot, d.chunk_tot, d.chunk_cnt, d.ntiles,
-                          w.tile, v) &&
+    park_partials<1>(v, it);
+    prev_sys = sys;
+    prev_tile = tile;
+  }
+  __device__ void flush(int it) {
+    if ((threadIdx.x >> 5) != 0) return;
+    const SysDev<V>& d = D[prev_sys];
+    double v[1];
+    if (flush_partials<1>(v, it, &st[prev_sys].cnt_spmv, d.tile_tot, d.chunk_tot, d.chunk_cnt,
+                          d.ntiles, prev_tile) &&
         (threadIdx.x & 31) == 0) {
-      SysState& s = st[w.sys];
+      SysState& s = st[prev_sys];
       if (!(v[0] > 0.0)) s.status = kBreakdown;   // p.q <= 0 or NaN
       else s.alpha = __ddiv_rn(s.rho, v[0]);
     }
@@ -498,7 +524,8 @@ template <typename V, typename VT>
 __global__ void __launch_bounds__(kCsr2Threads, 2) kb_spmv(BatchArgs a) {
   if constexpr (sizeof(VT) == 8) {
     BatchTiles<V, 0> src{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, *a.nwork};
-    SpmvOp2<V> op{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, 0.0};
+    SpmvOp2<V> op{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, 0.0, nullptr, nullptr,
+                  0, 0, 0, 0};
     stream_csr2<kRows, kNnzCap, kStages>(src, op);
   } else {
     // FP32 values: the one-thread-per-row streamer (kRows threads do the
@@ -606,13 +633,14 @@ struct ResOp2 {
   SysState* st;
   const Work* work;
   double rr, rho, bb;
-  Work w;
   const SysDev<V>* d;
   bool init;
-  __device__ void begin(int k) {
-    w = work[k];
-    d = &D[w.sys];
-    init = st[w.sys].status == kInit;
+  int sys, tile, prev_sys, prev_tile;
+  __device__ void begin(int, TileAux aux) {
+    d = static_cast<const SysDev<V>*>(aux.a0);
+    sys = aux.i2;
+    tile = aux.i3;
+    init = st[sys].status == kInit;
   }
   __device__ double gather(int c) const { return d->x[c]; }
   __device__ double row_init(int i) const { return d->b[i]; }
@@ -629,20 +657,29 @@ struct ResOp2 {
     rr = __dadd_rn(rr, __dmul_rn(s, s));
     rho = __dadd_rn(rho, __dmul_rn((double)zi, (double)ri));
   }
-  __device__ void tile_end(int) {
+  __device__ void tile_end(int it) {
     double v[3] = {rr, rho, bb};
     rr = rho = bb = 0.0;
-    if (cons_tile_done<3>(&st[w.sys].cnt_res, d->tile_tot, d->chunk_tot, d->chunk_cnt,
-                          d->ntiles, w.tile, v) &&
+    park_partials<3>(v, it);
+    prev_sys = sys;
+    prev_tile = tile;
+  }
+  __device__ void flush(int it) {
+    if ((threadIdx.x >> 5) != 0) return;
+    const SysDev<V>& dd = D[prev_sys];
+    double v[3];
+    if (flush_partials<3>(v, it, &st[prev_sys].cnt_res, dd.tile_tot, dd.chunk_tot,
+                          dd.chunk_cnt, dd.ntiles, prev_tile) &&
         (threadIdx.x & 31) == 0)
-      res_finish(st[w.sys], *d, v);
+      res_finish(st[prev_sys], dd, v);
   }
 };
 
 template <typename V>
 __global__ void __launch_bounds__(kCsr2Threads, 2) kb_ru_res(BatchArgs a) {
   BatchTiles<V, 1> src{static_cast<const SysDev<V>*>(a.desc), a.st, a.ru.items, *a.ru.count};
-  ResOp2<V> op{static_cast<const SysDev<V>*>(a.desc), a.st, a.ru.items, 0.0, 0.0, 0.0};
+  ResOp2<V> op{static_cast<const SysDev<V>*>(a.desc), a.st, a.ru.items, 0.0, 0.0, 0.0,
+               nullptr, false, 0, 0, 0, 0};
   stream_csr2<kRows, kNnzCap, kStages>(src, op);
   // The last CTA to leave empties the refinement list for the next iteration.
   if (threadIdx.x == 0) {

@@ -208,7 +208,8 @@ struct OpSpmvDot {
     body(i, v, [i, o](int k) { return i + o[k]; }, len);
   }
   // two-phase streamer
-  __device__ __forceinline__ void begin(int) {}
+  __device__ __forceinline__ void begin(int, TileAux) {}
+  __device__ __forceinline__ void flush(int) {}
   __device__ __forceinline__ double gather(int c) const { return __ldg(p + c); }
   __device__ __forceinline__ double row_init(int) const { return 0.0; }
   __device__ __forceinline__ double combine(double acc, double prod) const {
@@ -263,7 +264,8 @@ struct OpResidual {
     body(i, v, [i, o](int k) { return i + o[k]; }, len);
   }
   // two-phase streamer
-  __device__ __forceinline__ void begin(int) {}
+  __device__ __forceinline__ void begin(int, TileAux) {}
+  __device__ __forceinline__ void flush(int) {}
   __device__ __forceinline__ double gather(int c) const { return __ldg(x + c); }
   __device__ __forceinline__ double row_init(int i) const { return b[i]; }
   __device__ __forceinline__ double combine(double acc, double prod) const {
@@ -301,6 +303,9 @@ struct FixedTiles {
     d.j0 = __ldg(row + d.r0);
     d.j1 = __ldg(row + d.r1);
     d.skip = 0;
+    d.aux0 = nullptr;
+    d.aux1 = nullptr;
+    d.aux2 = d.aux3 = 0;
     return d;
   }
 };

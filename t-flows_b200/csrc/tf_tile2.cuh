@@ -32,13 +32,16 @@
 //   int count()                    -- tiles (items) to walk
 //   TileDesc desc(int k)           -- arrays and row/entry range of item k
 // and the operator `Op` (consumer threads):
-//   void begin(int k)              -- item k starts (cache pointers)
+//   void begin(int k, TileAux aux) -- item k starts (aux: the descriptor's aux)
 //   double gather(int c)           -- the vector entry multiplied by column c
 //   double row_init(int i)         -- 0.0 or b_i
 //   double combine(double acc, double prod)  -- acc + prod or acc - prod
 //   void row_done(int i, double acc)
-//   void tile_end(int k)           -- consumer warps, after the rows (may be
-//                                     empty; must not use CTA barriers)
+//   void tile_end(int it)          -- after the rows of the tile of consumer
+//                                     iteration `it` (no barriers)
+//   void flush(int it)             -- the same tile, later: after a barrier
+//                                     that every consumer has passed since
+//                                     tile_end(it) (reductions over warps)
 #pragma once
 #include "tf_common.cuh"
 
@@ -53,6 +56,17 @@ struct TileDesc {
   const double* val;
   int r0, r1, j0, j1;
   int skip;
+  const void* aux0;   // handed to op.begin through the stage (e.g. x, y vectors)
+  void* aux1;
+  int aux2, aux3;
+};
+
+// What op.begin receives about its tile (copied by the producer into the
+// stage's metadata, so consumers need no global loads to start a tile).
+struct TileAux {
+  const void* a0;
+  void* a1;
+  int i2, i3;
 };
 
 template <int ROWCAP, int NNZCAP, int STAGES>
@@ -63,7 +77,7 @@ struct Csr2Layout {
   static constexpr size_t kStageBytes = kValBytes + kColBytes + kRowBytes;
   static constexpr size_t kBarOffset = STAGES * kStageBytes;   // full[S], empty[S]
   static constexpr size_t kMetaOffset = kBarOffset + 16 * STAGES;
-  static constexpr int kMetaInts = 12;
+  static constexpr int kMetaInts = 16;   // 0-8 tile, 9-10 aux ints, 12-15 aux pointers
   static constexpr size_t kSmemBytes = kMetaOffset + 4 * kMetaInts * STAGES + 16;
 };
 
@@ -142,6 +156,10 @@ __device__ bool stream_csr2(S& src, Op& op) {
         int* m = meta + L::kMetaInts * s;
         m[7] = d.skip;
         m[8] = k;
+        m[9] = d.aux2;
+        m[10] = d.aux3;
+        *reinterpret_cast<const void**>(m + 12) = d.aux0;
+        *reinterpret_cast<void**>(m + 14) = d.aux1;
         if (d.skip) {
           mbar_arrive_expect_tx(&full[s], 0);
           continue;
@@ -164,7 +182,7 @@ __device__ bool stream_csr2(S& src, Op& op) {
   } else {
     // ---- consumer warps ----
     const int t = threadIdx.x;
-    int it = 0;
+    int it = 0, pending = -1;   // iteration whose tile awaits op.flush
     for (int k = blockIdx.x; k < count; k += gridDim.x, ++it) {
       const int s = it % STAGES;
       bool stop = !mbar_wait_bounded(&full[s], (unsigned)(it / STAGES) & 1u);
@@ -176,12 +194,18 @@ __device__ bool stream_csr2(S& src, Op& op) {
         *abort_flag = 1;
         break;
       }
+      // Past this barrier every consumer has finished the previous tile:
+      // its deferred reduction (op.flush) can run without a barrier of its own.
+      if (pending >= 0) op.flush(pending);
+      pending = -1;
       const int* m = meta + L::kMetaInts * s;
       if (!m[7]) {
         const int a0 = m[0], c0 = m[1], p0 = m[2], r0 = m[3], r1 = m[4], j0 = m[5];
         double* prod = sval(s) + (j0 - a0);
         const int* cc = scol(s) + (j0 - c0);
-        op.begin(k);
+        const TileAux aux{*reinterpret_cast<const void* const*>(m + 12),
+                          *reinterpret_cast<void* const*>(m + 14), m[9], m[10]};
+        op.begin(k, aux);
         const int* sr = srow(s);
         const int nr = r1 - r0;
         if (nr > kCons / 2) {
@@ -236,11 +260,16 @@ __device__ bool stream_csr2(S& src, Op& op) {
             op.row_done(i, acc);
           }
         }
-        op.tile_end(k);
+        op.tile_end(it);
+        pending = it;
       }
       fence_proxy_async_smem();   // product writes before the next bulk copy
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    if (ok && pending >= 0) {   // the last tile's deferred reduction
+      consumer_bar();
+      op.flush(pending);
     }
   }
   __syncthreads();
