@@ -819,12 +819,11 @@ int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* co
     int r1 = r0;
     while (r1 < n && r1 - r0 < kRows && h.row[r1 + 1] - h.row[r0] <= kNnzCap) ++r1;
     if (r1 == r0) return TF_ERR_LAYOUT;   // one row longer than a tile stage
-    // A tile cut short by its entry cap is trimmed to kRows/2 or kRows/4
-    // rows, so the streamer can give each row 2 or 4 threads.
-    if (r1 < n) {
-      if (r1 - r0 > kRows / 2 && r1 - r0 < kRows) r1 = r0 + kRows / 2;
-      else if (r1 - r0 > kRows / 4 && r1 - r0 < kRows / 2) r1 = r0 + kRows / 4;
-    }
+    // A tile cut short by its entry cap between kRows/2 and kRows rows is
+    // trimmed to kRows/2, so the streamer can give each row 2 threads;
+    // shorter tiles keep their rows (2 or 4 threads per row as they are:
+    // halving them would double the per-tile costs).
+    if (r1 < n && r1 - r0 > kRows / 2 && r1 - r0 < kRows) r1 = r0 + kRows / 2;
     h.tiles.push_back(r1);
     r0 = r1;
   }
