@@ -440,15 +440,17 @@ struct BatchTiles {
 // iteration parity); flush, after the streamer's next barrier, has warp 0
 // sum the kWarps partials in warp order -- the order cta_tile_done uses --
 // and report the tile, one fence and one atomic per tile.
-// Tile reduction for the producer-warp streamer (tf_tile2.cuh), in two
-// halves.  tile_end: every consumer warp parks its partials in shared
-// memory (slot it & 1).  flush, after the streamer's next consumer barrier:
-// warp 0 sums the kWarps partials in warp order -- the order cta_tile_done
-// uses -- and reports the tile (one fence and one atomic per tile).  The
-// streamer's own per-tile barrier orders the two halves, so the reduction
-// costs no barrier of its own; two slots let tile it+1 park while warp 0
-// still flushes tile it.
+// Tile reduction for the producer-warp streamer (tf_tile2.cuh), by its
+// reducer warp: every consumer warp sums its lanes and parks the result in
+// shared memory (slot it & 1, tile_end), consumer thread 0 adds the tile's
+// system and index (tile_id); the reducer warp sums the kWarps partials in
+// warp order -- the order cta_tile_done uses -- and reports the tile.  The
+// consumers never wait for a report.
 __shared__ double g_tile_part[2][kPartQ][kWarps];
+struct TileId {
+  int sys, tile, skip;
+};
+__shared__ TileId g_tile_id[2];
 
 template <int NQ>
 __device__ __forceinline__ void park_partials(double (&v)[NQ], int it) {
@@ -461,35 +463,29 @@ __device__ __forceinline__ void park_partials(double (&v)[NQ], int it) {
   }
 }
 
-// Warp 0 only; true when the tile completed its system (v = totals).
+// The reducer warp: the parked tile's totals, in warp order.
 template <int NQ>
-__device__ __forceinline__ bool flush_partials(double (&v)[NQ], int it, unsigned* sys_cnt,
-                                               double* tile_tot, double* chunk_tot,
-                                               unsigned* chunk_cnt, int ntiles, int tile) {
+__device__ __forceinline__ void sum_partials(double (&v)[NQ], int it) {
   const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
     const double w = lane < kWarps ? g_tile_part[it & 1][q][lane] : 0.0;
     v[q] = warp_sum(w);
   }
-  return warp_tile_done<NQ>(sys_cnt, tile_tot, chunk_tot, chunk_cnt, ntiles, tile, v);
 }
 
-// q = A p (FP64 values, FP64 row sums), p.q per tile, alpha per system.
 template <typename V>
 struct SpmvOp2 {
+  static constexpr bool kReducer = true;
   const SysDev<V>* D;
   SysState* st;
   const Work* work;
   double acc;
   const V* p;
   V* q;
-  int sys, tile, prev_sys, prev_tile;
   __device__ void begin(int, TileAux aux) {
     p = static_cast<const V*>(aux.a0);
     q = static_cast<V*>(aux.a1);
-    sys = aux.i2;
-    tile = aux.i3;
   }
   __device__ double gather(int c) const { return (double)__ldg(p + c); }
   __device__ double row_init(int) const { return 0.0; }
@@ -503,17 +499,21 @@ struct SpmvOp2 {
     double v[1] = {acc};
     acc = 0.0;
     park_partials<1>(v, it);
-    prev_sys = sys;
-    prev_tile = tile;
   }
-  __device__ void flush(int it) {
-    if ((threadIdx.x >> 5) != 0) return;
-    const SysDev<V>& d = D[prev_sys];
+  __device__ void flush(int) {}
+  __device__ void tile_id(int it, int skip, TileAux aux) {
+    g_tile_id[it & 1] = TileId{aux.i2, aux.i3, skip};
+  }
+  __device__ void reduce_tile(int it) {
+    const TileId id = g_tile_id[it & 1];
+    if (id.skip) return;
     double v[1];
-    if (flush_partials<1>(v, it, &st[prev_sys].cnt_spmv, d.tile_tot, d.chunk_tot, d.chunk_cnt,
-                          d.ntiles, prev_tile) &&
+    sum_partials<1>(v, it);
+    const SysDev<V>& d = D[id.sys];
+    if (warp_tile_done<1>(&st[id.sys].cnt_spmv, d.tile_tot, d.chunk_tot, d.chunk_cnt, d.ntiles,
+                          id.tile, v) &&
         (threadIdx.x & 31) == 0) {
-      SysState& s = st[prev_sys];
+      SysState& s = st[id.sys];
       if (!(v[0] > 0.0)) s.status = kBreakdown;   // p.q <= 0 or NaN
       else s.alpha = __ddiv_rn(s.rho, v[0]);
     }
@@ -521,11 +521,10 @@ struct SpmvOp2 {
 };
 
 template <typename V, typename VT>
-__global__ void __launch_bounds__(kCsr2Threads, 2) kb_spmv(BatchArgs a) {
+__global__ void __launch_bounds__(kCsr2RedThreads, 2) kb_spmv(BatchArgs a) {
   if constexpr (sizeof(VT) == 8) {
     BatchTiles<V, 0> src{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, *a.nwork};
-    SpmvOp2<V> op{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, 0.0, nullptr, nullptr,
-                  0, 0, 0, 0};
+    SpmvOp2<V> op{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, 0.0, nullptr, nullptr};
     stream_csr2<kRows, kNnzCap, kStages>(src, op);
   } else {
     // FP32 values: the one-thread-per-row streamer (kRows threads do the
@@ -629,18 +628,16 @@ struct ResWork {
 // r = b - A x in FP64 for the producer-warp streamer (see ResWork).
 template <typename V>
 struct ResOp2 {
+  static constexpr bool kReducer = true;
   const SysDev<V>* D;
   SysState* st;
   const Work* work;
   double rr, rho, bb;
   const SysDev<V>* d;
   bool init;
-  int sys, tile, prev_sys, prev_tile;
   __device__ void begin(int, TileAux aux) {
     d = static_cast<const SysDev<V>*>(aux.a0);
-    sys = aux.i2;
-    tile = aux.i3;
-    init = st[sys].status == kInit;
+    init = st[aux.i2].status == kInit;
   }
   __device__ double gather(int c) const { return d->x[c]; }
   __device__ double row_init(int i) const { return d->b[i]; }
@@ -661,25 +658,29 @@ struct ResOp2 {
     double v[3] = {rr, rho, bb};
     rr = rho = bb = 0.0;
     park_partials<3>(v, it);
-    prev_sys = sys;
-    prev_tile = tile;
   }
-  __device__ void flush(int it) {
-    if ((threadIdx.x >> 5) != 0) return;
-    const SysDev<V>& dd = D[prev_sys];
+  __device__ void flush(int) {}
+  __device__ void tile_id(int it, int skip, TileAux aux) {
+    g_tile_id[it & 1] = TileId{aux.i2, aux.i3, skip};
+  }
+  __device__ void reduce_tile(int it) {
+    const TileId id = g_tile_id[it & 1];
+    if (id.skip) return;
     double v[3];
-    if (flush_partials<3>(v, it, &st[prev_sys].cnt_res, dd.tile_tot, dd.chunk_tot,
-                          dd.chunk_cnt, dd.ntiles, prev_tile) &&
+    sum_partials<3>(v, it);
+    const SysDev<V>& dd = D[id.sys];
+    if (warp_tile_done<3>(&st[id.sys].cnt_res, dd.tile_tot, dd.chunk_tot, dd.chunk_cnt,
+                          dd.ntiles, id.tile, v) &&
         (threadIdx.x & 31) == 0)
-      res_finish(st[prev_sys], dd, v);
+      res_finish(st[id.sys], dd, v);
   }
 };
 
 template <typename V>
-__global__ void __launch_bounds__(kCsr2Threads, 2) kb_ru_res(BatchArgs a) {
+__global__ void __launch_bounds__(kCsr2RedThreads, 2) kb_ru_res(BatchArgs a) {
   BatchTiles<V, 1> src{static_cast<const SysDev<V>*>(a.desc), a.st, a.ru.items, *a.ru.count};
   ResOp2<V> op{static_cast<const SysDev<V>*>(a.desc), a.st, a.ru.items, 0.0, 0.0, 0.0,
-               nullptr, false, 0, 0, 0, 0};
+               nullptr, false};
   stream_csr2<kRows, kNnzCap, kStages>(src, op);
   // The last CTA to leave empties the refinement list for the next iteration.
   if (threadIdx.x == 0) {
@@ -949,10 +950,10 @@ struct tf_batch_s {
   void launch_iteration(cudaStream_t s, const BatchArgs& a) {
     kb_pupdate<V><<<grid_plain, 256, 0, s>>>(a);
     if (opts.val_fp32) kb_spmv<V, float><<<grid_tile, kRows, smem_rows32(), s>>>(a);
-    else kb_spmv<V, double><<<grid_tile, kCsr2Threads, smem_csr2(), s>>>(a);
+    else kb_spmv<V, double><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
     kb_update<V><<<grid_plain, 256, 0, s>>>(a);
     kb_ru_fold<V><<<grid_plain, 256, 0, s>>>(a);
-    kb_ru_res<V><<<grid_tile, kCsr2Threads, smem_csr2(), s>>>(a);
+    kb_ru_res<V><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
   }
 
   template <typename V>
@@ -968,7 +969,7 @@ struct tf_batch_s {
                                      (int)smem_csr2()));
     int per_sm = 1;
     TF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_spmv<V, double>,
-                                                              kCsr2Threads, smem_csr2()));
+                                                              kCsr2RedThreads, smem_csr2()));
     grid_tile = std::max(1, per_sm) * ctx->sm_count;
     grid_plain = ctx->sm_count * 8;
     return TF_OK;

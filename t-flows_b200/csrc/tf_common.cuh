@@ -298,6 +298,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar,
   }
   return true;
 }
+// The same wait, also ending (false) once *abort_flag is set.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, unsigned parity,
+                                                   volatile int* abort_flag) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*abort_flag || globaltimer_ns() - t0 > kWaitLimitNs) return false;
+  }
+  return true;
+}
 // Global -> shared bulk copy completing on `bar`.  dst, src 16-byte aligned,
 // bytes a multiple of 16.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src,

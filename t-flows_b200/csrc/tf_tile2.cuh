@@ -42,6 +42,13 @@
 //   void flush(int it)             -- the same tile, later: after a barrier
 //                                     that every consumer has passed since
 //                                     tile_end(it) (reductions over warps)
+//   static constexpr bool kReducer -- true: a reducer warp (one more warp,
+//                                     kCsr2RedThreads per CTA) takes over
+//                                     the tile reductions:
+//   void tile_id(int it, int skip, TileAux aux) -- consumer warp 0, lane 0,
+//                                     before the tile's partials are parked
+//   void reduce_tile(int it)       -- the reducer warp, once every consumer
+//                                     warp has parked tile it (tile_end)
 #pragma once
 #include "tf_common.cuh"
 
@@ -49,6 +56,7 @@ namespace tf {
 
 constexpr int kCons = 512;               // consumer threads per CTA
 constexpr int kCsr2Threads = kCons + 32;  // + the producer warp
+constexpr int kCsr2RedThreads = kCsr2Threads + 32;   // + a reducer warp
 
 struct TileDesc {
   const int* row;
@@ -78,7 +86,9 @@ struct Csr2Layout {
   static constexpr size_t kBarOffset = STAGES * kStageBytes;   // full[S], empty[S]
   static constexpr size_t kMetaOffset = kBarOffset + 16 * STAGES;
   static constexpr int kMetaInts = 16;   // 0-8 tile, 9-10 aux ints, 12-15 aux pointers
-  static constexpr size_t kSmemBytes = kMetaOffset + 4 * kMetaInts * STAGES + 16;
+  // parked[2], freed[2]: the reducer warp's hand-over (after the abort flag)
+  static constexpr size_t kRedBarOffset = kMetaOffset + 4 * kMetaInts * STAGES + 16;
+  static constexpr size_t kSmemBytes = kRedBarOffset + 4 * 8;
 };
 
 // Named barrier 1 over the consumer threads only (the producer warp never
@@ -108,6 +118,11 @@ __device__ bool stream_csr2(S& src, Op& op) {
   extern __shared__ __align__(128) unsigned char tf_smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(tf_smem + L::kBarOffset);
   uint64_t* empty = full + STAGES;
+  // Reducer hand-over, by tile parity: parked (every consumer warp has
+  // parked the tile's partials), freed (the reducer is done with them).
+  uint64_t* parked = reinterpret_cast<uint64_t*>(tf_smem + L::kRedBarOffset);
+  uint64_t* freed = parked + 2;
+  constexpr bool kRed = Op::kReducer;
   int* meta = reinterpret_cast<int*>(tf_smem + L::kMetaOffset);
   volatile int* abort_flag = meta + L::kMetaInts * STAGES;
   auto sval = [&](int s) { return reinterpret_cast<double*>(tf_smem + s * L::kStageBytes); };
@@ -125,6 +140,12 @@ __device__ bool stream_csr2(S& src, Op& op) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], kConsWarps);
+    }
+    if constexpr (kRed) {
+      for (int s = 0; s < 2; ++s) {
+        mbar_init(&parked[s], kConsWarps);
+        mbar_init(&freed[s], 1);
+      }
     }
     *abort_flag = 0;
     mbar_fence_init();
@@ -178,6 +199,21 @@ __device__ bool stream_csr2(S& src, Op& op) {
       }
       for (int k = (issued > STAGES ? issued - STAGES : 0); k < issued; ++k)
         mbar_wait_bounded(&full[k % STAGES], (unsigned)(k / STAGES) & 1u);
+    }
+  } else if (warp > kConsWarps) {
+    // ---- reducer warp (Op::kReducer) ----
+    if constexpr (kRed) {
+      int it = 0;
+      for (int k = blockIdx.x; k < count; k += gridDim.x, ++it) {
+        if (!mbar_wait_or_abort(&parked[it & 1], (unsigned)(it >> 1) & 1u, abort_flag)) {
+          ok = false;
+          *abort_flag = 1;
+          break;
+        }
+        op.reduce_tile(it);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&freed[it & 1]);
+      }
     }
   } else {
     // ---- consumer warps ----
@@ -260,8 +296,26 @@ __device__ bool stream_csr2(S& src, Op& op) {
             op.row_done(i, acc);
           }
         }
-        op.tile_end(it);
-        pending = it;
+        if constexpr (!kRed) {
+          op.tile_end(it);
+          pending = it;
+        }
+      }
+      if constexpr (kRed) {
+        // Hand the tile to the reducer warp: its parity slot is free once
+        // the reducer is done with tile it - 2.  A timeout here stops the
+        // CTA at the next tile (every consumer still passes this tile's
+        // barriers).
+        if (it >= 2 && !mbar_wait_bounded(&freed[it & 1], (unsigned)((it >> 1) - 1) & 1u)) {
+          ok = false;
+          *abort_flag = 1;
+        }
+        if (!m[7]) op.tile_end(it);
+        if (t == 0)
+          op.tile_id(it, m[7], TileAux{*reinterpret_cast<const void* const*>(m + 12),
+                                       *reinterpret_cast<void* const*>(m + 14), m[9], m[10]});
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&parked[it & 1]);
       }
       fence_proxy_async_smem();   // product writes before the next bulk copy
       __syncwarp();
