@@ -303,14 +303,19 @@ __device__ bool stream_csr2(S& src, Op& op) {
       }
       if constexpr (kRed) {
         // Hand the tile to the reducer warp: its parity slot is free once
-        // the reducer is done with tile it - 2.  A timeout here stops the
-        // CTA at the next tile (every consumer still passes this tile's
-        // barriers).
-        if (it >= 2 && !mbar_wait_bounded(&freed[it & 1], (unsigned)((it >> 1) - 1) & 1u)) {
+        // the reducer is done with tile it - 2.  A timeout or an abort here
+        // stops the CTA at the next tile (every consumer still passes this
+        // tile's barriers; the tile is not parked).
+        // (Warp-uniform: tile_end shuffles across the warp.)
+        const bool slot_free = __all_sync(
+            0xffffffffu,
+            it < 2 ||
+                mbar_wait_or_abort(&freed[it & 1], (unsigned)((it >> 1) - 1) & 1u, abort_flag));
+        if (!slot_free) {
           ok = false;
           *abort_flag = 1;
         }
-        if (!m[7]) op.tile_end(it);
+        if (!m[7] && slot_free) op.tile_end(it);
         if (t == 0)
           op.tile_id(it, m[7], TileAux{*reinterpret_cast<const void* const*>(m + 12),
                                        *reinterpret_cast<void* const*>(m + 14), m[9], m[10]});
