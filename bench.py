@@ -162,7 +162,7 @@ def _batch_solve(ctx, sysl, **opts):
                     max_systems=len(sysl) + 8, **opts)
     try:
         t0 = time.perf_counter()
-        ids = [b.add(s, tol=1e-10, maxit=100000) for s in sysl]
+        ids = b.add_many(sysl, tol=1e-10, maxit=100000)   # host preparation on all cores
         t_add = time.perf_counter() - t0
         t1 = time.perf_counter()
         b.run()

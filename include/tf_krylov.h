@@ -192,6 +192,18 @@ int tf_batch_destroy(tf_batch b);
 int tf_batch_add(tf_batch b, int n, int64_t nnz, const int* row, const int* col,
                  const int* dia, const double* val, const double* rhs,
                  const double* x0, double tol, int maxit, int* sys);
+/* Several systems at once (array i holds system i's arguments of
+ * tf_batch_add; x0 may be NULL, or x0[i] NULL for zeros).  The host
+ * preparation runs on `threads` threads (0: one per hardware thread);
+ * systems are admitted in order, so sys[] and the results equal count calls
+ * of tf_batch_add.  On an error the systems before the failing one stay
+ * added (sys[i] >= 0), the rest get sys[i] = -1.  No reference counterpart
+ * (the reference solves one system per call). */
+int tf_batch_add_many(tf_batch b, int count, const int* n, const int64_t* nnz,
+                      const int* const* row, const int* const* col, const int* const* dia,
+                      const double* const* val, const double* const* rhs,
+                      const double* const* x0, const double* tol, const int* maxit,
+                      int threads, int* sys);
 /* Iterate until every system has converged or stopped. */
 int tf_batch_run(tf_batch b);
 /* x (host, n doubles) may be NULL; true_rel_res = ||b-Ax||_2/||b||_2 in FP64;

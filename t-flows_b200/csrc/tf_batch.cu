@@ -1279,6 +1279,82 @@ extern "C" int tf_batch_add(tf_batch bt, int n, int64_t nnz, const int* row, con
   return bt->admit(h, sys);
 }
 
+// Several systems in one call: the host preparation (conversion,
+// renumbering, tiling) runs on `threads` worker threads (0: one per
+// hardware thread) while this thread admits the prepared systems in order,
+// so slots, results and errors are those of tf_batch_add called for each
+// system in turn.  At most 2 x threads prepared systems wait for admission.
+extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int64_t* nnz,
+                                 const int* const* row, const int* const* col,
+                                 const int* const* dia, const double* const* val,
+                                 const double* const* rhs, const double* const* x0,
+                                 const double* tol, const int* maxit, int threads, int* sys) {
+  if (!bt || count < 0) return TF_ERR_ARG;
+  if (count == 0) return TF_OK;
+  if (!n || !nnz || !row || !col || !dia || !val || !rhs || !tol || !maxit || !sys)
+    return TF_ERR_ARG;
+  for (int i = 0; i < count; ++i) sys[i] = -1;
+  TF_CUDA_TRY(cudaSetDevice(bt->ctx->device));
+  int nt = threads > 0 ? threads : (int)std::thread::hardware_concurrency();
+  nt = std::max(1, std::min(std::min(nt, count), 64));
+  const int window = 2 * nt;
+  std::vector<HostSys> hs(count);
+  std::vector<int> st(count, TF_OK);
+  std::vector<char> ready(count, 0);
+  std::mutex mu;
+  std::condition_variable cv_ready, cv_room;
+  int next = 0, admitted = 0;
+  bool stop = false;
+  auto worker = [&]() {
+    for (;;) {
+      int i;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_room.wait(lk, [&] { return stop || next >= count || next < admitted + window; });
+        if (stop || next >= count) return;
+        i = next++;
+      }
+      const int r = prepare_host(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
+                                 x0 ? x0[i] : nullptr, tol[i], maxit[i], bt->opts.val_fp32);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        st[i] = r;
+        ready[i] = 1;
+      }
+      cv_ready.notify_all();
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t) pool.emplace_back(worker);
+  int result = TF_OK;
+  for (int i = 0; i < count; ++i) {
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv_ready.wait(lk, [&] { return ready[i] != 0; });
+    }
+    int r = st[i];
+    if (r == TF_OK) r = bt->admit(hs[i], &sys[i]);
+    hs[i] = HostSys();   // its host copy is on the device now
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      admitted = i + 1;
+      if (r != TF_OK) stop = true;
+    }
+    cv_room.notify_all();
+    if (r != TF_OK) {
+      result = r;
+      break;
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    stop = true;
+  }
+  cv_room.notify_all();
+  for (auto& t : pool) t.join();
+  return result;
+}
+
 extern "C" int tf_batch_run(tf_batch bt) {
   if (!bt) return TF_ERR_ARG;
   TF_CUDA_TRY(cudaSetDevice(bt->ctx->device));

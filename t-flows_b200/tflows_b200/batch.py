@@ -24,6 +24,8 @@ def _lib():
     L.tf_batch_destroy.argtypes = [_vp]
     L.tf_batch_add.argtypes = [_vp, ctypes.c_int, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp,
                                _vp, ctypes.c_double, ctypes.c_int, ip]
+    L.tf_batch_add_many.argtypes = [_vp, ctypes.c_int, ip, ctypes.POINTER(ctypes.c_int64),
+                                    _vp, _vp, _vp, _vp, _vp, _vp, dp, ip, ctypes.c_int, ip]
     L.tf_batch_run.argtypes = [_vp]
     L.tf_batch_result.argtypes = [_vp, ctypes.c_int, _vp, ip, dp, ip, ip, dp]
     L.tf_batch_remove.argtypes = [_vp, ctypes.c_int]
@@ -75,6 +77,30 @@ class Batch:
                                           ctypes.byref(sid)), "tf_batch_add")
         self.n[sid.value] = s.n
         return sid.value
+
+    def add_many(self, systems, tol=1e-10, maxit=20000, threads=0):
+        """tf_batch_add_many: the host preparation of the systems runs on
+        `threads` threads (0: all hardware threads); ids and results equal
+        add() called for each system in order."""
+        cnt = len(systems)
+        if cnt == 0:
+            return []
+        packed = [_sys_args(s) for s in systems]
+        keep = [k for k, _ in packed]
+        cols = list(zip(*[a for _, a in packed]))   # n, nnz, row, col, dia, val, b, x0
+        ptrs = [(_vp * cnt)(*c) for c in cols[2:]]
+        n = (ctypes.c_int * cnt)(*cols[0])
+        nnz = (ctypes.c_int64 * cnt)(*cols[1])
+        tols = (ctypes.c_double * cnt)(*([float(tol)] * cnt))
+        its = (ctypes.c_int * cnt)(*([int(maxit)] * cnt))
+        sid = (ctypes.c_int * cnt)()
+        st = self.L.tf_batch_add_many(self.h, cnt, n, nnz, *ptrs, tols, its, int(threads), sid)
+        del keep
+        for s, i in zip(systems, sid):
+            if i >= 0:
+                self.n[i] = s.n
+        native._check(st, "tf_batch_add_many")
+        return list(sid)
 
     def run(self):
         native._check(self.L.tf_batch_run(self.h), "tf_batch_run")

@@ -33,7 +33,7 @@ EXPORTS = [
     "tf_ctx_sync", "tf_ctx_stream", "tf_last_error_message", "tf_matrix_tile_config",
     "tf_matrix_row_patterns", "tf_matrix_renumbered",
     "tf_faces_register", "tf_assemble_pressure", "tf_assemble_momentum",
-    "tf_solve_multi", "tf_solve_multi_device",
+    "tf_solve_multi", "tf_solve_multi_device", "tf_batch_add_many",
 ]
 
 

@@ -98,6 +98,45 @@ def test_batch_alone_equals_in_mix(gpu_ctx):
         assert np.array_equal(mix[k]["x"], alone[k]["x"])
 
 
+@pytest.mark.parametrize("threads", [1, 3, 0])
+def test_batch_add_many_equals_adds(gpu_ctx, threads):
+    """tf_batch_add_many prepares on worker threads and admits in order:
+    the same ids, iterations and bits as one tf_batch_add per system."""
+    sysl = mixed_systems()
+    out = []
+    for many in (False, True):
+        b = batch.Batch(gpu_ctx, mem_budget=1 << 30)
+        try:
+            ids = b.add_many(sysl, threads=threads) if many else [b.add(s) for s in sysl]
+            b.run()
+            out.append((ids, [b.result(i) for i in ids]))
+        finally:
+            b.close()
+    (ids0, r0), (ids1, r1) = out
+    assert ids0 == ids1
+    for a, c in zip(r0, r1):
+        assert a["iters"] == c["iters"] and a["status"] == c["status"] == "converged"
+        assert np.array_equal(a["x"], c["x"])
+
+
+def test_batch_add_many_stops_at_the_budget(gpu_ctx):
+    """Systems before the first that does not fit stay added; the rest get -1."""
+    from tflows_b200 import native
+    small = [systems.small_hex(4, seed=k, kind="pressure") for k in (1, 2)]
+    big = systems.small_hex(40, seed=3, kind="pressure")
+    b = batch.Batch(gpu_ctx, mem_budget=1 << 20)
+    try:
+        with pytest.raises(native.TFError) as e:
+            b.add_many(small + [big] + small, threads=2)
+        assert e.value.status == 7     # TF_ERR_BUSY
+        b.run()
+        assert len(b.n) == 2
+        for i in b.n:
+            assert b.result(i)["status"] == "converged"
+    finally:
+        b.close()
+
+
 def test_batch_memory_budget(gpu_ctx):
     big = systems.small_hex(40, seed=1, kind="pressure")
     b = batch.Batch(gpu_ctx, mem_budget=1 << 20)
