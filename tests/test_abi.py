@@ -60,3 +60,7 @@ def test_null_arguments_rejected(lib):
     r = ctypes.c_double()
     assert lib.tf_solve(None, None, 0, 1, None, None, None, 10, ctypes.byref(n), 1e-6,
                         ctypes.byref(r), None) == 3
+    # batched entry points reject a missing handle before touching a device
+    assert lib.tf_batch_add_many(None, 0, None, None, None, None, None, None, None, None,
+                                 None, None, 0, None) == 3
+    assert lib.tf_batch_run(None) == 3
