@@ -435,11 +435,6 @@ struct BatchTiles {
   }
 };
 
-// Per-tile partials of the producer-warp streamer's consumer warps: each
-// warp sums its lanes and parks the result in a double buffer (by consumer
-// iteration parity); flush, after the streamer's next barrier, has warp 0
-// sum the kWarps partials in warp order -- the order cta_tile_done uses --
-// and report the tile, one fence and one atomic per tile.
 // Tile reduction for the producer-warp streamer (tf_tile2.cuh), by its
 // reducer warp: every consumer warp sums its lanes and parks the result in
 // shared memory (slot it & 1, tile_end), consumer thread 0 adds the tile's
@@ -500,7 +495,6 @@ struct SpmvOp2 {
     acc = 0.0;
     park_partials<1>(v, it);
   }
-  __device__ void flush(int) {}
   __device__ void tile_id(int it, int skip, TileAux aux) {
     g_tile_id[it & 1] = TileId{aux.i2, aux.i3, skip};
   }
@@ -659,7 +653,6 @@ struct ResOp2 {
     rr = rho = bb = 0.0;
     park_partials<3>(v, it);
   }
-  __device__ void flush(int) {}
   __device__ void tile_id(int it, int skip, TileAux aux) {
     g_tile_id[it & 1] = TileId{aux.i2, aux.i3, skip};
   }

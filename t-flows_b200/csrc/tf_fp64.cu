@@ -209,7 +209,6 @@ struct OpSpmvDot {
   }
   // two-phase streamer
   __device__ __forceinline__ void begin(int, TileAux) {}
-  __device__ __forceinline__ void flush(int) {}
   static constexpr bool kReducer = false;
   __device__ __forceinline__ double gather(int c) const { return __ldg(p + c); }
   __device__ __forceinline__ double row_init(int) const { return 0.0; }
@@ -266,7 +265,6 @@ struct OpResidual {
   }
   // two-phase streamer
   __device__ __forceinline__ void begin(int, TileAux) {}
-  __device__ __forceinline__ void flush(int) {}
   static constexpr bool kReducer = false;
   __device__ __forceinline__ double gather(int c) const { return __ldg(x + c); }
   __device__ __forceinline__ double row_init(int i) const { return b[i]; }

@@ -39,9 +39,6 @@
 //   void row_done(int i, double acc)
 //   void tile_end(int it)          -- after the rows of the tile of consumer
 //                                     iteration `it` (no barriers)
-//   void flush(int it)             -- the same tile, later: after a barrier
-//                                     that every consumer has passed since
-//                                     tile_end(it) (reductions over warps)
 //   static constexpr bool kReducer -- true: a reducer warp (one more warp,
 //                                     kCsr2RedThreads per CTA) takes over
 //                                     the tile reductions:
@@ -218,7 +215,7 @@ __device__ bool stream_csr2(S& src, Op& op) {
   } else {
     // ---- consumer warps ----
     const int t = threadIdx.x;
-    int it = 0, pending = -1;   // iteration whose tile awaits op.flush
+    int it = 0;
     for (int k = blockIdx.x; k < count; k += gridDim.x, ++it) {
       const int s = it % STAGES;
       bool stop = !mbar_wait_bounded(&full[s], (unsigned)(it / STAGES) & 1u);
@@ -230,10 +227,6 @@ __device__ bool stream_csr2(S& src, Op& op) {
         *abort_flag = 1;
         break;
       }
-      // Past this barrier every consumer has finished the previous tile:
-      // its deferred reduction (op.flush) can run without a barrier of its own.
-      if (pending >= 0) op.flush(pending);
-      pending = -1;
       const int* m = meta + L::kMetaInts * s;
       if (!m[7]) {
         const int a0 = m[0], c0 = m[1], p0 = m[2], r0 = m[3], r1 = m[4], j0 = m[5];
@@ -296,10 +289,7 @@ __device__ bool stream_csr2(S& src, Op& op) {
             op.row_done(i, acc);
           }
         }
-        if constexpr (!kRed) {
-          op.tile_end(it);
-          pending = it;
-        }
+        if constexpr (!kRed) op.tile_end(it);
       }
       if constexpr (kRed) {
         // Hand the tile to the reducer warp: its parity slot is free once
@@ -325,10 +315,6 @@ __device__ bool stream_csr2(S& src, Op& op) {
       fence_proxy_async_smem();   // product writes before the next bulk copy
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
-    }
-    if (ok && pending >= 0) {   // the last tile's deferred reduction
-      consumer_bar();
-      op.flush(pending);
     }
   }
   __syncthreads();
