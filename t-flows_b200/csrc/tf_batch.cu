@@ -774,8 +774,9 @@ int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* co
     h.dia[i] = d;
   }
   // Scattered numbering: renumber by reverse Cuthill-McKee, each row keeping
-  // its entries in storage order (the same row sums; see tf_renumber.cu).
-  std::vector<long long> src;   // entry j here is entry src[j] of the caller's
+  // its entries (and values) in storage order (the same row sums; see
+  // tf_renumber.cu).
+  bool have_val = false;
   h.perm.clear();
   if (n >= kRenumberMinRows && !getenv("TF_NO_RENUMBER")) {
     const double before = tf_gather_lines_per_warp(h.row.data(), h.col.data(), n, 0);
@@ -784,16 +785,17 @@ int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* co
       tf_rcm_order(h.row, h.col, n, order);
       for (int i = 0; i < n; ++i) inv[order[i]] = i;
       std::vector<int> row2(h.row.size()), col2(h.col.size(), 0), dia2(h.dia.size(), 0);
-      std::vector<long long> src2((size_t)nnz);
+      std::vector<double> val2((size_t)nnz + 8, 0.0);
       row2[0] = 0;
       for (int i = 0; i < n; ++i) {
         const int o = order[i], js = h.row[o], len = h.row[o + 1] - js;
+        const int r = row2[i];
         for (int k = 0; k < len; ++k) {
-          src2[row2[i] + k] = js + k;
-          col2[row2[i] + k] = inv[h.col[js + k]];
+          col2[r + k] = inv[h.col[js + k]];
+          val2[r + k] = val[js + k];
         }
-        dia2[i] = row2[i] + (h.dia[o] - js);
-        row2[i + 1] = row2[i] + len;
+        dia2[i] = r + (h.dia[o] - js);
+        row2[i + 1] = r + len;
       }
       for (size_t i = n + 1; i < row2.size(); ++i) row2[i] = row2[n];
       if (tf_gather_lines_per_warp(row2.data(), col2.data(), n, 0) <= 0.8 * before) {
@@ -801,7 +803,8 @@ int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* co
         h.col.swap(col2);
         h.dia.swap(dia2);
         h.perm.swap(order);
-        src.swap(src2);
+        h.val.swap(val2);
+        have_val = true;
       }
     }
   }
@@ -821,13 +824,10 @@ int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* co
     h.tiles.push_back(r1);
     r0 = r1;
   }
-  if (src.empty()) {
+  if (!have_val) {
     h.val.assign(val, val + nnz);
-  } else {
-    h.val.resize((size_t)nnz);
-    for (long long j = 0; j < nnz; ++j) h.val[j] = val[src[j]];
+    h.val.resize((size_t)nnz + 8, 0.0);
   }
-  h.val.resize((size_t)nnz + 8, 0.0);
   if (use_val32) {
     h.val32.resize((size_t)nnz + 8);
     for (long long j = 0; j < nnz + 8; ++j) h.val32[j] = (float)h.val[j];
