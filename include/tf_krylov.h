@@ -194,7 +194,8 @@ int tf_batch_add(tf_batch b, int n, int64_t nnz, const int* row, const int* col,
                  const double* x0, double tol, int maxit, int* sys);
 /* Several systems at once (array i holds system i's arguments of
  * tf_batch_add; x0 may be NULL, or x0[i] NULL for zeros).  The host
- * preparation runs on `threads` threads (0: one per hardware thread);
+ * preparation runs on `threads` threads (0: one per hardware thread, at
+ * most 64), holding at most 2 x threads prepared host copies at a time;
  * systems are admitted in order, so sys[] and the results equal count calls
  * of tf_batch_add.  On an error the systems before the failing one stay
  * added (sys[i] >= 0), the rest get sys[i] = -1.  No reference counterpart
