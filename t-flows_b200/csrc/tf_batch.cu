@@ -52,6 +52,9 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <new>
+#include <stdexcept>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -749,9 +752,9 @@ struct HostSys {
   int maxit = 10000;
 };
 
-int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* col,
-                 const int* dia, const double* val, const double* b, const double* x0,
-                 double tol, int maxit, int use_val32) {
+int prepare_host_impl(HostSys& h, int n, long long nnz, const int* row, const int* col,
+                      const int* dia, const double* val, const double* b, const double* x0,
+                      double tol, int maxit, int use_val32) {
   if (n < 1 || nnz < n || !row || !col || !dia || !val || !b) return TF_ERR_ARG;
   if (row[0] != 1 || (long long)row[n] - 1 != nnz) return TF_ERR_LAYOUT;
   h.n = n;
@@ -845,6 +848,22 @@ int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* co
     }
   }
   return TF_OK;
+}
+
+// prepare_host_impl without exceptions across the C ABI: a host
+// allocation that fails is TF_ERR_OOM.
+int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* col,
+                 const int* dia, const double* val, const double* b, const double* x0,
+                 double tol, int maxit, int use_val32) {
+  try {
+    return prepare_host_impl(h, n, nnz, row, col, dia, val, b, x0, tol, maxit, use_val32);
+  } catch (const std::bad_alloc&) {
+    h = HostSys();
+    return TF_ERR_OOM;
+  } catch (const std::length_error&) {
+    h = HostSys();
+    return TF_ERR_OOM;
+  }
 }
 
 // Byte layout of one system's segment.
@@ -1318,10 +1337,18 @@ extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int
     }
   };
   std::vector<std::thread> pool;
-  for (int t = 0; t < nt; ++t) pool.emplace_back(worker);
+  try {
+    for (int t = 0; t < nt; ++t) pool.emplace_back(worker);
+  } catch (const std::system_error&) {
+    // fewer workers than asked for (none: this thread prepares each system)
+  }
+  const bool inline_prep = pool.empty();
   int result = TF_OK;
   for (int i = 0; i < count; ++i) {
-    {
+    if (inline_prep) {
+      st[i] = prepare_host(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
+                           x0 ? x0[i] : nullptr, tol[i], maxit[i], bt->opts.val_fp32);
+    } else {
       std::unique_lock<std::mutex> lk(mu);
       cv_ready.wait(lk, [&] { return ready[i] != 0; });
     }
