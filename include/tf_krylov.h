@@ -35,13 +35,16 @@ extern "C" {
 enum tf_status {
   TF_OK = 0,
   TF_ERR_CUDA = 1,           /* a CUDA runtime call failed                       */
-  TF_ERR_OOM = 2,            /* device allocation failed or over memory budget   */
+  TF_ERR_OOM = 2,            /* device (or host) allocation failed, or over the
+                                memory budget                                  */
   TF_ERR_ARG = 3,            /* bad argument (null pointer, size, index range)   */
   TF_ERR_TIMEOUT = 4,        /* a bounded device-side wait gave up               */
   TF_ERR_LAYOUT = 5,         /* CSR layout violates Matrix_Type's contract       */
   TF_ERR_NO_DEVICE = 6,      /* no CUDA device / driver                          */
   TF_ERR_BUSY = 7,           /* serving queue full or handle in use              */
   TF_ERR_CANCELLED = 8,      /* request cancelled before it finished             */
+  TF_ERR_HOST = 9,           /* host-side failure (no entry point lets a C++
+                                exception escape; host out-of-memory is OOM)  */
   TF_ERR_UNKNOWN_SOLVER = 64,
   TF_ERR_UNKNOWN_PREC = 72
 };

@@ -41,13 +41,14 @@ extern "C" const char* tf_status_string(int status) {
   switch (status) {
     case TF_OK: return "ok";
     case TF_ERR_CUDA: return "CUDA runtime error";
-    case TF_ERR_OOM: return "out of device memory";
+    case TF_ERR_OOM: return "out of memory";
     case TF_ERR_ARG: return "invalid argument";
     case TF_ERR_TIMEOUT: return "bounded device wait timed out";
     case TF_ERR_LAYOUT: return "CSR layout violates Matrix_Type contract";
     case TF_ERR_NO_DEVICE: return "no CUDA device";
     case TF_ERR_BUSY: return "busy";
     case TF_ERR_CANCELLED: return "cancelled";
+    case TF_ERR_HOST: return "host-side failure";
     case TF_ERR_UNKNOWN_SOLVER: return "unknown native solver";
     case TF_ERR_UNKNOWN_PREC: return "unknown preconditioner";
     default: return "unknown status";
@@ -60,6 +61,7 @@ extern "C" const char* tf_version(void) { return "tfkrylov 0.1 sm_100a"; }
 // Contexts
 // ---------------------------------------------------------------------------
 extern "C" int tf_ctx_create(int device, tf_ctx* out) {
+  TF_API_BEGIN
   if (!out) return TF_ERR_ARG;
   *out = nullptr;
   int ndev = 0;
@@ -84,49 +86,62 @@ extern "C" int tf_ctx_create(int device, tf_ctx* out) {
   }
   *out = c;
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_ctx_destroy(tf_ctx ctx) {
+  TF_API_BEGIN
   if (!ctx) return TF_ERR_ARG;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_ctx_sync(tf_ctx ctx) {
+  TF_API_BEGIN
   if (!ctx) return TF_ERR_ARG;
   TF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" void* tf_ctx_stream(tf_ctx ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 extern "C" int tf_ctx_set_history(tf_ctx ctx, int enable) {
+  TF_API_BEGIN
   if (!ctx) return TF_ERR_ARG;
   ctx->history = enable ? 1 : 0;
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_last_history(tf_ctx ctx, double* hist, int cap, int* count) {
+  TF_API_BEGIN
   if (!ctx || !count || (cap > 0 && !hist)) return TF_ERR_ARG;
   const int n = std::min(cap, ctx->last_count);
   for (int i = 0; i < n; ++i) hist[i] = ctx->last_hist[i];
   *count = ctx->last_count;
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_host_pin(void* ptr, size_t bytes) {
+  TF_API_BEGIN
   if (!ptr || bytes == 0) return TF_ERR_ARG;
   TF_CUDA_TRY(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_host_unpin(void* ptr) {
+  TF_API_BEGIN
   if (!ptr) return TF_ERR_ARG;
   TF_CUDA_TRY(cudaHostUnregister(ptr));
   return TF_OK;
+  TF_API_END
 }
 
 // ---------------------------------------------------------------------------
@@ -260,8 +275,10 @@ int64_t max_tile_nnz(const std::vector<int>& row0, int ni, int rows) {
 extern "C" int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own,
                                   int64_t nnz, const int* row, const int* col,
                                   const int* dia, tf_matrix* out) {
+  TF_API_BEGIN
   if (!ctx || !out) return TF_ERR_ARG;
   return tf_matrix_create(ctx, n_cells, n_own, nnz, row, col, dia, 1, out);
+  TF_API_END
 }
 
 namespace {
@@ -472,29 +489,37 @@ int matrix_create_impl(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const
 }  // namespace
 
 extern "C" int tf_matrix_release(tf_matrix m) {
+  TF_API_BEGIN
   if (!m) return TF_ERR_ARG;
   cudaSetDevice(m->ctx->device);
   cudaStreamSynchronize(m->ctx->stream);
   tf_matrix_free(m);
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_matrix_row_patterns(tf_matrix m) {
+  TF_API_BEGIN
   return m ? m->npat : TF_ERR_ARG;
+  TF_API_END
 }
 
 extern "C" int tf_matrix_renumbered(tf_matrix m) {
+  TF_API_BEGIN
   return m ? (m->ren != nullptr) : TF_ERR_ARG;
+  TF_API_END
 }
 
 extern "C" int tf_matrix_info(tf_matrix m, int* n_cells, int* n_own,
                               int64_t* nnz, int* max_row_len) {
+  TF_API_BEGIN
   if (!m) return TF_ERR_ARG;
   if (n_cells) *n_cells = m->nt;
   if (n_own) *n_own = m->ni;
   if (nnz) *nnz = m->nnz;
   if (max_row_len) *max_row_len = m->max_row_len;
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_matrix_tile_config(tf_matrix m) { return m ? m->tile_cfg : -1; }
@@ -594,6 +619,7 @@ extern "C" int tf_solve(tf_ctx ctx, tf_matrix m, int solver, int prec,
                         double* val, double* x, double* b, int miter,
                         int* niter, double tol, double* fin_res,
                         const double* norm) {
+  TF_API_BEGIN
   int st = check_solve_args(ctx, m, solver, prec, niter, fin_res);
   if (st != TF_OK) return st;
   if (m->nt == 0) {
@@ -618,12 +644,14 @@ extern "C" int tf_solve(tf_ctx ctx, tf_matrix m, int solver, int prec,
   TF_CUDA_TRY(cudaMemcpyAsync(x, m->d_x, nb, cudaMemcpyDeviceToHost, s));
   TF_CUDA_TRY(cudaMemcpyAsync(b, m->d_b, nb, cudaMemcpyDeviceToHost, s));
   return finish_solve(m, niter, fin_res);
+  TF_API_END
 }
 
 extern "C" int tf_solve_device(tf_ctx ctx, tf_matrix m, int solver, int prec,
                                double* d_val, double* d_x, double* d_b,
                                int miter, int* niter, double tol,
                                double* fin_res, const double* norm) {
+  TF_API_BEGIN
   int st = check_solve_args(ctx, m, solver, prec, niter, fin_res);
   if (st != TF_OK) return st;
   if (m->nt == 0) {
@@ -648,6 +676,7 @@ extern "C" int tf_solve_device(tf_ctx ctx, tf_matrix m, int solver, int prec,
   TF_CUDA_TRY(cudaMemcpyAsync(d_x, m->d_x, nb, cudaMemcpyDeviceToDevice, s));
   TF_CUDA_TRY(cudaMemcpyAsync(d_b, m->d_b, nb, cudaMemcpyDeviceToDevice, s));
   return finish_solve(m, niter, fin_res);
+  TF_API_END
 }
 
 // ---------------------------------------------------------------------------
@@ -714,6 +743,7 @@ int check_multi_args(tf_ctx ctx, tf_matrix m, int solver, int prec, int nrhs, in
 extern "C" int tf_solve_multi(tf_ctx ctx, tf_matrix m, int solver, int prec, int nrhs,
                               double* val, double* x, double* b, int miter, int* niter,
                               double tol, double* fin_res, const double* norm) {
+  TF_API_BEGIN
   int st = check_multi_args(ctx, m, solver, prec, nrhs, niter, fin_res);
   if (st != TF_OK) return st;
   if (m->nt == 0) {
@@ -747,12 +777,14 @@ extern "C" int tf_solve_multi(tf_ctx ctx, tf_matrix m, int solver, int prec, int
                                 cudaMemcpyDeviceToHost, s));
   }
   return finish_multi(m, nrhs, niter, fin_res);
+  TF_API_END
 }
 
 extern "C" int tf_solve_multi_device(tf_ctx ctx, tf_matrix m, int solver, int prec, int nrhs,
                                      double* d_val, double* d_x, double* d_b, int miter,
                                      int* niter, double tol, double* fin_res,
                                      const double* norm) {
+  TF_API_BEGIN
   int st = check_multi_args(ctx, m, solver, prec, nrhs, niter, fin_res);
   if (st != TF_OK) return st;
   if (m->nt == 0) {
@@ -783,6 +815,7 @@ extern "C" int tf_solve_multi_device(tf_ctx ctx, tf_matrix m, int solver, int pr
     TF_CUDA_TRY(cudaMemcpyAsync(d_b + (size_t)i * m->nt, rhs_b(m, i), nb, dd, s));
   }
   return finish_multi(m, nrhs, niter, fin_res);
+  TF_API_END
 }
 
 namespace {
@@ -798,6 +831,7 @@ extern "C" int tf_solve_native(tf_ctx ctx, tf_matrix m, const char* solver,
                                const char* prec, double* val, double* x,
                                double* b, int miter, int* niter, double tol,
                                double* fin_res, const double* norm) {
+  TF_API_BEGIN
   if (!solver || !prec) return TF_ERR_ARG;
   int s;
   if (name_is(solver, "bicg")) s = TF_SOLVER_BICG;        // Solve_Native.f90:33
@@ -809,6 +843,7 @@ extern "C" int tf_solve_native(tf_ctx ctx, tf_matrix m, const char* solver,
   else if (name_is(prec, "none")) p = TF_PREC_NONE;
   else return TF_ERR_UNKNOWN_PREC;
   return tf_solve(ctx, m, s, p, val, x, b, miter, niter, tol, fin_res, norm);
+  TF_API_END
 }
 
 // ---------------------------------------------------------------------------
@@ -816,29 +851,35 @@ extern "C" int tf_solve_native(tf_ctx ctx, tf_matrix m, const char* solver,
 // ---------------------------------------------------------------------------
 extern "C" int tf_spmv(tf_ctx ctx, tf_matrix m, const double* d_val,
                        const double* d_p, double* d_q, double* d_pq) {
+  TF_API_BEGIN
   if (!ctx || !m || m->ctx != ctx) return TF_ERR_ARG;
   if (m->nt == 0) return TF_OK;
   if (!d_val || !d_p || !d_q) return TF_ERR_ARG;
   if (((uintptr_t)d_val & 15) != 0) return TF_ERR_ARG;  // bulk copies need 16 B
   TF_CUDA_TRY(cudaSetDevice(ctx->device));
   return tf_fp64_spmv(m, d_val, d_p, d_q, d_pq);
+  TF_API_END
 }
 
 extern "C" int tf_residual(tf_ctx ctx, tf_matrix m, const double* d_val,
                            const double* d_b, const double* d_x, double* d_r) {
+  TF_API_BEGIN
   if (!ctx || !m || m->ctx != ctx) return TF_ERR_ARG;
   if (m->nt == 0) return TF_OK;
   if (!d_val || !d_b || !d_x || !d_r) return TF_ERR_ARG;
   if (((uintptr_t)d_val & 15) != 0) return TF_ERR_ARG;
   TF_CUDA_TRY(cudaSetDevice(ctx->device));
   return tf_fp64_residual(m, d_val, d_b, d_x, d_r);
+  TF_API_END
 }
 
 extern "C" int tf_nrms(tf_ctx ctx, tf_matrix m, const double* d_val,
                        const double* d_r, const double* d_x,
                        const double* norm, double* d_out) {
+  TF_API_BEGIN
   if (!ctx || !m || m->ctx != ctx || !d_val || !d_r || !d_x || !d_out) return TF_ERR_ARG;
   if (m->nt == 0) return TF_ERR_ARG;
   TF_CUDA_TRY(cudaSetDevice(ctx->device));
   return tf_fp64_nrms(m, d_val, d_r, d_x, norm ? 1 : 0, norm ? *norm : 0.0, d_out);
+  TF_API_END
 }

@@ -144,6 +144,7 @@ using namespace tf;
 
 extern "C" int tf_faces_register(tf_ctx ctx, tf_matrix m, int n_faces, const int* faces_c,
                                  const int* pos) {
+  TF_API_BEGIN
   if (!ctx || !m || m->ctx != ctx || n_faces < 0 || (n_faces > 0 && (!faces_c || !pos)))
     return TF_ERR_ARG;
   const int n = m->nt;
@@ -197,6 +198,7 @@ extern "C" int tf_faces_register(tf_ctx ctx, tf_matrix m, int n_faces, const int
   TF_CUDA_TRY(cudaStreamSynchronize(s));
   m->n_faces = n_faces;
   return TF_OK;
+  TF_API_END
 }
 
 namespace {
@@ -208,6 +210,7 @@ int grid_for(tf_matrix_s* m, int items) {
 extern "C" int tf_assemble_pressure(tf_ctx ctx, tf_matrix m, const double* d_fc,
                                     const double* d_fw, const double* d_vm,
                                     const int* d_bnd_open, double* d_val) {
+  TF_API_BEGIN
   if (!ctx || !m || m->ctx != ctx || !m->d_cf_ptr || !d_fc || !d_fw || !d_val)
     return TF_ERR_ARG;
   std::lock_guard<std::mutex> lk(m->mu);
@@ -222,11 +225,13 @@ extern "C" int tf_assemble_pressure(tf_ctx ctx, tf_matrix m, const double* d_fc,
                                                    d_val);
   TF_CUDA_TRY(cudaGetLastError());
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_assemble_momentum(tf_ctx ctx, tf_matrix m, const double* d_fc,
                                     const double* d_flux, const int* d_bnd_wall, double vis,
                                     double rho, const double* d_vol, double dt, double* d_val) {
+  TF_API_BEGIN
   if (!ctx || !m || m->ctx != ctx || !m->d_cf_ptr || !d_fc || !d_flux || !d_vol || !d_val)
     return TF_ERR_ARG;
   std::lock_guard<std::mutex> lk(m->mu);
@@ -242,4 +247,5 @@ extern "C" int tf_assemble_momentum(tf_ctx ctx, tf_matrix m, const double* d_fc,
                                                    d_vol, dt, d_val);
   TF_CUDA_TRY(cudaGetLastError());
   return TF_OK;
+  TF_API_END
 }

@@ -1262,6 +1262,7 @@ struct tf_batch_s {
 // C ABI: batches
 // ---------------------------------------------------------------------------
 extern "C" int tf_batch_create(tf_ctx ctx, const tf_batch_opts* opts, tf_batch* out) {
+  TF_API_BEGIN
   if (!ctx || !out) return TF_ERR_ARG;
   *out = nullptr;
   auto* b = new tf_batch_s();
@@ -1272,23 +1273,28 @@ extern "C" int tf_batch_create(tf_ctx ctx, const tf_batch_opts* opts, tf_batch* 
   }
   *out = b;
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_batch_destroy(tf_batch b) {
+  TF_API_BEGIN
   if (!b) return TF_ERR_ARG;
   delete b;
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_batch_add(tf_batch bt, int n, int64_t nnz, const int* row, const int* col,
                             const int* dia, const double* val, const double* b,
                             const double* x0, double tol, int maxit, int* sys) {
+  TF_API_BEGIN
   if (!bt || !sys) return TF_ERR_ARG;
   HostSys h;
   int st = prepare_host(h, n, nnz, row, col, dia, val, b, x0, tol, maxit, bt->opts.val_fp32);
   if (st != TF_OK) return st;
   TF_CUDA_TRY(cudaSetDevice(bt->ctx->device));
   return bt->admit(h, sys);
+  TF_API_END
 }
 
 // Several systems in one call: the host preparation (conversion,
@@ -1301,6 +1307,7 @@ extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int
                                  const int* const* dia, const double* const* val,
                                  const double* const* rhs, const double* const* x0,
                                  const double* tol, const int* maxit, int threads, int* sys) {
+  TF_API_BEGIN
   if (!bt || count < 0) return TF_ERR_ARG;
   if (count == 0) return TF_OK;
   if (!n || !nnz || !row || !col || !dia || !val || !rhs || !tol || !maxit || !sys)
@@ -1373,17 +1380,21 @@ extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int
   cv_room.notify_all();
   for (auto& t : pool) t.join();
   return result;
+  TF_API_END
 }
 
 extern "C" int tf_batch_run(tf_batch bt) {
+  TF_API_BEGIN
   if (!bt) return TF_ERR_ARG;
   TF_CUDA_TRY(cudaSetDevice(bt->ctx->device));
   return bt->run_all();
+  TF_API_END
 }
 
 extern "C" int tf_batch_result(tf_batch bt, int sys, double* x, int* iters,
                                double* true_rel_res, int* status, int* n_updates,
                                double* done_ms) {
+  TF_API_BEGIN
   if (!bt || sys < 0 || sys >= bt->max_sys || !bt->slots[sys].used) return TF_ERR_ARG;
   const SysState& s = bt->h_state[sys];
   if (done_ms) *done_ms = bt->slots[sys].done_ms;
@@ -1393,20 +1404,25 @@ extern "C" int tf_batch_result(tf_batch bt, int sys, double* x, int* iters,
   if (n_updates) *n_updates = s.n_ru;
   if (x) return bt->fetch_x(sys, x);
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_batch_remove(tf_batch bt, int sys) {
+  TF_API_BEGIN
   if (!bt || sys < 0 || sys >= bt->max_sys || !bt->slots[sys].used) return TF_ERR_ARG;
   bt->retire(sys);
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_batch_info(tf_batch bt, int* sweeps, int* work_items, size_t* free_bytes) {
+  TF_API_BEGIN
   if (!bt) return TF_ERR_ARG;
   if (sweeps) *sweeps = bt->sweeps;
   if (work_items) *work_items = bt->nwork;
   if (free_bytes) *free_bytes = bt->arena.free_bytes();
   return TF_OK;
+  TF_API_END
 }
 
 // ---------------------------------------------------------------------------
@@ -1536,6 +1552,7 @@ struct tf_server_s {
 };
 
 extern "C" int tf_server_create(tf_ctx ctx, const tf_batch_opts* opts, tf_server* out) {
+  TF_API_BEGIN
   if (!ctx || !out) return TF_ERR_ARG;
   *out = nullptr;
   auto* s = new tf_server_s();
@@ -1547,12 +1564,14 @@ extern "C" int tf_server_create(tf_ctx ctx, const tf_batch_opts* opts, tf_server
   s->worker = std::thread([s] { s->loop(); });
   *out = s;
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_server_submit(tf_server sv, int n, int64_t nnz, const int* row,
                                 const int* col, const int* dia, const double* val,
                                 const double* b, const double* x0, double tol, int maxit,
                                 int64_t* req) {
+  TF_API_BEGIN
   if (!sv || !req) return TF_ERR_ARG;
   auto r = std::make_shared<Request>();
   const int st = prepare_host(r->h, n, nnz, row, col, dia, val, b, x0, tol, maxit,
@@ -1567,11 +1586,13 @@ extern "C" int tf_server_submit(tf_server sv, int n, int64_t nnz, const int* row
   *req = r->id;
   sv->cv_work.notify_one();
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_server_wait(tf_server sv, int64_t req, double* x, int* iters,
                               double* true_rel_res, int* status, double* latency_ms,
                               double* queue_ms) {
+  TF_API_BEGIN
   if (!sv) return TF_ERR_ARG;
   std::unique_lock<std::mutex> lk(sv->mu);
   auto it = sv->live.find(req);
@@ -1590,10 +1611,12 @@ extern "C" int tf_server_wait(tf_server sv, int64_t req, double* x, int* iters,
   if (r->status < 0) return -r->status;
   if (x && !r->x.empty()) memcpy(x, r->x.data(), r->x.size() * sizeof(double));
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_server_stats(tf_server sv, long long* admitted, long long* completed,
                                int* peak_running, int* sweeps) {
+  TF_API_BEGIN
   if (!sv) return TF_ERR_ARG;
   std::lock_guard<std::mutex> lk(sv->mu);
   if (admitted) *admitted = sv->admitted;
@@ -1601,9 +1624,11 @@ extern "C" int tf_server_stats(tf_server sv, long long* admitted, long long* com
   if (peak_running) *peak_running = sv->peak_running;
   if (sweeps) *sweeps = sv->eng.sweeps;
   return sv->error;
+  TF_API_END
 }
 
 extern "C" int tf_server_destroy(tf_server sv) {
+  TF_API_BEGIN
   if (!sv) return TF_ERR_ARG;
   {
     std::lock_guard<std::mutex> lk(sv->mu);
@@ -1619,4 +1644,5 @@ extern "C" int tf_server_destroy(tf_server sv) {
   if (sv->worker.joinable()) sv->worker.join();
   delete sv;
   return TF_OK;
+  TF_API_END
 }

@@ -3,12 +3,25 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <mutex>
+#include <new>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "../../include/tf_krylov.h"
 #include "tf_common.cuh"
+
 #include "tf_tile.cuh"
+
+// Every int-returning C-ABI entry point runs its body between TF_API_BEGIN
+// and TF_API_END, so no C++ exception crosses the C ABI: a failed host
+// allocation returns TF_ERR_OOM, any other exception TF_ERR_HOST.
+#define TF_API_BEGIN try {
+#define TF_API_END                                              \
+  }                                                             \
+  catch (const std::bad_alloc&) { return TF_ERR_OOM; }          \
+  catch (const std::length_error&) { return TF_ERR_OOM; }       \
+  catch (...) { return TF_ERR_HOST; }
 
 #define TF_CUDA_TRY(expr)                                       \
   do {                                                          \

@@ -99,6 +99,7 @@ int scratch_for_current_device(unsigned char** out) {
 extern "C" int tf_spmv_noalloc(int n, const int* d_row, const int* d_col,
                                const double* d_val, const double* d_p,
                                double* d_q, double* d_pq, void* stream) {
+  TF_API_BEGIN
   if (n < 0 || (n > 0 && (!d_row || !d_col || !d_val || !d_p || !d_q || !d_pq)))
     return TF_ERR_ARG;
   if ((long long)n > kNoAllocMaxRows) {
@@ -124,4 +125,5 @@ extern "C" int tf_spmv_noalloc(int n, const int* d_row, const int* d_col,
                                                          d_pq, scratch);
   TF_CUDA_TRY(cudaGetLastError());
   return TF_OK;
+  TF_API_END
 }

@@ -245,6 +245,7 @@ struct tf_pool_s {
 };
 
 extern "C" int tf_pool_create(int device, int workers, size_t mem_budget, tf_pool* out) {
+  TF_API_BEGIN
   if (!out || workers < 1 || workers > 256) return TF_ERR_ARG;
   *out = nullptr;
   auto* p = new tf_pool_s();
@@ -276,12 +277,14 @@ extern "C" int tf_pool_create(int device, int workers, size_t mem_budget, tf_poo
   for (int w = 0; w < workers; ++w) p->workers.emplace_back([p, w] { p->loop(w); });
   *out = p;
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_pool_submit(tf_pool p, int solver, int prec, int n, int64_t nnz,
                               const int* row, const int* col, const int* dia,
                               const double* val, const double* b, double* x,
                               int miter, double tol, const double* norm, int64_t* req) {
+  TF_API_BEGIN
   if (!p || !req || n < 1 || nnz < n || !row || !col || !dia || !val || !b || !x)
     return TF_ERR_ARG;
   if (solver != TF_SOLVER_CG && solver != TF_SOLVER_BICG) return TF_ERR_UNKNOWN_SOLVER;
@@ -321,10 +324,12 @@ extern "C" int tf_pool_submit(tf_pool p, int solver, int prec, int n, int64_t nn
   }
   *req = r->id;
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_pool_wait(tf_pool p, int64_t req, int* niter, double* fin_res,
                             double* latency_ms, double* queue_ms) {
+  TF_API_BEGIN
   if (!p) return TF_ERR_ARG;
   std::unique_lock<std::mutex> lk(p->mu);
   auto it = p->live.find(req);
@@ -339,10 +344,12 @@ extern "C" int tf_pool_wait(tf_pool p, int64_t req, int* niter, double* fin_res,
   if (niter) *niter = r->niter;
   if (fin_res) *fin_res = r->fin_res;
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_pool_stats(tf_pool p, long long* submitted, long long* completed,
                              long long* rejected, size_t* peak_bytes) {
+  TF_API_BEGIN
   if (!p) return TF_ERR_ARG;
   std::lock_guard<std::mutex> lk(p->mu);
   if (submitted) *submitted = p->submitted;
@@ -350,9 +357,11 @@ extern "C" int tf_pool_stats(tf_pool p, long long* submitted, long long* complet
   if (rejected) *rejected = p->rejected;
   if (peak_bytes) *peak_bytes = p->peak;
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_pool_resident(tf_pool p, long long* reused, int* held, size_t* held_bytes) {
+  TF_API_BEGIN
   if (!p) return TF_ERR_ARG;
   std::lock_guard<std::mutex> lk(p->mu);
   if (reused) *reused = p->reused;
@@ -363,9 +372,11 @@ extern "C" int tf_pool_resident(tf_pool p, long long* reused, int* held, size_t*
     *held_bytes = b;
   }
   return TF_OK;
+  TF_API_END
 }
 
 extern "C" int tf_pool_destroy(tf_pool p) {
+  TF_API_BEGIN
   if (!p) return TF_ERR_ARG;
   {
     std::lock_guard<std::mutex> lk(p->mu);
@@ -392,4 +403,5 @@ extern "C" int tf_pool_destroy(tf_pool p) {
   }
   delete p;
   return TF_OK;
+  TF_API_END
 }

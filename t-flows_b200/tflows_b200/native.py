@@ -18,7 +18,7 @@ TF_OK = 0
 STATUS = {
     0: "TF_OK", 1: "TF_ERR_CUDA", 2: "TF_ERR_OOM", 3: "TF_ERR_ARG",
     4: "TF_ERR_TIMEOUT", 5: "TF_ERR_LAYOUT", 6: "TF_ERR_NO_DEVICE",
-    7: "TF_ERR_BUSY", 8: "TF_ERR_CANCELLED", 64: "TF_ERR_UNKNOWN_SOLVER",
+    7: "TF_ERR_BUSY", 8: "TF_ERR_CANCELLED", 9: "TF_ERR_HOST", 64: "TF_ERR_UNKNOWN_SOLVER",
     72: "TF_ERR_UNKNOWN_PREC",
 }
 SOLVERS = {"cg": 0, "bicg": 1}

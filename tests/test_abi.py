@@ -39,6 +39,7 @@ def test_status_strings(lib):
     assert lib.tf_status_string(0) == b"ok"
     assert lib.tf_status_string(64) == b"unknown native solver"
     assert lib.tf_status_string(72) == b"unknown preconditioner"
+    assert lib.tf_status_string(9) == b"host-side failure"
     assert b"sm_100a" in lib.tf_version()
 
 
