@@ -1360,7 +1360,7 @@ extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int
       cv_ready.wait(lk, [&] { return ready[i] != 0; });
     }
     int r = st[i];
-    if (r == TF_OK) r = bt->admit(hs[i], &sys[i]);
+    if (r == TF_OK) r = tf_guarded([&] { return bt->admit(hs[i], &sys[i]); });
     hs[i] = HostSys();   // its host copy is on the device now
     {
       std::lock_guard<std::mutex> lk(mu);
@@ -1478,7 +1478,7 @@ struct tf_server_s {
           r = queue.front();
         }
         int slot = -1;
-        const int st = eng.admit(r->h, &slot);
+        const int st = tf_guarded([&] { return eng.admit(r->h, &slot); });
         if (st == TF_ERR_BUSY) {
           if (by_slot.empty()) {   // cannot ever fit: fail the request
             std::lock_guard<std::mutex> lk(mu);
@@ -1510,8 +1510,8 @@ struct tf_server_s {
       if (by_slot.empty()) continue;
       peak_running = std::max(peak_running, (int)by_slot.size());
       int st = TF_OK;
-      if (changed) st = eng.rebuild_work();
-      if (st == TF_OK) st = eng.run_sweep();
+      if (changed) st = tf_guarded([&] { return eng.rebuild_work(); });
+      if (st == TF_OK) st = tf_guarded([&] { return eng.run_sweep(); });
       if (st != TF_OK) {
         std::lock_guard<std::mutex> lk(mu);
         error = st;

@@ -23,6 +23,21 @@
   catch (const std::length_error&) { return TF_ERR_OOM; }       \
   catch (...) { return TF_ERR_HOST; }
 
+// The same for work done on the library's own threads (pool workers, the
+// server loop): f's status, or the status of the exception it threw.
+template <class F>
+int tf_guarded(F&& f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc&) {
+    return TF_ERR_OOM;
+  } catch (const std::length_error&) {
+    return TF_ERR_OOM;
+  } catch (...) {
+    return TF_ERR_HOST;
+  }
+}
+
 #define TF_CUDA_TRY(expr)                                       \
   do {                                                          \
     cudaError_t _e = (expr);                                    \

@@ -211,7 +211,7 @@ struct tf_pool_s {
         }
         r->t_start = Clock::now();
       }
-      const int st = run(ctx, *r, &m);
+      const int st = tf_guarded([&] { return run(ctx, *r, &m); });
       {
         std::lock_guard<std::mutex> lk(mu);
         if (h >= 0) {
