@@ -24,9 +24,12 @@
 // released the stage (empty[s]).  Consumers meet at a named barrier before
 // each tile (to agree on stopping) and between the two phases (the
 // products of a row come from other threads) -- the producer never waits
-// there.  All waits are bounded; on a
-// timeout the CTA stops, the producer drains its armed copies and the
-// streamer returns false.
+// there.  With Op::kReducer a third role, the reducer warp (after the
+// producer), takes each tile's parked partials over two mbarriers (parked:
+// every consumer warp has parked the tile; freed: the reducer is done with
+// its slot), so no consumer waits for a tile's report.  All waits are
+// bounded; on a timeout the CTA stops, the producer drains its armed copies
+// and the streamer returns false.
 //
 // The tile source `S` provides (producer lane only):
 //   int count()                    -- tiles (items) to walk
