@@ -1,16 +1,25 @@
 """Generate the golden fixtures under tests/golden/ (committed).
 
-Each fixture is a small seeded system in Matrix_Type layout plus the
-expected outputs of Native_Mod's Cg/Bicg.  The expected outputs come from
-the C++ restatement (oracle/tf_oracle.cpp, one thread) and are cross-checked
-here, bit for bit, against the independent pure-Python transliteration
-(oracle/pyref.py); the script refuses to write a fixture on any mismatch.
-The reference itself cannot be run here (it is Fortran and no Fortran
-compiler exists), so these fixtures pin the restatements against each other
-and against the hand example of Matrix_Mod.f90:44-55, not against reference
-output.
+Each fixture is a seeded system in Matrix_Type layout plus the expected
+outputs of Native_Mod's Solve_Native (Cg/Bicg).  The expected outputs are
+those of the reference's own Fortran source
+(Sources/Process/Cpu/Native_Mod/*.f90, executed by oracle/f90exec.py,
+which needs the T-Flows tree), and the script refuses to write a fixture
+unless three other evaluations agree with it bit for bit (x, val, b, niter,
+fin_res): the C++ restatement (oracle/tf_oracle.cpp, one thread) and the
+pure-Python transliteration (oracle/pyref.py).
 
-    python tests/golden/make_golden.py
+Two kinds of fixture:
+  * small systems stored whole (row, col, dia, val, b, x0 and outputs);
+  * `gen_*` fixtures of the 30^3 lid-driven-cavity pressure system (27,000
+    cells), stored as the generator call that rebuilds the inputs, a SHA-256
+    of those inputs, and the reference source's outputs.  The singular
+    system is made solvable both ways the workload allows: one cell pinned
+    by an open pressure-boundary face, and the reference's own Set_Singular
+    (Solver_Mod/Set_Singular.f90, executed too).
+
+    python tests/golden/make_golden.py            # everything (~2 minutes)
+    python tests/golden/make_golden.py --small    # the small fixtures only
 """
 import os
 import sys
@@ -22,6 +31,9 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "t-flows_b200"))
 
+import hashlib  # noqa: E402
+
+from oracle import f90exec  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 from oracle import pyref  # noqa: E402
 from tflows_b200 import grids, systems  # noqa: E402
@@ -84,26 +96,93 @@ def run_oracle(c):
     return x, val, b, r
 
 
-def main():
+def run_reference(c):
+    """The reference's Solve_Native on the case, from its Fortran source."""
+    r = f90exec.solve_native(c["solver"], c["prec"], c["row"], c["col"], c["dia"], c["val"],
+                             c["x0"], c["b"], c["miter"], c["tol"], c["norm"])
+    return np.array(r["x"]), np.array(r["val"]), np.array(r["b"]), r["niter"], r["fin_res"]
+
+
+def same(a, b):
+    return (np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+            and np.array_equal(a[2], b[2]) and a[3] == b[3] and a[4] == b[4])
+
+
+def input_sha(row, col, dia, val, b, x0):
+    h = hashlib.sha256()
+    for a in (row, col, dia):
+        h.update(np.ascontiguousarray(a, dtype=np.int32).tobytes())
+    for a in (val, b, x0):
+        h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def ldc30(singular):
+    """The 30^3 lid-driven-cavity pressure system; `set_singular` applies the
+    reference's own Set_Singular to the unshifted matrix and checks that the
+    generator's numpy version gives the same values."""
+    if singular == "pin":
+        return systems.ldc_pressure_30(seed=1, singular="pin")
+    s = systems.ldc_pressure_30(seed=1, singular="none")
+    ref_val = np.array(f90exec.set_singular(s.csr.row, s.csr.dia, s.val))
+    systems.set_singular(s.csr, s.val)
+    if not np.array_equal(ref_val, s.val):
+        raise SystemExit("Set_Singular: reference source and generator differ")
+    return s
+
+
+def generated_cases():
+    out = []
+    for singular in ("pin", "set_singular"):
+        out.append(dict(name=f"gen_ldc30_{singular}_cg_jacobi",
+                        generator=f"ldc_pressure_30(seed=1, singular={singular!r})",
+                        build=lambda singular=singular: ldc30(singular)))
+    return out
+
+
+def main(small_only=False):
+    if not f90exec.available():
+        raise SystemExit("the T-Flows sources are needed to generate the fixtures")
     for c in cases():
         x, val, b, r = run_oracle(c)
-        px, pval, pb, pit, pres = pyref.solve(c["solver"], c["prec"], c["row"], c["col"],
-                                              c["dia"], c["val"], c["x0"], c["b"],
-                                              c["miter"], c["tol"], c["norm"])
-        same = (np.array_equal(x, np.array(px)) and np.array_equal(val, np.array(pval))
-                and np.array_equal(b, np.array(pb)) and r["niter"] == pit
-                and r["fin_res"] == pres)
-        if not same:
-            raise SystemExit(f"{c['name']}: C++ oracle and Python transliteration differ")
+        ref = run_reference(c)
+        py = pyref.solve(c["solver"], c["prec"], c["row"], c["col"], c["dia"], c["val"],
+                         c["x0"], c["b"], c["miter"], c["tol"], c["norm"])
+        py = (np.array(py[0]), np.array(py[1]), np.array(py[2]), py[3], py[4])
+        if not same(ref, (x, val, b, r["niter"], r["fin_res"])):
+            raise SystemExit(f"{c['name']}: reference source and C++ oracle differ")
+        if not same(ref, py):
+            raise SystemExit(f"{c['name']}: reference source and Python transliteration differ")
         path = os.path.join(HERE, c["name"] + ".npz")
         np.savez_compressed(
             path, row=c["row"], col=c["col"], dia=c["dia"], val=c["val"], b=c["b"],
             x0=c["x0"], solver=c["solver"], prec=c["prec"], miter=c["miter"], tol=c["tol"],
-            norm=np.nan if c["norm"] is None else c["norm"], x_out=x, val_out=val,
-            b_out=b, niter=r["niter"], fin_res=r["fin_res"], hist=r["hist"])
+            norm=np.nan if c["norm"] is None else c["norm"], x_out=ref[0], val_out=ref[1],
+            b_out=ref[2], niter=ref[3], fin_res=ref[4], hist=r["hist"],
+            source="reference Fortran source via oracle/f90exec.py")
         print(f"{c['name']}: n={len(c['row']) - 1} niter={r['niter']} "
-              f"fin_res={r['fin_res']:.3e}")
+              f"fin_res={r['fin_res']:.3e} (reference source = C++ oracle = pyref)")
+    if small_only:
+        return
+    for g in generated_cases():
+        s = g["build"]()
+        c = dict(row=s.csr.row, col=s.csr.col, dia=s.csr.dia, val=s.val, b=s.b, x0=s.x0,
+                 solver=s.solver, prec=s.prec, miter=s.miter, tol=s.tol, norm=s.norm)
+        x, val, b, r = run_oracle(c)
+        ref = run_reference(c)
+        if not same(ref, (x, val, b, r["niter"], r["fin_res"])):
+            raise SystemExit(f"{g['name']}: reference source and C++ oracle differ")
+        path = os.path.join(HERE, g["name"] + ".npz")
+        np.savez_compressed(
+            path, generator=g["generator"],
+            input_sha256=input_sha(c["row"], c["col"], c["dia"], c["val"], c["b"], c["x0"]),
+            solver=c["solver"], prec=c["prec"], miter=c["miter"], tol=c["tol"],
+            norm=np.nan if c["norm"] is None else c["norm"], x_out=ref[0], niter=ref[3],
+            fin_res=ref[4], hist=r["hist"],
+            source="reference Fortran source via oracle/f90exec.py")
+        print(f"{g['name']}: n={s.n} niter={ref[3]} fin_res={ref[4]:.3e} "
+              f"(reference source = C++ oracle)")
 
 
 if __name__ == "__main__":
-    main()
+    main(small_only="--small" in sys.argv)

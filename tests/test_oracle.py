@@ -5,7 +5,7 @@ import pytest
 import scipy.sparse as sps
 import scipy.sparse.linalg as spla
 
-from conftest import golden_cases
+from conftest import build_generated, generated_cases, golden_cases
 from oracle import oracle as O
 from oracle import pyref
 from tflows_b200 import grids, systems
@@ -173,3 +173,16 @@ def test_nrms_definition():
     assert abs(got - want) <= 1e-13 * want
     assert O.nrms(s.csr.row, s.csr.col, s.csr.dia, s.val, r, x, norm=2.0) == pytest.approx(
         np.sqrt(np.sum(r * r / (a * a))) / 2.0, rel=1e-13)
+
+
+@pytest.mark.parametrize("case", generated_cases(), ids=lambda c: c["name"])
+def test_generated_fixture_inputs_are_reproducible(case):
+    """The 30^3 fixtures hold the reference source's outputs; their inputs
+    are rebuilt from the generator (SHA-256 checked) -- here without the
+    reference: the oracle must reproduce them bit for bit."""
+    s = build_generated(case)
+    v, x, bb = s.val.copy(), s.x0.copy(), s.b.copy()
+    o = O.solve_native(case["solver"], case["prec"], s.csr.row, s.csr.col, s.csr.dia, v, x,
+                       bb, case["miter"], case["tol"], norm=case["norm"], threads=1)
+    assert o["niter"] == case["niter"] and o["fin_res"] == case["fin_res"]
+    assert np.array_equal(x, case["x_out"])
