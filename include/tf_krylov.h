@@ -29,9 +29,12 @@
 extern "C" {
 #endif
 
-/* Status codes.  64 and 72 are the codes the reference passes to
- * Message % Error for an unknown solver (Solve_Native.f90:38) and an unknown
- * preconditioner (Shared/Control_Mod/Native/Preconditioner_For_System_Matrix.f90:36). */
+/* Status codes.  64 is the code the reference passes to Message % Error for
+ * an unknown solver (Solve_Native.f90:38); 72 the one its control reader uses
+ * for an unknown preconditioner keyword
+ * (Shared/Control_Mod/Native/Preconditioner_For_System_Matrix.f90:36), here
+ * returned for a preconditioner code outside enum tf_prec.  A preconditioner
+ * NAME that is not known runs unpreconditioned, as Solve_Native does. */
 enum tf_status {
   TF_OK = 0,
   TF_ERR_CUDA = 1,           /* a CUDA runtime call failed                       */
@@ -112,9 +115,12 @@ int tf_solve(tf_ctx ctx, tf_matrix m, int solver, int prec, double* val,
 
 /* Same, with the solver and preconditioner given by name as in
  * Solve_Native.f90:33-44 ('cg', 'bicg') and Prec_Form.f90:47-89 ('jacobi',
- * 'icc', anything else = none).  The control-file spellings 'diagonal' and
- * 'incomplete_cholesky' are mapped as Preconditioner_For_System_Matrix.f90:43-44
- * maps them.  Unknown solver -> TF_ERR_UNKNOWN_SOLVER (the reference's 64). */
+ * 'icc', anything else = none: the else branches of Prec_Form and
+ * Prec_Solve, so an unknown name is not an error, as in the reference).
+ * The control-file spellings 'diagonal' and 'incomplete_cholesky' are
+ * mapped as Preconditioner_For_System_Matrix.f90:43-44 maps them.  Trailing
+ * blanks are ignored.  Unknown solver -> TF_ERR_UNKNOWN_SOLVER (the
+ * reference's 64). */
 int tf_solve_native(tf_ctx ctx, tf_matrix m, const char* solver,
                     const char* prec, double* val, double* x, double* b,
                     int miter, int* niter, double tol, double* fin_res,
@@ -122,7 +128,13 @@ int tf_solve_native(tf_ctx ctx, tf_matrix m, const char* solver,
 
 /* Same as tf_solve with val, x and b already in device memory (e.g. an
  * OpenACC `host_data use_device` region).  Nothing crosses PCIe except the
- * two result scalars. */
+ * two result scalars.  When all three are 16-byte aligned (as cudaMalloc'd
+ * arrays are) the solve runs on them in place: the first call with a new
+ * set of arrays builds the solve's CUDA graph on them, later calls with the
+ * same arrays reuse it.  val is then read in 16-byte units, so up to 8
+ * bytes past its last entry are read (inside any cudaMalloc allocation).
+ * Arrays off a 16-byte boundary are copied into the matrix's own buffers
+ * and back (same results). */
 int tf_solve_device(tf_ctx ctx, tf_matrix m, int solver, int prec,
                     double* d_val, double* d_x, double* d_b, int miter,
                     int* niter, double tol, double* fin_res,
@@ -151,6 +163,15 @@ int tf_solve_multi_device(tf_ctx ctx, tf_matrix m, int solver, int prec, int nrh
  * on the device, one extra copy on the host). */
 int tf_ctx_set_history(tf_ctx ctx, int enable);
 int tf_last_history(tf_ctx ctx, double* hist, int cap, int* count);
+
+/* Limit of every bounded device-side wait in this context's solves (a
+ * tile's copies, a free pipeline stage), in seconds; 0 restores the default
+ * of 2 s.  A wait that runs out ends the solve cleanly with TF_ERR_TIMEOUT
+ * (the CTA still waits for the copies it started before it exits, with the
+ * default limit); the context stays usable.  A watchdog against a stalled
+ * device; the reference has none (its failures stop the run,
+ * Shared/Message_Mod/Error.f90:74). */
+int tf_ctx_set_wait_limit(tf_ctx ctx, double seconds);
 
 /* Pin (page-lock) a host array the caller will pass to tf_solve on every
  * call, e.g. A % val, so its copies run at full PCIe/C2C bandwidth.
@@ -337,8 +358,11 @@ void* tf_ctx_stream(tf_ctx ctx);
  *  loads the library keeps until exit.  It bounds n to
  *  TF_SPMV_NOALLOC_MAX_ROWS; larger n returns TF_ERR_ARG (the reason is in
  *  tf_last_error_message).  The first call on a device looks up the array's
- *  device address (cudaGetSymbolAddress, with that device current); make
- *  that first call before any stream capture.  Work is queued on `stream`
+ *  device address (cudaGetSymbolAddress, with that device current) and keeps
+ *  it for the life of the process; make that first call before any stream
+ *  capture.  A cudaDeviceReset of a device the entry point was used on is
+ *  not supported (the kept address would be stale): do not call it on that
+ *  device afterwards.  Work is queued on `stream`
  *  (a cudaStream_t, NULL = legacy default stream) and the call returns
  *  without waiting.  Every call shares the one array: calls that can
  *  overlap on the GPU (different streams, or different host threads on one

@@ -118,6 +118,15 @@ extern "C" int tf_ctx_set_history(tf_ctx ctx, int enable) {
   TF_API_END
 }
 
+extern "C" int tf_ctx_set_wait_limit(tf_ctx ctx, double seconds) {
+  TF_API_BEGIN
+  if (!ctx || !(seconds >= 0.0) || seconds > 3600.0) return TF_ERR_ARG;
+  ctx->wait_ns = (unsigned long long)(seconds * 1e9);
+  if (seconds > 0.0 && ctx->wait_ns == 0) ctx->wait_ns = 1;
+  return TF_OK;
+  TF_API_END
+}
+
 extern "C" int tf_last_history(tf_ctx ctx, double* hist, int cap, int* count) {
   TF_API_BEGIN
   if (!ctx || !count || (cap > 0 && !hist)) return TF_ERR_ARG;
@@ -178,6 +187,8 @@ void tf_matrix_free(tf_matrix_s* m) {
   cudaSetDevice(m->ctx->device);
   tf_matrix_free(m->ren);
   for (auto& g : m->graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto& g : m->ext_graph)
     if (g) cudaGraphExecDestroy(g);
   tf_slices_free(m);
   void* ptrs[] = {m->d_row, m->d_col, m->d_dia, m->d_val, m->d_x, m->d_b,
@@ -552,6 +563,7 @@ int run_solve_core(tf_matrix_s* m, int prec, int miter, double tol,
   hp->miter = miter;
   hp->hist = nullptr;
   hp->hist_cap = 0;
+  hp->wait_ns = c->wait_ns;
   if (c->history && miter >= 0) {
     int st = ensure_hist(a, miter + 1);
     if (st != TF_OK) return st;
@@ -604,6 +616,40 @@ int tf_solve_resident(tf_matrix_s* m, int prec, int miter, double tol, const dou
 }
 
 namespace {
+
+// tf_solve_device on the caller's own arrays: the matrix's val/x/b pointers
+// are bound to them for the length of the solve, and the graphs built on
+// them are kept while the caller passes the same arrays (one rebuild when
+// the arrays change).  A renumbered matrix gathers from and scatters to
+// them directly.  Called with m->mu held.
+int solve_in_place(tf_matrix_s* m, int prec, double* d_val, double* d_x, double* d_b,
+                   int miter, int* niter, double tol, double* fin_res, const double* norm) {
+  if (m->ext_key[0] != d_val || m->ext_key[1] != d_x || m->ext_key[2] != d_b) {
+    for (auto& g : m->ext_graph)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+    m->ext_key[0] = d_val;
+    m->ext_key[1] = d_x;
+    m->ext_key[2] = d_b;
+  }
+  double* own[3] = {m->d_val, m->d_x, m->d_b};
+  m->d_val = d_val;
+  m->d_x = d_x;
+  m->d_b = d_b;
+  m->ext_bound = 1;
+  const int st = run_solve_core(m, prec, miter, tol, norm);
+  m->d_val = own[0];
+  m->d_x = own[1];
+  m->d_b = own[2];
+  m->ext_bound = 0;
+  if (st != TF_OK) {
+    cudaStreamSynchronize(m->ctx->stream);
+    return st;
+  }
+  return finish_solve(m, niter, fin_res);
+}
 
 int check_solve_args(tf_ctx ctx, tf_matrix m, int solver, int prec, int* niter,
                      double* fin_res) {
@@ -663,6 +709,9 @@ extern "C" int tf_solve_device(tf_ctx ctx, tf_matrix m, int solver, int prec,
   std::lock_guard<std::mutex> lk(m->mu);
   TF_CUDA_TRY(cudaSetDevice(ctx->device));
   cudaStream_t s = ctx->stream;
+  if ((((uintptr_t)d_val | (uintptr_t)d_x | (uintptr_t)d_b) & 15) == 0)
+    return solve_in_place(m, prec, d_val, d_x, d_b, miter, niter, tol, fin_res, norm);
+  // Arrays off a 16-byte boundary: solve on the matrix's own buffers.
   const size_t vb = (size_t)m->nnz * sizeof(double), nb = (size_t)m->nt * sizeof(double);
   TF_CUDA_TRY(cudaMemcpyAsync(m->d_val, d_val, vb, cudaMemcpyDeviceToDevice, s));
   TF_CUDA_TRY(cudaMemcpyAsync(m->d_x, d_x, nb, cudaMemcpyDeviceToDevice, s));
@@ -703,6 +752,7 @@ int run_multi_core(tf_matrix_s* m, int prec, int nrhs, int miter, double tol,
   hp->miter = miter;
   hp->hist = nullptr;
   hp->hist_cap = 0;
+  hp->wait_ns = c->wait_ns;
   TF_CUDA_TRY(cudaMemcpyAsync(m->d_params, hp, sizeof(*hp), cudaMemcpyHostToDevice, c->stream));
   int st = tf_fp64_run_multi(m, prec, nrhs);
   if (st != TF_OK) return st;
@@ -837,11 +887,12 @@ extern "C" int tf_solve_native(tf_ctx ctx, tf_matrix m, const char* solver,
   if (name_is(solver, "bicg")) s = TF_SOLVER_BICG;        // Solve_Native.f90:33
   else if (name_is(solver, "cg")) s = TF_SOLVER_CG;       // Solve_Native.f90:35
   else return TF_ERR_UNKNOWN_SOLVER;                      // Solve_Native.f90:38
+  // Prec_Form.f90:47-89 / Prec_Solve.f90:44-102: 'jacobi', 'icc', and any
+  // other name runs unpreconditioned (their else branches).
   int p;
   if (name_is(prec, "jacobi") || name_is(prec, "diagonal")) p = TF_PREC_JACOBI;
   else if (name_is(prec, "icc") || name_is(prec, "incomplete_cholesky")) p = TF_PREC_ICC;
-  else if (name_is(prec, "none")) p = TF_PREC_NONE;
-  else return TF_ERR_UNKNOWN_PREC;
+  else p = TF_PREC_NONE;
   return tf_solve(ctx, m, s, p, val, x, b, miter, niter, tol, fin_res, norm);
   TF_API_END
 }

@@ -1333,8 +1333,10 @@ extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int
         if (stop || next >= count) return;
         i = next++;
       }
-      const int r = prepare_host(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
-                                 x0 ? x0[i] : nullptr, tol[i], maxit[i], bt->opts.val_fp32);
+      const int r = tf_guarded([&] {
+        return prepare_host(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
+                            x0 ? x0[i] : nullptr, tol[i], maxit[i], bt->opts.val_fp32);
+      });
       {
         std::lock_guard<std::mutex> lk(mu);
         st[i] = r;
@@ -1353,8 +1355,10 @@ extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int
   int result = TF_OK;
   for (int i = 0; i < count; ++i) {
     if (inline_prep) {
-      st[i] = prepare_host(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
-                           x0 ? x0[i] : nullptr, tol[i], maxit[i], bt->opts.val_fp32);
+      st[i] = tf_guarded([&] {
+        return prepare_host(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
+                            x0 ? x0[i] : nullptr, tol[i], maxit[i], bt->opts.val_fp32);
+      });
     } else {
       std::unique_lock<std::mutex> lk(mu);
       cv_ready.wait(lk, [&] { return ready[i] != 0; });

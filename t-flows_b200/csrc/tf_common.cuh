@@ -14,7 +14,10 @@ constexpr double kMicro = 1.0e-6;
 
 // Upper bound on CTAs of any grid-reduced kernel (size of partial arrays).
 constexpr int kMaxBlocks = 4096;
-// A bounded device-side wait gives up after this many nanoseconds.
+// A bounded device-side wait gives up after this many nanoseconds unless
+// the caller set another limit (tf_ctx_set_wait_limit).  Draining the bulk
+// copies a CTA armed before it exits always uses this default: a kernel
+// never returns with a copy into its shared memory in flight.
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
 
 enum Prec : int { kPrecNone = 0, kPrecJacobi = 1, kPrecIcc = 2 };
@@ -28,7 +31,12 @@ struct SolveParams {
   int hist_cap;       // entries available in hist
   int pad;
   double* hist;       // per-iteration residuals (may be null)
+  unsigned long long wait_ns;   // bounded-wait limit (0: kWaitLimitNs)
 };
+
+__host__ __device__ __forceinline__ unsigned long long wait_limit(const SolveParams* p) {
+  return (p && p->wait_ns) ? p->wait_ns : kWaitLimitNs;
+}
 
 // Device-resident solver state; one per matrix handle.
 struct SolveState {
@@ -289,24 +297,31 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   return ok != 0;
 }
 // Wait for `parity` with a time limit.  Returns false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar,
-                                                  unsigned parity) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity,
+                                                  unsigned long long limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = globaltimer_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
   }
   return true;
 }
 // The same wait, also ending (false) once *abort_flag is set.
 __device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, unsigned parity,
-                                                   volatile int* abort_flag) {
+                                                   volatile int* abort_flag,
+                                                   unsigned long long limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = globaltimer_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (*abort_flag || globaltimer_ns() - t0 > kWaitLimitNs) return false;
+    if (*abort_flag || globaltimer_ns() - t0 > limit_ns) return false;
   }
   return true;
+}
+// Wait for the bulk copies armed on `bar` before the CTA exits: always the
+// default limit (never the caller's), so a short caller limit cannot end a
+// CTA with copies into its shared memory still in flight.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, unsigned parity) {
+  mbar_wait_bounded(bar, parity, kWaitLimitNs);
 }
 // Global -> shared bulk copy completing on `bar`.  dst, src 16-byte aligned,
 // bytes a multiple of 16.

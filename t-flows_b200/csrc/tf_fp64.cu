@@ -326,8 +326,8 @@ struct SpArgs {
 template <int CFG, int PAT, class Op>
 __device__ __forceinline__ bool run_rows(const SpArgs& a, Op& op) {
   if constexpr (CFG != kTileNone && PAT) {
-    return stream_tiles_pat<kTileRows[CFG], kTileNnzCap[CFG], kPatStages>(a.row, a.pt, a.val,
-                                                                          a.nrows, op);
+    return stream_tiles_pat<kTileRows[CFG], kTileNnzCap[CFG], kPatStages>(
+        a.row, a.pt, a.val, a.nrows, op, wait_limit(a.v.prm));
   } else if constexpr (CFG == kTileNone) {
     const int stride = gridDim.x * blockDim.x;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nrows; i += stride) {
@@ -337,7 +337,7 @@ __device__ __forceinline__ bool run_rows(const SpArgs& a, Op& op) {
     return true;
   } else {
     FixedTiles<kTileRows[CFG]> src{a.row, a.col, a.val, a.nrows};
-    return stream_csr2<kTileRows[CFG], kTileNnzCap[CFG], 2>(src, op);
+    return stream_csr2<kTileRows[CFG], kTileNnzCap[CFG], 2>(src, op, wait_limit(a.v.prm));
   }
 }
 
@@ -977,7 +977,7 @@ int tf_fp64_run(tf_matrix_s* m, int prec) {
     if (prec == kPrecNone) return run_host_loop_p<kPrecNone>(m, xdef);
     return run_host_loop_p<kPrecIcc>(m, 0);
   }
-  cudaGraphExec_t& g = m->graph[2 * prec + xdef];
+  cudaGraphExec_t& g = (m->ext_bound ? m->ext_graph : m->graph)[2 * prec + xdef];
   if (!g) {
     int st;
     if (prec == kPrecJacobi) st = build_graph_p<kPrecJacobi>(m, xdef, &g);

@@ -58,6 +58,7 @@ struct tf_ctx_s {
   size_t l2_bytes = 0;
   cudaStream_t stream = nullptr;
   int history = 0;
+  unsigned long long wait_ns = 0;   // bounded-wait limit of this context's solves (0: default)
   std::vector<double> last_hist;
   int last_count = 0;
   // Stream-ordered allocation (cudaMallocAsync / cudaFreeAsync on `stream`)
@@ -129,6 +130,12 @@ struct tf_matrix_s {
   double* d_icc_dinv = nullptr;  // Prec_Form's d_inv
   // cached graphs, one per (preconditioner, x update deferred or not)
   cudaGraphExec_t graph[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  // The same graphs bound to a caller's device val/x/b (tf_solve_device in
+  // place): d_val, d_x, d_b point at the caller's arrays while such a solve
+  // runs (ext_bound), and ext_key names the arrays ext_graph was built on.
+  cudaGraphExec_t ext_graph[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  const void* ext_key[3] = {nullptr, nullptr, nullptr};
+  int ext_bound = 0;
   std::mutex mu;
   int async_alloc = 0;   // device arrays from cudaMallocAsync on ctx->stream
   int host_lent = 0;     // h_state / h_params belong to the context

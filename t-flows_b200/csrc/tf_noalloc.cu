@@ -83,7 +83,13 @@ unsigned char* g_ptr[kMaxDevices] = {};
 int scratch_for_current_device(unsigned char** out) {
   int dev = 0;
   TF_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return TF_ERR_ARG;
+  if (dev < 0 || dev >= kMaxDevices) {
+    char msg[128];
+    snprintf(msg, sizeof msg, "tf_spmv_noalloc: device ordinal %d is not below %d", dev,
+             kMaxDevices);
+    tf_set_last_message(msg);
+    return TF_ERR_ARG;
+  }
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_ptr[dev]) {
     void* p = nullptr;

@@ -164,7 +164,7 @@ __device__ bool stream_items(W& w) {
       const int itk = it_no + d;
       const int k = blockIdx.x + itk * G;
       if (k >= count) break;
-      mbar_wait_bounded(&bars[itk % STAGES], (unsigned)(itk / STAGES) & 1u);
+      mbar_drain(&bars[itk % STAGES], (unsigned)(itk / STAGES) & 1u);
     }
   }
   __syncthreads();
@@ -232,7 +232,8 @@ constexpr int pat_threads() { return ROWS + 32; }
 // stage it armed.  Returns false on a timeout (the caller records it).
 template <int ROWS, int NNZCAP, int STAGES, class Op>
 __device__ bool stream_tiles_pat(const int* __restrict__ row, const PatTable& pt,
-                                 const double* __restrict__ val, int nrows, Op& op) {
+                                 const double* __restrict__ val, int nrows, Op& op,
+                                 unsigned long long wait_ns = kWaitLimitNs) {
   using L = PatLayout<ROWS, NNZCAP, STAGES>;
   constexpr int kConsumerWarps = ROWS / 32;
   extern __shared__ __align__(128) unsigned char tf_smem[];
@@ -274,7 +275,7 @@ __device__ bool stream_tiles_pat(const int* __restrict__ row, const PatTable& pt
       for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++issued) {
         const int s = issued % STAGES;
         if (issued >= STAGES) {
-          if (!mbar_wait_bounded(&empty[s], (unsigned)(issued / STAGES - 1) & 1u)) {
+          if (!mbar_wait_bounded(&empty[s], (unsigned)(issued / STAGES - 1) & 1u, wait_ns)) {
             ok = false;
             *abort_flag = 1;
             break;
@@ -300,14 +301,14 @@ __device__ bool stream_tiles_pat(const int* __restrict__ row, const PatTable& pt
       }
       // Drain: the copies of the last armed phase of every stage.
       for (int k = (issued > STAGES ? issued - STAGES : 0); k < issued; ++k)
-        mbar_wait_bounded(&full[k % STAGES], (unsigned)(k / STAGES) & 1u);
+        mbar_drain(&full[k % STAGES], (unsigned)(k / STAGES) & 1u);
     }
   } else {
     // ---- consumer warps ----
     int it = 0;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
       const int s = it % STAGES;
-      if (!mbar_wait_bounded(&full[s], (unsigned)(it / STAGES) & 1u)) {
+      if (!mbar_wait_bounded(&full[s], (unsigned)(it / STAGES) & 1u, wait_ns)) {
         ok = false;
         *abort_flag = 1;
         break;

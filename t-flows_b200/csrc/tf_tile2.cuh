@@ -112,7 +112,7 @@ __device__ __forceinline__ bool consumer_bar_or(bool v) {
 }
 
 template <int ROWCAP, int NNZCAP, int STAGES, class S, class Op>
-__device__ bool stream_csr2(S& src, Op& op) {
+__device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLimitNs) {
   using L = Csr2Layout<ROWCAP, NNZCAP, STAGES>;
   constexpr int kConsWarps = kCons / 32;
   extern __shared__ __align__(128) unsigned char tf_smem[];
@@ -166,7 +166,7 @@ __device__ bool stream_csr2(S& src, Op& op) {
         const TileDesc d = nxt;
         if (k + (int)gridDim.x < count) nxt = src.desc(k + gridDim.x);
         if (issued >= STAGES) {
-          if (!mbar_wait_bounded(&empty[s], (unsigned)(issued / STAGES - 1) & 1u)) {
+          if (!mbar_wait_bounded(&empty[s], (unsigned)(issued / STAGES - 1) & 1u, wait_ns)) {
             ok = false;
             *abort_flag = 1;
             break;
@@ -198,14 +198,15 @@ __device__ bool stream_csr2(S& src, Op& op) {
         bulk_g2s(srow(s), d.row + p0, br, &full[s]);
       }
       for (int k = (issued > STAGES ? issued - STAGES : 0); k < issued; ++k)
-        mbar_wait_bounded(&full[k % STAGES], (unsigned)(k / STAGES) & 1u);
+        mbar_drain(&full[k % STAGES], (unsigned)(k / STAGES) & 1u);
     }
   } else if (warp > kConsWarps) {
     // ---- reducer warp (Op::kReducer) ----
     if constexpr (kRed) {
       int it = 0;
       for (int k = blockIdx.x; k < count; k += gridDim.x, ++it) {
-        if (!mbar_wait_or_abort(&parked[it & 1], (unsigned)(it >> 1) & 1u, abort_flag)) {
+        if (!mbar_wait_or_abort(&parked[it & 1], (unsigned)(it >> 1) & 1u, abort_flag,
+                                wait_ns)) {
           ok = false;
           *abort_flag = 1;
           break;
@@ -221,7 +222,7 @@ __device__ bool stream_csr2(S& src, Op& op) {
     int it = 0;
     for (int k = blockIdx.x; k < count; k += gridDim.x, ++it) {
       const int s = it % STAGES;
-      bool stop = !mbar_wait_bounded(&full[s], (unsigned)(it / STAGES) & 1u);
+      bool stop = !mbar_wait_bounded(&full[s], (unsigned)(it / STAGES) & 1u, wait_ns);
       stop = stop || *abort_flag;
       // Consumers must pass the named barrier equally often: they decide
       // together whether to stop here.
@@ -303,7 +304,8 @@ __device__ bool stream_csr2(S& src, Op& op) {
         const bool slot_free = __all_sync(
             0xffffffffu,
             it < 2 ||
-                mbar_wait_or_abort(&freed[it & 1], (unsigned)((it >> 1) - 1) & 1u, abort_flag));
+                mbar_wait_or_abort(&freed[it & 1], (unsigned)((it >> 1) - 1) & 1u, abort_flag,
+                                   wait_ns));
         if (!slot_free) {
           ok = false;
           *abort_flag = 1;

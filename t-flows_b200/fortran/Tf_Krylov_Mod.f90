@@ -3,9 +3,13 @@
 !------------------------------------------------------------------------------!
 !>  ISO_C_BINDING interface to libtfkrylov.so, the B200 implementation of
 !>  Native_Mod's Cg/Bicg (include/tf_krylov.h).  Solve_Native keeps its
-!>  argument list; its body calls Tf_Solve_Native_Gpu below instead of
-!>  Nat % Cg / Nat % Bicg.  Not compiled in this repository (no Fortran
-!>  compiler is available where it was written); see INTEGRATION.md.
+!>  argument list; its body calls Tf_Solve below instead of Nat % Cg /
+!>  Nat % Bicg.  Matrix_Type (Matrix_Mod.f90:57-76) gains one component,
+!>      type(c_ptr) :: dev = c_null_ptr   ! device copy of row/col/dia
+!>  which Tf_Register sets once after Create_Matrix, so Solve_Native finds
+!>  the registration of whichever matrix (Nat % A or Nat % M) it is given.
+!>  Not compiled: neither the machine this was written on nor the GPU
+!>  machines it was tested on have a Fortran compiler.
 !------------------------------------------------------------------------------!
   use iso_c_binding
 !------------------------------------------------------------------------------!
@@ -61,21 +65,19 @@
   end interface
 
   type(c_ptr), save :: tf_ctx = c_null_ptr
-  type(c_ptr), save :: tf_mat_a = c_null_ptr   ! Nat % A
-  type(c_ptr), save :: tf_mat_m = c_null_ptr   ! Nat % M
 
   contains
 
   !============================================================================!
-  subroutine Tf_Register(A, n_cells, n_own, mat)
+  subroutine Tf_Register(A, n_cells, n_own)
   !----------------------------------------------------------------------------!
-  !>  Uploads the structure of one Matrix_Type once (after Create_Matrix).
+  !>  Uploads the structure of one Matrix_Type once (after Create_Matrix) and
+  !>  keeps the handle in A % dev.
   !----------------------------------------------------------------------------!
     use Matrix_Mod
-    type(Matrix_Type), intent(in)    :: A
+    type(Matrix_Type), intent(inout) :: A
     integer,           intent(in)    :: n_cells, n_own
-    type(c_ptr),       intent(inout) :: mat
-    integer(c_int) :: st
+    integer(c_int)     :: st
     integer(c_int64_t) :: nnz
 
     if(.not. c_associated(tf_ctx)) then
@@ -84,8 +86,39 @@
     end if
     nnz = int(A % row(n_cells + 1) - 1, c_int64_t)
     st = tf_matrix_register(tf_ctx, int(n_cells, c_int), int(n_own, c_int),  &
-                            nnz, A % row, A % col, A % dia, mat)
+                            nnz, A % row, A % col, A % dia, A % dev)
     if(st .ne. TF_OK) stop 'tf_matrix_register failed'
   end subroutine
+
+  !============================================================================!
+  integer function Tf_Solve(solver, prec, A, x, b, miter, niter, tol,  &
+                            fin_res, norm)
+  !----------------------------------------------------------------------------!
+  !>  Solve_Native's arguments (Solve_Native.f90:2-27) in, the library's
+  !>  status out (0, or 64 for an unknown solver as Solve_Native.f90:38).
+  !>  x is x(-nb:n) as Solve_Native declares it; the library reads and
+  !>  writes x(1:n) only.  An absent norm stays absent.
+  !----------------------------------------------------------------------------!
+    use Matrix_Mod
+    character(*),      intent(in)    :: solver, prec
+    type(Matrix_Type), intent(inout) :: A
+    real,              intent(inout) :: x(:)      ! x(1:n) of Solve_Native's x
+    real,              intent(inout) :: b(:)
+    integer,           intent(in)    :: miter
+    integer,           intent(out)   :: niter
+    real,              intent(in)    :: tol
+    real,              intent(out)   :: fin_res
+    real,    optional, intent(in)    :: norm
+    integer(c_int) :: it
+    real(c_double) :: res
+
+    Tf_Solve = tf_solve_native(tf_ctx, A % dev,                           &
+                               trim(solver)//c_null_char,                 &
+                               trim(prec)//c_null_char,                   &
+                               A % val, x, b, int(miter, c_int), it,      &
+                               real(tol, c_double), res, norm)
+    niter   = it
+    fin_res = res
+  end function
 
   end module

@@ -29,6 +29,7 @@ EXPORTS = [
     "tf_status_string", "tf_version", "tf_ctx_create", "tf_ctx_destroy",
     "tf_matrix_register", "tf_matrix_release", "tf_matrix_info", "tf_solve",
     "tf_solve_native", "tf_solve_device", "tf_ctx_set_history", "tf_last_history",
+    "tf_ctx_set_wait_limit",
     "tf_host_pin", "tf_host_unpin", "tf_spmv", "tf_residual", "tf_nrms",
     "tf_ctx_sync", "tf_ctx_stream", "tf_last_error_message", "tf_matrix_tile_config",
     "tf_matrix_row_patterns", "tf_matrix_renumbered",
@@ -76,6 +77,7 @@ def load(path=LIB_PATH):
     L.tf_ctx_stream.argtypes = [_vp]
     L.tf_ctx_stream.restype = _vp
     L.tf_ctx_set_history.argtypes = [_vp, ctypes.c_int]
+    L.tf_ctx_set_wait_limit.argtypes = [_vp, ctypes.c_double]
     L.tf_last_history.argtypes = [_vp, _c_dbl_p, ctypes.c_int, _c_int_p]
     L.tf_matrix_register.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int64,
                                      _c_int_p, _c_int_p, _c_int_p, ctypes.POINTER(_vp)]
@@ -130,6 +132,10 @@ class Context:
         _check(L.tf_ctx_create(device, ctypes.byref(h)), "tf_ctx_create")
         self.h = h
         self.set_history(history)
+
+    def set_wait_limit(self, seconds):
+        """Limit of the device-side bounded waits (0: the 2 s default)."""
+        _check(load().tf_ctx_set_wait_limit(self.h, float(seconds)), "tf_ctx_set_wait_limit")
 
     def set_history(self, on):
         _check(load().tf_ctx_set_history(self.h, 1 if on else 0), "tf_ctx_set_history")

@@ -66,6 +66,12 @@ def run_both(ctx, s, miter, tol):
     return (x, it, res), (ox, r["niter"], r["fin_res"])
 
 
+def report(what, g, o):
+    (x, it, res), (ox, oit, ores) = g, o
+    print(f"\n{what}: niter {it} (oracle {oit}), rel-L2(x) {rel_l2(x, ox):.2e}, "
+          f"fin_res {res:.6e} (oracle {ores:.6e})")
+
+
 def check_prefix(g, o):
     (x, it, res), (ox, oit, ores) = g, o
     assert it == oit == PREFIX
@@ -83,19 +89,27 @@ def check_whole(g, o, tol):
 @pytest.mark.parametrize("kind", ["pressure", "momentum"])
 def test_stretched200_prefix(gpu_ctx, stretched200, kind):
     s = stretched200[kind]
-    check_prefix(*run_both(gpu_ctx, s, PREFIX, 0.0))
+    r = run_both(gpu_ctx, s, PREFIX, 0.0)
+    report(f"stretched 200^3 {kind}, {PREFIX}-iteration prefix", *r)
+    check_prefix(*r)
 
 
 @pytest.mark.parametrize("kind", ["momentum", "pressure"])
 def test_stretched200_whole_solve(gpu_ctx, stretched200, kind):
     s = stretched200[kind]
-    check_whole(*run_both(gpu_ctx, s, s.miter, s.tol), s.tol)
+    r = run_both(gpu_ctx, s, s.miter, s.tol)
+    report(f"stretched 200^3 {kind}, whole solve", *r)
+    check_whole(*r, s.tol)
 
 
 def test_delaunay2m_prefix(gpu_ctx, delaunay2m):
-    check_prefix(*run_both(gpu_ctx, delaunay2m, PREFIX, 0.0))
+    r = run_both(gpu_ctx, delaunay2m, PREFIX, 0.0)
+    report(f"Delaunay dual {delaunay2m.n} cells, {PREFIX}-iteration prefix", *r)
+    check_prefix(*r)
 
 
 def test_delaunay2m_whole_solve(gpu_ctx, delaunay2m):
     s = delaunay2m
-    check_whole(*run_both(gpu_ctx, s, s.miter, s.tol), s.tol)
+    r = run_both(gpu_ctx, s, s.miter, s.tol)
+    report(f"Delaunay dual {s.n} cells, whole solve", *r)
+    check_whole(*r, s.tol)

@@ -403,8 +403,16 @@ def test_error_codes(gpu_ctx):
         with pytest.raises(native.TFError) as e:
             native.solve_native(gpu_ctx, m, "gmres", "jacobi", v, x, b, 10, 1e-6)
         assert e.value.status == 64
+        # An unknown preconditioner name runs unpreconditioned, as the
+        # else branches of Prec_Form.f90 / Prec_Solve.f90 do.
+        res = []
+        for pname in ("ilu", "none"):
+            vv, xx, bb = s.val.copy(), s.x0.copy(), s.b.copy()
+            res.append((native.solve_native(gpu_ctx, m, "cg", pname, vv, xx, bb, 300, 1e-9,
+                                            1.0), xx))
+        assert res[0][0] == res[1][0] and np.array_equal(res[0][1], res[1][1])
         with pytest.raises(native.TFError) as e:
-            native.solve_native(gpu_ctx, m, "cg", "ilu", v, x, b, 10, 1e-6)
+            native.solve(gpu_ctx, m, "cg", 7, v, x, b, 10, 1e-6)
         assert e.value.status == 72
         it, res = native.solve_native(gpu_ctx, m, "cg   ", "diagonal", v, x, b, 100, 1e-8, 1.0)
         assert it > 0
@@ -441,6 +449,39 @@ def test_solve_device_pointers(gpu_ctx):
     o = oracle_solve(s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, "cg", "jacobi", 1000,
                      1e-10, 1.0)
     check_parity((dx.cpu().numpy(), dval.cpu().numpy(), db.cpu().numpy(), it, res), o, 1e-10)
+
+
+@pytest.mark.parametrize("kind,prec,norm", [("hex", "jacobi", 1.0), ("hex", "none", None),
+                                             ("hex", "icc", 1.0), ("poly", "jacobi", 1.0)])
+def test_solve_device_in_place_equals_host_solve(gpu_ctx, kind, prec, norm):
+    """tf_solve_device works on the caller's arrays (16-byte aligned: in
+    place; renumbered matrices gather from and scatter to them) and gives
+    the bits of tf_solve; a second set of arrays rebuilds its graph, and
+    arrays off a 16-byte boundary take the copy path with the same bits."""
+    torch = torch_dev()
+    if kind == "hex":
+        s = systems.small_hex(24, seed=9, kind="pressure", ratio=1.03)
+    else:
+        s = systems.poly_system(30000, seed=12, kind="pressure", tol=1e-10, miter=5000,
+                                norm=1.0)
+    m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia)
+    try:
+        v, x, b = s.val.copy(), s.x0.copy(), s.b.copy()
+        want = native.solve(gpu_ctx, m, "cg", prec, v, x, b, 5000, 1e-10, norm)
+        for offset in (0, 0, 1):   # twice on fresh aligned arrays, then off by 8 bytes
+            bufs = []
+            for a in (s.val, s.x0, s.b):
+                t = torch.zeros(len(a) + 2, dtype=torch.float64, device="cuda")
+                t[offset:offset + len(a)] = torch.from_numpy(a).cuda()
+                bufs.append(t)
+            torch.cuda.synchronize()
+            ptr = [t.data_ptr() + 8 * offset for t in bufs]
+            got = native.solve_device(gpu_ctx, m, "cg", prec, *ptr, 5000, 1e-10, norm)
+            assert got == want
+            for t, ref in zip(bufs, (v, x, b)):
+                assert np.array_equal(t[offset:offset + len(ref)].cpu().numpy(), ref)
+    finally:
+        m.close()
 
 
 def test_history_matches_oracle(gpu_ctx):

@@ -135,3 +135,13 @@ def test_unknown_solver_is_error_64():
         F.solve_native("gmres", "jacobi", s.csr.row, s.csr.col, s.csr.dia, s.val, s.x0,
                        s.b, 10, 1e-8, 1.0)
     assert e.value.code == 64
+
+
+def test_unknown_preconditioner_name_runs_unpreconditioned():
+    """Prec_Form / Prec_Solve's else branches: any other name is 'none'
+    (tf_solve_native maps names the same way)."""
+    s = systems.small_hex(3, seed=3, kind="pressure")
+    a = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.x0, s.b, 60, 1e-10, 1.0)
+    r1 = F.solve_native("cg", "ilu", *a)
+    r2 = F.solve_native("cg", "none", *a)
+    assert (r1["niter"], r1["fin_res"], r1["x"]) == (r2["niter"], r2["fin_res"], r2["x"])

@@ -63,19 +63,35 @@ def _noalloc_spmv(torch, L, s, p):
     return dq.cpu().numpy(), dpq.item()
 
 
+def _one_by_one():
+    """The 1 x 1 system: one row, one tile that is first and last at once."""
+    csr = systems.Csr(n=1, row=np.array([1, 2], np.int32), col=np.array([1], np.int32),
+                      dia=np.array([1], np.int32), pos=np.zeros((0, 2), np.int32))
+    return systems.System(name="1x1", solver="cg", prec="jacobi", csr=csr,
+                          val=np.array([2.5]), b=np.array([1.0]), x0=np.zeros(1),
+                          tol=1e-8, miter=10, norm=1.0, meta={})
+
+
 def test_noalloc_matches_regular_spmv_twice(gpu_ctx):
     import torch
     assert torch.cuda.is_available()
     L = _lib()
-    cases = [systems.small_hex(40, seed=3, kind="momentum", ratio=1.02),
+    cases = [_one_by_one(),                                                 # n = 1
+             systems.small_hex(5, seed=2, kind="pressure"),                 # n = 125 < 256
+             systems.small_hex(7, seed=2, kind="momentum", peclet=1.0),     # 343: a partial tile
+             systems.small_hex(40, seed=3, kind="momentum", ratio=1.02),    # 250 whole tiles
              systems.poly_system(5000, seed=4, kind="pressure")]
     rng = np.random.default_rng(11)
-    for s, p in [(cases[0], rng.standard_normal(cases[0].n)),
-                 (cases[1], rng.standard_normal(cases[1].n))]:
+    for s in cases:
+        p = rng.standard_normal(s.n)
         q_ref, pq_ref = _reference_spmv(torch, gpu_ctx, s, p)
-        q, pq = _noalloc_spmv(torch, L, s, p)
-        assert np.array_equal(q, q_ref)
-        assert pq == pytest.approx(pq_ref, rel=1e-13)
+        # The same input twice in a row: the second call starts from the
+        # scratch the first one left, and must give the same bits.
+        q1, pq1 = _noalloc_spmv(torch, L, s, p)
+        q2, pq2 = _noalloc_spmv(torch, L, s, p)
+        assert np.array_equal(q1, q_ref) and np.array_equal(q2, q_ref), s.name
+        assert pq1 == pytest.approx(pq_ref, rel=1e-13), s.name
+        assert pq2 == pq1, s.name
 
 
 def test_noalloc_rejects_oversize():
