@@ -60,14 +60,17 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--count", type=int, default=512)
     ap.add_argument("--parts", default="all",
-                    help="batched: comma list of mixed, fp64_batched, drop_in, streams, pool "
-                         "(default all)")
+                    help="batched: comma list of mixed, fp64_batched, mixed_row_groups, drop_in, "
+                         "streams, pool (default all)")
     ap.add_argument("--rate", type=float, default=200.0, help="served: arrivals per second")
     ap.add_argument("--seconds", type=float, default=60.0, help="served: window length")
     ap.add_argument("--iters", type=int, default=30, help="iters: Cg iterations per solve")
     ap.add_argument("--mesh", default="hex", choices=["hex", "poly-lattice", "poly-delaunay"],
                     help="spmv: hex (--size^3 cells) or a polyhedral mesh of --cells cells")
     ap.add_argument("--cells", type=int, default=2000000)
+    ap.add_argument("--tile-cfgs", default="auto",
+                    help="spmv: comma list of SpMV layouts to time (tf_matrix_tile_config "
+                         "ids, or auto for the tuner's choice)")
     ap.add_argument("--rcm", action="store_true",
                     help="spmv: renumber the cells by reverse Cuthill-McKee first")
     ap.add_argument("--mode", default="solve",
@@ -195,9 +198,11 @@ def run_batched(args):
                        "polyhedral upwind convection-diffusion (Bicg, Pe U[1,50], CFL 0.1); "
                        "Jacobi; target ||b-Ax||/||b|| <= 1e-10"}
     smallest = sorted(sysl, key=lambda s: s.n)[:4]
-    parts = set(("mixed,fp64_batched,drop_in,streams,pool" if args.parts == "all"
+    parts = set(("mixed,fp64_batched,mixed_row_groups,drop_in,streams,pool"
+                 if args.parts == "all"
                  else args.parts).split(","))
-    for label, opts in (("mixed", dict(vec_fp32=True)), ("fp64_batched", dict(vec_fp32=False))):
+    for label, opts in (("mixed", dict(vec_fp32=True)), ("fp64_batched", dict(vec_fp32=False)),
+                        ("mixed_row_groups", dict(vec_fp32=True, row_groups=1))):
         if label not in parts:
             continue
         _drop = _batch_solve(ctx, smallest, **opts)   # warm-up (module load, graphs)
@@ -257,6 +262,8 @@ def run_batched(args):
     ratio("fp64_drop_in_8streams", "fp64_drop_in")
     ratio("mixed", "fp64_drop_in")
     ratio("mixed", "fp64_batched")
+    ratio("mixed_row_groups", "fp64_drop_in")
+    ratio("mixed_row_groups", "mixed")
     print(json.dumps(out), flush=True)
     ctx.close()
 
@@ -342,6 +349,88 @@ def _serve_stream(req_sys, rhs, rate, seconds, workers, budget, seed, max_outsta
             "peak_device_bytes": stats["peak_bytes"]}
 
 
+def _serve_stream_mixed(req_sys, rhs, rate, seconds, budget, seed, max_outstanding=256,
+                        submit_threads=8, row_groups=0):
+    """The same Poisson stream into the continuous-batching server
+    (tf_server_*: the mixed-precision engine, requests admitted into free
+    slots between sweeps, Krylov state resident).  Submission copies and
+    prepares each system on the caller's thread, so arrivals are handed to
+    `submit_threads` submitter threads.  Latency is counted from arrival:
+    time until the submit call returned plus the server's own latency
+    (submit to result)."""
+    import concurrent.futures as cf
+    import copy
+    import math
+    from tflows_b200 import batch, native
+    rng = np.random.default_rng(seed)
+    sizes = np.array([s.n for s in req_sys])
+    kinds = np.array([s.solver for s in req_sys])
+    ctx = native.Context(0)
+    srv = batch.Server(ctx, mem_budget=budget, max_systems=max_outstanding + 8,
+                       sweep_iters=8, row_groups=row_groups)
+    results, lock = [], threading.Lock()
+    state = {"outstanding": 0}
+
+    def handle(t_arr, idx, v):
+        s = copy.copy(req_sys[idx])
+        s.b = rhs[idx][v][0]
+        s.x0 = np.zeros(s.n)
+        try:
+            rid = srv.submit(s, tol=1e-10, maxit=100000)
+            t_ret = time.perf_counter()
+            r = srv.wait(rid)
+            ok = r["status"] == "converged"
+            lat = (t_ret - t_arr) * 1e3 + r["latency_ms"]
+            with lock:
+                results.append((t_arr, lat, r["queue_ms"], s.n * r["iters"], ok))
+        finally:
+            with lock:
+                state["outstanding"] -= 1
+
+    ex = cf.ThreadPoolExecutor(max_outstanding + submit_threads)
+    t_start = time.perf_counter()
+    stop_at = t_start + seconds
+    t_next, offered, shed = t_start, 0, 0
+    futs = []
+    while True:
+        t_next += rng.exponential(1.0 / rate)
+        if t_next > stop_at:
+            break
+        delay = t_next - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        kind = "cg" if rng.random() < 0.5 else "bicg"
+        n = math.exp(rng.uniform(math.log(1e4), math.log(4e6)))
+        cand = np.nonzero(kinds == kind)[0]
+        idx = int(cand[np.argmin(np.abs(np.log(sizes[cand]) - math.log(n)))])
+        offered += 1
+        with lock:
+            if state["outstanding"] >= max_outstanding:
+                shed += 1
+                continue
+            state["outstanding"] += 1
+        futs.append(ex.submit(handle, time.perf_counter(), idx, offered % len(rhs[idx])))
+    for f in futs:
+        f.result()
+    ex.shutdown()
+    st = srv.stats()
+    srv.close()
+    ctx.close()
+    inwin = [r for r in results if r[0] + r[1] * 1e-3 <= stop_at]
+    lat = np.array([r[1] for r in inwin]) if inwin else np.zeros(1)
+    qms = np.array([r[2] for r in inwin]) if inwin else np.zeros(1)
+    return {"rate_per_s": rate, "seconds": seconds, "submit_threads": submit_threads,
+            "offered": offered, "shed": shed, "admitted": offered - shed,
+            "completed_in_window": len(inwin),
+            "converged_to_1e-10": int(sum(r[4] for r in inwin)),
+            "solves_per_s": len(inwin) / seconds,
+            "mcell_iters_per_s": sum(r[3] for r in inwin) / seconds / 1e6,
+            "latency_ms_p50": float(np.percentile(lat, 50)),
+            "latency_ms_p99": float(np.percentile(lat, 99)),
+            "queue_ms_p50": float(np.percentile(qms, 50)),
+            "peak_running": st["peak_running"], "sweeps": st["sweeps"]}
+
+
 def run_served(args):
     """Served stream through the request pool (each request one Solve_Native
     on the FP64 drop-in): Poisson arrivals at `--rate`/s of hex Poisson (Cg)
@@ -377,6 +466,17 @@ def run_served(args):
                                                     budget, 3)
     out["throughput_ratio_pool_vs_one_at_a_time"] = (
         sat["solves_per_s"] / max(out["one_at_a_time"]["solves_per_s"], 1e-9))
+    # The mixed-precision continuous-batching server on the same streams
+    # (tol: ||b - A x|| / ||b|| <= 1e-10 in FP64).
+    _serve_stream_mixed(req_sys, rhs, 5.0, 3.0, budget, 1)     # warm-up
+    mixed = _serve_stream_mixed(req_sys, rhs, args.rate, args.seconds, budget, 2)
+    out["mixed_server"] = mixed
+    out["mixed_server_half_load"] = _serve_stream_mixed(
+        req_sys, rhs, max(1.0, 0.5 * mixed["solves_per_s"]), args.seconds / 2, budget, 3)
+    out["throughput_ratio_mixed_server_vs_one_at_a_time"] = (
+        mixed["solves_per_s"] / max(out["one_at_a_time"]["solves_per_s"], 1e-9))
+    out["throughput_ratio_mixed_server_vs_pool"] = (
+        mixed["solves_per_s"] / max(sat["solves_per_s"], 1e-9))
     print(json.dumps(out), flush=True)
 
 
@@ -395,27 +495,38 @@ def run_spmv_only(args):
     if args.rcm:
         s = systems.renumber_rcm(s)
     ctx = native.Context(0)
-    m = native.Matrix(ctx, s.csr.row, s.csr.col, s.csr.dia)
     val = torch.from_numpy(s.val).cuda()
     p = torch.randn(s.n, dtype=torch.float64, device="cuda")
     q = torch.empty_like(p)
     torch.cuda.synchronize()
     stream = torch.cuda.ExternalStream(ctx.stream)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    native.spmv(ctx, m, val.data_ptr(), p.data_ptr(), q.data_ptr())
-    e0.record(stream)
-    for _ in range(args.steps):
+    peak, peak_kind = measured_peak()
+    # --tile-cfgs: each layout in turn (TF_TILE_CFG at registration); "auto":
+    # the layout the tuner picks.
+    for cfg in args.tile_cfgs.split(","):
+        if cfg == "auto":
+            os.environ.pop("TF_TILE_CFG", None)
+        else:
+            os.environ["TF_TILE_CFG"] = cfg
+        m = native.Matrix(ctx, s.csr.row, s.csr.col, s.csr.dia)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         native.spmv(ctx, m, val.data_ptr(), p.data_ptr(), q.data_ptr())
-    e1.record(stream)
-    e1.synchronize()
-    t = e0.elapsed_time(e1) / 1e3 / max(args.steps, 1)
-    by = SPMV_BYTES(s.n, s.nnz, m.row_patterns > 0)
-    print(json.dumps({"mode": "spmv", "mesh": args.mesh, "n": s.n, "nnz": s.nnz,
-                      "tile_cfg": m.tile_config,
-                      "row_patterns": m.row_patterns, "launch_ms": t * 1e3,
-                      "bytes_per_launch": by, "csr_bytes_per_launch": SPMV_BYTES(s.n, s.nnz),
-                      "achieved_gbs": by / t / 1e9}), flush=True)
-    m.close()
+        e0.record(stream)
+        for _ in range(args.steps):
+            native.spmv(ctx, m, val.data_ptr(), p.data_ptr(), q.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / max(args.steps, 1)
+        by = SPMV_BYTES(s.n, s.nnz, m.row_patterns > 0)
+        print(json.dumps({"mode": "spmv", "mesh": args.mesh, "n": s.n, "nnz": s.nnz,
+                          "requested": cfg, "tile_cfg": m.tile_config,
+                          "row_patterns": m.row_patterns, "tuning": m.tuning(),
+                          "launch_ms": t * 1e3, "bytes_per_launch": by,
+                          "csr_bytes_per_launch": SPMV_BYTES(s.n, s.nnz),
+                          "achieved_gbs": by / t / 1e9, "frac": by / t / 1e9 / peak,
+                          "peak_kind": peak_kind}), flush=True)
+        m.close()
+    os.environ.pop("TF_TILE_CFG", None)
     ctx.close()
 
 
@@ -566,7 +677,8 @@ def run_poly_system(args):
     m.close()
     out["fp64_drop_in"] = {"ms": best[0], "iters": best[1], "true_rel": best[2],
                            "mcell_iters_per_s": s.n * best[1] / best[0] / 1e3}
-    for label, opts in (("batch_fp64", dict(vec_fp32=False)), ("batch_mixed", dict(vec_fp32=True))):
+    for label, opts in (("batch_fp64", dict(vec_fp32=False)), ("batch_mixed", dict(vec_fp32=True)),
+                        ("batch_mixed_row_groups", dict(vec_fp32=True, row_groups=1))):
         runs = [_batch_solve(ctx, [s], **opts) for _ in range(1 + args.steps)][1:]
         t_add, t_run, res, info = min(runs, key=lambda r: r[1])
         out[label] = {"ms": t_run * 1e3, "iters": res[0]["iters"], "true_rel": res[0]["rel"],
@@ -901,10 +1013,11 @@ def main():
     launches = sum(args.steps * (4 + 3 * it) for it, _ in iters)
 
     if rank == 0:
-        cpu = None
+        cpu = cpu1 = None
         if not args.no_cpu_baseline and world == 1:
             from oracle import oracle as O
             cpu = cpu_baseline(sysl, args.cpu_seconds, O.max_threads())
+            cpu1 = cpu_baseline(sysl, args.cpu_seconds / 2, 1)
         ms = np.array(step_ms)
         solve_count = args.steps * len(sysl) * world
         line = {
@@ -934,6 +1047,7 @@ def main():
                              "achieved": bytes_iter / t_iter / 1e9,
                              "frac": bytes_iter / t_iter / 1e9 / peak}},
             "cpu_baseline": cpu,
+            "cpu_baseline_1core": cpu1,
             "clocks": clk,
             "gpu_launches": launches,
         }

@@ -85,9 +85,27 @@ int tf_matrix_register(tf_ctx ctx, int n_cells, int n_own, int64_t nnz,
 int tf_matrix_release(tf_matrix m);
 int tf_matrix_info(tf_matrix m, int* n_cells, int* n_own, int64_t* nnz,
                    int* max_row_len);
-/* SpMV tile configuration chosen at registration: 0/1/2 = 512/256/128-row
- * shared-memory tiles, 3 = rows read straight from global memory. */
+/* SpMV layout chosen at registration: 0/1/2 = fixed tiles of 512/256/128
+ * rows staged in shared memory (row-pattern or CSR columns), 3 = rows read
+ * straight from global memory, 4/5/6/7 = CSR tiles of variable length (at
+ * most 512 rows and 4096 entries) whose rows are summed by groups of
+ * 1/2/4/8 lanes.  Every layout gives the same row sums bit for bit.  The
+ * layout is chosen by timing the candidates on the device when the matrix
+ * is registered (tf_matrix_tuning), once per class of matrix (size, mean
+ * and longest row, row patterns or not) per process; the environment
+ * variable TF_TILE_CFG forces one, TF_NO_TUNE skips the timing. */
 int tf_matrix_tile_config(tf_matrix m);
+/* The candidates timed when m was registered: cfg[i] (as
+ * tf_matrix_tile_config) and us[i], the median microseconds of one q = A p
+ * launch, for i < min(cap, *count).  *count = 0 when the layout came from
+ * the cache of an earlier registration of the same class, from
+ * TF_TILE_CFG, or from the rule used for small matrices (under 16,384 rows)
+ * and row-pattern matrices.  No reference counterpart (the reference has a
+ * single loop order). */
+int tf_matrix_tuning(tf_matrix m, int* cfg, double* us, int cap, int* count);
+/* Forget the layouts chosen for earlier registrations, so the next matrix
+ * of each class is timed again. */
+int tf_tuning_cache_clear(void);
 /* Number of row patterns of the compressed column layout chosen at
  * registration (rows whose column offsets relative to the row index repeat,
  * as on structured hex blocks: one byte per row instead of four per entry;
@@ -164,13 +182,14 @@ int tf_solve_multi_device(tf_ctx ctx, tf_matrix m, int solver, int prec, int nrh
 int tf_ctx_set_history(tf_ctx ctx, int enable);
 int tf_last_history(tf_ctx ctx, double* hist, int cap, int* count);
 
-/* Limit of every bounded device-side wait in this context's solves (a
- * tile's copies, a free pipeline stage), in seconds; 0 restores the default
- * of 2 s.  A wait that runs out ends the solve cleanly with TF_ERR_TIMEOUT
- * (the CTA still waits for the copies it started before it exits, with the
- * default limit); the context stays usable.  A watchdog against a stalled
- * device; the reference has none (its failures stop the run,
- * Shared/Message_Mod/Error.f90:74). */
+/* Watchdog of this context's solves, in seconds (0 restores the default of
+ * 2 s): a streaming kernel of the solve (the SpMV and residual passes) stops
+ * at its first wait for a tile's copies or a free pipeline stage after this
+ * much time since its start -- or once such a wait has been blocked that
+ * long -- and the solve ends with TF_ERR_TIMEOUT.  Before a stopped CTA
+ * exits it still waits for the copies it started (with the default limit),
+ * and the context stays usable.  The reference has no counterpart (its
+ * failures stop the run, Shared/Message_Mod/Error.f90:74). */
 int tf_ctx_set_wait_limit(tf_ctx ctx, double seconds);
 
 /* Pin (page-lock) a host array the caller will pass to tf_solve on every
@@ -198,6 +217,10 @@ typedef struct tf_batch_opts {
   int max_systems;    /* system slots (default 1024)                          */
   double ru_delta;    /* refinement when |r| fell by this factor (0.1)        */
   size_t mem_budget;  /* device bytes for all systems' data (default 4 GiB)   */
+  int row_groups;     /* SpMV consumers: 0 = two phases (products staged in
+                         shared memory, then one thread per row), 1 = warp
+                         groups of 1/2/4 lanes per row by each tile's mean
+                         row length; the same row sums bit for bit          */
 } tf_batch_opts;
 
 typedef struct tf_batch_s* tf_batch;
@@ -256,6 +279,12 @@ int tf_server_wait(tf_server s, int64_t req, double* x, int* iters,
                    double* queue_ms);
 int tf_server_stats(tf_server s, long long* admitted, long long* completed,
                     int* peak_running, int* sweeps);
+/* Cancel a request: a queued one is dropped at once, an admitted one is
+ * retired at the end of the current sweep (its Krylov state and slot are
+ * freed); tf_server_wait then returns TF_ERR_CANCELLED.  Returns TF_OK,
+ * TF_ERR_BUSY when the request had already finished (its result stands),
+ * or TF_ERR_ARG for an unknown or collected id.  No reference counterpart. */
+int tf_server_cancel(tf_server s, int64_t req);
 int tf_server_destroy(tf_server s);
 
 /* ---------------------------------------------------------------------------
@@ -284,6 +313,12 @@ int tf_pool_wait(tf_pool p, int64_t req, int* niter, double* fin_res,
                  double* latency_ms, double* queue_ms);
 int tf_pool_stats(tf_pool p, long long* submitted, long long* completed,
                   long long* rejected, size_t* peak_bytes);
+/* Cancel a request not yet taken by a worker (tf_pool_wait then returns
+ * TF_ERR_CANCELLED and x is left untouched).  A request already running
+ * is one Solve_Native graph on the device and runs to its end: TF_ERR_BUSY,
+ * as for a finished one.  TF_ERR_ARG for an unknown or collected id.  No
+ * reference counterpart. */
+int tf_pool_cancel(tf_pool p, int64_t req);
 /* Resident structures: requests reusing a held registration (`reused`),
  * registrations currently held and their budgeted bytes.  A request whose
  * row/col/dia arrays (same addresses, same sampled contents, same sizes)

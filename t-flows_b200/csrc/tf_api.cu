@@ -191,7 +191,7 @@ void tf_matrix_free(tf_matrix_s* m) {
   for (auto& g : m->ext_graph)
     if (g) cudaGraphExecDestroy(g);
   tf_slices_free(m);
-  void* ptrs[] = {m->d_row, m->d_col, m->d_dia, m->d_val, m->d_x, m->d_b,
+  void* ptrs[] = {m->d_row, m->d_col, m->d_dia, m->d_tiles, m->d_val, m->d_x, m->d_b,
                   m->d_r, m->d_p, m->d_q, m->d_z, m->d_adiag, m->d_part,
                   m->d_hist, m->d_state, m->d_params, m->d_levf_rows, m->d_levb_rows,
                   m->d_icc_d, m->d_icc_dinv, m->d_pat, m->d_pat_tab, m->d_perm, m->d_src,
@@ -272,6 +272,23 @@ int find_row_patterns(const std::vector<int>& row0, const std::vector<int>& col0
 }
 
 // Largest nnz of any tile of `rows` consecutive rows among the first ni.
+// Variable tiles: consecutive rows, at most kTileRows / kTileNnzCap of the
+// var configurations each.  False when one row alone exceeds the entry cap.
+bool var_tiles(const std::vector<int>& row0, int ni, std::vector<int>& tiles) {
+  const int rows = tf::kTileRows[tf::kTileVar1], cap = tf::kTileNnzCap[tf::kTileVar1];
+  tiles.clear();
+  tiles.push_back(0);
+  int r0 = 0;
+  while (r0 < ni) {
+    if (row0[r0 + 1] - row0[r0] > cap) return false;
+    int r1 = r0 + 1;
+    while (r1 < ni && r1 - r0 < rows && row0[r1 + 1] - row0[r0] <= cap) ++r1;
+    tiles.push_back(r1);
+    r0 = r1;
+  }
+  return ni > 0;
+}
+
 int64_t max_tile_nnz(const std::vector<int>& row0, int ni, int rows) {
   int64_t mx = 0;
   for (int r0 = 0; r0 < ni; r0 += rows) {
@@ -447,23 +464,17 @@ int matrix_create_impl(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const
       st = TF_ERR_CUDA;
     }
   }
-  if (st == TF_OK) {
-    // Tile configuration: the widest tile whose nnz fits its stage.
-    m->tile_cfg = tf::kTileNone;
-    for (int c = 0; c < 3 && n_cells > 0; ++c) {
+  if (st == TF_OK && n_cells > 0) {
+    // Fixed tiles whose entries fit their stage.
+    unsigned fit_mask = 0;
+    int fixed = tf::kTileNone;
+    for (int c = 2; c >= 0; --c)
       if (max_tile_nnz(row0, n_own, tf::kTileRows[c]) <= tf::kTileNnzCap[c]) {
-        m->tile_cfg = c;
-        break;
+        fit_mask |= 1u << c;
+        fixed = c;
       }
-    }
-    if (const char* f = getenv("TF_TILE_CFG")) {
-      const int c = atoi(f);
-      if (c >= 0 && c <= 3 &&
-          (c == 3 || max_tile_nnz(row0, n_own, tf::kTileRows[c]) <= tf::kTileNnzCap[c]))
-        m->tile_cfg = c;
-    }
     // Row-pattern columns for tiled matrices (TF_NO_ROW_PATTERNS keeps CSR).
-    if (n_cells > 0 && m->tile_cfg != tf::kTileNone && !getenv("TF_NO_ROW_PATTERNS")) {
+    if (fixed != tf::kTileNone && !getenv("TF_NO_ROW_PATTERNS")) {
       std::vector<unsigned char> pat;
       std::vector<int> tab;
       const int np = find_row_patterns(row0, col0, n_own, pat, tab);
@@ -485,9 +496,23 @@ int matrix_create_impl(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const
         if (st == TF_OK) m->npat = np;
       }
     }
-    if (st == TF_OK && n_cells > 0) st = tf_fp64_prepare(m);
-  }
-  if (st == TF_OK && n_cells > 0 && diag_first && want_icc)
+    // Variable-length CSR tiles (every row fits a stage).
+    std::vector<int> tiles;
+    if (st == TF_OK && var_tiles(row0, n_own, tiles)) {
+      st = dev_alloc(ctx, &m->d_tiles, tiles.size() + 8);
+      if (st == TF_OK) {
+        cudaError_t e = cudaMemcpyAsync(m->d_tiles, tiles.data(), tiles.size() * sizeof(int),
+                                        cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess && !ctx->async_alloc) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) {
+          tf_set_last_cuda_error(e, "cudaMemcpy(tiles)", __FILE__, __LINE__);
+          st = TF_ERR_CUDA;
+        }
+        m->ntiles = (int)tiles.size() - 1;
+      }
+    }
+    if (st == TF_OK) st = tf_choose_tiles(m, fit_mask);
+  }  if (st == TF_OK && n_cells > 0 && diag_first && want_icc)
     st = tf_icc_build(m, row0.data(), col0.data());
   if (st == TF_OK && allow_renumber) st = attach_renumbered(m, row0, col0, dia0);
   if (st != TF_OK) {
@@ -534,6 +559,26 @@ extern "C" int tf_matrix_info(tf_matrix m, int* n_cells, int* n_own,
 }
 
 extern "C" int tf_matrix_tile_config(tf_matrix m) { return m ? m->tile_cfg : -1; }
+
+extern "C" int tf_matrix_tuning(tf_matrix m, int* cfg, double* us, int cap, int* count) {
+  TF_API_BEGIN
+  if (!m || !count || (cap > 0 && (!cfg || !us))) return TF_ERR_ARG;
+  const int n = std::min<int>(cap, (int)m->tune.size());
+  for (int i = 0; i < n; ++i) {
+    cfg[i] = m->tune[i].first;
+    us[i] = m->tune[i].second;
+  }
+  *count = (int)m->tune.size();
+  return TF_OK;
+  TF_API_END
+}
+
+extern "C" int tf_tuning_cache_clear(void) {
+  TF_API_BEGIN
+  tf_tune_cache_clear();
+  return TF_OK;
+  TF_API_END
+}
 
 // ---------------------------------------------------------------------------
 // Solves

@@ -517,12 +517,13 @@ struct SpmvOp2 {
   }
 };
 
-template <typename V, typename VT>
+// G = 0: the two-phase consumers; G = -1: warp groups, width per tile.
+template <typename V, typename VT, int G>
 __global__ void __launch_bounds__(kCsr2RedThreads, 2) kb_spmv(BatchArgs a) {
   if constexpr (sizeof(VT) == 8) {
     BatchTiles<V, 0> src{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, *a.nwork};
     SpmvOp2<V> op{static_cast<const SysDev<V>*>(a.desc), a.st, a.work, 0.0, nullptr, nullptr};
-    stream_csr2<kRows, kNnzCap, kStages>(src, op);
+    stream_csr2<kRows, kNnzCap, kStages, G>(src, op);
   } else {
     // FP32 values: the one-thread-per-row streamer (kRows threads do the
     // work; the extra warp only joins the CTA-wide barriers).
@@ -672,12 +673,12 @@ struct ResOp2 {
   }
 };
 
-template <typename V>
+template <typename V, int G>
 __global__ void __launch_bounds__(kCsr2RedThreads, 2) kb_ru_res(BatchArgs a) {
   BatchTiles<V, 1> src{static_cast<const SysDev<V>*>(a.desc), a.st, a.ru.items, *a.ru.count};
   ResOp2<V> op{static_cast<const SysDev<V>*>(a.desc), a.st, a.ru.items, 0.0, 0.0, 0.0,
                nullptr, false};
-  stream_csr2<kRows, kNnzCap, kStages>(src, op);
+  stream_csr2<kRows, kNnzCap, kStages, G>(src, op);
   // The last CTA to leave empties the refinement list for the next iteration.
   if (threadIdx.x == 0) {
     __threadfence();
@@ -961,26 +962,26 @@ struct tf_batch_s {
   template <typename V>
   void launch_iteration(cudaStream_t s, const BatchArgs& a) {
     kb_pupdate<V><<<grid_plain, 256, 0, s>>>(a);
-    if (opts.val_fp32) kb_spmv<V, float><<<grid_tile, kRows, smem_rows32(), s>>>(a);
-    else kb_spmv<V, double><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
+    if (opts.val_fp32) kb_spmv<V, float, 0><<<grid_tile, kRows, smem_rows32(), s>>>(a);
+    else if (opts.row_groups) kb_spmv<V, double, -1><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
+    else kb_spmv<V, double, 0><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
     kb_update<V><<<grid_plain, 256, 0, s>>>(a);
     kb_ru_fold<V><<<grid_plain, 256, 0, s>>>(a);
-    kb_ru_res<V><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
+    if (opts.row_groups) kb_ru_res<V, -1><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
+    else kb_ru_res<V, 0><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
   }
 
   template <typename V>
   int setup_kernels() {
-    TF_CUDA_TRY(cudaFuncSetAttribute(kb_spmv<V, double>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem_csr2()));
-    TF_CUDA_TRY(cudaFuncSetAttribute(kb_spmv<V, float>,
+    for (const void* f : {(const void*)kb_spmv<V, double, 0>, (const void*)kb_spmv<V, double, -1>,
+                          (const void*)kb_ru_res<V, 0>, (const void*)kb_ru_res<V, -1>})
+      TF_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_csr2()));
+    TF_CUDA_TRY(cudaFuncSetAttribute(kb_spmv<V, float, 0>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem_rows32()));
-    TF_CUDA_TRY(cudaFuncSetAttribute(kb_ru_res<V>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem_csr2()));
     int per_sm = 1;
-    TF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_spmv<V, double>,
+    TF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_spmv<V, double, 0>,
                                                               kCsr2RedThreads, smem_csr2()));
     grid_tile = std::max(1, per_sm) * ctx->sm_count;
     grid_plain = ctx->sm_count * 8;
@@ -1445,6 +1446,7 @@ struct Request {
   double res = 0.0;
   std::vector<double> x;
   bool done = false;
+  bool cancel = false;  // set by tf_server_cancel while the request runs
 };
 }  // namespace
 
@@ -1486,6 +1488,7 @@ struct tf_server_s {
         if (st == TF_ERR_BUSY) {
           if (by_slot.empty()) {   // cannot ever fit: fail the request
             std::lock_guard<std::mutex> lk(mu);
+            if (queue.empty() || queue.front() != r) continue;   // cancelled meanwhile
             queue.pop_front();
             r->status = -TF_ERR_OOM;
             r->done = true;
@@ -1497,6 +1500,10 @@ struct tf_server_s {
           break;
         }
         std::lock_guard<std::mutex> lk(mu);
+        if (queue.empty() || queue.front() != r) {   // cancelled while being admitted
+          if (st == TF_OK) eng.retire(slot);
+          continue;
+        }
         queue.pop_front();
         if (st != TF_OK) {
           r->status = -st;
@@ -1527,11 +1534,25 @@ struct tf_server_s {
         cv_done.notify_all();
         continue;
       }
-      // Retire finished systems.
-      std::vector<int> fin;
-      for (auto& kv : by_slot) {
-        const int s = eng.h_state[kv.first].status;
-        if (s != kInit && s != kActive) fin.push_back(kv.first);
+      // Retire finished systems, and cancelled ones that have not finished.
+      std::vector<int> fin, cancelled;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        for (auto& kv : by_slot) {
+          const int s = eng.h_state[kv.first].status;
+          if (s != kInit && s != kActive) fin.push_back(kv.first);
+          else if (kv.second->cancel) cancelled.push_back(kv.first);
+        }
+      }
+      for (int slot : cancelled) {
+        auto r = by_slot[slot];
+        std::lock_guard<std::mutex> lk(mu);
+        r->status = -TF_ERR_CANCELLED;
+        r->t_done = Clock::now();
+        r->done = true;
+        eng.retire(slot);
+        by_slot.erase(slot);
+        cv_done.notify_all();
       }
       for (int slot : fin) {
         auto r = by_slot[slot];
@@ -1550,7 +1571,7 @@ struct tf_server_s {
         ++completed;
         cv_done.notify_all();
       }
-      if (!fin.empty()) eng.rebuild_work();
+      if (!fin.empty() || !cancelled.empty()) eng.rebuild_work();
     }
   }
 };
@@ -1614,6 +1635,29 @@ extern "C" int tf_server_wait(tf_server sv, int64_t req, double* x, int* iters,
                              : ms(r->t_done - r->t_submit).count();
   if (r->status < 0) return -r->status;
   if (x && !r->x.empty()) memcpy(x, r->x.data(), r->x.size() * sizeof(double));
+  return TF_OK;
+  TF_API_END
+}
+
+extern "C" int tf_server_cancel(tf_server sv, int64_t req) {
+  TF_API_BEGIN
+  if (!sv) return TF_ERR_ARG;
+  std::lock_guard<std::mutex> lk(sv->mu);
+  auto it = sv->live.find(req);
+  if (it == sv->live.end()) return TF_ERR_ARG;
+  auto r = it->second;
+  if (r->done) return TF_ERR_BUSY;            // finished: its result stands
+  for (auto q = sv->queue.begin(); q != sv->queue.end(); ++q)
+    if (*q == r) {                            // still queued
+      sv->queue.erase(q);
+      r->status = -TF_ERR_CANCELLED;
+      r->t_done = Clock::now();
+      r->done = true;
+      sv->cv_done.notify_all();
+      return TF_OK;
+    }
+  r->cancel = true;                           // admitted: retired after this sweep
+  sv->cv_work.notify_one();
   return TF_OK;
   TF_API_END
 }

@@ -14,10 +14,11 @@ constexpr double kMicro = 1.0e-6;
 
 // Upper bound on CTAs of any grid-reduced kernel (size of partial arrays).
 constexpr int kMaxBlocks = 4096;
-// A bounded device-side wait gives up after this many nanoseconds unless
-// the caller set another limit (tf_ctx_set_wait_limit).  Draining the bulk
-// copies a CTA armed before it exits always uses this default: a kernel
-// never returns with a copy into its shared memory in flight.
+// A bounded device-side wait gives up after this many nanoseconds; the
+// streaming kernels of a solve stop at this deadline past their start
+// unless the caller set another limit (tf_ctx_set_wait_limit).  Draining
+// the bulk copies a CTA armed before it exits always allows this default:
+// a kernel never returns with a copy into its shared memory in flight.
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
 
 enum Prec : int { kPrecNone = 0, kPrecJacobi = 1, kPrecIcc = 2 };
@@ -297,31 +298,45 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   return ok != 0;
 }
 // Wait for `parity` with a time limit.  Returns false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity,
-                                                  unsigned long long limit_ns = kWaitLimitNs) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = globaltimer_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (globaltimer_ns() - t0 > limit_ns) return false;
+    if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
   }
   return true;
 }
-// The same wait, also ending (false) once *abort_flag is set.
+
+// Waits of the streaming kernels run against a deadline: the kernel's
+// start (globaltimer) plus the limit of the solve (tf_ctx_set_wait_limit,
+// 2 s by default).  A wait fails when its barrier has not completed by the
+// deadline, and also when it completes after the deadline, so a kernel that
+// outlives its limit stops at its next wait whether or not its data keeps
+// arriving (mbarrier.try_wait suspends in hardware until the phase
+// completes, so a limit on the time spent inside one wait alone would
+// rarely be reached).
+__device__ __forceinline__ unsigned long long deadline_after(unsigned long long limit_ns) {
+  return globaltimer_ns() + limit_ns;
+}
+__device__ __forceinline__ bool mbar_wait_deadline(uint64_t* bar, unsigned parity,
+                                                   unsigned long long deadline) {
+  while (!mbar_try_wait(bar, parity))
+    if (globaltimer_ns() > deadline) return false;
+  return globaltimer_ns() <= deadline;
+}
+// The same, also ending (false) once *abort_flag is set.
 __device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, unsigned parity,
                                                    volatile int* abort_flag,
-                                                   unsigned long long limit_ns = kWaitLimitNs) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const unsigned long long t0 = globaltimer_ns();
-  while (!mbar_try_wait(bar, parity)) {
-    if (*abort_flag || globaltimer_ns() - t0 > limit_ns) return false;
-  }
-  return true;
+                                                   unsigned long long deadline) {
+  while (!mbar_try_wait(bar, parity))
+    if (*abort_flag || globaltimer_ns() > deadline) return false;
+  return globaltimer_ns() <= deadline;
 }
 // Wait for the bulk copies armed on `bar` before the CTA exits: always the
 // default limit (never the caller's), so a short caller limit cannot end a
 // CTA with copies into its shared memory still in flight.
 __device__ __forceinline__ void mbar_drain(uint64_t* bar, unsigned parity) {
-  mbar_wait_bounded(bar, parity, kWaitLimitNs);
+  mbar_wait_bounded(bar, parity);
 }
 // Global -> shared bulk copy completing on `bar`.  dst, src 16-byte aligned,
 // bytes a multiple of 16.

@@ -36,6 +36,10 @@
 #include <stdio.h>
 
 #include <algorithm>
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "tf_icc.cuh"
@@ -310,11 +314,39 @@ struct FixedTiles {
   }
 };
 
+// Variable-length tiles over one matrix: tile k is rows [tiles[k],
+// tiles[k+1]) (the drop-in's tile source for the var configurations).
+struct VarTiles {
+  const int* row;
+  const int* col;
+  const double* val;
+  const int* tiles;
+  int ntiles;
+  __device__ int count() const { return ntiles; }
+  __device__ TileDesc desc(int k) const {
+    TileDesc d;
+    d.row = row;
+    d.col = col;
+    d.val = val;
+    d.r0 = __ldg(tiles + k);
+    d.r1 = __ldg(tiles + k + 1);
+    d.j0 = __ldg(row + d.r0);
+    d.j1 = __ldg(row + d.r1);
+    d.skip = 0;
+    d.aux0 = nullptr;
+    d.aux1 = nullptr;
+    d.aux2 = d.aux3 = 0;
+    return d;
+  }
+};
+
 struct SpArgs {
   const int* row;
   const int* col;
   const double* val;
   PatTable pt;       // row patterns (pt.npat > 0 when the PAT kernels run)
+  const int* tiles;  // variable tiles (var configurations)
+  int ntiles;
   int nrows;
   VecArgs v;
   double* out_scalar;  // building-block mode: receives the dot product
@@ -335,6 +367,10 @@ __device__ __forceinline__ bool run_rows(const SpArgs& a, Op& op) {
       op(i, a.val + js, a.col + js, je - js);
     }
     return true;
+  } else if constexpr (tile_is_var(CFG)) {
+    VarTiles src{a.row, a.col, a.val, a.tiles, a.ntiles};
+    return stream_csr2<kTileRows[CFG], kTileNnzCap[CFG], 2, tile_var_g(CFG)>(
+        src, op, wait_limit(a.v.prm));
   } else {
     FixedTiles<kTileRows[CFG]> src{a.row, a.col, a.val, a.nrows};
     return stream_csr2<kTileRows[CFG], kTileNnzCap[CFG], 2>(src, op, wait_limit(a.v.prm));
@@ -606,6 +642,24 @@ using namespace tf;
 // ---------------------------------------------------------------------------
 namespace {
 
+template <int V>
+using IC = std::integral_constant<int, V>;
+
+// Calls f(IC<CFG>, IC<PAT>) for the matrix's tile configuration.
+template <class F>
+auto dispatch_cfg(int cfg, bool pat, F&& f) {
+  switch (cfg) {
+    case kTile512: return pat ? f(IC<kTile512>{}, IC<1>{}) : f(IC<kTile512>{}, IC<0>{});
+    case kTile256: return pat ? f(IC<kTile256>{}, IC<1>{}) : f(IC<kTile256>{}, IC<0>{});
+    case kTile128: return pat ? f(IC<kTile128>{}, IC<1>{}) : f(IC<kTile128>{}, IC<0>{});
+    case kTileVar1: return f(IC<kTileVar1>{}, IC<0>{});
+    case kTileVar2: return f(IC<kTileVar2>{}, IC<0>{});
+    case kTileVar4: return f(IC<kTileVar4>{}, IC<0>{});
+    case kTileVar8: return f(IC<kTileVar8>{}, IC<0>{});
+    default: return f(IC<kTileNone>{}, IC<0>{});
+  }
+}
+
 template <int CFG, int PAT>
 size_t cfg_smem() {
   if constexpr (CFG == kTileNone) return 0;
@@ -656,6 +710,8 @@ SpArgs make_sp_args(tf_matrix_s* m, const VecArgs& v) {
   s.pt.pat = m->d_pat;
   s.pt.tab = m->d_pat_tab;
   s.pt.npat = m->npat;
+  s.tiles = m->d_tiles;
+  s.ntiles = m->ntiles;
   s.nrows = m->ni;
   s.v = v;
   s.out_scalar = nullptr;
@@ -838,19 +894,9 @@ int build_graph_t(tf_matrix_s* m, int xdef, cudaGraphExec_t* out) {
 
 template <int PREC>
 int build_graph_p(tf_matrix_s* m, int xdef, cudaGraphExec_t* out) {
-  const bool pat = m->npat > 0;
-  switch (m->tile_cfg) {
-    case kTile512:
-      return pat ? build_graph_t<kTile512, PREC, 1>(m, xdef, out)
-                 : build_graph_t<kTile512, PREC, 0>(m, xdef, out);
-    case kTile256:
-      return pat ? build_graph_t<kTile256, PREC, 1>(m, xdef, out)
-                 : build_graph_t<kTile256, PREC, 0>(m, xdef, out);
-    case kTile128:
-      return pat ? build_graph_t<kTile128, PREC, 1>(m, xdef, out)
-                 : build_graph_t<kTile128, PREC, 0>(m, xdef, out);
-    default: return build_graph_t<kTileNone, PREC, 0>(m, xdef, out);
-  }
+  return dispatch_cfg(m->tile_cfg, m->npat > 0, [&](auto C, auto P) {
+    return build_graph_t<decltype(C)::value, PREC, decltype(P)::value>(m, xdef, out);
+  });
 }
 
 template <int CFG>
@@ -859,8 +905,9 @@ int occupancy_grid(tf_matrix_s* m, const void* fn, int threads, size_t smem,
   int per_sm = 0;
   TF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
   if (per_sm < 1) per_sm = 1;
-  int units = (CFG == kTileNone) ? (nrows + threads - 1) / threads
-                                 : (nrows + kTileRows[CFG > 2 ? 0 : CFG] - 1) / kTileRows[CFG > 2 ? 0 : CFG];
+  int units = (CFG == kTileNone)     ? (nrows + threads - 1) / threads
+              : tile_is_var(CFG)      ? m->ntiles
+                                      : (nrows + kTileRows[CFG] - 1) / kTileRows[CFG];
   int g = std::min(units, per_sm * m->ctx->sm_count);
   g = std::max(1, std::min(g, kMaxBlocks));
   *grid = g;
@@ -881,6 +928,122 @@ int prepare_cfg(tf_matrix_s* m) {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// SpMV layout choice: the autotuner
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kTuneMinRows = 16384;   // below: launch latency dominates, use the rule
+constexpr int kTuneReps = 5;
+
+std::mutex g_tune_mu;
+std::map<std::vector<long long>, int> g_tune_cache;
+
+// Matrices of one class share a layout: device, row patterns or not, size
+// (power of two of the rows), mean entries per row (halves), longest row
+// (eighths of 64).
+std::vector<long long> tune_key(const tf_matrix_s* m) {
+  const double mean = m->ni > 0 ? (double)m->nnz / (double)m->nt : 0.0;
+  int lg = 0;
+  while ((1 << (lg + 1)) <= m->ni) ++lg;
+  return {m->ctx->device, m->npat > 0, lg, (long long)std::lround(2.0 * mean),
+          std::min(m->max_row_len, 64) / 8};
+}
+
+// Without timing: patterns keep their fixed tile; CSR rows take variable
+// tiles with lanes per row by the mean row length.
+int tile_rule(const tf_matrix_s* m, const std::vector<int>& cands) {
+  if (m->npat > 0) return cands.front();
+  const double mean = m->nt > 0 ? (double)m->nnz / (double)m->nt : 0.0;
+  const int want = mean > 12.0 ? kTileVar4 : mean > 6.0 ? kTileVar2 : kTileVar1;
+  for (int c : cands)
+    if (c == want) return c;
+  return cands.front();
+}
+
+// Median microseconds of one q = A p launch with configuration cfg, timed
+// with CUDA events on the context's stream (values and p are the zeroed
+// registration buffers: the same memory traffic as real data).
+int time_cfg(tf_matrix_s* m, int cfg, int npat, double* us) {
+  m->tile_cfg = cfg;
+  m->npat = cfg <= kTile128 ? npat : 0;
+  int st = tf_fp64_prepare(m);
+  if (st != TF_OK) return st;
+  cudaEvent_t ev[kTuneReps + 1];
+  for (auto& e : ev) TF_CUDA_TRY(cudaEventCreate(&e));
+  for (int w = 0; w < 2 && st == TF_OK; ++w) st = tf_fp64_spmv(m, m->d_val, m->d_p, m->d_q, nullptr);
+  for (int k = 0; k < kTuneReps && st == TF_OK; ++k) {
+    cudaEventRecord(ev[k], m->ctx->stream);
+    st = tf_fp64_spmv(m, m->d_val, m->d_p, m->d_q, nullptr);
+  }
+  cudaEventRecord(ev[kTuneReps], m->ctx->stream);
+  cudaError_t e = cudaEventSynchronize(ev[kTuneReps]);
+  std::vector<float> t(kTuneReps, 0.0f);
+  for (int k = 0; k < kTuneReps && e == cudaSuccess; ++k)
+    e = cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]);
+  for (auto& x : ev) cudaEventDestroy(x);
+  if (st != TF_OK) return st;
+  TF_CUDA_TRY(e);
+  std::sort(t.begin(), t.end());
+  *us = 1e3 * (double)t[kTuneReps / 2];
+  return TF_OK;
+}
+
+}  // namespace
+
+void tf_tune_cache_clear() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache.clear();
+}
+
+int tf_choose_tiles(tf_matrix_s* m, unsigned fit_mask) {
+  const int npat = m->npat;
+  std::vector<int> cands;
+  for (int c = 0; c <= kTile128; ++c)
+    if (fit_mask & (1u << c)) cands.push_back(c);
+  if (npat == 0 || cands.empty()) {
+    if (m->ntiles > 0)
+      for (int c : {kTileVar1, kTileVar2, kTileVar4, kTileVar8}) cands.push_back(c);
+    cands.push_back(kTileNone);
+  } else {
+    cands.resize(1);   // row patterns: the widest fixed tile
+  }
+  m->tune.clear();
+  int choice = -1;
+  if (const char* f = getenv("TF_TILE_CFG")) {
+    const int c = atoi(f);
+    const bool ok = c == kTileNone || (c <= kTile128 && c >= 0 && (fit_mask & (1u << c))) ||
+                    (c < kNumTileCfgs && tile_is_var(c) && m->ntiles > 0);
+    if (ok) choice = c;
+  }
+  if (choice < 0 && cands.size() == 1) choice = cands[0];
+  if (choice < 0 && (m->ni < kTuneMinRows || getenv("TF_NO_TUNE"))) choice = tile_rule(m, cands);
+  const std::vector<long long> key = tune_key(m);
+  if (choice < 0) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) choice = it->second;
+  }
+  if (choice < 0) {
+    double best = 0.0;
+    for (int c : cands) {
+      double us = 0.0;
+      const int st = time_cfg(m, c, npat, &us);
+      if (st != TF_OK) return st;
+      m->tune.emplace_back(c, us);
+      if (choice < 0 || us < best) {
+        best = us;
+        choice = c;
+      }
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = choice;
+  }
+  m->tile_cfg = choice;
+  m->npat = choice <= kTile128 ? npat : 0;
+  return tf_fp64_prepare(m);
+}
+
 int tf_fp64_prepare(tf_matrix_s* m) {
   const int n = std::max(m->nt, 1);
   int per_sm = 0;
@@ -890,13 +1053,9 @@ int tf_fp64_prepare(tf_matrix_s* m) {
   m->vec_grid = std::max(1, std::min({(n + 511) / 512, m->ctx->sm_count * per_sm, kMaxBlocks}));
   if (const char* e = getenv("TF_VEC_DIR")) m->vec_dir = atoi(e) ? 1 : 0;
   if (m->tile_cfg == kTileNone) m->npat = 0;
-  const bool pat = m->npat > 0;
-  switch (m->tile_cfg) {
-    case kTile512: return pat ? prepare_cfg<kTile512, 1>(m) : prepare_cfg<kTile512, 0>(m);
-    case kTile256: return pat ? prepare_cfg<kTile256, 1>(m) : prepare_cfg<kTile256, 0>(m);
-    case kTile128: return pat ? prepare_cfg<kTile128, 1>(m) : prepare_cfg<kTile128, 0>(m);
-    default: return prepare_cfg<kTileNone, 0>(m);
-  }
+  return dispatch_cfg(m->tile_cfg, m->npat > 0, [&](auto C, auto P) {
+    return prepare_cfg<decltype(C)::value, decltype(P)::value>(m);
+  });
 }
 
 namespace {
@@ -950,19 +1109,9 @@ int run_host_loop_t(tf_matrix_s* m, int xdef) {
 
 template <int PREC>
 int run_host_loop_p(tf_matrix_s* m, int xdef) {
-  const bool pat = m->npat > 0;
-  switch (m->tile_cfg) {
-    case kTile512:
-      return pat ? run_host_loop_t<kTile512, PREC, 1>(m, xdef)
-                 : run_host_loop_t<kTile512, PREC, 0>(m, xdef);
-    case kTile256:
-      return pat ? run_host_loop_t<kTile256, PREC, 1>(m, xdef)
-                 : run_host_loop_t<kTile256, PREC, 0>(m, xdef);
-    case kTile128:
-      return pat ? run_host_loop_t<kTile128, PREC, 1>(m, xdef)
-                 : run_host_loop_t<kTile128, PREC, 0>(m, xdef);
-    default: return run_host_loop_t<kTileNone, PREC, 0>(m, xdef);
-  }
+  return dispatch_cfg(m->tile_cfg, m->npat > 0, [&](auto C, auto P) {
+    return run_host_loop_t<decltype(C)::value, PREC, decltype(P)::value>(m, xdef);
+  });
 }
 }  // namespace
 
@@ -1031,23 +1180,9 @@ static double* bb_scalar(tf_matrix_s* m) { return m->d_part + 8 * kMaxBlocks; }
 int tf_fp64_spmv(tf_matrix_s* m, const double* val, const double* p, double* q,
                  double* pq) {
   double* scal = bb_scalar(m);
-  int st;
-  const bool pat = m->npat > 0;
-  switch (m->tile_cfg) {
-    case kTile512:
-      st = pat ? launch_spmv<kTile512, 1>(m, val, p, q, scal)
-               : launch_spmv<kTile512, 0>(m, val, p, q, scal);
-      break;
-    case kTile256:
-      st = pat ? launch_spmv<kTile256, 1>(m, val, p, q, scal)
-               : launch_spmv<kTile256, 0>(m, val, p, q, scal);
-      break;
-    case kTile128:
-      st = pat ? launch_spmv<kTile128, 1>(m, val, p, q, scal)
-               : launch_spmv<kTile128, 0>(m, val, p, q, scal);
-      break;
-    default: st = launch_spmv<kTileNone, 0>(m, val, p, q, scal); break;
-  }
+  const int st = dispatch_cfg(m->tile_cfg, m->npat > 0, [&](auto C, auto P) {
+    return launch_spmv<decltype(C)::value, decltype(P)::value>(m, val, p, q, scal);
+  });
   if (st == TF_OK && pq)
     TF_CUDA_TRY(cudaMemcpyAsync(pq, scal, sizeof(double), cudaMemcpyDeviceToDevice,
                                 m->ctx->stream));
@@ -1057,19 +1192,9 @@ int tf_fp64_spmv(tf_matrix_s* m, const double* val, const double* p, double* q,
 int tf_fp64_residual(tf_matrix_s* m, const double* val, const double* b,
                      const double* x, double* r) {
   double* scal = bb_scalar(m);
-  const bool pat = m->npat > 0;
-  switch (m->tile_cfg) {
-    case kTile512:
-      return pat ? launch_resid<kTile512, 1>(m, val, b, x, r, scal)
-                 : launch_resid<kTile512, 0>(m, val, b, x, r, scal);
-    case kTile256:
-      return pat ? launch_resid<kTile256, 1>(m, val, b, x, r, scal)
-                 : launch_resid<kTile256, 0>(m, val, b, x, r, scal);
-    case kTile128:
-      return pat ? launch_resid<kTile128, 1>(m, val, b, x, r, scal)
-                 : launch_resid<kTile128, 0>(m, val, b, x, r, scal);
-    default: return launch_resid<kTileNone, 0>(m, val, b, x, r, scal);
-  }
+  return dispatch_cfg(m->tile_cfg, m->npat > 0, [&](auto C, auto P) {
+    return launch_resid<decltype(C)::value, decltype(P)::value>(m, val, b, x, r, scal);
+  });
 }
 
 namespace tf {
@@ -1356,19 +1481,9 @@ int build_multi_graph_t(tf_matrix_s* m, int nr, int xdef, cudaGraphExec_t* out) 
 
 template <int PREC>
 int build_multi_graph_p(tf_matrix_s* m, int nr, int xdef, cudaGraphExec_t* out) {
-  const bool pat = m->npat > 0;
-  switch (m->tile_cfg) {
-    case kTile512:
-      return pat ? build_multi_graph_t<kTile512, 1, PREC>(m, nr, xdef, out)
-                 : build_multi_graph_t<kTile512, 0, PREC>(m, nr, xdef, out);
-    case kTile256:
-      return pat ? build_multi_graph_t<kTile256, 1, PREC>(m, nr, xdef, out)
-                 : build_multi_graph_t<kTile256, 0, PREC>(m, nr, xdef, out);
-    case kTile128:
-      return pat ? build_multi_graph_t<kTile128, 1, PREC>(m, nr, xdef, out)
-                 : build_multi_graph_t<kTile128, 0, PREC>(m, nr, xdef, out);
-    default: return build_multi_graph_t<kTileNone, 0, PREC>(m, nr, xdef, out);
-  }
+  return dispatch_cfg(m->tile_cfg, m->npat > 0, [&](auto C, auto P) {
+    return build_multi_graph_t<decltype(C)::value, decltype(P)::value, PREC>(m, nr, xdef, out);
+  });
 }
 
 int alloc_slice(tf_matrix_s* m, tf_slice_s** out) {

@@ -6,6 +6,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/tf_krylov.h"
@@ -116,8 +117,13 @@ struct tf_matrix_s {
   unsigned char* d_pat = nullptr;
   int* d_pat_tab = nullptr;
   int npat = 0;
-  // SpMV tiling picked at registration
+  // SpMV tiling picked at registration; variable tiles (tile_cfg 4-7):
+  // ntiles + 1 row boundaries
   int tile_cfg = tf::kTileNone;
+  int* d_tiles = nullptr;
+  int ntiles = 0;
+  // SpMV layouts timed at registration (configuration, median us per launch)
+  std::vector<std::pair<int, double>> tune;
   int spmv_grid = 1;
   int vec_grid = 1;
   int vec_dir = 0;       // walking direction of the vector kernels (see tf_fp64.cu)
@@ -169,6 +175,13 @@ void tf_slices_free(tf_matrix_s* m);
 
 // FP64 drop-in entry points implemented in tf_fp64.cu
 int tf_fp64_prepare(tf_matrix_s* m);
+// Picks the SpMV layout of a freshly registered matrix (tf_fp64.cu): the
+// TF_TILE_CFG override when valid, else the fastest of the candidate
+// layouts timed on the device (cached per matrix class), else a rule for
+// small matrices; then prepares the kernels.  fit_mask bit c: fixed tile
+// configuration c (0-2) holds every tile of the matrix.
+int tf_choose_tiles(tf_matrix_s* m, unsigned fit_mask);
+void tf_tune_cache_clear();
 int tf_fp64_run(tf_matrix_s* m, int prec);   // runs on m->ctx->stream
 int tf_fp64_spmv(tf_matrix_s* m, const double* val, const double* p,
                  double* q, double* pq);

@@ -347,6 +347,28 @@ extern "C" int tf_pool_wait(tf_pool p, int64_t req, int* niter, double* fin_res,
   TF_API_END
 }
 
+extern "C" int tf_pool_cancel(tf_pool p, int64_t req) {
+  TF_API_BEGIN
+  if (!p) return TF_ERR_ARG;
+  std::lock_guard<std::mutex> lk(p->mu);
+  auto it = p->live.find(req);
+  if (it == p->live.end()) return TF_ERR_ARG;
+  auto r = it->second;
+  if (r->done) return TF_ERR_BUSY;            // finished: its result stands
+  for (auto q = p->queue.begin(); q != p->queue.end(); ++q)
+    if (*q == r) {                            // not yet taken by a worker
+      p->queue.erase(q);
+      r->status = TF_ERR_CANCELLED;
+      r->t_start = r->t_done = Clock::now();
+      r->done = true;
+      p->cv_done.notify_all();
+      p->cv_work.notify_all();
+      return TF_OK;
+    }
+  return TF_ERR_BUSY;                         // running: a solve runs to its end
+  TF_API_END
+}
+
 extern "C" int tf_pool_stats(tf_pool p, long long* submitted, long long* completed,
                              long long* rejected, size_t* peak_bytes) {
   TF_API_BEGIN

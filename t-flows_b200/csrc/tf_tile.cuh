@@ -266,6 +266,7 @@ __device__ bool stream_tiles_pat(const int* __restrict__ row, const PatTable& pt
   __syncthreads();
   const int* tab_len = tab + pt.npat * kPatMaxLen;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned long long deadline = deadline_after(wait_ns);
   bool ok = true;
 
   if (warp == kConsumerWarps) {
@@ -275,7 +276,7 @@ __device__ bool stream_tiles_pat(const int* __restrict__ row, const PatTable& pt
       for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++issued) {
         const int s = issued % STAGES;
         if (issued >= STAGES) {
-          if (!mbar_wait_bounded(&empty[s], (unsigned)(issued / STAGES - 1) & 1u, wait_ns)) {
+          if (!mbar_wait_deadline(&empty[s], (unsigned)(issued / STAGES - 1) & 1u, deadline)) {
             ok = false;
             *abort_flag = 1;
             break;
@@ -308,7 +309,7 @@ __device__ bool stream_tiles_pat(const int* __restrict__ row, const PatTable& pt
     int it = 0;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
       const int s = it % STAGES;
-      if (!mbar_wait_bounded(&full[s], (unsigned)(it / STAGES) & 1u, wait_ns)) {
+      if (!mbar_wait_deadline(&full[s], (unsigned)(it / STAGES) & 1u, deadline)) {
         ok = false;
         *abort_flag = 1;
         break;
@@ -330,9 +331,21 @@ __device__ bool stream_tiles_pat(const int* __restrict__ row, const PatTable& pt
   return !__syncthreads_or(!ok);
 }
 
-// Tile configurations the host may pick (rows per tile = threads per CTA).
-enum TileCfgId { kTile512 = 0, kTile256 = 1, kTile128 = 2, kTileNone = 3 };
-constexpr int kTileRows[3] = {512, 256, 128};
-constexpr int kTileNnzCap[3] = {4096, 4096, 2048};
+// Tile configurations the host may pick.
+//   0-2  fixed tiles of 512 / 256 / 128 rows (row patterns, or CSR with the
+//        two-phase consumers of tf_tile2.cuh);
+//   3    no tiles: one thread per row straight from global memory;
+//   4-7  CSR tiles of variable length (at most 512 rows and 4096 entries,
+//        boundaries listed at registration) with warp-group consumers of
+//        G = 1, 2, 4, 8 lanes per row.
+enum TileCfgId { kTile512 = 0, kTile256 = 1, kTile128 = 2, kTileNone = 3,
+                 kTileVar1 = 4, kTileVar2 = 5, kTileVar4 = 6, kTileVar8 = 7 };
+constexpr int kNumTileCfgs = 8;
+constexpr int kTileRows[kNumTileCfgs] = {512, 256, 128, 512, 512, 512, 512, 512};
+constexpr int kTileNnzCap[kNumTileCfgs] = {4096, 4096, 2048, 0, 4096, 4096, 4096, 4096};
+__host__ __device__ constexpr bool tile_is_var(int c) { return c >= kTileVar1; }
+__host__ __device__ constexpr int tile_var_g(int c) {
+  return c == kTileVar1 ? 1 : c == kTileVar2 ? 2 : c == kTileVar4 ? 4 : 8;
+}
 
 }  // namespace tf

@@ -111,7 +111,64 @@ __device__ __forceinline__ bool consumer_bar_or(bool v) {
   return r != 0;
 }
 
-template <int ROWCAP, int NNZCAP, int STAGES, class S, class Op>
+// Warp-group consumers (G = 1, 2, 4 or 8; G = 0 selects the two-phase
+// consumers above).  Each warp takes 32/G rows of the staged tile at a
+// time, G lanes per row: lane g of a row's group forms the products of
+// the row's entries g, g+G, g+2G, ... of a 16-entry chunk (16/G gathers in
+// flight per lane), and the group's first lane adds the 16 products in
+// entry order, fetched by warp shuffles, before the next chunk.  The sum is
+// the one-thread-per-row sum in storage order, bit for bit; no barrier
+// joins the consumer warps, so each warp moves on as soon as its rows are
+// done.  Rows of any length up to the tile's entry cap are handled.
+template <int G, class Op>
+__device__ __forceinline__ void wg_rows(Op& op, const double* prod, const int* cc,
+                                        const int* sr, int p0, int r0, int r1, int j0,
+                                        int warp, int lane, int nwarps) {
+  constexpr int kRpw = 32 / G;   // rows per warp pass
+  constexpr int kU = 16 / G;     // products per lane per 16-entry chunk
+  const int grp = lane / G, g = lane & (G - 1);
+  const int gbase = lane & ~(G - 1);
+  for (int rb = r0 + warp * kRpw; rb < r1; rb += nwarps * kRpw) {
+    const int i = rb + grp;
+    int js = 0, len = 0;
+    if (i < r1) {
+      js = sr[i - p0] - j0;
+      len = sr[i + 1 - p0] - j0 - js;
+    }
+    const int maxlen = __reduce_max_sync(0xffffffffu, len);
+    double acc = (i < r1) ? op.row_init(i) : 0.0;
+    for (int k0 = 0; k0 < maxlen; k0 += 16) {
+      double pr[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int q = k0 + u * G + g;
+        pr[u] = (q < len) ? __dmul_rn(prod[js + q], op.gather(cc[js + q])) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if constexpr (G == 1) {
+          if (k0 + u < len) acc = op.combine(acc, pr[u]);
+        } else {
+#pragma unroll
+          for (int gg = 0; gg < G; ++gg) {
+            const double v = __shfl_sync(0xffffffffu, pr[u], gbase + gg);
+            if (k0 + u * G + gg < len) acc = op.combine(acc, v);
+          }
+        }
+      }
+    }
+    if (g == 0 && i < r1) op.row_done(i, acc);
+  }
+}
+
+// G = -1: the group width is picked per tile from its mean row length
+// (the same for every warp of the CTA), for sources whose tiles mix short
+// and long rows (the batch engine's systems).
+__device__ __forceinline__ int tile_group_width(int rows, int entries) {
+  return entries > 12 * rows ? 4 : entries > 6 * rows ? 2 : 1;
+}
+
+template <int ROWCAP, int NNZCAP, int STAGES, int G = 0, class S, class Op>
 __device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLimitNs) {
   using L = Csr2Layout<ROWCAP, NNZCAP, STAGES>;
   constexpr int kConsWarps = kCons / 32;
@@ -152,6 +209,7 @@ __device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLi
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned long long deadline = deadline_after(wait_ns);
   bool ok = true;
 
   if (warp == kConsWarps) {
@@ -166,7 +224,7 @@ __device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLi
         const TileDesc d = nxt;
         if (k + (int)gridDim.x < count) nxt = src.desc(k + gridDim.x);
         if (issued >= STAGES) {
-          if (!mbar_wait_bounded(&empty[s], (unsigned)(issued / STAGES - 1) & 1u, wait_ns)) {
+          if (!mbar_wait_deadline(&empty[s], (unsigned)(issued / STAGES - 1) & 1u, deadline)) {
             ok = false;
             *abort_flag = 1;
             break;
@@ -206,7 +264,7 @@ __device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLi
       int it = 0;
       for (int k = blockIdx.x; k < count; k += gridDim.x, ++it) {
         if (!mbar_wait_or_abort(&parked[it & 1], (unsigned)(it >> 1) & 1u, abort_flag,
-                                wait_ns)) {
+                                deadline)) {
           ok = false;
           *abort_flag = 1;
           break;
@@ -216,13 +274,64 @@ __device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLi
         if (lane == 0) mbar_arrive(&freed[it & 1]);
       }
     }
+  } else if constexpr (G != 0) {
+    // ---- consumer warps, G lanes per row (wg_rows) ----
+    int it = 0;
+    for (int k = blockIdx.x; k < count; k += gridDim.x, ++it) {
+      const int s = it % STAGES;
+      bool stop = !mbar_wait_deadline(&full[s], (unsigned)(it / STAGES) & 1u, deadline);
+      stop = __any_sync(0xffffffffu, stop || *abort_flag);   // warp-uniform
+      if (stop) {
+        ok = false;
+        *abort_flag = 1;
+        break;
+      }
+      const int* m = meta + L::kMetaInts * s;
+      if (!m[7]) {
+        const int a0 = m[0], c0 = m[1], p0 = m[2], r0 = m[3], r1 = m[4], j0 = m[5];
+        const TileAux aux{*reinterpret_cast<const void* const*>(m + 12),
+                          *reinterpret_cast<void* const*>(m + 14), m[9], m[10]};
+        op.begin(k, aux);
+        const double* prod = sval(s) + (j0 - a0);
+        const int* cc = scol(s) + (j0 - c0);
+        if constexpr (G > 0) {
+          wg_rows<G>(op, prod, cc, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+        } else {
+          switch (tile_group_width(r1 - r0, m[6] - j0)) {
+            case 1: wg_rows<1>(op, prod, cc, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps); break;
+            case 2: wg_rows<2>(op, prod, cc, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps); break;
+            default: wg_rows<4>(op, prod, cc, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+          }
+        }
+        if constexpr (!kRed) op.tile_end(it);
+      }
+      if constexpr (kRed) {
+        const bool slot_free = __all_sync(
+            0xffffffffu,
+            it < 2 ||
+                mbar_wait_or_abort(&freed[it & 1], (unsigned)((it >> 1) - 1) & 1u, abort_flag,
+                                   deadline));
+        if (!slot_free) {
+          ok = false;
+          *abort_flag = 1;
+        }
+        if (!m[7] && slot_free) op.tile_end(it);
+        if (threadIdx.x == 0)
+          op.tile_id(it, m[7], TileAux{*reinterpret_cast<const void* const*>(m + 12),
+                                       *reinterpret_cast<void* const*>(m + 14), m[9], m[10]});
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&parked[it & 1]);
+      }
+      __syncwarp();   // the stage is only read here: the producer's proxy fence suffices
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
   } else {
     // ---- consumer warps ----
     const int t = threadIdx.x;
     int it = 0;
     for (int k = blockIdx.x; k < count; k += gridDim.x, ++it) {
       const int s = it % STAGES;
-      bool stop = !mbar_wait_bounded(&full[s], (unsigned)(it / STAGES) & 1u, wait_ns);
+      bool stop = !mbar_wait_deadline(&full[s], (unsigned)(it / STAGES) & 1u, deadline);
       stop = stop || *abort_flag;
       // Consumers must pass the named barrier equally often: they decide
       // together whether to stop here.
@@ -305,7 +414,7 @@ __device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLi
             0xffffffffu,
             it < 2 ||
                 mbar_wait_or_abort(&freed[it & 1], (unsigned)((it >> 1) - 1) & 1u, abort_flag,
-                                   wait_ns));
+                                   deadline));
         if (!slot_free) {
           ok = false;
           *abort_flag = 1;

@@ -12,7 +12,8 @@ STATUS = {0: "free", 1: "init", 2: "active", 3: "converged", 4: "maxiter", 5: "b
 class BatchOpts(ctypes.Structure):
     _fields_ = [("vec_fp32", ctypes.c_int), ("val_fp32", ctypes.c_int),
                 ("sweep_iters", ctypes.c_int), ("max_systems", ctypes.c_int),
-                ("ru_delta", ctypes.c_double), ("mem_budget", ctypes.c_size_t)]
+                ("ru_delta", ctypes.c_double), ("mem_budget", ctypes.c_size_t),
+                ("row_groups", ctypes.c_int)]
 
 
 def _lib():
@@ -38,14 +39,15 @@ def _lib():
     L.tf_server_stats.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong),
                                   ctypes.POINTER(ctypes.c_longlong), ip, ip]
     L.tf_server_destroy.argtypes = [_vp]
+    L.tf_server_cancel.argtypes = [_vp, ctypes.c_int64]
     L._tf_batch_bound = True
     return L
 
 
 def _opts(vec_fp32=True, val_fp32=False, sweep_iters=8, max_systems=1024, ru_delta=0.1,
-          mem_budget=4 << 30):
+          mem_budget=4 << 30, row_groups=0):
     return BatchOpts(int(vec_fp32), int(val_fp32), int(sweep_iters), int(max_systems),
-                     float(ru_delta), int(mem_budget))
+                     float(ru_delta), int(mem_budget), int(row_groups))
 
 
 def _sys_args(s):
@@ -162,6 +164,10 @@ class Server:
         native._check(rc, "tf_server_wait")
         return dict(x=x, iters=it.value, res=res.value, status=STATUS.get(st.value, st.value),
                     latency_ms=lat.value, queue_ms=qms.value)
+
+    def cancel(self, rid):
+        """tf_server_cancel: 0 (will end cancelled), 7 (already finished)."""
+        return self.L.tf_server_cancel(self.h, rid)
 
     def stats(self):
         a, c = ctypes.c_longlong(), ctypes.c_longlong()

@@ -32,7 +32,8 @@ EXPORTS = [
     "tf_ctx_set_wait_limit",
     "tf_host_pin", "tf_host_unpin", "tf_spmv", "tf_residual", "tf_nrms",
     "tf_ctx_sync", "tf_ctx_stream", "tf_last_error_message", "tf_matrix_tile_config",
-    "tf_matrix_row_patterns", "tf_matrix_renumbered",
+    "tf_matrix_row_patterns", "tf_matrix_renumbered", "tf_matrix_tuning",
+    "tf_tuning_cache_clear", "tf_pool_cancel", "tf_server_cancel",
     "tf_faces_register", "tf_assemble_pressure", "tf_assemble_momentum",
     "tf_solve_multi", "tf_solve_multi_device", "tf_batch_add_many",
 ]
@@ -85,6 +86,7 @@ def load(path=LIB_PATH):
     L.tf_matrix_info.argtypes = [_vp, _c_int_p, _c_int_p,
                                  ctypes.POINTER(ctypes.c_int64), _c_int_p]
     L.tf_matrix_tile_config.argtypes = [_vp]
+    L.tf_matrix_tuning.argtypes = [_vp, _c_int_p, _c_dbl_p, ctypes.c_int, _c_int_p]
     L.tf_matrix_row_patterns.argtypes = [_vp]
     L.tf_matrix_renumbered.argtypes = [_vp]
     solve_args = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int,
@@ -167,6 +169,11 @@ class Context:
         self.close()
 
 
+def tuning_cache_clear():
+    """tf_tuning_cache_clear: the next matrix of every class is timed again."""
+    _check(load().tf_tuning_cache_clear(), "tf_tuning_cache_clear")
+
+
 class Matrix:
     """Device-resident structure of one Matrix_Type (tf_matrix)."""
 
@@ -188,6 +195,18 @@ class Matrix:
     @property
     def tile_config(self):
         return load().tf_matrix_tile_config(self.h)
+
+    def tuning(self):
+        """[(tile configuration, median us per SpMV)] timed at registration
+        (empty when the layout came from the cache, TF_TILE_CFG or the rule)."""
+        L = load()
+        cnt = ctypes.c_int(0)
+        _check(L.tf_matrix_tuning(self.h, None, None, 0, ctypes.byref(cnt)), "tf_matrix_tuning")
+        cfg = (ctypes.c_int * max(cnt.value, 1))()
+        us = (ctypes.c_double * max(cnt.value, 1))()
+        _check(L.tf_matrix_tuning(self.h, cfg, us, cnt.value, ctypes.byref(cnt)),
+               "tf_matrix_tuning")
+        return [(cfg[i], us[i]) for i in range(cnt.value)]
 
     @property
     def renumbered(self):

@@ -25,6 +25,7 @@ def _lib():
     L.tf_pool_resident.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong),
                                    ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_size_t)]
     L.tf_pool_destroy.argtypes = [_vp]
+    L.tf_pool_cancel.argtypes = [_vp, ctypes.c_int64]
     L._tf_pool_bound = True
     return L
 
@@ -75,6 +76,10 @@ class Pool:
             arrs = self.keep.pop(rid)
         return dict(x=arrs[5], niter=it.value, fin_res=res.value, latency_ms=lat.value,
                     queue_ms=qms.value)
+
+    def cancel(self, rid):
+        """tf_pool_cancel: 0 (dropped from the queue), 7 (running or finished)."""
+        return self.L.tf_pool_cancel(self.h, rid)
 
     def stats(self):
         a, c, r = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()

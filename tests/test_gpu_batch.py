@@ -13,7 +13,7 @@ import pytest
 import scipy.sparse as sps
 import scipy.sparse.linalg as spla
 
-from tflows_b200 import batch, systems
+from tflows_b200 import batch, native, systems
 
 pytestmark = pytest.mark.gpu
 
@@ -198,5 +198,33 @@ def test_server_continuous_batching(gpu_ctx):
             assert r["latency_ms"] >= r["queue_ms"] >= 0.0
         st = srv.stats()
         assert st["completed"] == len(sysl) * 2 and st["error"] == 0
+    finally:
+        srv.close()
+
+
+def test_server_cancel_running_and_queued(gpu_ctx):
+    """A running request is retired at the end of its sweep and its slot
+    reused; a queued one is dropped; a finished one keeps its result."""
+    slow = systems.small_hex(40, seed=21, kind="pressure", ratio=1.05)
+    quick = systems.small_hex(8, seed=22, kind="pressure")
+    srv = batch.Server(gpu_ctx, mem_budget=1 << 30, sweep_iters=4, max_systems=1)
+    try:
+        # tol 0: the slow request can only stop at its iteration limit
+        running = srv.submit(slow, tol=0.0, maxit=10 ** 7)
+        queued = srv.submit(quick)          # one slot: waits behind the slow one
+        t0 = time.perf_counter()
+        while srv.stats()["admitted"] < 1 and time.perf_counter() - t0 < 5.0:
+            time.sleep(0.001)
+        assert srv.stats()["admitted"] == 1  # the slow one holds the only slot
+        assert srv.cancel(queued) == 0
+        assert srv.cancel(running) == 0
+        for rid in (queued, running):
+            with pytest.raises(native.TFError) as e:
+                srv.wait(rid)
+            assert e.value.status == 8      # TF_ERR_CANCELLED
+        done = srv.submit(quick)
+        r = srv.wait(done)
+        assert r["status"] == "converged"
+        assert srv.cancel(done) == 3        # collected: unknown id
     finally:
         srv.close()

@@ -1,10 +1,11 @@
 """Failure paths of the drop-in, made without faulting the GPU.
 
-* A bounded device-side wait that runs out: the context's wait limit is set
-  to a nanosecond, so the SpMV streamers' first waits for a tile's copies
+* The watchdog: the context's limit is set to a nanosecond, so the SpMV
+  streamers' first waits for a tile's copies come after their deadline and
   give up; the solve must end with TF_ERR_TIMEOUT (the CTAs still wait for
   the copies they started, with the default limit, before exiting), and
-  the same context must then solve normally again.
+  the same context must then solve normally again.  Run on the row-pattern
+  streamer (hex) and on the CSR streamer (polyhedral).
 * Degenerate input the reference does not reject (Message_Mod/Error.f90 is
   never reached for it): NaN in b and a zero diagonal.  The numbers
   propagate; the drop-in must run the same iterations as the oracle (which
@@ -33,11 +34,12 @@ def gpu(ctx, m, s, val, b, miter, tol, norm, prec="jacobi"):
     return x, it, res
 
 
-@pytest.mark.parametrize("kind", ["hex-row-patterns", "poly-csr"])
-def test_wait_limit_runs_out_then_context_recovers(kind):
+@pytest.mark.parametrize("kind", ["hex-row-patterns", "poly-csr-tiles"])
+def test_wait_limit_runs_out_then_context_recovers(kind, monkeypatch):
     if kind == "hex-row-patterns":
         s = systems.small_hex(64, seed=4, kind="pressure", ratio=1.02)
     else:
+        monkeypatch.setenv("TF_TILE_CFG", "6")   # variable CSR tiles, 4 lanes per row
         s = systems.poly_system(60000, seed=5, kind="pressure", tol=1e-10, miter=5000,
                                 norm=1.0)
     ctx = native.Context(0)

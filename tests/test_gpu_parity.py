@@ -151,11 +151,12 @@ def test_spmv_and_residual_bitwise(gpu_ctx, kind, n, ratio, patterns, monkeypatc
         m.close()
 
 
-@pytest.mark.parametrize("cfg", [0, 1, 2, 3])
+@pytest.mark.parametrize("cfg", [0, 1, 2, 3, 4, 5, 6, 7])
 @pytest.mark.parametrize("patterns", [True, False])
 def test_every_tile_configuration(gpu_ctx, cfg, patterns, monkeypatch):
-    """Tile widths 512/256/128 (row-pattern or CSR columns) and the
-    direct-from-global path agree."""
+    """Tile widths 512/256/128 (row-pattern or CSR columns), the
+    direct-from-global path and the variable CSR tiles with 1/2/4/8 lanes
+    per row agree."""
     torch = torch_dev()
     monkeypatch.setenv("TF_TILE_CFG", str(cfg))
     if not patterns:
@@ -164,7 +165,7 @@ def test_every_tile_configuration(gpu_ctx, cfg, patterns, monkeypatch):
     m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia)
     try:
         assert m.tile_config == cfg
-        assert (m.row_patterns > 0) == (patterns and cfg != 3)
+        assert (m.row_patterns > 0) == (patterns and cfg <= 2)
         p = np.random.default_rng(1).standard_normal(s.n)
         dval, dp, dq = _dev_arrays(torch, s.val, p, np.zeros(s.n))
         torch.cuda.synchronize()
@@ -176,10 +177,69 @@ def test_every_tile_configuration(gpu_ctx, cfg, patterns, monkeypatch):
         m.close()
 
 
+@pytest.mark.parametrize("mesh,n", [("delaunay", 3000), ("delaunay", 40000), ("lattice", 20000)])
+@pytest.mark.parametrize("cfg", [3, 4, 5, 6, 7])
+def test_variable_tiles_bitwise(gpu_ctx, mesh, n, cfg, monkeypatch):
+    """Polyhedral rows (10-49 entries) on variable CSR tiles, every group
+    width: q and r equal the oracle's bit for bit, and a whole solve agrees
+    with the oracle (dot products are summed in another order per layout)."""
+    torch = torch_dev()
+    monkeypatch.setenv("TF_TILE_CFG", str(cfg))
+    s = (systems.poly_system(n, seed=8, kind="pressure", tol=1e-10, miter=5000, norm=1.0)
+         if mesh == "delaunay" else _lattice_poly(n, 8))
+    rng = np.random.default_rng(9)
+    p, xx = rng.standard_normal(s.n), rng.standard_normal(s.n)
+    m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia)
+    try:
+        assert m.tile_config == cfg
+        dval, dp, dq, db, dx, dr = _dev_arrays(torch, s.val, p, np.zeros(s.n), s.b, xx,
+                                               np.zeros(s.n))
+        dpq = torch.zeros(1, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        native.spmv(gpu_ctx, m, dval.data_ptr(), dp.data_ptr(), dq.data_ptr(), dpq.data_ptr())
+        native.residual(gpu_ctx, m, dval.data_ptr(), db.data_ptr(), dx.data_ptr(),
+                        dr.data_ptr())
+        gpu_ctx.sync()
+        q = dq.cpu().numpy()
+        assert np.array_equal(q, O.spmv(s.csr.row, s.csr.col, s.csr.dia, s.val, p))
+        assert np.array_equal(dr.cpu().numpy(),
+                              O.residual(s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, xx))
+        assert dpq.item() == pytest.approx(float(np.dot(p, q)), rel=1e-13)
+    finally:
+        m.close()
+    args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, "cg", "jacobi", 5000, 1e-10, 1.0)
+    check_parity(gpu_solve(gpu_ctx, *args), oracle_solve(*args), 1e-10)
+
+
+def test_autotuner_picks_the_fastest_candidate(gpu_ctx, monkeypatch):
+    """Registration times every candidate layout and keeps the fastest; a
+    second matrix of the same class reuses the choice without timing."""
+    monkeypatch.delenv("TF_TILE_CFG", raising=False)
+    monkeypatch.delenv("TF_NO_TUNE", raising=False)
+    native.tuning_cache_clear()
+    s = systems.poly_system(40000, seed=13, kind="pressure", tol=1e-10, miter=5000, norm=1.0)
+    m = native.Matrix(gpu_ctx, s.csr.row, s.csr.col, s.csr.dia)
+    try:
+        t = m.tuning()
+        assert {c for c, _ in t} >= {3, 4, 5, 6, 7}
+        assert all(us > 0 for _, us in t)
+        best = min(t, key=lambda cu: cu[1])[0]
+        assert m.tile_config == best
+    finally:
+        m.close()
+    m2 = native.Matrix(gpu_ctx, s.csr.row.copy(), s.csr.col.copy(), s.csr.dia.copy())
+    try:
+        assert m2.tuning() == [] and m2.tile_config == best
+    finally:
+        m2.close()
+
+
 @pytest.mark.parametrize("prec,norm", [("jacobi", 1.0), ("jacobi", None), ("icc", 1.0)])
 def test_row_patterns_do_not_change_the_solve(gpu_ctx, prec, norm, monkeypatch):
     """The row-pattern layout feeds the same operands in the same order to
-    every row sum, so a whole solve is bit-identical with the CSR columns."""
+    every row sum, so a whole solve is bit-identical with the CSR columns on
+    the same tiles (512-row tiles for both)."""
+    monkeypatch.setenv("TF_TILE_CFG", "0")
     s = systems.small_hex(23, seed=9, kind="pressure", ratio=1.04)
     args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, "cg", prec, 3000, 1e-10, norm)
     g1 = gpu_solve(gpu_ctx, *args)

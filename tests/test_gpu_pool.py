@@ -125,3 +125,28 @@ def test_pool_releases_held_structures_for_new_requests(gpu_ctx):
         assert p.stats()["peak_bytes"] <= budget
     finally:
         p.close()
+
+
+def test_pool_cancel_queued_request(gpu_ctx):
+    """A request still in the queue is dropped (TF_ERR_CANCELLED, x left as
+    given); one that ran keeps its result; the pool keeps serving."""
+    big = systems.small_hex(48, seed=6, kind="pressure", ratio=1.02)
+    small = systems.small_hex(10, seed=7, kind="pressure")
+    want = _reference(gpu_ctx, small)
+    p = pool.Pool(workers=1, mem_budget=1 << 30)
+    try:
+        first = [p.submit(big) for _ in range(3)]     # one worker: these run in turn
+        last = p.submit(small)
+        assert p.cancel(last) == 0                     # still queued behind them
+        with pytest.raises(native.TFError) as e:
+            p.wait(last)
+        assert e.value.status == 8                     # TF_ERR_CANCELLED
+        for rid in first:
+            p.wait(rid)
+        assert p.cancel(first[0]) == 3                 # collected: unknown id
+        again = p.submit(small)
+        r = p.wait(again)
+        assert p.cancel(again) == 3
+        assert r["niter"] == want[1] and np.array_equal(r["x"], want[0])
+    finally:
+        p.close()
