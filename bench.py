@@ -74,7 +74,8 @@ def parse():
     ap.add_argument("--rcm", action="store_true",
                     help="spmv: renumber the cells by reverse Cuthill-McKee first")
     ap.add_argument("--mode", default="solve",
-                    choices=["solve", "spmv", "iters", "multi", "poly", "batched", "served"],
+                    choices=["solve", "spmv", "iters", "multi", "poly", "batched", "served",
+                             "icc"],
                     help="spmv: only the pressure matrix and `--steps` SpMV launches "
                          "(the small case profiled with ncu); iters: `--steps` Cg solves "
                          "of exactly `--iters` iterations on the pressure matrix (launch "
@@ -569,6 +570,46 @@ def run_fixed_iterations(args):
     ctx.close()
 
 
+def run_icc(args):
+    """The reference's default preconditioner (incomplete Cholesky,
+    Prec_Form.f90:68-78, Prec_Solve.f90:64-92) against Jacobi on the bench's
+    pressure matrix (--size^3 stretched hex): iterations, time per solve and
+    per iteration, and the kernel launches per iteration."""
+    import torch
+    from tflows_b200 import native
+    p = make_workload(args.size, args.peclet)[0]
+    ctx = native.Context(0)
+    m = native.Matrix(ctx, p.csr.row, p.csr.col, p.csr.dia)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    val0, b0 = torch.from_numpy(p.val).cuda(), torch.from_numpy(p.b).cuda()
+    out = {"mode": "icc", "n": p.n, "nnz": p.nnz, "tol": p.tol,
+           "levels": m.icc_levels()}
+    for prec in ("jacobi", "icc"):
+        best = None
+        for _ in range(max(1, args.steps)):
+            val, b = val0.clone(), b0.clone()
+            x = torch.zeros(p.n, dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            it, res = native.solve_device(ctx, m, "cg", prec, val.data_ptr(), x.data_ptr(),
+                                          b.data_ptr(), p.miter, p.tol, p.norm)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            if best is None or ms < best[0]:
+                best = (ms, it, res)
+        out[prec] = {"ms": best[0], "iters": best[1], "fin_res": best[2],
+                     "us_per_iteration": 1e3 * best[0] / max(best[1], 1)}
+    lv = out["levels"]
+    out["jacobi"]["launches_per_iteration"] = 3
+    out["icc"]["launches_per_iteration"] = m.icc_launches_per_iteration()
+    out["icc_vs_jacobi_time"] = out["icc"]["ms"] / out["jacobi"]["ms"]
+    print(json.dumps(out), flush=True)
+    m.close()
+    ctx.close()
+
+
 def run_multi_rhs(args):
     """Three velocity components with one momentum matrix (the bench's
     200^3 Bicg system, three seeded right-hand sides): one tf_solve_multi
@@ -856,6 +897,9 @@ def main():
         return
     if args.mode == "spmv":
         run_spmv_only(args)
+        return
+    if args.mode == "icc":
+        run_icc(args)
         return
     if args.mode == "iters":
         run_fixed_iterations(args)

@@ -106,6 +106,11 @@ int tf_matrix_tuning(tf_matrix m, int* cfg, double* us, int cap, int* count);
 /* Forget the layouts chosen for earlier registrations, so the next matrix
  * of each class is timed again. */
 int tf_tuning_cache_clear(void);
+/* Levels of the incomplete-Cholesky sweeps built at registration (rows of
+ * one level depend only on rows of earlier levels in Prec_Form.f90:69-78 /
+ * Prec_Solve.f90:67-92's recurrences): forward and backward counts, 0 when
+ * ICC is unavailable (diagonal not first).  No reference counterpart. */
+int tf_matrix_icc_levels(tf_matrix m, int* forward, int* backward);
 /* Number of row patterns of the compressed column layout chosen at
  * registration (rows whose column offsets relative to the row index repeat,
  * as on structured hex blocks: one byte per row instead of four per entry;

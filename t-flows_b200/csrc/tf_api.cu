@@ -194,7 +194,8 @@ void tf_matrix_free(tf_matrix_s* m) {
   void* ptrs[] = {m->d_row, m->d_col, m->d_dia, m->d_tiles, m->d_val, m->d_x, m->d_b,
                   m->d_r, m->d_p, m->d_q, m->d_z, m->d_adiag, m->d_part,
                   m->d_hist, m->d_state, m->d_params, m->d_levf_rows, m->d_levb_rows,
-                  m->d_icc_d, m->d_icc_dinv, m->d_pat, m->d_pat_tab, m->d_perm, m->d_src,
+                  m->d_icc_d, m->d_icc_dinv, m->d_icc_units_f, m->d_icc_units_b,
+                  m->d_icc_flag, m->d_pat, m->d_pat_tab, m->d_perm, m->d_src,
                   m->d_face_cell, m->d_face_pos, m->d_cf_ptr, m->d_cf};
   for (void* p : ptrs)
     if (p) {
@@ -569,6 +570,15 @@ extern "C" int tf_matrix_tuning(tf_matrix m, int* cfg, double* us, int cap, int*
     us[i] = m->tune[i].second;
   }
   *count = (int)m->tune.size();
+  return TF_OK;
+  TF_API_END
+}
+
+extern "C" int tf_matrix_icc_levels(tf_matrix m, int* forward, int* backward) {
+  TF_API_BEGIN
+  if (!m || !forward || !backward) return TF_ERR_ARG;
+  *forward = m->icc_ready ? (int)m->h_levf_ptr.size() - 1 : 0;
+  *backward = m->icc_ready ? (int)m->h_levb_ptr.size() - 1 : 0;
   return TF_OK;
   TF_API_END
 }

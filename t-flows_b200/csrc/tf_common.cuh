@@ -55,12 +55,24 @@ struct SolveState {
   int done;
   int status;         // TF_OK or TF_ERR_TIMEOUT
   int x_pend;         // x still lacks the last alpha * p (deferred update)
-  int pad;
+  unsigned icc_epoch;  // sweeps of the persistent ICC kernels so far (flags' epoch)
   unsigned counter[8];  // last-block-done counters, one per kernel kind
 };
 
 enum CounterSlot { kCntDiag = 0, kCntScale, kCntResid, kCntSpmv, kCntUpdate,
-                   kCntZ, kCntAux, kCntAux2 };
+                   kCntZ, kCntAux, kCntSweep };
+
+// Acquire / release accesses at GPU scope: a flag read with ld_acquire_gpu
+// that returns the value st_release_gpu stored makes every write the
+// storing thread made before it visible to the reader's later loads.
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
   unsigned long long t;

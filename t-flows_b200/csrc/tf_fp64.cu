@@ -739,7 +739,41 @@ struct NodeBuilder {
     }
     return node;
   }
+  // A kernel node launched cooperatively (all its CTAs resident at once).
+  cudaGraphNode_t add_coop(const void* fn, dim3 grid, dim3 block, void** args,
+                           cudaGraphNode_t dep) {
+    cudaGraphNode_t node = add(fn, grid, block, 0, args, dep);
+    if (status != TF_OK) return nullptr;
+    cudaKernelNodeAttrValue v{};
+    v.cooperative = 1;
+    cudaError_t e = cudaGraphKernelNodeSetAttribute(node, cudaKernelNodeAttributeCooperative, &v);
+    if (e != cudaSuccess) {
+      tf_set_last_cuda_error(e, "cudaGraphKernelNodeSetAttribute(cooperative)", __FILE__,
+                             __LINE__);
+      status = TF_ERR_CUDA;
+    }
+    return node;
+  }
 };
+
+// Arguments of the persistent ICC sweeps.
+struct IccSweeps {
+  IccSweepArgs form, fwd, bwd;
+};
+IccArgs icc_args(tf_matrix_s* m);
+IccSweeps icc_sweep_args(tf_matrix_s* m) {
+  IccSweeps w{};
+  IccArgs a = icc_args(m);
+  a.rows = m->d_levf_rows;
+  w.fwd = IccSweepArgs{a, m->d_icc_units_f, m->icc_nunits_f, m->d_icc_flag, m->d_state,
+                       m->d_params};
+  w.form = w.fwd;
+  w.form.a.st = nullptr;
+  a.rows = m->d_levb_rows;
+  w.bwd = IccSweepArgs{a, m->d_icc_units_b, m->icc_nunits_b, m->d_icc_flag, m->d_state,
+                       m->d_params};
+  return w;
+}
 
 IccArgs icc_args(tf_matrix_s* m) {
   IccArgs a{};
@@ -834,26 +868,41 @@ int build_graph_t(tf_matrix_s* m, int xdef, cudaGraphExec_t* out) {
   RhoArgs ra{m->ni, m->d_z, m->d_r, m->d_part, m->d_state};
   void* rargs[] = {&ra.ni, &ra.z, &ra.r, &ra.part, &ra.st};
   std::vector<void*> form_args, fwd_args, bwd_args;
+  IccSweeps sw{};
+  void* sw_form[] = {&sw.form};
+  void* sw_fwd[] = {&sw.fwd};
+  void* sw_bwd[] = {&sw.bwd};
+  const bool sweeps = PREC == kPrecIcc && m->icc_sweep_grid > 0;
+  const dim3 swg(std::max(1, m->icc_sweep_grid));
   if (PREC == kPrecIcc) {
     lv = icc_level_args(m);
+    sw = icc_sweep_args(m);
     for (auto& a : lv.form) form_args.push_back(&a);
     for (auto& a : lv.fwd) fwd_args.push_back(&a);
     for (auto& a : lv.bwd) bwd_args.push_back(&a);
   }
   auto lgrid = [](int count) { return dim3(std::max(1, (count + 255) / 256)); };
-  // z = M^-1 r by the two level-scheduled sweeps, then rho = z.r
+  // z = M^-1 r by the two triangular sweeps (persistent kernels, or one
+  // kernel per level), then rho = z.r
   auto add_icc_apply = [&](NodeBuilder& b, cudaGraphNode_t dep) {
-    for (size_t l = 0; l < lv.fwd.size(); ++l)
-      dep = b.add((const void*)k_icc_fwd_level, lgrid(lv.fwd[l].count), dim3(256), 0,
-                  &fwd_args[l], dep);
-    for (size_t l = 0; l < lv.bwd.size(); ++l)
-      dep = b.add((const void*)k_icc_bwd_level, lgrid(lv.bwd[l].count), dim3(256), 0,
-                  &bwd_args[l], dep);
+    if (sweeps) {
+      dep = b.add_coop((const void*)k_icc_sweep<kSweepFwd>, swg, dim3(256), sw_fwd, dep);
+      dep = b.add_coop((const void*)k_icc_sweep<kSweepBwd>, swg, dim3(256), sw_bwd, dep);
+    } else {
+      for (size_t l = 0; l < lv.fwd.size(); ++l)
+        dep = b.add((const void*)k_icc_fwd_level, lgrid(lv.fwd[l].count), dim3(256), 0,
+                    &fwd_args[l], dep);
+      for (size_t l = 0; l < lv.bwd.size(); ++l)
+        dep = b.add((const void*)k_icc_bwd_level, lgrid(lv.bwd[l].count), dim3(256), 0,
+                    &bwd_args[l], dep);
+    }
     return b.add((const void*)k_icc_rho, vg, vb, 0, rargs, dep);
   };
   cudaGraphNode_t n1 = nb.add((const void*)k_diag, vg, vb, 0, vargs, nullptr);
   cudaGraphNode_t n2 = nb.add((const void*)k_scale, vg, vb, 0, vargs, n1);
-  if (PREC == kPrecIcc)   // Prec_Form (Cg.f90:89) on the scaled matrix
+  if (PREC == kPrecIcc && sweeps)   // Prec_Form (Cg.f90:89) on the scaled matrix
+    n2 = nb.add_coop((const void*)k_icc_sweep<kSweepForm>, swg, dim3(256), sw_form, n2);
+  else if (PREC == kPrecIcc)
     for (size_t l = 0; l < lv.form.size(); ++l)
       n2 = nb.add((const void*)k_icc_form_level, lgrid(lv.form[l].count), dim3(256), 0,
                   &form_args[l], n2);
@@ -927,6 +976,25 @@ int prepare_cfg(tf_matrix_s* m) {
 }
 
 }  // namespace
+
+int tf_icc_prepare_sweeps(tf_matrix_s* m) {
+  m->icc_sweep_grid = 0;
+  if (getenv("TF_ICC_LEVELS")) return TF_OK;
+  int coop = 0;
+  TF_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, m->ctx->device));
+  if (!coop) return TF_OK;
+  int per_sm = 1 << 30;
+  for (const void* fn : {(const void*)k_icc_sweep<kSweepForm>, (const void*)k_icc_sweep<kSweepFwd>,
+                         (const void*)k_icc_sweep<kSweepBwd>}) {
+    int b = 0;
+    TF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, 256, 0));
+    per_sm = std::min(per_sm, b);
+  }
+  if (per_sm < 1) return TF_OK;
+  const int units = std::max(m->icc_nunits_f, m->icc_nunits_b);
+  m->icc_sweep_grid = std::max(1, std::min(per_sm * m->ctx->sm_count, (units + 7) / 8));
+  return TF_OK;
+}
 
 // ---------------------------------------------------------------------------
 // SpMV layout choice: the autotuner
@@ -1074,16 +1142,32 @@ int run_host_loop_t(tf_matrix_s* m, int xdef) {
   const IterFns fns = iter_fns<PREC>(xdef, m->vec_dir);
   void* vargs[] = {&va};
   IccLevelArgs lv;
-  if (PREC == kPrecIcc) lv = icc_level_args(m);
+  IccSweeps sw{};
+  const bool sweeps = PREC == kPrecIcc && m->icc_sweep_grid > 0;
+  if (PREC == kPrecIcc) {
+    lv = icc_level_args(m);
+    sw = icc_sweep_args(m);
+  }
   auto lgrid = [](int count) { return std::max(1, (count + 255) / 256); };
+  auto coop = [&](const void* fn, IccSweepArgs* a) {
+    void* args[] = {a};
+    return cudaLaunchCooperativeKernel(fn, dim3(m->icc_sweep_grid), dim3(256), args, 0, s);
+  };
   auto icc_apply = [&]() {
-    for (auto& a : lv.fwd) k_icc_fwd_level<<<lgrid(a.count), 256, 0, s>>>(a);
-    for (auto& a : lv.bwd) k_icc_bwd_level<<<lgrid(a.count), 256, 0, s>>>(a);
+    if (sweeps) {
+      coop((const void*)k_icc_sweep<kSweepFwd>, &sw.fwd);
+      coop((const void*)k_icc_sweep<kSweepBwd>, &sw.bwd);
+    } else {
+      for (auto& a : lv.fwd) k_icc_fwd_level<<<lgrid(a.count), 256, 0, s>>>(a);
+      for (auto& a : lv.bwd) k_icc_bwd_level<<<lgrid(a.count), 256, 0, s>>>(a);
+    }
     k_icc_rho<<<vg, 256, 0, s>>>(m->ni, m->d_z, m->d_r, m->d_part, m->d_state);
   };
   k_diag<<<vg, 256, 0, s>>>(va);
   k_scale<<<vg, 256, 0, s>>>(va);
-  if (PREC == kPrecIcc)
+  if (PREC == kPrecIcc && sweeps)
+    TF_CUDA_TRY(coop((const void*)k_icc_sweep<kSweepForm>, &sw.form));
+  else if (PREC == kPrecIcc)
     for (auto& a : lv.form) k_icc_form_level<<<lgrid(a.count), 256, 0, s>>>(a);
   k_residual<CFG, PREC, PAT><<<sg, cfg_threads<CFG, PAT>(), ssm, s>>>(sa);
   if (PREC == kPrecIcc) icc_apply();

@@ -134,6 +134,13 @@ struct tf_matrix_s {
   std::vector<int> h_levf_ptr, h_levb_ptr;
   double* d_icc_d = nullptr;     // Prec_Form's d
   double* d_icc_dinv = nullptr;  // Prec_Form's d_inv
+  // Persistent sweeps (k_icc_sweep): units of <= 32 rows of one level, in
+  // level order, per sweep direction; a per-row epoch flag.
+  int2* d_icc_units_f = nullptr;
+  int2* d_icc_units_b = nullptr;
+  int icc_nunits_f = 0, icc_nunits_b = 0;
+  unsigned* d_icc_flag = nullptr;
+  int icc_sweep_grid = 0;        // 0: per-level kernels
   // cached graphs, one per (preconditioner, x update deferred or not)
   cudaGraphExec_t graph[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   // The same graphs bound to a caller's device val/x/b (tf_solve_device in
@@ -190,6 +197,11 @@ int tf_fp64_residual(tf_matrix_s* m, const double* val, const double* b,
 int tf_fp64_nrms(tf_matrix_s* m, const double* val, const double* r,
                  const double* x, int has_norm, double norm, double* out);
 int tf_icc_build(tf_matrix_s* m, const int* h_row0, const int* h_col0);
+// Grid of the persistent ICC sweeps (tf_fp64.cu): the CTAs that fit on the
+// device at once (they wait on one another); icc_sweep_grid stays 0, and
+// the per-level kernels are used, when TF_ICC_LEVELS is set or the device
+// cannot launch cooperatively.
+int tf_icc_prepare_sweeps(tf_matrix_s* m);
 // Registration behind tf_matrix_register; want_icc = 0 skips the ICC level
 // schedule.  Device bytes the matrix will hold, for budgeting.
 int tf_matrix_create(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const int* row,

@@ -33,7 +33,7 @@ EXPORTS = [
     "tf_host_pin", "tf_host_unpin", "tf_spmv", "tf_residual", "tf_nrms",
     "tf_ctx_sync", "tf_ctx_stream", "tf_last_error_message", "tf_matrix_tile_config",
     "tf_matrix_row_patterns", "tf_matrix_renumbered", "tf_matrix_tuning",
-    "tf_tuning_cache_clear", "tf_pool_cancel", "tf_server_cancel",
+    "tf_tuning_cache_clear", "tf_pool_cancel", "tf_server_cancel", "tf_matrix_icc_levels",
     "tf_faces_register", "tf_assemble_pressure", "tf_assemble_momentum",
     "tf_solve_multi", "tf_solve_multi_device", "tf_batch_add_many",
 ]
@@ -87,6 +87,7 @@ def load(path=LIB_PATH):
                                  ctypes.POINTER(ctypes.c_int64), _c_int_p]
     L.tf_matrix_tile_config.argtypes = [_vp]
     L.tf_matrix_tuning.argtypes = [_vp, _c_int_p, _c_dbl_p, ctypes.c_int, _c_int_p]
+    L.tf_matrix_icc_levels.argtypes = [_vp, _c_int_p, _c_int_p]
     L.tf_matrix_row_patterns.argtypes = [_vp]
     L.tf_matrix_renumbered.argtypes = [_vp]
     solve_args = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int,
@@ -207,6 +208,19 @@ class Matrix:
         _check(L.tf_matrix_tuning(self.h, cfg, us, cnt.value, ctypes.byref(cnt)),
                "tf_matrix_tuning")
         return [(cfg[i], us[i]) for i in range(cnt.value)]
+
+    def icc_levels(self):
+        """(forward, backward) level counts of the incomplete-Cholesky sweeps."""
+        f, b = ctypes.c_int(0), ctypes.c_int(0)
+        _check(load().tf_matrix_icc_levels(self.h, ctypes.byref(f), ctypes.byref(b)),
+               "tf_matrix_icc_levels")
+        return f.value, b.value
+
+    def icc_launches_per_iteration(self):
+        """Kernel launches of one ICC-preconditioned Cg iteration: the three
+        iteration kernels, one per sweep level, and the rho reduction."""
+        f, b = self.icc_levels()
+        return 3 + f + b + 1
 
     @property
     def renumbered(self):

@@ -582,6 +582,25 @@ def test_icc_parity_medium_and_poly(gpu_ctx):
     check_parity(gpu_solve(gpu_ctx, *args), oracle_solve(*args), 1e-10)
 
 
+@pytest.mark.parametrize("kind", ["hex", "poly"])
+def test_icc_persistent_sweeps_equal_level_kernels(gpu_ctx, kind, monkeypatch):
+    """The persistent ICC sweeps (one cooperative kernel per sweep, rows
+    waiting on their neighbours' flags) give the per-level kernels' bits."""
+    if kind == "hex":
+        s = systems.small_hex(30, seed=4, kind="pressure", ratio=1.03)
+    else:
+        s = systems.poly_system(20000, seed=6, kind="pressure", tol=1e-10, miter=3000,
+                                norm=1.0)
+    args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, "cg", "icc", 3000, 1e-10, 1.0)
+    g1 = gpu_solve(gpu_ctx, *args)
+    monkeypatch.setenv("TF_ICC_LEVELS", "1")
+    g2 = gpu_solve(gpu_ctx, *args)
+    assert g1[3] == g2[3] and g1[4] == g2[4]
+    for u, w in zip(g1[:3], g2[:3]):
+        assert np.array_equal(u, w)
+    check_parity(g1, oracle_solve(*args), 1e-10)
+
+
 def test_icc_needs_diagonal_first(gpu_ctx):
     """The 4x4 example of Matrix_Mod.f90 stores rows in column order."""
     from golden.make_golden import example_4x4
