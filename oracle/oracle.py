@@ -1,10 +1,9 @@
 """ctypes loader of the CPU oracle (oracle/libtforacle.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
-bench.py's CPU-baseline leg, never by the product.  PARITY UNPINNED: the
-reference (Fortran) cannot be compiled or run here, so the oracle is pinned
-by scipy's PCG iterates, the Bicg == Cg identity, the 4x4 example of
-Matrix_Mod.f90:44-55 and a pure-Python transliteration (see tf_oracle.cpp).
+bench.py's CPU-baseline leg, never by the product.  Pinned to the reference:
+the reference's own Fortran source, executed by oracle/f90exec.py, produced
+the golden fixtures this oracle reproduces bit for bit (see tf_oracle.cpp).
 """
 import ctypes
 import os

@@ -6,14 +6,16 @@
 //  baseline leg load it; the product library (libtfkrylov.so) never links it
 //  and never falls back to it.
 //
-//  PARITY UNPINNED: the reference is Fortran 2008 and no Fortran compiler is
-//  available, so the reference cannot be run to produce outputs, and the
-//  reference ships no golden vectors, known-answer tests or fixtures for this
-//  path.  This restatement is pinned instead by (i) scipy's independent PCG,
-//  compared iterate by iterate, (ii) the identity Bicg(A) == Cg(A) bitwise
-//  (Bicg.f90:129-133 copies r1 into r2 and never uses A^T), (iii) the 4x4
-//  CSR example of Matrix_Mod.f90:44-55, and (iv) a pure-Python line-by-line
-//  transliteration run on small cases (tests/golden/make_golden.py).
+//  PINNED TO THE REFERENCE: the reference is Fortran 2008 and no Fortran
+//  compiler is available, so its source is executed instead by
+//  oracle/f90exec.py (a translator of the Fortran subset the path's files
+//  use); the golden fixtures are that execution's outputs, and this
+//  restatement reproduces them bit for bit, as it does the executed source
+//  on every case of tests/test_reference_exec.py.  Further pins: scipy's
+//  independent PCG, compared iterate by iterate, the identity
+//  Bicg(A) == Cg(A) bitwise (Bicg.f90:129-133 copies r1 into r2 and never
+//  uses A^T), the 4x4 CSR example of Matrix_Mod.f90:44-55, and a pure-Python
+//  line-by-line transliteration (oracle/pyref.py).
 //
 //  Conventions follow the reference exactly:
 //    * all `real` are FP64 (REAL=double build, makefile -fdefault-real-8);

@@ -194,8 +194,8 @@ void tf_matrix_free(tf_matrix_s* m) {
   void* ptrs[] = {m->d_row, m->d_col, m->d_dia, m->d_tiles, m->d_val, m->d_x, m->d_b,
                   m->d_r, m->d_p, m->d_q, m->d_z, m->d_adiag, m->d_part,
                   m->d_hist, m->d_state, m->d_params, m->d_levf_rows, m->d_levb_rows,
-                  m->d_icc_d, m->d_icc_dinv, m->d_icc_units_f, m->d_icc_units_b,
-                  m->d_icc_flag, m->d_pat, m->d_pat_tab, m->d_perm, m->d_src,
+                  m->d_icc_d, m->d_icc_dinv, m->d_icc_levf_ptr, m->d_icc_levb_ptr,
+                  m->d_pat, m->d_pat_tab, m->d_perm, m->d_src,
                   m->d_face_cell, m->d_face_pos, m->d_cf_ptr, m->d_cf};
   for (void* p : ptrs)
     if (p) {

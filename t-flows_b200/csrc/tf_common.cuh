@@ -55,12 +55,14 @@ struct SolveState {
   int done;
   int status;         // TF_OK or TF_ERR_TIMEOUT
   int x_pend;         // x still lacks the last alpha * p (deferred update)
-  unsigned icc_epoch;  // sweeps of the persistent ICC kernels so far (flags' epoch)
+  int pad;
   unsigned counter[8];  // last-block-done counters, one per kernel kind
+  unsigned bar_count;   // grid barrier of the persistent ICC sweeps: arrivals
+  unsigned bar_gen;     // ... and generation
 };
 
 enum CounterSlot { kCntDiag = 0, kCntScale, kCntResid, kCntSpmv, kCntUpdate,
-                   kCntZ, kCntAux, kCntSweep };
+                   kCntZ, kCntAux, kCntAux2 };
 
 // Acquire / release accesses at GPU scope: a flag read with ld_acquire_gpu
 // that returns the value st_release_gpu stored makes every write the

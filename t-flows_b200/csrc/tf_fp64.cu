@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(256) k_diag(VecArgs a) {
     st->iter = 0;
     st->niter = 0;
     st->status = 0;
+    st->bar_count = 0u;   // a timed-out ICC sweep may have left arrivals behind
     st->res = 0.0;
     st->rho = 0.0;
     st->rho_old = 0.0;
@@ -211,7 +212,8 @@ struct OpSpmvDot {
   __device__ __forceinline__ void pat(int i, const double* v, const int* o, int len) {
     body(i, v, [i, o](int k) { return i + o[k]; }, len);
   }
-  // two-phase streamer
+  // per-row hooks (row-pattern and CSR streamers)
+  static constexpr bool kRowOps = true;
   __device__ __forceinline__ void begin(int, TileAux) {}
   static constexpr bool kReducer = false;
   __device__ __forceinline__ double gather(int c) const { return __ldg(p + c); }
@@ -267,7 +269,8 @@ struct OpResidual {
   __device__ __forceinline__ void pat(int i, const double* v, const int* o, int len) {
     body(i, v, [i, o](int k) { return i + o[k]; }, len);
   }
-  // two-phase streamer
+  // per-row hooks (row-pattern and CSR streamers)
+  static constexpr bool kRowOps = true;
   __device__ __forceinline__ void begin(int, TileAux) {}
   static constexpr bool kReducer = false;
   __device__ __forceinline__ double gather(int c) const { return __ldg(x + c); }
@@ -765,12 +768,12 @@ IccSweeps icc_sweep_args(tf_matrix_s* m) {
   IccSweeps w{};
   IccArgs a = icc_args(m);
   a.rows = m->d_levf_rows;
-  w.fwd = IccSweepArgs{a, m->d_icc_units_f, m->icc_nunits_f, m->d_icc_flag, m->d_state,
+  w.fwd = IccSweepArgs{a, m->d_icc_levf_ptr, (int)m->h_levf_ptr.size() - 1, m->d_state,
                        m->d_params};
   w.form = w.fwd;
   w.form.a.st = nullptr;
   a.rows = m->d_levb_rows;
-  w.bwd = IccSweepArgs{a, m->d_icc_units_b, m->icc_nunits_b, m->d_icc_flag, m->d_state,
+  w.bwd = IccSweepArgs{a, m->d_icc_levb_ptr, (int)m->h_levb_ptr.size() - 1, m->d_state,
                        m->d_params};
   return w;
 }
@@ -991,8 +994,12 @@ int tf_icc_prepare_sweeps(tf_matrix_s* m) {
     per_sm = std::min(per_sm, b);
   }
   if (per_sm < 1) return TF_OK;
-  const int units = std::max(m->icc_nunits_f, m->icc_nunits_b);
-  m->icc_sweep_grid = std::max(1, std::min(per_sm * m->ctx->sm_count, (units + 7) / 8));
+  // One CTA of 256 threads per SM: a level of a 200^3 hex grid has at most
+  // ~30,000 rows (about one per thread), and every CTA joins every barrier.
+  int widest = 1;
+  for (const auto* ptr : {&m->h_levf_ptr, &m->h_levb_ptr})
+    for (size_t l = 0; l + 1 < ptr->size(); ++l) widest = std::max(widest, (*ptr)[l + 1] - (*ptr)[l]);
+  m->icc_sweep_grid = std::max(1, std::min(m->ctx->sm_count, (widest + 255) / 256));
   return TF_OK;
 }
 
@@ -1019,11 +1026,12 @@ std::vector<long long> tune_key(const tf_matrix_s* m) {
 }
 
 // Without timing: patterns keep their fixed tile; CSR rows take variable
-// tiles with lanes per row by the mean row length.
+// tiles, one lane per row unless rows are long (one lane per row measured
+// fastest on polyhedral rows of 16.5 entries on average).
 int tile_rule(const tf_matrix_s* m, const std::vector<int>& cands) {
   if (m->npat > 0) return cands.front();
   const double mean = m->nt > 0 ? (double)m->nnz / (double)m->nt : 0.0;
-  const int want = mean > 12.0 ? kTileVar4 : mean > 6.0 ? kTileVar2 : kTileVar1;
+  const int want = mean > 48.0 ? kTileVar4 : mean > 24.0 ? kTileVar2 : kTileVar1;
   for (int c : cands)
     if (c == want) return c;
   return cands.front();
@@ -1350,6 +1358,7 @@ struct MultiCond {
 constexpr int kMultiChunk = 2;
 template <int NR>
 struct OpSpmvMulti {
+  static constexpr bool kRowOps = false;
   const double* p[NR];
   double* q[NR];
   double pq[NR];

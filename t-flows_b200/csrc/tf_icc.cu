@@ -19,14 +19,6 @@ void bucket(const std::vector<int>& lev, int nlev, std::vector<int>& ptr,
   for (int i = 0; i < (int)lev.size(); ++i) rows[fill[lev[i]]++] = i;
 }
 
-// Units of <= 32 consecutive rows of one level, in level order.
-std::vector<int2> units(const std::vector<int>& ptr) {
-  std::vector<int2> u;
-  for (size_t l = 0; l + 1 < ptr.size(); ++l)
-    for (int s = ptr[l]; s < ptr[l + 1]; s += 32) u.push_back(make_int2(s, std::min(32, ptr[l + 1] - s)));
-  return u;
-}
-
 }  // namespace
 
 // Levels of the sweeps in Prec_Form.f90:69-78 / Prec_Solve.f90:67-92.
@@ -73,29 +65,25 @@ int tf_icc_build(tf_matrix_s* m, const int* row0, const int* col0) {
   if (st == TF_OK) st = tf_dev_alloc_bytes(m->ctx, &p, nv * sizeof(double));
   m->d_icc_dinv = (double*)p;
   if (st != TF_OK) return st;
-  // Units of the persistent sweeps: at most 32 rows of one level each.
-  std::vector<int2> uf = units(m->h_levf_ptr), ub = units(m->h_levb_ptr);
+  // Level pointers of the persistent sweeps.
   void* q = nullptr;
-  st = tf_dev_alloc_bytes(m->ctx, &q, std::max<size_t>(uf.size(), 1) * sizeof(int2));
+  st = tf_dev_alloc_bytes(m->ctx, &q, m->h_levf_ptr.size() * sizeof(int));
   if (st != TF_OK) return st;
-  m->d_icc_units_f = (int2*)q;
-  st = tf_dev_alloc_bytes(m->ctx, &q, std::max<size_t>(ub.size(), 1) * sizeof(int2));
+  m->d_icc_levf_ptr = (int*)q;
+  st = tf_dev_alloc_bytes(m->ctx, &q, m->h_levb_ptr.size() * sizeof(int));
   if (st != TF_OK) return st;
-  m->d_icc_units_b = (int2*)q;
-  st = tf_dev_alloc_bytes(m->ctx, &q, nv * sizeof(unsigned));   // zeroed: epoch 0
-  if (st != TF_OK) return st;
-  m->d_icc_flag = (unsigned*)q;
-  m->icc_nunits_f = (int)uf.size();
-  m->icc_nunits_b = (int)ub.size();
+  m->d_icc_levb_ptr = (int*)q;
   // From pageable memory these return once the source has been staged.
   TF_CUDA_TRY(cudaMemcpyAsync(m->d_levf_rows, rf.data(), rf.size() * sizeof(int),
                               cudaMemcpyHostToDevice, m->ctx->stream));
   TF_CUDA_TRY(cudaMemcpyAsync(m->d_levb_rows, rb.data(), rb.size() * sizeof(int),
                               cudaMemcpyHostToDevice, m->ctx->stream));
-  TF_CUDA_TRY(cudaMemcpyAsync(m->d_icc_units_f, uf.data(), uf.size() * sizeof(int2),
-                              cudaMemcpyHostToDevice, m->ctx->stream));
-  TF_CUDA_TRY(cudaMemcpyAsync(m->d_icc_units_b, ub.data(), ub.size() * sizeof(int2),
-                              cudaMemcpyHostToDevice, m->ctx->stream));
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_icc_levf_ptr, m->h_levf_ptr.data(),
+                              m->h_levf_ptr.size() * sizeof(int), cudaMemcpyHostToDevice,
+                              m->ctx->stream));
+  TF_CUDA_TRY(cudaMemcpyAsync(m->d_icc_levb_ptr, m->h_levb_ptr.data(),
+                              m->h_levb_ptr.size() * sizeof(int), cudaMemcpyHostToDevice,
+                              m->ctx->stream));
   if (!m->ctx->async_alloc) TF_CUDA_TRY(cudaStreamSynchronize(m->ctx->stream));
   m->icc_ready = 1;
   return tf_icc_prepare_sweeps(m);

@@ -85,99 +85,112 @@ __global__ void __launch_bounds__(256) k_icc_bwd_level(IccArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// The same three recurrences as single persistent kernels.  One kernel
-// per sweep instead of one per level: its warps walk units of at most 32
-// rows of one level, in level order (warp w takes units w, w + W, ...).
-// Before reading a row k's value a lane waits until flag[k] holds this
-// sweep's epoch; after writing row i's value it publishes flag[i] = epoch
-// with release semantics, and readers acquire it, reading the value from
-// L2.  The arithmetic of every row is the per-level kernels' (and so the
-// reference's) in the same order, so the bits are the same.  A unit waits
-// only on rows of earlier levels, i.e. of earlier units, and every warp
-// walks its units in order, so the lowest unfinished unit can always
-// proceed -- provided every CTA is resident: the kernel is launched
-// cooperatively, with no more CTAs than fit at once.  Waits are bounded by
-// the solve's deadline (a timeout is recorded in the solve status).  The
-// kernel's last CTA advances the epoch for the next sweep.
+// The same three recurrences as single persistent kernels, level by level:
+// one kernel per sweep instead of one per level.  Every thread of the grid
+// takes rows t, t + T, ... of the current level (T threads in all), then
+// all CTAs meet at a grid barrier before the next level, so the rows of a
+// level read only values written before the barrier (read from L2, since
+// other SMs wrote them).  The arithmetic of every row is the per-level
+// kernels' (and so the reference's) in the same order: the same bits.
+// The barrier needs every CTA resident: the kernel is launched
+// cooperatively with no more CTAs than fit at once.  It is a counter and a
+// generation word in the solve state; its waits are bounded by the solve's
+// deadline, and a timeout is recorded in the solve status (the other CTAs
+// then time out at the next barrier too).
 // ---------------------------------------------------------------------------
 enum IccSweepKind { kSweepForm = 0, kSweepFwd = 1, kSweepBwd = 2 };
 
 struct IccSweepArgs {
   IccArgs a;             // arrays; a.rows = rows in this sweep's level order
-  const int2* units;     // (first index into rows, count <= 32), level order
-  int nunits;
-  unsigned* flag;        // per row: epoch of the last sweep that computed it
-  SolveState* st;        // solve state (epoch, status); never null here
+  const int* lev_ptr;    // level l is a.rows[lev_ptr[l] .. lev_ptr[l+1])
+  int nlev;
+  SolveState* st;        // solve state (barrier, status); never null here
   const SolveParams* prm;
 };
 
-__device__ __forceinline__ bool icc_wait(const unsigned* f, unsigned epoch,
-                                         unsigned long long deadline) {
-  while ((int)(epoch - ld_acquire_gpu(f)) > 0)
-    if (globaltimer_ns() > deadline) return false;
-  return true;
+// Grid barrier: every CTA's thread 0 arrives on bar_count; the last one
+// resets it and advances bar_gen, which the others wait for.  Writes before the barrier are visible after it (fences at
+// GPU scope around the arrival).  Returns false, CTA-uniformly, on timeout.
+__device__ __forceinline__ bool icc_grid_barrier(SolveState* st, unsigned long long deadline) {
+  __syncthreads();
+  int ok = 1;
+  if (threadIdx.x == 0) {
+    const unsigned g = ld_acquire_gpu(&st->bar_gen);
+    __threadfence();
+    if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
+      st->bar_count = 0u;
+      __threadfence();
+      st_release_gpu(&st->bar_gen, g + 1u);
+    } else {
+      // One poller per CTA, polling at full rate: a sleep's wake-up
+      // granularity would add to every level of the sweep.
+      while (ld_acquire_gpu(&st->bar_gen) == g) {
+        if (globaltimer_ns() > deadline) {
+          ok = 0;
+          break;
+        }
+      }
+    }
+  }
+  return __syncthreads_and(ok) != 0;
+}
+
+template <int KIND>
+__device__ __forceinline__ void icc_sweep_row(const IccArgs& a, int i) {
+  const int js = a.row[i], je = a.row[i + 1];
+  if (KIND == kSweepForm) {             // Prec_Form.f90:69-78
+    double sum = a.val[js];
+    for (int j = js + 1; j < je; ++j) {
+      const int k = a.col[j];
+      if (k > i) break;
+      const double v = a.val[j];
+      sum = __dsub_rn(sum, __dmul_rn(__dmul_rn(__ldcg(a.d + k), v), v));
+    }
+    a.d_inv[i] = sum;
+    a.d[i] = __ddiv_rn(1.0, sum);
+  } else if (KIND == kSweepFwd) {       // Prec_Solve.f90:67-81
+    double sum = a.r[i];
+    for (int j = js + 1; j < je; ++j) {
+      const int k = a.col[j];
+      if (k > i) break;
+      sum = __dsub_rn(sum, __dmul_rn(a.val[j], __ldcg(a.y + k)));
+    }
+    const double yi = __dmul_rn(sum, a.d[i]);
+    a.y[i] = yi;
+    a.z[i] = __dmul_rn(yi, a.d_inv[i]);
+  } else {                              // Prec_Solve.f90:84-92
+    double sum = __ldcg(a.z + i);
+    for (int j = je - 1; j >= js + 1; --j) {
+      const int k = a.col[j];
+      if (k < i) break;
+      if (k < a.ni) sum = __dsub_rn(sum, __dmul_rn(a.val[j], __ldcg(a.z + k)));
+    }
+    a.z[i] = __dmul_rn(sum, a.d[i]);
+  }
 }
 
 template <int KIND>
 __global__ void __launch_bounds__(256) k_icc_sweep(IccSweepArgs s) {
   SolveState* st = s.st;
-  if (KIND != kSweepForm && st->done) return;
-  const IccArgs& a = s.a;
-  const unsigned epoch = st->icc_epoch + 1u;
+  if (KIND != kSweepForm && st->done) return;   // the same for every CTA
   const unsigned long long deadline = deadline_after(wait_limit(s.prm));
-  const int lane = threadIdx.x & 31;
-  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
-  bool ok = true;
-  for (int u = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); u < s.nunits; u += nw) {
-    const int2 un = s.units[u];
-    if (lane < un.y && ok) {
-      const int i = a.rows[un.x + lane];
-      const int js = a.row[i], je = a.row[i + 1];
-      if (KIND == kSweepForm) {           // Prec_Form.f90:69-78
-        double sum = a.val[js];
-        for (int j = js + 1; j < je; ++j) {
-          const int k = a.col[j];
-          if (k > i) break;
-          if (!icc_wait(s.flag + k, epoch, deadline)) { ok = false; break; }
-          const double v = a.val[j];
-          sum = __dsub_rn(sum, __dmul_rn(__dmul_rn(__ldcg(a.d + k), v), v));
-        }
-        a.d_inv[i] = sum;
-        a.d[i] = __ddiv_rn(1.0, sum);
-      } else if (KIND == kSweepFwd) {     // Prec_Solve.f90:67-81
-        double sum = a.r[i];
-        for (int j = js + 1; j < je; ++j) {
-          const int k = a.col[j];
-          if (k > i) break;
-          if (!icc_wait(s.flag + k, epoch, deadline)) { ok = false; break; }
-          sum = __dsub_rn(sum, __dmul_rn(a.val[j], __ldcg(a.y + k)));
-        }
-        const double yi = __dmul_rn(sum, a.d[i]);
-        a.y[i] = yi;
-        a.z[i] = __dmul_rn(yi, a.d_inv[i]);
-      } else {                            // Prec_Solve.f90:84-92
-        double sum = __ldcg(a.z + i);
-        for (int j = je - 1; j >= js + 1; --j) {
-          const int k = a.col[j];
-          if (k < i) break;
-          if (k < a.ni) {
-            if (!icc_wait(s.flag + k, epoch, deadline)) { ok = false; break; }
-            sum = __dsub_rn(sum, __dmul_rn(a.val[j], __ldcg(a.z + k)));
-          }
-        }
-        a.z[i] = __dmul_rn(sum, a.d[i]);
+  const int T = (int)(gridDim.x * blockDim.x);
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  // The next level's first row of this thread is looked up before the
+  // barrier, so after it only the neighbours' values are waited for.
+  int b = __ldg(s.lev_ptr), e = __ldg(s.lev_ptr + 1);
+  int i0 = (b + t < e) ? __ldg(s.a.rows + b + t) : -1;
+  for (int l = 0; l < s.nlev; ++l) {
+    if (i0 >= 0) icc_sweep_row<KIND>(s.a, i0);
+    for (int q = b + t + T; q < e; q += T) icc_sweep_row<KIND>(s.a, __ldg(s.a.rows + q));
+    if (l + 1 < s.nlev) {
+      b = __ldg(s.lev_ptr + l + 1);
+      e = __ldg(s.lev_ptr + l + 2);
+      i0 = (b + t < e) ? __ldg(s.a.rows + b + t) : -1;
+      if (!icc_grid_barrier(st, deadline)) {
+        if (threadIdx.x == 0) atomicExch(&st->status, (int)TF_ERR_TIMEOUT);
+        return;
       }
-      st_release_gpu(s.flag + i, epoch);
-    }
-  }
-  if (!ok) atomicExch(&st->status, (int)TF_ERR_TIMEOUT);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(&st->counter[kCntSweep], 1u) == gridDim.x - 1) {
-      st->counter[kCntSweep] = 0u;
-      st->icc_epoch = epoch;
-      __threadfence();
     }
   }
 }

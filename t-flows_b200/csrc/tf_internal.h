@@ -134,12 +134,9 @@ struct tf_matrix_s {
   std::vector<int> h_levf_ptr, h_levb_ptr;
   double* d_icc_d = nullptr;     // Prec_Form's d
   double* d_icc_dinv = nullptr;  // Prec_Form's d_inv
-  // Persistent sweeps (k_icc_sweep): units of <= 32 rows of one level, in
-  // level order, per sweep direction; a per-row epoch flag.
-  int2* d_icc_units_f = nullptr;
-  int2* d_icc_units_b = nullptr;
-  int icc_nunits_f = 0, icc_nunits_b = 0;
-  unsigned* d_icc_flag = nullptr;
+  // Persistent sweeps (k_icc_sweep): the level pointers on the device.
+  int* d_icc_levf_ptr = nullptr;
+  int* d_icc_levb_ptr = nullptr;
   int icc_sweep_grid = 0;        // 0: per-level kernels
   // cached graphs, one per (preconditioner, x update deferred or not)
   cudaGraphExec_t graph[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};

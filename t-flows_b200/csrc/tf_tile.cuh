@@ -211,6 +211,25 @@ struct PatTable {
   int npat;
 };
 
+// One row of a row-pattern tile for operators with per-row hooks
+// (kRowOps: gather / row_init / combine / row_done): all of the row's
+// (at most kPatMaxLen) gathers are issued before the first product is
+// added, so a thread keeps its row's loads in flight together; the sum is
+// the one-entry-at-a-time sum in storage order, bit for bit.
+template <class Op>
+__device__ __forceinline__ void pat_row(Op& op, int i, const double* v, const int* off,
+                                        int len) {
+  double acc = op.row_init(i);
+  double pr[kPatMaxLen];
+#pragma unroll
+  for (int u = 0; u < kPatMaxLen; ++u)
+    pr[u] = (u < len) ? __dmul_rn(v[u], op.gather(i + off[u])) : 0.0;
+#pragma unroll
+  for (int u = 0; u < kPatMaxLen; ++u)
+    if (u < len) acc = op.combine(acc, pr[u]);
+  op.row_done(i, acc);
+}
+
 // Threads of a row-pattern CTA: ROWS consumer threads (one row each) and
 // one producer warp.
 template <int ROWS>
@@ -320,7 +339,10 @@ __device__ bool stream_tiles_pat(const int* __restrict__ row, const PatTable& pt
       if (r < r1) {
         const int js = srow(s)[r - p0];
         const int pid = spat(s)[r - b0];
-        op.pat(r, sval(s) + (js - a0), tab + pid * kPatMaxLen, tab_len[pid]);
+        if constexpr (Op::kRowOps)
+          pat_row(op, r, sval(s) + (js - a0), tab + pid * kPatMaxLen, tab_len[pid]);
+        else
+          op.pat(r, sval(s) + (js - a0), tab + pid * kPatMaxLen, tab_len[pid]);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);

@@ -165,7 +165,9 @@ __device__ __forceinline__ void wg_rows(Op& op, const double* prod, const int* c
 // (the same for every warp of the CTA), for sources whose tiles mix short
 // and long rows (the batch engine's systems).
 __device__ __forceinline__ int tile_group_width(int rows, int entries) {
-  return entries > 12 * rows ? 4 : entries > 6 * rows ? 2 : 1;
+  // One lane per row measured fastest up to polyhedral rows (16.5 entries
+  // on average, up to 49); groups pay off only for long rows.
+  return entries > 48 * rows ? 4 : entries > 24 * rows ? 2 : 1;
 }
 
 template <int ROWCAP, int NNZCAP, int STAGES, int G = 0, class S, class Op>
