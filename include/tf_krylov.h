@@ -376,6 +376,40 @@ int tf_residual(tf_ctx ctx, tf_matrix m, const double* d_val,
 int tf_nrms(tf_ctx ctx, tf_matrix m, const double* d_val, const double* d_r,
             const double* d_x, const double* norm, double* d_out);
 int tf_ctx_sync(tf_ctx ctx);
+
+/* Vector kernels for callers that run their own Krylov loop around tf_spmv,
+ * e.g. one system split by rows over several GPUs (the reference's MPI
+ * sub-domains: Cg.f90 with Exchange_Cells_Real before each SpMV and the
+ * Global % Sum_Real of every dot product), where the caller exchanges the
+ * buffer cells and sums the partial results over processes between these
+ * calls.  Device pointers, n entries, asynchronous on ctx's stream; every
+ * expression is rounded as the reference's loop rounds it, and every sum is
+ * deterministic (fixed grid, partials combined in block order), written to
+ * device memory (d_out).
+ *   tf_vec_axpby:  y = a x + b y (first != 0: y = a x; a == 0: y = b y) --
+ *                  p = z + beta p, x + alfa p, r - alfa q (Cg.f90:166-209);
+ *   tf_vec_gather / tf_vec_scatter: out[k] = src[idx[k]] / dst[idx[k]] =
+ *                  vals[k] (packing and unpacking buffer cells);
+ *   tf_vec_recip:  out = 1 / x (Prec_Form.f90:51);
+ *   tf_vec_dot:    d_out[0] = sum a_i b_i (b NULL: sum a_i);
+ *   tf_vec_nrms_sum: d_out[0] = sum r_i^2 / d_i^2
+ *                  (Normalized_Root_Mean_Square.f90:33-36, before the sum
+ *                  over processes, the root and the scaling);
+ *   tf_vec_jacobi: z = r d_inv and d_out[0] = sum z_i r_i (Prec_Solve.f90:
+ *                  44-49, Cg.f90:151-155);
+ *   tf_vec_minmax: d_out[0], d_out[1] = min and max of x
+ *                  (Normalized_Root_Mean_Square.f90:42-48). */
+int tf_vec_axpby(tf_ctx ctx, int n, double a, const double* d_x, double b, double* d_y,
+                 int first);
+int tf_vec_gather(tf_ctx ctx, int n, const double* d_src, const int64_t* d_idx, double* d_out);
+int tf_vec_scatter(tf_ctx ctx, int n, double* d_dst, const int64_t* d_idx,
+                   const double* d_vals);
+int tf_vec_recip(tf_ctx ctx, int n, const double* d_x, double* d_out);
+int tf_vec_dot(tf_ctx ctx, int n, const double* d_a, const double* d_b, double* d_out);
+int tf_vec_nrms_sum(tf_ctx ctx, int n, const double* d_r, const double* d_diag, double* d_out);
+int tf_vec_jacobi(tf_ctx ctx, int n, const double* d_r, const double* d_dinv, double* d_z,
+                  double* d_out);
+int tf_vec_minmax(tf_ctx ctx, int n, const double* d_x, double* d_out2);
 /* The CUDA stream of ctx (a cudaStream_t), for callers that order their
  * own work with it. */
 void* tf_ctx_stream(tf_ctx ctx);

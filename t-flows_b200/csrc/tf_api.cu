@@ -94,6 +94,11 @@ extern "C" int tf_ctx_destroy(tf_ctx ctx) {
   if (!ctx) return TF_ERR_ARG;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->d_vec_scratch) {
+    if (ctx->async_alloc) cudaFreeAsync(ctx->d_vec_scratch, ctx->stream);
+    else cudaFree(ctx->d_vec_scratch);
+    cudaStreamSynchronize(ctx->stream);
+  }
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return TF_OK;

@@ -982,7 +982,7 @@ int prepare_cfg(tf_matrix_s* m) {
 
 int tf_icc_prepare_sweeps(tf_matrix_s* m) {
   m->icc_sweep_grid = 0;
-  if (getenv("TF_ICC_LEVELS")) return TF_OK;
+  if (!getenv("TF_ICC_PERSISTENT")) return TF_OK;
   int coop = 0;
   TF_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, m->ctx->device));
   if (!coop) return TF_OK;

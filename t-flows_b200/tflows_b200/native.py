@@ -34,6 +34,8 @@ EXPORTS = [
     "tf_ctx_sync", "tf_ctx_stream", "tf_last_error_message", "tf_matrix_tile_config",
     "tf_matrix_row_patterns", "tf_matrix_renumbered", "tf_matrix_tuning",
     "tf_tuning_cache_clear", "tf_pool_cancel", "tf_server_cancel", "tf_matrix_icc_levels",
+    "tf_vec_axpby", "tf_vec_gather", "tf_vec_scatter", "tf_vec_recip", "tf_vec_dot",
+    "tf_vec_nrms_sum", "tf_vec_jacobi", "tf_vec_minmax",
     "tf_faces_register", "tf_assemble_pressure", "tf_assemble_momentum",
     "tf_solve_multi", "tf_solve_multi_device", "tf_batch_add_many",
 ]
@@ -88,6 +90,15 @@ def load(path=LIB_PATH):
     L.tf_matrix_tile_config.argtypes = [_vp]
     L.tf_matrix_tuning.argtypes = [_vp, _c_int_p, _c_dbl_p, ctypes.c_int, _c_int_p]
     L.tf_matrix_icc_levels.argtypes = [_vp, _c_int_p, _c_int_p]
+    ci, cd = ctypes.c_int, ctypes.c_double
+    L.tf_vec_axpby.argtypes = [_vp, ci, cd, _vp, cd, _vp, ci]
+    L.tf_vec_gather.argtypes = [_vp, ci, _vp, _vp, _vp]
+    L.tf_vec_scatter.argtypes = [_vp, ci, _vp, _vp, _vp]
+    L.tf_vec_recip.argtypes = [_vp, ci, _vp, _vp]
+    for f in (L.tf_vec_dot, L.tf_vec_nrms_sum):
+        f.argtypes = [_vp, ci, _vp, _vp, _vp]
+    L.tf_vec_jacobi.argtypes = [_vp, ci, _vp, _vp, _vp, _vp]
+    L.tf_vec_minmax.argtypes = [_vp, ci, _vp, _vp]
     L.tf_matrix_row_patterns.argtypes = [_vp]
     L.tf_matrix_renumbered.argtypes = [_vp]
     solve_args = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int,
@@ -168,6 +179,50 @@ class Context:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def _dptr(t):
+    """Device pointer of a torch tensor (or None / int)."""
+    if t is None or isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+def vec_axpby(ctx, n, a, x, b, y, first=False):
+    _check(load().tf_vec_axpby(ctx.h, int(n), float(a), _dptr(x), float(b), _dptr(y),
+                               1 if first else 0), "tf_vec_axpby")
+
+
+def vec_gather(ctx, n, src, idx, out):
+    _check(load().tf_vec_gather(ctx.h, int(n), _dptr(src), _dptr(idx), _dptr(out)),
+           "tf_vec_gather")
+
+
+def vec_scatter(ctx, n, dst, idx, vals):
+    _check(load().tf_vec_scatter(ctx.h, int(n), _dptr(dst), _dptr(idx), _dptr(vals)),
+           "tf_vec_scatter")
+
+
+def vec_recip(ctx, n, x, out):
+    _check(load().tf_vec_recip(ctx.h, int(n), _dptr(x), _dptr(out)), "tf_vec_recip")
+
+
+def vec_dot(ctx, n, a, b, out):
+    _check(load().tf_vec_dot(ctx.h, int(n), _dptr(a), _dptr(b), _dptr(out)), "tf_vec_dot")
+
+
+def vec_nrms_sum(ctx, n, r, diag, out):
+    _check(load().tf_vec_nrms_sum(ctx.h, int(n), _dptr(r), _dptr(diag), _dptr(out)),
+           "tf_vec_nrms_sum")
+
+
+def vec_jacobi(ctx, n, r, dinv, z, out):
+    _check(load().tf_vec_jacobi(ctx.h, int(n), _dptr(r), _dptr(dinv), _dptr(z), _dptr(out)),
+           "tf_vec_jacobi")
+
+
+def vec_minmax(ctx, n, x, out):
+    _check(load().tf_vec_minmax(ctx.h, int(n), _dptr(x), _dptr(out)), "tf_vec_minmax")
 
 
 def tuning_cache_clear():

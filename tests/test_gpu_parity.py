@@ -584,8 +584,8 @@ def test_icc_parity_medium_and_poly(gpu_ctx):
 
 @pytest.mark.parametrize("kind", ["hex", "poly"])
 def test_icc_persistent_sweeps_equal_level_kernels(gpu_ctx, kind, monkeypatch):
-    """The persistent ICC sweeps (one cooperative kernel per sweep, rows
-    waiting on their neighbours' flags) give the per-level kernels' bits."""
+    """The persistent ICC sweeps (one cooperative kernel per sweep, a grid
+    barrier between levels; opt-in) give the per-level kernels' bits."""
     if kind == "hex":
         s = systems.small_hex(30, seed=4, kind="pressure", ratio=1.03)
     else:
@@ -593,7 +593,7 @@ def test_icc_persistent_sweeps_equal_level_kernels(gpu_ctx, kind, monkeypatch):
                                 norm=1.0)
     args = (s.csr.row, s.csr.col, s.csr.dia, s.val, s.b, s.x0, "cg", "icc", 3000, 1e-10, 1.0)
     g1 = gpu_solve(gpu_ctx, *args)
-    monkeypatch.setenv("TF_ICC_LEVELS", "1")
+    monkeypatch.setenv("TF_ICC_PERSISTENT", "1")
     g2 = gpu_solve(gpu_ctx, *args)
     assert g1[3] == g2[3] and g1[4] == g2[4]
     for u, w in zip(g1[:3], g2[:3]):
