@@ -179,9 +179,26 @@ def _batch_solve(ctx, sysl, **opts):
             res.append(dict(iters=r["iters"], status=r["status"], rel=rr, done_ms=r["done_ms"],
                             n_updates=r["n_updates"]))
         info = b.info()
+        info["trace"] = b.trace()
     finally:
         b.close()
     return t_add, t_run, res, info
+
+
+def _trace_deciles(trace):
+    """The sweep timeline in ten slices of equal wall time: running systems
+    and work items at the slice's first sweep, and its share of the run."""
+    if not trace:
+        return []
+    total = sum(t for _, _, t in trace)
+    out, acc, nxt = [], 0.0, 0.0
+    for a, w, t in trace:
+        if acc >= nxt:
+            out.append({"at_ms": round(acc, 1), "running": a, "work_items": w,
+                        "sweep_ms": round(t, 3)})
+            nxt += total / 10
+        acc += t
+    return out
 
 
 def run_batched(args):
@@ -218,7 +235,8 @@ def run_batched(args):
                       "done_ms_p50": float(np.percentile(done, 50)),
                       "done_ms_p99": float(np.percentile(done, 99)),
                       "sweeps": info["sweeps"],
-                      "iters_total": int(sum(r["iters"] for r in res))}
+                      "iters_total": int(sum(r["iters"] for r in res)),
+                      "trace_deciles": _trace_deciles(info["trace"])}
     if "drop_in" in parts:
         _drop_in_solve_times(ctx, smallest[:2], 1e-10)   # warm-up
         t = _drop_in_solve_times(ctx, sysl, 1e-10)

@@ -267,6 +267,10 @@ int tf_batch_result(tf_batch b, int sys, double* x, int* iters,
                     double* true_rel_res, int* status, int* n_updates,
                     double* done_ms);
 int tf_batch_remove(tf_batch b, int sys);
+/* Timeline of the last tf_batch_run, one record per sweep: systems running
+ * when it was launched, work items (row tiles) in its list, and its wall
+ * time in milliseconds (launch to the state read back); *count = sweeps. */
+int tf_batch_trace(tf_batch b, int* active, int* items, double* ms, int cap, int* count);
 int tf_batch_info(tf_batch b, int* sweeps, int* work_items, size_t* free_bytes);
 
 /* Continuous batching: a worker thread admits queued requests whenever the

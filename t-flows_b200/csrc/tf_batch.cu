@@ -942,6 +942,13 @@ struct tf_batch_s {
   int grid_plain = 1, grid_tile = 1;
   int sweeps = 0;
   long long total_iters = 0;
+  // Per sweep of the last tf_batch_run: systems running at its launch, work
+  // items (tiles) of the list, wall time of the sweep (launch to state read).
+  struct SweepRec {
+    int active, items;
+    double ms;
+  };
+  std::vector<SweepRec> trace;
 
   ~tf_batch_s() {
     cudaSetDevice(ctx->device);
@@ -1214,12 +1221,15 @@ struct tf_batch_s {
     int st = rebuild_work();
     if (st != TF_OK) return st;
     int running = n_running();
+    trace.clear();
     while (running > 0) {
+      const auto ts = std::chrono::steady_clock::now();
       st = run_sweep();
       if (st != TF_OK) return st;
-      const double ms =
-          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
-              .count();
+      const auto te = std::chrono::steady_clock::now();
+      trace.push_back(SweepRec{running, nwork,
+                               std::chrono::duration<double, std::milli>(te - ts).count()});
+      const double ms = std::chrono::duration<double, std::milli>(te - t0).count();
       for (int i = 0; i < max_sys; ++i)
         if (slots[i].used && slots[i].done_ms < 0.0 && h_state[i].status != kInit &&
             h_state[i].status != kActive)
@@ -1408,6 +1418,21 @@ extern "C" int tf_batch_result(tf_batch bt, int sys, double* x, int* iters,
   if (status) *status = s.status;
   if (n_updates) *n_updates = s.n_ru;
   if (x) return bt->fetch_x(sys, x);
+  return TF_OK;
+  TF_API_END
+}
+
+extern "C" int tf_batch_trace(tf_batch bt, int* active, int* items, double* ms, int cap,
+                              int* count) {
+  TF_API_BEGIN
+  if (!bt || !count || (cap > 0 && (!active || !items || !ms))) return TF_ERR_ARG;
+  const int n = std::min<int>(cap, (int)bt->trace.size());
+  for (int i = 0; i < n; ++i) {
+    active[i] = bt->trace[i].active;
+    items[i] = bt->trace[i].items;
+    ms[i] = bt->trace[i].ms;
+  }
+  *count = (int)bt->trace.size();
   return TF_OK;
   TF_API_END
 }

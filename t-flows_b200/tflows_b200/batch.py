@@ -30,6 +30,7 @@ def _lib():
     L.tf_batch_run.argtypes = [_vp]
     L.tf_batch_result.argtypes = [_vp, ctypes.c_int, _vp, ip, dp, ip, ip, dp]
     L.tf_batch_remove.argtypes = [_vp, ctypes.c_int]
+    L.tf_batch_trace.argtypes = [_vp, ip, ip, dp, ctypes.c_int, ip]
     L.tf_batch_info.argtypes = [_vp, ip, ip, ctypes.POINTER(ctypes.c_size_t)]
     L.tf_server_create.argtypes = [_vp, ctypes.POINTER(BatchOpts), ctypes.POINTER(_vp)]
     L.tf_server_submit.argtypes = [_vp, ctypes.c_int, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp,
@@ -118,6 +119,18 @@ class Batch:
                       "tf_batch_result")
         return dict(x=x, iters=it.value, res=res.value, status=STATUS[st.value],
                     n_updates=nru.value, done_ms=dms.value)
+
+    def trace(self):
+        """[(systems running, work items, ms)] per sweep of the last run."""
+        cnt = ctypes.c_int(0)
+        native._check(self.L.tf_batch_trace(self.h, None, None, None, 0, ctypes.byref(cnt)),
+                      "tf_batch_trace")
+        n = cnt.value
+        a, w = (ctypes.c_int * max(n, 1))(), (ctypes.c_int * max(n, 1))()
+        t = (ctypes.c_double * max(n, 1))()
+        native._check(self.L.tf_batch_trace(self.h, a, w, t, n, ctypes.byref(cnt)),
+                      "tf_batch_trace")
+        return [(a[i], w[i], t[i]) for i in range(n)]
 
     def remove(self, sid):
         native._check(self.L.tf_batch_remove(self.h, sid), "tf_batch_remove")

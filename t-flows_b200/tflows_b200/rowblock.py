@@ -265,10 +265,13 @@ class DeviceKernels:
         self.idx = {}
 
     def _idx(self, idx):
-        key = (id(idx), len(idx))
+        """Device copy of an index list, kept per content (the exchange
+        passes the same few lists every iteration)."""
+        a = np.ascontiguousarray(idx, dtype=np.int64)
+        key = a.tobytes()
         t = self.idx.get(key)
         if t is None:
-            t = self.torch.from_numpy(np.asarray(idx, dtype=np.int64)).cuda()
+            t = self.torch.from_numpy(a).cuda()
             self.idx[key] = t
         return t
 
