@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--count", type=int, default=512)
+    ap.add_argument("--batched-count", type=int, default=512,
+                    help="default mode: systems of the batched leg (0: skip it)")
     ap.add_argument("--parts", default="all",
                     help="batched: comma list of mixed, fp64_batched, mixed_row_groups, drop_in, "
                          "streams, pool (default all)")
@@ -180,6 +182,8 @@ def _batch_solve(ctx, sysl, **opts):
                             n_updates=r["n_updates"]))
         info = b.info()
         info["trace"] = b.trace()
+        if os.environ.get("TF_BATCH_PROFILE"):
+            info["kernel_ms"] = b.kernel_ms()
     finally:
         b.close()
     return t_add, t_run, res, info
@@ -204,11 +208,20 @@ def _trace_deciles(trace):
 def run_batched(args):
     """Many independent systems: mixed-precision batch vs the FP64 drop-in
     solving the same systems one at a time."""
-    from tflows_b200 import native, workloads
-    t0 = time.perf_counter()
-    sysl = workloads.batched(count=args.count, seed=4)
-    t_gen = time.perf_counter() - t0
+    from tflows_b200 import native
     ctx = native.Context(0)
+    out = batched_comparison(ctx, args.count, args.parts)
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
+def batched_comparison(ctx, count, parts_arg):
+    """The batched workload (`count` systems): the engines named in
+    parts_arg, each on the same systems, as one dict."""
+    from tflows_b200 import workloads
+    t0 = time.perf_counter()
+    sysl = workloads.batched(count=count, seed=4)
+    t_gen = time.perf_counter() - t0
     cells = sum(s.n for s in sysl)
     out = {"mode": "batched", "systems": len(sysl), "cells": cells,
            "nnz": sum(s.nnz for s in sysl), "gen_s": t_gen,
@@ -217,8 +230,8 @@ def run_batched(args):
                        "Jacobi; target ||b-Ax||/||b|| <= 1e-10"}
     smallest = sorted(sysl, key=lambda s: s.n)[:4]
     parts = set(("mixed,fp64_batched,mixed_row_groups,drop_in,streams,pool"
-                 if args.parts == "all"
-                 else args.parts).split(","))
+                 if parts_arg == "all"
+                 else parts_arg).split(","))
     for label, opts in (("mixed", dict(vec_fp32=True)), ("fp64_batched", dict(vec_fp32=False)),
                         ("mixed_row_groups", dict(vec_fp32=True, row_groups=1))):
         if label not in parts:
@@ -236,7 +249,8 @@ def run_batched(args):
                       "done_ms_p99": float(np.percentile(done, 99)),
                       "sweeps": info["sweeps"],
                       "iters_total": int(sum(r["iters"] for r in res)),
-                      "trace_deciles": _trace_deciles(info["trace"])}
+                      "trace_deciles": _trace_deciles(info["trace"]),
+                      "kernel_ms": info.get("kernel_ms")}
     if "drop_in" in parts:
         _drop_in_solve_times(ctx, smallest[:2], 1e-10)   # warm-up
         t = _drop_in_solve_times(ctx, sysl, 1e-10)
@@ -283,8 +297,8 @@ def run_batched(args):
     ratio("mixed", "fp64_batched")
     ratio("mixed_row_groups", "fp64_drop_in")
     ratio("mixed_row_groups", "mixed")
-    print(json.dumps(out), flush=True)
-    ctx.close()
+    ratio("mixed", "fp64_drop_in_8streams")
+    return out
 
 
 def _serve_stream(req_sys, rhs, rate, seconds, workers, budget, seed, max_outstanding=256):
@@ -1080,6 +1094,24 @@ def main():
             from oracle import oracle as O
             cpu = cpu_baseline(sysl, args.cpu_seconds, O.max_threads())
             cpu1 = cpu_baseline(sysl, args.cpu_seconds / 2, 1)
+        batched = None
+        if world == 1 and args.batched_count > 0:
+            # The batched workload (512 systems): the mixed-precision batch
+            # engine against the FP64 drop-in one request at a time and on 8
+            # concurrent streams, same systems, same run.
+            b = batched_comparison(ctx, args.batched_count, "mixed,drop_in,streams")
+            keep = ("run_s", "upload_s", "solves_per_s", "solves_per_s_incl_upload",
+                    "mcell_iters_per_s", "converged_to_1e-10", "max_true_rel",
+                    "done_ms_p50", "done_ms_p99", "solve_ms_p50", "solve_ms_p99",
+                    "iters_total")
+            batched = {"workload": b["workload"], "systems": b["systems"], "cells": b["cells"],
+                       "nnz": b["nnz"]}
+            for k in ("mixed", "fp64_drop_in", "fp64_drop_in_8streams"):
+                if k in b:
+                    batched[k] = {kk: v for kk, v in b[k].items() if kk in keep}
+            for k, v in b.items():
+                if k.startswith("speedup_"):
+                    batched[k] = v
         ms = np.array(step_ms)
         solve_count = args.steps * len(sysl) * world
         line = {
@@ -1110,6 +1142,7 @@ def main():
                              "frac": bytes_iter / t_iter / 1e9 / peak}},
             "cpu_baseline": cpu,
             "cpu_baseline_1core": cpu1,
+            "batched": batched,
             "clocks": clk,
             "gpu_launches": launches,
         }

@@ -271,6 +271,12 @@ int tf_batch_remove(tf_batch b, int sys);
  * when it was launched, work items (row tiles) in its list, and its wall
  * time in milliseconds (launch to the state read back); *count = sweeps. */
 int tf_batch_trace(tf_batch b, int* active, int* items, double* ms, int cap, int* count);
+/* With TF_BATCH_PROFILE set when the batch was created, sweeps run as direct
+ * launches with CUDA events around every kernel: ms5 receives the time spent
+ * in the five kernels of an iteration (p update, SpMV, update, refinement
+ * fold, refinement residual) over all runs so far.  TF_ERR_ARG when the
+ * batch was not created for profiling. */
+int tf_batch_kernel_ms(tf_batch b, double* ms5);
 int tf_batch_info(tf_batch b, int* sweeps, int* work_items, size_t* free_bytes);
 
 /* Continuous batching: a worker thread admits queued requests whenever the

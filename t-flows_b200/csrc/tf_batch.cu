@@ -966,16 +966,54 @@ struct tf_batch_s {
   static size_t smem_csr2() { return Csr2Layout<kRows, kNnzCap, kStages>::kSmemBytes; }
   static size_t smem_rows32() { return TileLayout<kRows, kNnzCap, float, kStages>::kSmemBytes; }
 
+  // ev (profiling only): events recorded before each of the five kernels
+  // and after the last.
   template <typename V>
-  void launch_iteration(cudaStream_t s, const BatchArgs& a) {
+  void launch_iteration(cudaStream_t s, const BatchArgs& a, cudaEvent_t* ev = nullptr) {
+    if (ev) cudaEventRecord(ev[0], s);
     kb_pupdate<V><<<grid_plain, 256, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[1], s);
     if (opts.val_fp32) kb_spmv<V, float, 0><<<grid_tile, kRows, smem_rows32(), s>>>(a);
     else if (opts.row_groups) kb_spmv<V, double, -1><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
     else kb_spmv<V, double, 0><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
+    if (ev) cudaEventRecord(ev[2], s);
     kb_update<V><<<grid_plain, 256, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[3], s);
     kb_ru_fold<V><<<grid_plain, 256, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[4], s);
     if (opts.row_groups) kb_ru_res<V, -1><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
     else kb_ru_res<V, 0><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
+    if (ev) cudaEventRecord(ev[5], s);
+  }
+
+  // Profiling (TF_BATCH_PROFILE set when the batch was created): sweeps run
+  // as direct launches with events around every kernel; kern_ms accumulates
+  // the time of pupdate, spmv, update, ru_fold, ru_res over the run.
+  bool profile = false;
+  double kern_ms[5] = {0, 0, 0, 0, 0};
+  int run_sweep_profiled() {
+    cudaStream_t s = ctx->stream;
+    BatchArgs a{d_desc, d_state, d_work, d_nwork, opts.ru_delta * opts.ru_delta,
+                RuList{d_ru, d_ru_count, d_ru_exit}};
+    std::vector<cudaEvent_t> ev(6 * opts.sweep_iters);
+    for (auto& e : ev) TF_CUDA_TRY(cudaEventCreate(&e));
+    for (int it = 0; it < opts.sweep_iters; ++it) {
+      if (vsz == 4) launch_iteration<float>(s, a, &ev[6 * it]);
+      else launch_iteration<double>(s, a, &ev[6 * it]);
+    }
+    TF_CUDA_TRY(cudaGetLastError());
+    TF_CUDA_TRY(cudaMemcpyAsync(h_state, d_state, (size_t)max_sys * sizeof(SysState),
+                                cudaMemcpyDeviceToHost, s));
+    TF_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int it = 0; it < opts.sweep_iters; ++it)
+      for (int k = 0; k < 5; ++k) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ev[6 * it + k], ev[6 * it + k + 1]);
+        kern_ms[k] += ms;
+      }
+    for (auto& e : ev) cudaEventDestroy(e);
+    ++sweeps;
+    return TF_OK;
   }
 
   template <typename V>
@@ -1034,6 +1072,7 @@ struct tf_batch_s {
     }
     vsz = opts.vec_fp32 ? 4 : 8;
     max_sys = opts.max_systems;
+    profile = getenv("TF_BATCH_PROFILE") != nullptr;
     TF_CUDA_TRY(cudaSetDevice(ctx->device));
     int st = arena.init(opts.mem_budget);
     if (st != TF_OK) return st;
@@ -1200,6 +1239,7 @@ struct tf_batch_s {
 
   // One sweep (sweep_iters iterations), then refresh the host state mirror.
   int run_sweep() {
+    if (profile) return run_sweep_profiled();
     cudaStream_t s = ctx->stream;
     TF_CUDA_TRY(cudaGraphLaunch(sweep, s));
     TF_CUDA_TRY(cudaMemcpyAsync(h_state, d_state, (size_t)max_sys * sizeof(SysState),
@@ -1419,6 +1459,14 @@ extern "C" int tf_batch_result(tf_batch bt, int sys, double* x, int* iters,
   if (n_updates) *n_updates = s.n_ru;
   if (x) return bt->fetch_x(sys, x);
   return TF_OK;
+  TF_API_END
+}
+
+extern "C" int tf_batch_kernel_ms(tf_batch bt, double* ms5) {
+  TF_API_BEGIN
+  if (!bt || !ms5) return TF_ERR_ARG;
+  for (int k = 0; k < 5; ++k) ms5[k] = bt->kern_ms[k];
+  return bt->profile ? TF_OK : TF_ERR_ARG;
   TF_API_END
 }
 

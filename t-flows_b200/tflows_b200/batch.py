@@ -31,6 +31,7 @@ def _lib():
     L.tf_batch_result.argtypes = [_vp, ctypes.c_int, _vp, ip, dp, ip, ip, dp]
     L.tf_batch_remove.argtypes = [_vp, ctypes.c_int]
     L.tf_batch_trace.argtypes = [_vp, ip, ip, dp, ctypes.c_int, ip]
+    L.tf_batch_kernel_ms.argtypes = [_vp, dp]
     L.tf_batch_info.argtypes = [_vp, ip, ip, ctypes.POINTER(ctypes.c_size_t)]
     L.tf_server_create.argtypes = [_vp, ctypes.POINTER(BatchOpts), ctypes.POINTER(_vp)]
     L.tf_server_submit.argtypes = [_vp, ctypes.c_int, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp,
@@ -131,6 +132,12 @@ class Batch:
         native._check(self.L.tf_batch_trace(self.h, a, w, t, n, ctypes.byref(cnt)),
                       "tf_batch_trace")
         return [(a[i], w[i], t[i]) for i in range(n)]
+
+    def kernel_ms(self):
+        """{kernel: ms} over the runs so far (batch created with TF_BATCH_PROFILE)."""
+        out = (ctypes.c_double * 5)()
+        native._check(self.L.tf_batch_kernel_ms(self.h, out), "tf_batch_kernel_ms")
+        return dict(zip(("pupdate", "spmv", "update", "ru_fold", "ru_res"), list(out)))
 
     def remove(self, sid):
         native._check(self.L.tf_batch_remove(self.h, sid), "tf_batch_remove")
