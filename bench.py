@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--batched-count", type=int, default=512,
                     help="default mode: systems of the batched leg (0: skip it)")
     ap.add_argument("--parts", default="all",
-                    help="batched: comma list of mixed, fp64_batched, mixed_row_groups, drop_in, "
+                    help="batched: comma list of mixed, fp64_batched, mixed_two_phase, drop_in, "
                          "streams, pool (default all)")
     ap.add_argument("--rate", type=float, default=200.0, help="served: arrivals per second")
     ap.add_argument("--seconds", type=float, default=60.0, help="served: window length")
@@ -189,19 +189,33 @@ def _batch_solve(ctx, sysl, **opts):
     return t_add, t_run, res, info
 
 
-def _trace_deciles(trace):
-    """The sweep timeline in ten slices of equal wall time: running systems
-    and work items at the slice's first sweep, and its share of the run."""
+def _trace_deciles(trace, vec_bytes, sweep_iters=8):
+    """The sweep timeline in ten slices of equal wall time, at each slice's
+    first sweep: running systems, work items, their rows and entries, the
+    sweep's wall ms, and the HBM rate the sweep would reach if every listed
+    system ran all its iterations (bytes of an inner iteration: 12 per entry,
+    4 per row pointer, 13 vectors of vec_bytes per row) -- an upper bound,
+    since systems that finish inside the sweep stop.  When the batch was
+    profiled, the SpMV kernel's rate over the same bytes model (entries, row
+    pointers, p and q) is added."""
     if not trace:
         return []
-    total = sum(t for _, _, t in trace)
+    total = sum(t["ms"] for t in trace)
     out, acc, nxt = [], 0.0, 0.0
-    for a, w, t in trace:
+    for t in trace:
         if acc >= nxt:
-            out.append({"at_ms": round(acc, 1), "running": a, "work_items": w,
-                        "sweep_ms": round(t, 3)})
+            it_bytes = 12 * t["nnz"] + 4 * (t["rows"] + 1) + 13 * vec_bytes * t["rows"]
+            d = {"at_ms": round(acc, 1), "running": t["active"], "work_items": t["items"],
+                 "rows": t["rows"], "nnz": t["nnz"], "sweep_ms": round(t["ms"], 3),
+                 "gbs_if_all_iterate": round(sweep_iters * it_bytes / t["ms"] / 1e6, 1)}
+            k = t["kernel_ms"]
+            if k["spmv"] > 0:
+                sp_bytes = 12 * t["nnz"] + 4 * (t["rows"] + 1) + 2 * vec_bytes * t["rows"]
+                d["kernel_ms"] = {n: round(v, 3) for n, v in k.items()}
+                d["spmv_gbs_if_all_iterate"] = round(sweep_iters * sp_bytes / k["spmv"] / 1e6, 1)
+            out.append(d)
             nxt += total / 10
-        acc += t
+        acc += t["ms"]
     return out
 
 
@@ -229,11 +243,11 @@ def batched_comparison(ctx, count, parts_arg):
                        "polyhedral upwind convection-diffusion (Bicg, Pe U[1,50], CFL 0.1); "
                        "Jacobi; target ||b-Ax||/||b|| <= 1e-10"}
     smallest = sorted(sysl, key=lambda s: s.n)[:4]
-    parts = set(("mixed,fp64_batched,mixed_row_groups,drop_in,streams,pool"
+    parts = set(("mixed,fp64_batched,mixed_two_phase,drop_in,streams,pool"
                  if parts_arg == "all"
                  else parts_arg).split(","))
     for label, opts in (("mixed", dict(vec_fp32=True)), ("fp64_batched", dict(vec_fp32=False)),
-                        ("mixed_row_groups", dict(vec_fp32=True, row_groups=1))):
+                        ("mixed_two_phase", dict(vec_fp32=True, two_phase_rows=1))):
         if label not in parts:
             continue
         _drop = _batch_solve(ctx, smallest, **opts)   # warm-up (module load, graphs)
@@ -249,7 +263,7 @@ def batched_comparison(ctx, count, parts_arg):
                       "done_ms_p99": float(np.percentile(done, 99)),
                       "sweeps": info["sweeps"],
                       "iters_total": int(sum(r["iters"] for r in res)),
-                      "trace_deciles": _trace_deciles(info["trace"]),
+                      "trace_deciles": _trace_deciles(info["trace"], 4 if opts["vec_fp32"] else 8),
                       "kernel_ms": info.get("kernel_ms")}
     if "drop_in" in parts:
         _drop_in_solve_times(ctx, smallest[:2], 1e-10)   # warm-up
@@ -295,8 +309,7 @@ def batched_comparison(ctx, count, parts_arg):
     ratio("fp64_drop_in_8streams", "fp64_drop_in")
     ratio("mixed", "fp64_drop_in")
     ratio("mixed", "fp64_batched")
-    ratio("mixed_row_groups", "fp64_drop_in")
-    ratio("mixed_row_groups", "mixed")
+    ratio("mixed", "mixed_two_phase")
     ratio("mixed", "fp64_drop_in_8streams")
     return out
 
@@ -383,7 +396,7 @@ def _serve_stream(req_sys, rhs, rate, seconds, workers, budget, seed, max_outsta
 
 
 def _serve_stream_mixed(req_sys, rhs, rate, seconds, budget, seed, max_outstanding=256,
-                        submit_threads=8, row_groups=0):
+                        submit_threads=8):
     """The same Poisson stream into the continuous-batching server
     (tf_server_*: the mixed-precision engine, requests admitted into free
     slots between sweeps, Krylov state resident).  Submission copies and
@@ -400,7 +413,7 @@ def _serve_stream_mixed(req_sys, rhs, rate, seconds, budget, seed, max_outstandi
     kinds = np.array([s.solver for s in req_sys])
     ctx = native.Context(0)
     srv = batch.Server(ctx, mem_budget=budget, max_systems=max_outstanding + 8,
-                       sweep_iters=8, row_groups=row_groups)
+                       sweep_iters=8)
     results, lock = [], threading.Lock()
     state = {"outstanding": 0}
 
@@ -751,7 +764,7 @@ def run_poly_system(args):
     out["fp64_drop_in"] = {"ms": best[0], "iters": best[1], "true_rel": best[2],
                            "mcell_iters_per_s": s.n * best[1] / best[0] / 1e3}
     for label, opts in (("batch_fp64", dict(vec_fp32=False)), ("batch_mixed", dict(vec_fp32=True)),
-                        ("batch_mixed_row_groups", dict(vec_fp32=True, row_groups=1))):
+                        ("batch_mixed_two_phase", dict(vec_fp32=True, two_phase_rows=1))):
         runs = [_batch_solve(ctx, [s], **opts) for _ in range(1 + args.steps)][1:]
         t_add, t_run, res, info = min(runs, key=lambda r: r[1])
         out[label] = {"ms": t_run * 1e3, "iters": res[0]["iters"], "true_rel": res[0]["rel"],

@@ -222,10 +222,11 @@ typedef struct tf_batch_opts {
   int max_systems;    /* system slots (default 1024)                          */
   double ru_delta;    /* refinement when |r| fell by this factor (0.1)        */
   size_t mem_budget;  /* device bytes for all systems' data (default 4 GiB)   */
-  int row_groups;     /* SpMV consumers: 0 = two phases (products staged in
-                         shared memory, then one thread per row), 1 = warp
-                         groups of 1/2/4 lanes per row by each tile's mean
-                         row length; the same row sums bit for bit          */
+  int two_phase_rows; /* SpMV consumers: 0 (default) = warp groups of 1/2/4
+                         lanes per row by each tile's mean row length, no
+                         barrier between warps; 1 = two phases (products
+                         staged in shared memory, a barrier, then one thread
+                         per row).  The same row sums bit for bit           */
 } tf_batch_opts;
 
 typedef struct tf_batch_s* tf_batch;
@@ -267,16 +268,25 @@ int tf_batch_result(tf_batch b, int sys, double* x, int* iters,
                     double* true_rel_res, int* status, int* n_updates,
                     double* done_ms);
 int tf_batch_remove(tf_batch b, int sys);
-/* Timeline of the last tf_batch_run, one record per sweep: systems running
- * when it was launched, work items (row tiles) in its list, and its wall
- * time in milliseconds (launch to the state read back); *count = sweeps. */
-int tf_batch_trace(tf_batch b, int* active, int* items, double* ms, int cap, int* count);
+/* Timeline of the last tf_batch_run, one record per sweep; *count = sweeps,
+ * at most cap records are written. */
+typedef struct tf_batch_sweep {
+  int active;            /* systems iterating when the sweep was launched */
+  int items;             /* work items (row tiles) in its list */
+  int64_t rows, nnz;     /* rows and entries of those systems */
+  double ms;             /* wall time, launch to the state read back */
+  double kernel_ms[8];   /* TF_BATCH_PROFILE only (else 0): the sweep's time in
+                            the eight kernels of tf_batch_kernel_ms */
+} tf_batch_sweep;
+int tf_batch_trace(tf_batch b, tf_batch_sweep* out, int cap, int* count);
 /* With TF_BATCH_PROFILE set when the batch was created, sweeps run as direct
- * launches with CUDA events around every kernel: ms5 receives the time spent
- * in the five kernels of an iteration (p update, SpMV, update, refinement
- * fold, refinement residual) over all runs so far.  TF_ERR_ARG when the
+ * launches with CUDA events around every kernel: ms8 receives the time spent
+ * in the eight kernels of an iteration over all runs so far, in launch
+ * order: p update, SpMV (tile totals of p.q), alpha per system, x/r update
+ * (tile totals of rho and |r|^2), beta per system, refinement fold,
+ * refinement residual, refinement test per system.  TF_ERR_ARG when the
  * batch was not created for profiling. */
-int tf_batch_kernel_ms(tf_batch b, double* ms5);
+int tf_batch_kernel_ms(tf_batch b, double* ms8);
 int tf_batch_info(tf_batch b, int* sweeps, int* work_items, size_t* free_bytes);
 
 /* Continuous batching: a worker thread admits queued requests whenever the

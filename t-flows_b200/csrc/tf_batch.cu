@@ -22,23 +22,27 @@
 // while FP32 values need 1.3-1.75x (the perturbed operator breaks the
 // recurrence), so FP64 values are the default.
 //
-// Per-system reductions are warp-level, with no CTA-wide barrier: in the
-// elementwise kernels one warp owns a tile; in the tile-streaming kernels
-// each warp reports a partial, the tile's last warp sums them in warp order.
-// The warp that reports a system's last tile sums the tile totals in tile
-// order and finalises the system's scalars.  A system's arithmetic never
-// depends on which other systems share the batch: results are
-// bit-identical alone and in any mix.  The refinement kernels walk a compact
-// list of the tiles of the systems due an update, appended by the warp that
-// decides it.
+// Per-system reductions in two steps, with no atomics and no fences on the
+// tile passes: every tile pass stores its tile's totals (in the elementwise
+// kernels one warp owns a tile; in the tile streamers the reducer warp sums
+// the consumer warps' partials in warp order), and a finishing kernel, one
+// warp per system, sums the system's tile totals in a fixed order and
+// updates the system's scalars; the kernel boundary orders the two.  A
+// system's arithmetic never depends on which other systems share the
+// batch: results are bit-identical alone and in any mix.  The refinement
+// kernels walk a compact list of the tiles of the systems due an update,
+// appended by the warp that decides it.
 //
 // Kernels of one iteration (all skip systems with nothing to do):
-//   kb_pupdate  z = dinv r, p = z + beta p
-//   kb_spmv     q = A p (tile streamer), p.q, alpha
-//   kb_update   xlo += alpha p, r -= alpha q, rho, |r|^2, beta, RU trigger
-//   kb_ru_fold  x += xlo, xlo = 0                        (systems due an RU)
-//   kb_ru_res   r = b - A x in FP64 (tile streamer), |r|^2, rho, test;
-//               on a new system also forms dinv and |b|^2
+//   kb_pupdate   z = dinv r, p = z + beta p
+//   kb_spmv      q = A p (tile streamer), p.q per tile
+//   kb_alpha     alpha per system
+//   kb_update    xlo += alpha p, r -= alpha q, rho and |r|^2 per tile
+//   kb_beta      rho, beta, RU trigger per system
+//   kb_ru_fold   x += xlo, xlo = 0                       (systems due an RU)
+//   kb_ru_res    r = b - A x in FP64 (tile streamer), |r|^2, rho per tile;
+//                on a new system also forms dinv and |b|^2
+//   kb_ru_finish the refinement's test per system
 // A sweep of S iterations is captured once as a CUDA graph; the host only
 // looks at the state array between sweeps (retire, admit, rebuild the list).
 #include <cuda_runtime.h>
@@ -76,6 +80,8 @@ constexpr int kNnzCap = 4096;    // entries per tile stage
 constexpr int kStages = 2;
 constexpr int kPartQ = 4;        // partial sums kept per tile / warp
 constexpr int kRuEvery = 50;     // FP32 iterates: refine at least this often
+// Kernels of an iteration, in launch order (profiling: tf_batch_kernel_ms).
+constexpr int kKernels = 8;
 
 template <typename V>
 struct SysDev {
@@ -93,10 +99,8 @@ struct SysDev {
   V* q;
   V* dinv;
   double* tile_tot;     // ntiles * kPartQ: per-tile totals
-  double* warp_part;    // ntiles * kWarps * kPartQ: per-warp partials (tile kernels)
-  unsigned* tile_cnt;   // ntiles: warps of a tile that have reported
-  double* chunk_tot;    // n_chunks * kPartQ: per-chunk totals
-  unsigned* chunk_cnt;  // n_chunks: tiles of a chunk that have reported
+  double* warp_part;    // FP32 values: ntiles * kWarps * kPartQ per-warp partials
+  unsigned* tile_cnt;   // FP32 values: ntiles, warps of a tile that have reported
   int n, ntiles;
   int maxit, use_val32;
   double tol;
@@ -107,7 +111,6 @@ struct SysState {
   double rr, rr_ru, bnorm2, res_true;
   int status, iter, first, need_ru;
   int n_ru, iter_ru;   // refinements so far; iteration of the last one
-  unsigned cnt_spmv, cnt_upd, cnt_res, cnt_pad;
 };
 
 struct Work {
@@ -124,7 +127,6 @@ struct Work {
 struct RuList {
   Work* items;
   int* count;
-  unsigned* exit_cnt;
 };
 
 struct BatchArgs {
@@ -134,82 +136,30 @@ struct BatchArgs {
   const int* nwork;
   double ru_delta2;
   RuList ru;
+  const int* sys;         // the systems of the work list (finishing kernels)
+  const int* nsys;
 };
 
 __device__ __forceinline__ bool active(const SysState& s) { return s.status == kActive; }
 
 // ---------------------------------------------------------------------------
-// Warp-level per-system reductions (no CTA barriers).
+// Per-system reductions: tile totals, then one warp per system.
 // ---------------------------------------------------------------------------
-// One whole warp reports the total of tile `tile` (v, lane-independent).
-// Returns true in the warp that completes the system, with v = the system
-// totals.  Two levels keep the atomics spread: the tiles of a chunk of
-// kChunkTiles report to the chunk's counter, whose last arriver sums the
-// chunk's tile totals in tile order and reports the chunk to the system
-// counter; the system's last chunk sums the chunk totals in chunk order.
-// The order depends only on the system's tiling, never on the mix.
-constexpr int kChunkTiles = 64;
-
-__device__ __forceinline__ int n_chunks(int ntiles) {
-  return (ntiles + kChunkTiles - 1) / kChunkTiles;
-}
-
 template <int NQ>
-__device__ bool warp_tile_done(unsigned* sys_cnt, double* tile_tot, double* chunk_tot,
-                               unsigned* chunk_cnt, int ntiles, int tile, double (&v)[NQ]) {
-  const int lane = threadIdx.x & 31;
-  const int chunk = tile / kChunkTiles, t0 = chunk * kChunkTiles;
-  const int clen = min(kChunkTiles, ntiles - t0);
-  unsigned last = 0;
-  if (lane == 0) {
+__device__ __forceinline__ void put_tile_total(double* tile_tot, int tile,
+                                               const double (&v)[NQ]) {
+  if ((threadIdx.x & 31) == 0) {
 #pragma unroll
     for (int q = 0; q < NQ; ++q) tile_tot[(size_t)tile * kPartQ + q] = v[q];
-    __threadfence();
-    last = (atomicAdd(chunk_cnt + chunk, 1u) == (unsigned)clen - 1);
   }
-  last = __shfl_sync(0xffffffffu, last, 0);
-  if (!last) return false;
-  __threadfence();
-  double acc[NQ];
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
-  for (int t = lane; t < clen; t += 32)
-#pragma unroll
-    for (int q = 0; q < NQ; ++q)
-      acc[q] = __dadd_rn(acc[q], __ldcg(tile_tot + (size_t)(t0 + t) * kPartQ + q));
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) acc[q] = warp_sum(acc[q]);
-  const int nch = n_chunks(ntiles);
-  last = 0;
-  if (lane == 0) {
-    chunk_cnt[chunk] = 0u;   // ready for the next kernel
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) chunk_tot[(size_t)chunk * kPartQ + q] = acc[q];
-    __threadfence();
-    last = (atomicAdd(sys_cnt, 1u) == (unsigned)nch - 1);
-  }
-  last = __shfl_sync(0xffffffffu, last, 0);
-  if (!last) return false;
-  __threadfence();
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
-  for (int c = lane; c < nch; c += 32)
-#pragma unroll
-    for (int q = 0; q < NQ; ++q)
-      acc[q] = __dadd_rn(acc[q], __ldcg(chunk_tot + (size_t)c * kPartQ + q));
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) v[q] = warp_sum(acc[q]);
-  if (lane == 0) *sys_cnt = 0u;
-  return true;
 }
 
-// Tile kernels (one CTA of kWarps warps per tile): every warp reports its
-// partial; the tile's last warp sums the kWarps partials in warp order and
-// reports the tile through warp_tile_done.  v: this thread's values.
+// FP32-value SpMV (one CTA of kWarps warps per tile): every warp reports
+// its partial; the tile's last warp sums the kWarps partials in warp order
+// and returns true with v = the tile's totals.  v: this thread's values.
 template <int NQ>
-__device__ bool cta_tile_done(unsigned* sys_cnt, double* tile_tot, double* warp_part,
-                              unsigned* tile_cnt, double* chunk_tot, unsigned* chunk_cnt,
-                              int ntiles, int tile, double (&v)[NQ]) {
+__device__ bool cta_tile_total(double* warp_part, unsigned* tile_cnt, int tile,
+                               double (&v)[NQ]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < NQ; ++q) v[q] = warp_sum(v[q]);
@@ -232,7 +182,7 @@ __device__ bool cta_tile_done(unsigned* sys_cnt, double* tile_tot, double* warp_
     v[q] = warp_sum(w);
   }
   if (lane == 0) tile_cnt[tile] = 0u;
-  return warp_tile_done<NQ>(sys_cnt, tile_tot, chunk_tot, chunk_cnt, ntiles, tile, v);
+  return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -243,62 +193,215 @@ __device__ __forceinline__ int warp_global() {
 }
 __device__ __forceinline__ int warps_total() { return (int)((gridDim.x * blockDim.x) >> 5); }
 
+// A warp takes a whole tile (at most kRows rows): lane l owns rows
+// r0 + l + 32 u, u < kPerLane.  Every load of the tile is issued before the
+// first result is formed, so a warp keeps kPerLane loads per array in
+// flight.  The tile descriptors are software-pipelined: while a warp works
+// on item k it already holds the descriptor (system state and array
+// pointers) of item k + stride and the work entry of item k + 2 stride, so
+// only the data loads' latency is on its path.  Neither kernel changes a
+// system's state, so a descriptor read early is still current.
+constexpr int kPerLane = kRows / 32;
+
+// The work entries of a warp's items, one stride apart.
+struct WorkStream {
+  const Work* work;
+  int nw, k, stride;
+  __device__ Work at(int kk) const { return kk < nw ? work[kk] : Work{0, 0, 0, 0, 0, 0}; }
+};
+
 template <typename V>
-__global__ void __launch_bounds__(256) kb_pupdate(BatchArgs a) {
+struct PupdateDesc {
+  int r0, r1, go, first;
+  double beta;
+  const V* r;
+  const V* dinv;
+  V* p;
+  __device__ void load(const Work& w, const SysDev<V>* D, const SysState* st) {
+    const SysState& s = st[w.sys];
+    const SysDev<V>& d = D[w.sys];
+    r0 = w.r0;
+    r1 = w.r1;
+    go = active(s);
+    first = s.first;
+    beta = s.beta;
+    r = d.r;
+    dinv = d.dinv;
+    p = d.p;
+  }
+};
+
+// Resident CTAs per SM asked of the register allocator (FP32 iterates:
+// all of a tile's values fit in registers at this occupancy).
+template <typename V>
+constexpr int ew_min_blocks(int fp32) { return sizeof(V) == 4 ? fp32 : 1; }
+
+template <typename V>
+__global__ void __launch_bounds__(256, ew_min_blocks<V>(3)) kb_pupdate(BatchArgs a) {
   const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
-  const int nw = *a.nwork;
+  const WorkStream ws{a.work, *a.nwork, warp_global(), warps_total()};
+  if (ws.k >= ws.nw) return;
   const int lane = threadIdx.x & 31;
-  for (int k = warp_global(); k < nw; k += warps_total()) {
-    const Work w = a.work[k];
-    const SysState& s = a.st[w.sys];
-    if (!active(s)) continue;
-    const V* __restrict__ r = D[w.sys].r;
-    const V* __restrict__ dinv = D[w.sys].dinv;
-    V* __restrict__ p = D[w.sys].p;
-    const int first = s.first;
-    const double beta = s.beta;
-#pragma unroll 4
-    for (int i = w.r0 + lane; i < w.r1; i += 32) {
-      const V z = r[i] * dinv[i];
-      p[i] = first ? z : (V)((double)z + beta * (double)p[i]);
+  PupdateDesc<V> cur, nxt;
+  cur.load(ws.at(ws.k), D, a.st);
+  Work wn = ws.at(ws.k + ws.stride);
+  for (int k = ws.k; k < ws.nw; k += ws.stride) {
+    const Work wnn = ws.at(k + 2 * ws.stride);
+    if (k + ws.stride < ws.nw) nxt.load(wn, D, a.st);
+    if (cur.go) {
+      const V* __restrict__ r = cur.r;
+      const V* __restrict__ dinv = cur.dinv;
+      V* __restrict__ p = cur.p;
+      const int i0 = cur.r0 + lane, nr = cur.r1 - cur.r0;
+      V rv[kPerLane], dv[kPerLane], pv[kPerLane];
+#pragma unroll
+      for (int u = 0; u < kPerLane; ++u)
+        if (lane + 32 * u < nr) {
+          rv[u] = r[i0 + 32 * u];
+          dv[u] = dinv[i0 + 32 * u];
+          pv[u] = cur.first ? (V)0 : p[i0 + 32 * u];
+        }
+#pragma unroll
+      for (int u = 0; u < kPerLane; ++u)
+        if (lane + 32 * u < nr) {
+          const V z = rv[u] * dv[u];
+          p[i0 + 32 * u] = cur.first ? z : (V)((double)z + cur.beta * (double)pv[u]);
+        }
     }
+    cur = nxt;
+    wn = wnn;
   }
 }
 
 template <typename V>
-__global__ void __launch_bounds__(256) kb_update(BatchArgs a) {
+struct UpdateDesc {
+  int r0, r1, tile, go;
+  double alpha;
+  const SysDev<V>* d;
+  V* xlo;
+  V* r;
+  const V* p;
+  const V* q;
+  const V* dinv;
+  __device__ void load(const Work& w, const SysDev<V>* D, const SysState* st) {
+    const SysState& s = st[w.sys];
+    d = D + w.sys;
+    r0 = w.r0;
+    r1 = w.r1;
+    tile = w.tile;
+    go = active(s);
+    alpha = s.alpha;
+    xlo = d->xlo;
+    r = d->r;
+    p = d->p;
+    q = d->q;
+    dinv = d->dinv;
+  }
+};
+
+template <typename V>
+__global__ void __launch_bounds__(256, ew_min_blocks<V>(2)) kb_update(BatchArgs a) {
   const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
-  const int nw = *a.nwork;
+  const WorkStream ws{a.work, *a.nwork, warp_global(), warps_total()};
+  if (ws.k >= ws.nw) return;
   const int lane = threadIdx.x & 31;
-  for (int k = warp_global(); k < nw; k += warps_total()) {
-    const Work w = a.work[k];
-    SysState& s = a.st[w.sys];
-    if (!active(s)) continue;   // warp-uniform
-    const SysDev<V>& d = D[w.sys];
-    V* __restrict__ xlo = d.xlo;
-    V* __restrict__ r = d.r;
-    const V* __restrict__ p = d.p;
-    const V* __restrict__ q = d.q;
-    const V* __restrict__ dinv = d.dinv;
-    const double al = s.alpha;
-    double v[2] = {0.0, 0.0};   // rho, |r|^2
-#pragma unroll 4
-    for (int i = w.r0 + lane; i < w.r1; i += 32) {
-      const V xl = (V)((double)xlo[i] + al * (double)p[i]);
-      const V ri = (V)((double)r[i] - al * (double)q[i]);
-      xlo[i] = xl;
-      r[i] = ri;
-      const V zi = ri * dinv[i];
-      v[0] = __dadd_rn(v[0], __dmul_rn((double)zi, (double)ri));
-      v[1] = __dadd_rn(v[1], __dmul_rn((double)ri, (double)ri));
+  UpdateDesc<V> cur, nxt;
+  cur.load(ws.at(ws.k), D, a.st);
+  Work wn = ws.at(ws.k + ws.stride);
+  for (int k = ws.k; k < ws.nw; k += ws.stride) {
+    const Work wnn = ws.at(k + 2 * ws.stride);
+    if (k + ws.stride < ws.nw) nxt.load(wn, D, a.st);
+    if (cur.go) {   // warp-uniform
+      V* __restrict__ xlo = cur.xlo;
+      V* __restrict__ r = cur.r;
+      const V* __restrict__ p = cur.p;
+      const V* __restrict__ q = cur.q;
+      const V* __restrict__ dinv = cur.dinv;
+      const double al = cur.alpha;
+      const int i0 = cur.r0 + lane, nr = cur.r1 - cur.r0;
+      V xv[kPerLane], pv[kPerLane], rv[kPerLane], qv[kPerLane], dv[kPerLane];
+#pragma unroll
+      for (int u = 0; u < kPerLane; ++u)
+        if (lane + 32 * u < nr) {
+          const int i = i0 + 32 * u;
+          xv[u] = xlo[i];
+          pv[u] = p[i];
+          rv[u] = r[i];
+          qv[u] = q[i];
+          dv[u] = dinv[i];
+        }
+      double v[2] = {0.0, 0.0};   // rho, |r|^2
+#pragma unroll
+      for (int u = 0; u < kPerLane; ++u)
+        if (lane + 32 * u < nr) {
+          const int i = i0 + 32 * u;
+          const V xl = (V)((double)xv[u] + al * (double)pv[u]);
+          const V ri = (V)((double)rv[u] - al * (double)qv[u]);
+          xlo[i] = xl;
+          r[i] = ri;
+          const V zi = ri * dv[u];
+          v[0] = __dadd_rn(v[0], __dmul_rn((double)zi, (double)ri));
+          v[1] = __dadd_rn(v[1], __dmul_rn((double)ri, (double)ri));
+        }
+      v[0] = warp_sum(v[0]);
+      v[1] = warp_sum(v[1]);
+      put_tile_total<2>(cur.d->tile_tot, cur.tile, v);
     }
-    v[0] = warp_sum(v[0]);
-    v[1] = warp_sum(v[1]);
-    if (!warp_tile_done<2>(&s.cnt_upd, d.tile_tot, d.chunk_tot, d.chunk_cnt, d.ntiles, w.tile,
-                           v))
-      continue;
-    int base = -1;
-    if (lane == 0) {
+    cur = nxt;
+    wn = wnn;
+  }
+}
+
+// The finishing kernels: one CTA of kFinThreads per listed system (a
+// grid-stride loop over the system list).
+constexpr int kFinThreads = 256;
+
+// A system's totals from its tile totals: thread t adds tiles t,
+// t + kFinThreads, ... in turn, each warp sums its lanes (butterfly), and
+// every warp then sums the warps' results in warp order, so all threads
+// hold the same bits.  The order depends only on the system's tiling.
+// Whole CTA (two barriers).
+template <int NQ, typename V>
+__device__ __forceinline__ void sum_tiles(const SysDev<V>& d, double (&v)[NQ]) {
+  constexpr int kW = kFinThreads / 32;
+  __shared__ double part[NQ][kW];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double acc[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
+#pragma unroll 4
+  for (int t = threadIdx.x; t < d.ntiles; t += kFinThreads)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+      acc[q] = __dadd_rn(acc[q], __ldcg(d.tile_tot + (size_t)t * kPartQ + q));
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    acc[q] = warp_sum(acc[q]);
+    if (lane == 0) part[q][warp] = acc[q];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) v[q] = warp_sum(lane < kW ? part[q][lane] : 0.0);
+  __syncthreads();   // part is reused by the next system
+}
+
+// Per system after kb_update: rho, beta, the iteration count and the
+// refinement trigger; a system due an update lists its tiles for the
+// refinement kernels.
+template <typename V>
+__global__ void __launch_bounds__(kFinThreads) kb_beta(BatchArgs a) {
+  const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
+  __shared__ int base_sh;
+  const int ns = *a.nsys;
+  for (int k = blockIdx.x; k < ns; k += gridDim.x) {
+    const int sys = a.sys[k];
+    SysState& s = a.st[sys];
+    if (!active(s)) continue;   // CTA-uniform
+    const SysDev<V>& d = D[sys];
+    double v[2];
+    sum_tiles<2>(d, v);
+    if (threadIdx.x == 0) {
+      int base = -1;
       s.rho_old = s.rho;
       s.rho = v[0];
       s.beta = __ddiv_rn(s.rho, s.rho_old);
@@ -316,12 +419,34 @@ __global__ void __launch_bounds__(256) kb_update(BatchArgs a) {
         s.need_ru = 1;
         base = atomicAdd(a.ru.count, d.ntiles);
       }
+      base_sh = base;
     }
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= 0)   // list this system's tiles for the refinement kernels
-      for (int t = lane; t < d.ntiles; t += 32)
-        a.ru.items[base + t] = Work{w.sys, t, d.tiles[t], d.tiles[t + 1],
+    __syncthreads();
+    const int base = base_sh;
+    __syncthreads();   // base_sh is reused by the next system
+    if (base >= 0)     // list this system's tiles for the refinement kernels
+      for (int t = threadIdx.x; t < d.ntiles; t += kFinThreads)
+        a.ru.items[base + t] = Work{sys, t, d.tiles[t], d.tiles[t + 1],
                                     d.row[d.tiles[t]], d.row[d.tiles[t + 1]]};
+  }
+}
+
+// Per system after kb_spmv: alpha = rho / p.q (breakdown when p.q <= 0 or
+// NaN).
+template <typename V>
+__global__ void __launch_bounds__(kFinThreads) kb_alpha(BatchArgs a) {
+  const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
+  const int ns = *a.nsys;
+  for (int k = blockIdx.x; k < ns; k += gridDim.x) {
+    const int sys = a.sys[k];
+    SysState& s = a.st[sys];
+    if (!active(s)) continue;   // CTA-uniform
+    double v[1];
+    sum_tiles<1>(D[sys], v);
+    if (threadIdx.x == 0) {
+      if (!(v[0] > 0.0)) s.status = kBreakdown;
+      else s.alpha = __ddiv_rn(s.rho, v[0]);
+    }
   }
 }
 
@@ -336,11 +461,21 @@ __global__ void __launch_bounds__(256) kb_ru_fold(BatchArgs a) {
     if (!(s.status == kActive && s.need_ru)) continue;
     double* __restrict__ x = D[w.sys].x;
     V* __restrict__ xlo = D[w.sys].xlo;
-#pragma unroll 4
-    for (int i = w.r0 + lane; i < w.r1; i += 32) {
-      x[i] = __dadd_rn(x[i], (double)xlo[i]);
-      xlo[i] = (V)0;
-    }
+    const int i0 = w.r0 + lane, nr = w.r1 - w.r0;
+    double xv[kPerLane];
+    V lv[kPerLane];
+#pragma unroll
+    for (int u = 0; u < kPerLane; ++u)
+      if (lane + 32 * u < nr) {
+        xv[u] = x[i0 + 32 * u];
+        lv[u] = xlo[i0 + 32 * u];
+      }
+#pragma unroll
+    for (int u = 0; u < kPerLane; ++u)
+      if (lane + 32 * u < nr) {
+        x[i0 + 32 * u] = __dadd_rn(xv[u], (double)lv[u]);
+        xlo[i0 + 32 * u] = (V)0;
+      }
   }
 }
 
@@ -397,14 +532,8 @@ struct SpmvWork {
     const SysDev<V>& d = D[w.sys];
     double v[1] = {acc};
     acc = 0.0;
-    if (cta_tile_done<1>(&st[w.sys].cnt_spmv, d.tile_tot, d.warp_part, d.tile_cnt, d.chunk_tot,
-                         d.chunk_cnt, d.ntiles,
-                         w.tile, v) &&
-        (threadIdx.x & 31) == 0) {
-      SysState& s = st[w.sys];
-      if (!(v[0] > 0.0)) s.status = kBreakdown;   // p.q <= 0 or NaN
-      else s.alpha = __ddiv_rn(s.rho, v[0]);
-    }
+    if (cta_tile_total<1>(d.warp_part, d.tile_cnt, w.tile, v))
+      put_tile_total<1>(d.tile_tot, w.tile, v);
   }
 };
 
@@ -442,8 +571,8 @@ struct BatchTiles {
 // reducer warp: every consumer warp sums its lanes and parks the result in
 // shared memory (slot it & 1, tile_end), consumer thread 0 adds the tile's
 // system and index (tile_id); the reducer warp sums the kWarps partials in
-// warp order -- the order cta_tile_done uses -- and reports the tile.  The
-// consumers never wait for a report.
+// warp order -- the order cta_tile_total uses -- and stores the tile's
+// totals.  The consumers never wait for a report.
 __shared__ double g_tile_part[2][kPartQ][kWarps];
 struct TileId {
   int sys, tile, skip;
@@ -506,14 +635,7 @@ struct SpmvOp2 {
     if (id.skip) return;
     double v[1];
     sum_partials<1>(v, it);
-    const SysDev<V>& d = D[id.sys];
-    if (warp_tile_done<1>(&st[id.sys].cnt_spmv, d.tile_tot, d.chunk_tot, d.chunk_cnt, d.ntiles,
-                          id.tile, v) &&
-        (threadIdx.x & 31) == 0) {
-      SysState& s = st[id.sys];
-      if (!(v[0] > 0.0)) s.status = kBreakdown;   // p.q <= 0 or NaN
-      else s.alpha = __ddiv_rn(s.rho, v[0]);
-    }
+    put_tile_total<1>(D[id.sys].tile_tot, id.tile, v);
   }
 };
 
@@ -562,68 +684,8 @@ __device__ void res_finish(SysState& s, const SysDev<V>& d, const double (&v)[3]
   }
 }
 
-// r = b - A x in FP64; new systems also form dinv and |b|^2.
-template <typename V>
-struct ResWork {
-  using Item = Work;
-  const SysDev<V>* D;
-  SysState* st;
-  const Work* work;
-  int nw;
-  double rr, rho, bb;
-  __device__ int count() const { return nw; }
-  __device__ Work item(int k) const { return work[k]; }
-  __device__ void resolve(const Work& w, TileRes<double>& rs) const {
-    const SysDev<V>& d = D[w.sys];
-    rs.row = d.row;
-    rs.col = d.col;
-    rs.val = d.val;
-    const SysState& s = st[w.sys];
-    rs.skip = !(s.status == kInit || (s.status == kActive && s.need_ru));
-  }
-  __device__ void row(int k, int i, const double* v, const int* c, int len) {
-    const Work w = work[k];
-    const SysDev<V>& d = D[w.sys];
-    const bool init = st[w.sys].status == kInit;
-    double s = d.b[i];
-#pragma unroll 1
-    for (int j0 = 0; j0 < len; j0 += 8) {
-      double xv[8], vv[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u)
-        if (j0 + u < len) {
-          vv[u] = v[j0 + u];
-          xv[u] = d.x[c[j0 + u]];
-        }
-#pragma unroll
-      for (int u = 0; u < 8; ++u)
-        if (j0 + u < len) s = __dsub_rn(s, __dmul_rn(vv[u], xv[u]));
-    }
-    if (init) {
-      const double aii = d.val[d.dia[i]];
-      d.dinv[i] = (V)__drcp_rn(aii);
-      bb = __dadd_rn(bb, __dmul_rn(d.b[i], d.b[i]));
-    }
-    const V ri = (V)s;
-    d.r[i] = ri;
-    const V zi = ri * d.dinv[i];
-    rr = __dadd_rn(rr, __dmul_rn(s, s));
-    rho = __dadd_rn(rho, __dmul_rn((double)zi, (double)ri));
-  }
-  __device__ void tile_end(int k) {
-    const Work w = work[k];
-    const SysDev<V>& d = D[w.sys];
-    double v[3] = {rr, rho, bb};
-    rr = rho = bb = 0.0;
-    if (cta_tile_done<3>(&st[w.sys].cnt_res, d.tile_tot, d.warp_part, d.tile_cnt, d.chunk_tot,
-                         d.chunk_cnt, d.ntiles,
-                         w.tile, v) &&
-        (threadIdx.x & 31) == 0)
-      res_finish(st[w.sys], d, v);
-  }
-};
-
-// r = b - A x in FP64 for the producer-warp streamer (see ResWork).
+// r = b - A x in FP64 for the producer-warp streamer; new systems also
+// form dinv and |b|^2.
 template <typename V>
 struct ResOp2 {
   static constexpr bool kReducer = true;
@@ -665,11 +727,7 @@ struct ResOp2 {
     if (id.skip) return;
     double v[3];
     sum_partials<3>(v, it);
-    const SysDev<V>& dd = D[id.sys];
-    if (warp_tile_done<3>(&st[id.sys].cnt_res, dd.tile_tot, dd.chunk_tot, dd.chunk_cnt,
-                          dd.ntiles, id.tile, v) &&
-        (threadIdx.x & 31) == 0)
-      res_finish(st[id.sys], dd, v);
+    put_tile_total<3>(D[id.sys].tile_tot, id.tile, v);
   }
 };
 
@@ -679,14 +737,24 @@ __global__ void __launch_bounds__(kCsr2RedThreads, 2) kb_ru_res(BatchArgs a) {
   ResOp2<V> op{static_cast<const SysDev<V>*>(a.desc), a.st, a.ru.items, 0.0, 0.0, 0.0,
                nullptr, false};
   stream_csr2<kRows, kNnzCap, kStages, G>(src, op);
-  // The last CTA to leave empties the refinement list for the next iteration.
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(a.ru.exit_cnt, 1u) == gridDim.x - 1) {
-      *a.ru.count = 0;
-      *a.ru.exit_cnt = 0u;
-    }
+}
+
+// Per system after kb_ru_res: the refinement's convergence test and the
+// restarted scalars (res_finish); then the refinement list is emptied for
+// the next iteration.
+template <typename V>
+__global__ void __launch_bounds__(kFinThreads) kb_ru_finish(BatchArgs a) {
+  const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
+  const int ns = *a.nsys;
+  for (int k = blockIdx.x; k < ns; k += gridDim.x) {
+    const int sys = a.sys[k];
+    SysState& s = a.st[sys];
+    if (!(s.status == kInit || (s.status == kActive && s.need_ru))) continue;   // CTA-uniform
+    double v[3];
+    sum_tiles<3>(D[sys], v);
+    if (threadIdx.x == 0) res_finish(s, D[sys], v);
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.ru.count = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -870,7 +938,7 @@ int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* co
 // Byte layout of one system's segment.
 struct Layout {
   size_t row, col, dia, tiles, val, val32, b, x, xlo, r, p, q, dinv, tile_tot, warp_part,
-      tile_cnt, chunk_tot, chunk_cnt, total;
+      tile_cnt, total;
 };
 
 Layout layout_for(const HostSys& h, size_t vsz, int use_val32) {
@@ -893,11 +961,10 @@ Layout layout_for(const HostSys& h, size_t vsz, int use_val32) {
   L.q = take(n8 * vsz);
   L.dinv = take(n8 * vsz);
   L.tile_tot = take((size_t)ntiles * kPartQ * 8);
-  L.warp_part = take((size_t)ntiles * kWarps * kPartQ * 8);
-  L.tile_cnt = take((size_t)ntiles * 4);
-  const size_t nch = (size_t)(ntiles + kChunkTiles - 1) / kChunkTiles;
-  L.chunk_tot = take(nch * kPartQ * 8);
-  L.chunk_cnt = take(nch * 4);
+  if (use_val32) {   // the FP32-value SpMV's per-warp partials
+    L.warp_part = take((size_t)ntiles * kWarps * kPartQ * 8);
+    L.tile_cnt = take((size_t)ntiles * 4);
+  }
   L.total = o;
   return L;
 }
@@ -934,21 +1001,22 @@ struct tf_batch_s {
   int* d_nwork = nullptr;
   Work* d_ru = nullptr;          // refinement work list (same capacity)
   int* d_ru_count = nullptr;
-  unsigned* d_ru_exit = nullptr;
+  int* d_sys = nullptr;          // the systems of the work list
+  int* d_nsys = nullptr;
+  std::vector<int> h_sys;
   int work_cap = 0;
   std::vector<Work> h_work, h_ru;
   int nwork = 0;
+  long long work_rows = 0, work_nnz = 0;   // rows and entries of the listed systems
   cudaGraphExec_t sweep = nullptr;
-  int grid_plain = 1, grid_tile = 1;
+  int grid_pupdate = 1, grid_update = 1, grid_fold = 1, grid_tile = 1, grid_sys = 1;
   int sweeps = 0;
   long long total_iters = 0;
-  // Per sweep of the last tf_batch_run: systems running at its launch, work
-  // items (tiles) of the list, wall time of the sweep (launch to state read).
-  struct SweepRec {
-    int active, items;
-    double ms;
-  };
-  std::vector<SweepRec> trace;
+  // Per sweep of the last tf_batch_run (tf_batch_sweep): systems running at
+  // its launch with their rows and entries, work items (tiles) of the list,
+  // wall time of the sweep (launch to state read), kernel times (profiling).
+  std::vector<tf_batch_sweep> trace;
+  double sweep_kms[kKernels] = {};   // the last profiled sweep's kernel times
 
   ~tf_batch_s() {
     cudaSetDevice(ctx->device);
@@ -956,7 +1024,7 @@ struct tf_batch_s {
     if (sweep) cudaGraphExecDestroy(sweep);
     if (arena.base) cudaFree(arena.base);
     for (void* p : {d_desc, (void*)d_state, (void*)d_work, (void*)d_nwork, (void*)d_ru,
-                    (void*)d_ru_count, (void*)d_ru_exit})
+                    (void*)d_ru_count, (void*)d_sys, (void*)d_nsys})
       if (p) cudaFree(p);
     if (h_state) cudaFreeHost(h_state);
   }
@@ -966,50 +1034,65 @@ struct tf_batch_s {
   static size_t smem_csr2() { return Csr2Layout<kRows, kNnzCap, kStages>::kSmemBytes; }
   static size_t smem_rows32() { return TileLayout<kRows, kNnzCap, float, kStages>::kSmemBytes; }
 
-  // ev (profiling only): events recorded before each of the five kernels
-  // and after the last.
+  BatchArgs args() const {
+    return BatchArgs{d_desc, d_state, d_work, d_nwork, opts.ru_delta * opts.ru_delta,
+                     RuList{d_ru, d_ru_count}, d_sys, d_nsys};
+  }
+
+  // The kernels of one iteration (the order of tf_batch_kernel_ms).  ev
+  // (profiling only): events recorded before each kernel and after the last.
   template <typename V>
   void launch_iteration(cudaStream_t s, const BatchArgs& a, cudaEvent_t* ev = nullptr) {
-    if (ev) cudaEventRecord(ev[0], s);
-    kb_pupdate<V><<<grid_plain, 256, 0, s>>>(a);
-    if (ev) cudaEventRecord(ev[1], s);
+    int e = 0;
+    auto mark = [&]() { if (ev) cudaEventRecord(ev[e++], s); };
+    mark();
+    kb_pupdate<V><<<grid_pupdate, 256, 0, s>>>(a);
+    mark();
     if (opts.val_fp32) kb_spmv<V, float, 0><<<grid_tile, kRows, smem_rows32(), s>>>(a);
-    else if (opts.row_groups) kb_spmv<V, double, -1><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
-    else kb_spmv<V, double, 0><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
-    if (ev) cudaEventRecord(ev[2], s);
-    kb_update<V><<<grid_plain, 256, 0, s>>>(a);
-    if (ev) cudaEventRecord(ev[3], s);
-    kb_ru_fold<V><<<grid_plain, 256, 0, s>>>(a);
-    if (ev) cudaEventRecord(ev[4], s);
-    if (opts.row_groups) kb_ru_res<V, -1><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
-    else kb_ru_res<V, 0><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
-    if (ev) cudaEventRecord(ev[5], s);
+    else if (opts.two_phase_rows) kb_spmv<V, double, 0><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
+    else kb_spmv<V, double, -1><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
+    mark();
+    kb_alpha<V><<<grid_sys, kFinThreads, 0, s>>>(a);
+    mark();
+    kb_update<V><<<grid_update, 256, 0, s>>>(a);
+    mark();
+    kb_beta<V><<<grid_sys, kFinThreads, 0, s>>>(a);
+    mark();
+    kb_ru_fold<V><<<grid_fold, 256, 0, s>>>(a);
+    mark();
+    if (opts.two_phase_rows) kb_ru_res<V, 0><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
+    else kb_ru_res<V, -1><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
+    mark();
+    kb_ru_finish<V><<<grid_sys, kFinThreads, 0, s>>>(a);
+    mark();
   }
 
   // Profiling (TF_BATCH_PROFILE set when the batch was created): sweeps run
   // as direct launches with events around every kernel; kern_ms accumulates
-  // the time of pupdate, spmv, update, ru_fold, ru_res over the run.
+  // each kernel's time over the run.
   bool profile = false;
-  double kern_ms[5] = {0, 0, 0, 0, 0};
+  double kern_ms[kKernels] = {};
   int run_sweep_profiled() {
     cudaStream_t s = ctx->stream;
-    BatchArgs a{d_desc, d_state, d_work, d_nwork, opts.ru_delta * opts.ru_delta,
-                RuList{d_ru, d_ru_count, d_ru_exit}};
-    std::vector<cudaEvent_t> ev(6 * opts.sweep_iters);
+    const BatchArgs a = args();
+    constexpr int kEv = kKernels + 1;
+    std::vector<cudaEvent_t> ev(kEv * opts.sweep_iters);
     for (auto& e : ev) TF_CUDA_TRY(cudaEventCreate(&e));
     for (int it = 0; it < opts.sweep_iters; ++it) {
-      if (vsz == 4) launch_iteration<float>(s, a, &ev[6 * it]);
-      else launch_iteration<double>(s, a, &ev[6 * it]);
+      if (vsz == 4) launch_iteration<float>(s, a, &ev[kEv * it]);
+      else launch_iteration<double>(s, a, &ev[kEv * it]);
     }
     TF_CUDA_TRY(cudaGetLastError());
     TF_CUDA_TRY(cudaMemcpyAsync(h_state, d_state, (size_t)max_sys * sizeof(SysState),
                                 cudaMemcpyDeviceToHost, s));
     TF_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int k = 0; k < kKernels; ++k) sweep_kms[k] = 0.0;
     for (int it = 0; it < opts.sweep_iters; ++it)
-      for (int k = 0; k < 5; ++k) {
+      for (int k = 0; k < kKernels; ++k) {
         float ms = 0.0f;
-        cudaEventElapsedTime(&ms, ev[6 * it + k], ev[6 * it + k + 1]);
+        cudaEventElapsedTime(&ms, ev[kEv * it + k], ev[kEv * it + k + 1]);
         kern_ms[k] += ms;
+        sweep_kms[k] += ms;
       }
     for (auto& e : ev) cudaEventDestroy(e);
     ++sweeps;
@@ -1029,7 +1112,19 @@ struct tf_batch_s {
     TF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_spmv<V, double, 0>,
                                                               kCsr2RedThreads, smem_csr2()));
     grid_tile = std::max(1, per_sm) * ctx->sm_count;
-    grid_plain = ctx->sm_count * 8;
+    // The elementwise kernels keep a whole tile per warp in registers: one
+    // resident wave each, so no CTA waits for another to leave.
+    auto resident = [&](const void* f, int* grid) -> int {
+      int n = 1;
+      TF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, 256, 0));
+      *grid = std::max(1, n) * ctx->sm_count;
+      return TF_OK;
+    };
+    int st = resident((const void*)kb_pupdate<V>, &grid_pupdate);
+    if (st == TF_OK) st = resident((const void*)kb_update<V>, &grid_update);
+    if (st == TF_OK) st = resident((const void*)kb_ru_fold<V>, &grid_fold);
+    if (st != TF_OK) return st;
+    grid_sys = std::max(1, std::min(max_sys, ctx->sm_count * 8));   // one CTA per system
     return TF_OK;
   }
 
@@ -1039,8 +1134,7 @@ struct tf_batch_s {
       sweep = nullptr;
     }
     cudaStream_t s = ctx->stream;
-    BatchArgs a{d_desc, d_state, d_work, d_nwork, opts.ru_delta * opts.ru_delta,
-                RuList{d_ru, d_ru_count, d_ru_exit}};
+    const BatchArgs a = args();
     cudaGraph_t g = nullptr;
     TF_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int it = 0; it < opts.sweep_iters; ++it) {
@@ -1089,8 +1183,9 @@ struct tf_batch_s {
     TF_CUDA_TRY(cudaMemset(d_nwork, 0, sizeof(int)));
     TF_CUDA_TRY(cudaMalloc((void**)&d_ru_count, sizeof(int)));
     TF_CUDA_TRY(cudaMemset(d_ru_count, 0, sizeof(int)));
-    TF_CUDA_TRY(cudaMalloc((void**)&d_ru_exit, sizeof(unsigned)));
-    TF_CUDA_TRY(cudaMemset(d_ru_exit, 0, sizeof(unsigned)));
+    TF_CUDA_TRY(cudaMalloc((void**)&d_sys, (size_t)max_sys * sizeof(int)));
+    TF_CUDA_TRY(cudaMalloc((void**)&d_nsys, sizeof(int)));
+    TF_CUDA_TRY(cudaMemset(d_nsys, 0, sizeof(int)));
     st = (vsz == 4) ? setup_kernels<float>() : setup_kernels<double>();
     if (st != TF_OK) return st;
     return build_sweep();
@@ -1122,11 +1217,8 @@ struct tf_batch_s {
     if (e == cudaSuccess) e = up(L.x, h.x0.data(), (size_t)h.n * 8);
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.xlo, 0, n8 * vsz, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.p, 0, n8 * vsz, s);
-    if (e == cudaSuccess)
+    if (e == cudaSuccess && opts.val_fp32)
       e = cudaMemsetAsync(base + L.tile_cnt, 0, (h.tiles.size() - 1) * 4, s);
-    if (e == cudaSuccess)
-      e = cudaMemsetAsync(base + L.chunk_cnt, 0,
-                          ((h.tiles.size() - 1 + kChunkTiles - 1) / kChunkTiles) * 4, s);
     if (e != cudaSuccess) {
       arena.release(off, L.total);
       tf_set_last_cuda_error(e, "batch admit copies", __FILE__, __LINE__);
@@ -1149,10 +1241,8 @@ struct tf_batch_s {
       d.q = (VV*)(base + L.q);
       d.dinv = (VV*)(base + L.dinv);
       d.tile_tot = (double*)(base + L.tile_tot);
-      d.warp_part = (double*)(base + L.warp_part);
-      d.tile_cnt = (unsigned*)(base + L.tile_cnt);
-      d.chunk_tot = (double*)(base + L.chunk_tot);
-      d.chunk_cnt = (unsigned*)(base + L.chunk_cnt);
+      d.warp_part = opts.val_fp32 ? (double*)(base + L.warp_part) : nullptr;
+      d.tile_cnt = opts.val_fp32 ? (unsigned*)(base + L.tile_cnt) : nullptr;
       d.n = h.n;
       d.ntiles = ntiles;
       d.maxit = h.maxit;
@@ -1199,12 +1289,17 @@ struct tf_batch_s {
   int rebuild_work() {
     h_work.clear();
     h_ru.clear();
+    h_sys.clear();
+    work_rows = work_nnz = 0;
     for (int i = 0; i < max_sys; ++i) {
       if (!slots[i].used) continue;
       const int stt = h_state[i].status;
       if (stt != kInit && stt != kActive) continue;
       const std::vector<int>& tl = slots[i].tiles;
       const std::vector<int>& tj = slots[i].tile_j;
+      work_rows += slots[i].n;
+      work_nnz += tj[slots[i].ntiles];
+      h_sys.push_back(i);
       for (int t = 0; t < slots[i].ntiles; ++t) {
         const Work wk{i, t, tl[t], tl[t + 1], tj[t], tj[t + 1]};
         h_work.push_back(wk);
@@ -1232,6 +1327,11 @@ struct tf_batch_s {
       TF_CUDA_TRY(cudaMemcpyAsync(d_ru, h_ru.data(), (size_t)nru * sizeof(Work),
                                   cudaMemcpyHostToDevice, s));
     TF_CUDA_TRY(cudaMemcpyAsync(d_nwork, &nwork, sizeof(int), cudaMemcpyHostToDevice, s));
+    const int nsys = (int)h_sys.size();
+    if (nsys)
+      TF_CUDA_TRY(cudaMemcpyAsync(d_sys, h_sys.data(), (size_t)nsys * sizeof(int),
+                                  cudaMemcpyHostToDevice, s));
+    TF_CUDA_TRY(cudaMemcpyAsync(d_nsys, &nsys, sizeof(int), cudaMemcpyHostToDevice, s));
     TF_CUDA_TRY(cudaMemcpyAsync(d_ru_count, &nru, sizeof(int), cudaMemcpyHostToDevice, s));
     TF_CUDA_TRY(cudaStreamSynchronize(s));
     return TF_OK;
@@ -1267,8 +1367,15 @@ struct tf_batch_s {
       st = run_sweep();
       if (st != TF_OK) return st;
       const auto te = std::chrono::steady_clock::now();
-      trace.push_back(SweepRec{running, nwork,
-                               std::chrono::duration<double, std::milli>(te - ts).count()});
+      tf_batch_sweep rec{};
+      rec.active = running;
+      rec.items = nwork;
+      rec.rows = work_rows;
+      rec.nnz = work_nnz;
+      rec.ms = std::chrono::duration<double, std::milli>(te - ts).count();
+      if (profile)
+        for (int k = 0; k < kKernels; ++k) rec.kernel_ms[k] = sweep_kms[k];
+      trace.push_back(rec);
       const double ms = std::chrono::duration<double, std::milli>(te - t0).count();
       for (int i = 0; i < max_sys; ++i)
         if (slots[i].used && slots[i].done_ms < 0.0 && h_state[i].status != kInit &&
@@ -1462,24 +1569,19 @@ extern "C" int tf_batch_result(tf_batch bt, int sys, double* x, int* iters,
   TF_API_END
 }
 
-extern "C" int tf_batch_kernel_ms(tf_batch bt, double* ms5) {
+extern "C" int tf_batch_kernel_ms(tf_batch bt, double* ms8) {
   TF_API_BEGIN
-  if (!bt || !ms5) return TF_ERR_ARG;
-  for (int k = 0; k < 5; ++k) ms5[k] = bt->kern_ms[k];
+  if (!bt || !ms8) return TF_ERR_ARG;
+  for (int k = 0; k < kKernels; ++k) ms8[k] = bt->kern_ms[k];
   return bt->profile ? TF_OK : TF_ERR_ARG;
   TF_API_END
 }
 
-extern "C" int tf_batch_trace(tf_batch bt, int* active, int* items, double* ms, int cap,
-                              int* count) {
+extern "C" int tf_batch_trace(tf_batch bt, tf_batch_sweep* out, int cap, int* count) {
   TF_API_BEGIN
-  if (!bt || !count || (cap > 0 && (!active || !items || !ms))) return TF_ERR_ARG;
+  if (!bt || !count || cap < 0 || (cap > 0 && !out)) return TF_ERR_ARG;
   const int n = std::min<int>(cap, (int)bt->trace.size());
-  for (int i = 0; i < n; ++i) {
-    active[i] = bt->trace[i].active;
-    items[i] = bt->trace[i].items;
-    ms[i] = bt->trace[i].ms;
-  }
+  for (int i = 0; i < n; ++i) out[i] = bt->trace[i];
   *count = (int)bt->trace.size();
   return TF_OK;
   TF_API_END

@@ -13,7 +13,17 @@ class BatchOpts(ctypes.Structure):
     _fields_ = [("vec_fp32", ctypes.c_int), ("val_fp32", ctypes.c_int),
                 ("sweep_iters", ctypes.c_int), ("max_systems", ctypes.c_int),
                 ("ru_delta", ctypes.c_double), ("mem_budget", ctypes.c_size_t),
-                ("row_groups", ctypes.c_int)]
+                ("two_phase_rows", ctypes.c_int)]
+
+
+class SweepRec(ctypes.Structure):
+    """tf_batch_sweep: one sweep of a tf_batch_run."""
+    _fields_ = [("active", ctypes.c_int), ("items", ctypes.c_int),
+                ("rows", ctypes.c_int64), ("nnz", ctypes.c_int64), ("ms", ctypes.c_double),
+                ("kernel_ms", ctypes.c_double * 8)]
+
+
+KERNELS = ("pupdate", "spmv", "alpha", "update", "beta", "ru_fold", "ru_res", "ru_finish")
 
 
 def _lib():
@@ -30,7 +40,7 @@ def _lib():
     L.tf_batch_run.argtypes = [_vp]
     L.tf_batch_result.argtypes = [_vp, ctypes.c_int, _vp, ip, dp, ip, ip, dp]
     L.tf_batch_remove.argtypes = [_vp, ctypes.c_int]
-    L.tf_batch_trace.argtypes = [_vp, ip, ip, dp, ctypes.c_int, ip]
+    L.tf_batch_trace.argtypes = [_vp, ctypes.POINTER(SweepRec), ctypes.c_int, ip]
     L.tf_batch_kernel_ms.argtypes = [_vp, dp]
     L.tf_batch_info.argtypes = [_vp, ip, ip, ctypes.POINTER(ctypes.c_size_t)]
     L.tf_server_create.argtypes = [_vp, ctypes.POINTER(BatchOpts), ctypes.POINTER(_vp)]
@@ -47,9 +57,9 @@ def _lib():
 
 
 def _opts(vec_fp32=True, val_fp32=False, sweep_iters=8, max_systems=1024, ru_delta=0.1,
-          mem_budget=4 << 30, row_groups=0):
+          mem_budget=4 << 30, two_phase_rows=0):
     return BatchOpts(int(vec_fp32), int(val_fp32), int(sweep_iters), int(max_systems),
-                     float(ru_delta), int(mem_budget), int(row_groups))
+                     float(ru_delta), int(mem_budget), int(two_phase_rows))
 
 
 def _sys_args(s):
@@ -122,22 +132,25 @@ class Batch:
                     n_updates=nru.value, done_ms=dms.value)
 
     def trace(self):
-        """[(systems running, work items, ms)] per sweep of the last run."""
+        """One dict per sweep of the last run: systems running, work items,
+        rows and entries of the running systems, wall ms, and (profiling
+        only) the sweep's ms per kernel."""
         cnt = ctypes.c_int(0)
-        native._check(self.L.tf_batch_trace(self.h, None, None, None, 0, ctypes.byref(cnt)),
+        native._check(self.L.tf_batch_trace(self.h, None, 0, ctypes.byref(cnt)),
                       "tf_batch_trace")
         n = cnt.value
-        a, w = (ctypes.c_int * max(n, 1))(), (ctypes.c_int * max(n, 1))()
-        t = (ctypes.c_double * max(n, 1))()
-        native._check(self.L.tf_batch_trace(self.h, a, w, t, n, ctypes.byref(cnt)),
+        recs = (SweepRec * max(n, 1))()
+        native._check(self.L.tf_batch_trace(self.h, recs, n, ctypes.byref(cnt)),
                       "tf_batch_trace")
-        return [(a[i], w[i], t[i]) for i in range(n)]
+        return [dict(active=r.active, items=r.items, rows=r.rows, nnz=r.nnz, ms=r.ms,
+                     kernel_ms=dict(zip(KERNELS, list(r.kernel_ms))))
+                for r in recs[:n]]
 
     def kernel_ms(self):
         """{kernel: ms} over the runs so far (batch created with TF_BATCH_PROFILE)."""
-        out = (ctypes.c_double * 5)()
+        out = (ctypes.c_double * len(KERNELS))()
         native._check(self.L.tf_batch_kernel_ms(self.h, out), "tf_batch_kernel_ms")
-        return dict(zip(("pupdate", "spmv", "update", "ru_fold", "ru_res"), list(out)))
+        return dict(zip(KERNELS, list(out)))
 
     def remove(self, sid):
         native._check(self.L.tf_batch_remove(self.h, sid), "tf_batch_remove")

@@ -165,6 +165,45 @@ def test_batch_maxiter_reported(gpu_ctx):
         b.close()
 
 
+@pytest.mark.parametrize("profiled", [False, True], ids=["graph", "profiled"])
+def test_batch_trace_records(gpu_ctx, profiled, monkeypatch):
+    """One record per sweep: the first lists every system with its rows and
+    entries; running systems never grow; profiled sweeps (direct launches
+    with events) carry the per-kernel times and the same results."""
+    if profiled:
+        monkeypatch.setenv("TF_BATCH_PROFILE", "1")
+    sysl = mixed_systems()[:5]
+    b = batch.Batch(gpu_ctx, mem_budget=1 << 30)
+    try:
+        ids = [b.add(s, tol=TOL, maxit=20000) for s in sysl]
+        b.run()
+        tr = b.trace()
+        assert len(tr) == b.info()["sweeps"]
+        assert tr[0]["active"] == len(sysl)
+        assert tr[0]["rows"] == sum(s.n for s in sysl)
+        assert tr[0]["nnz"] == sum(s.nnz for s in sysl)
+        assert all(t["ms"] > 0 and t["items"] > 0 for t in tr)
+        assert all(a["active"] >= c["active"] and a["rows"] >= c["rows"]
+                   for a, c in zip(tr, tr[1:]))
+        total = {k: sum(t["kernel_ms"][k] for t in tr) for k in batch.KERNELS}
+        if profiled:
+            km = b.kernel_ms()
+            assert set(km) == set(batch.KERNELS)
+            assert km["spmv"] > 0 and km["update"] > 0 and km["alpha"] > 0
+            for k in batch.KERNELS:
+                assert total[k] == pytest.approx(km[k], rel=1e-9, abs=1e-9)
+            assert sum(km.values()) <= 1.05 * sum(t["ms"] for t in tr)
+        else:
+            assert all(v == 0.0 for v in total.values())
+            with pytest.raises(native.TFError):
+                b.kernel_ms()
+        for s, i in zip(sysl, ids):
+            r = b.result(i)
+            assert r["status"] == "converged" and _true_rel(s, r["x"]) <= 1.01 * TOL
+    finally:
+        b.close()
+
+
 def test_server_continuous_batching(gpu_ctx):
     """Requests arriving while others run join at the next sweep; each result
     equals the same system solved alone."""
