@@ -63,7 +63,7 @@ def parse():
                     help="default mode: systems of the batched leg (0: skip it)")
     ap.add_argument("--parts", default="all",
                     help="batched: comma list of mixed, fp64_batched, mixed_two_phase, drop_in, "
-                         "streams, pool (default all)")
+                         "streams, pool; served: pool, mixed (default all)")
     ap.add_argument("--rate", type=float, default=200.0, help="served: arrivals per second")
     ap.add_argument("--seconds", type=float, default=60.0, help="served: window length")
     ap.add_argument("--iters", type=int, default=30, help="iters: Cg iterations per solve")
@@ -182,6 +182,7 @@ def _batch_solve(ctx, sysl, **opts):
                             n_updates=r["n_updates"]))
         info = b.info()
         info["trace"] = b.trace()
+        info["upload_ms"] = {k: round(v, 1) for k, v in b.upload_ms().items()}
         if os.environ.get("TF_BATCH_PROFILE"):
             info["kernel_ms"] = b.kernel_ms()
     finally:
@@ -264,7 +265,8 @@ def batched_comparison(ctx, count, parts_arg):
                       "sweeps": info["sweeps"],
                       "iters_total": int(sum(r["iters"] for r in res)),
                       "trace_deciles": _trace_deciles(info["trace"], 4 if opts["vec_fp32"] else 8),
-                      "kernel_ms": info.get("kernel_ms")}
+                      "kernel_ms": info.get("kernel_ms"),
+                      "upload_ms": info["upload_ms"]}
     if "drop_in" in parts:
         _drop_in_solve_times(ctx, smallest[:2], 1e-10)   # warm-up
         t = _drop_in_solve_times(ctx, sysl, 1e-10)
@@ -460,6 +462,7 @@ def _serve_stream_mixed(req_sys, rhs, rate, seconds, budget, seed, max_outstandi
         f.result()
     ex.shutdown()
     st = srv.stats()
+    timing = srv.timing()
     srv.close()
     ctx.close()
     inwin = [r for r in results if r[0] + r[1] * 1e-3 <= stop_at]
@@ -474,7 +477,7 @@ def _serve_stream_mixed(req_sys, rhs, rate, seconds, budget, seed, max_outstandi
             "latency_ms_p50": float(np.percentile(lat, 50)),
             "latency_ms_p99": float(np.percentile(lat, 99)),
             "queue_ms_p50": float(np.percentile(qms, 50)),
-            "peak_running": st["peak_running"], "sweeps": st["sweeps"]}
+            "peak_running": st["peak_running"], "sweeps": st["sweeps"], "server_ms": timing}
 
 
 def run_served(args):
@@ -502,27 +505,31 @@ def run_served(args):
                        "tol 1e-10 x NRMS(b); FP64 Jacobi drop-in per request; 20 GB budget; "
                        "at most 256 requests outstanding (the rest shed)"}
     budget = 20 << 30
-    _serve_stream(req_sys, rhs, 5.0, 3.0, 8, budget, 1)          # warm-up
-    sat = _serve_stream(req_sys, rhs, args.rate, args.seconds, 8, budget, 2)
-    out["pool_8_streams"] = sat
-    out["one_at_a_time"] = _serve_stream(req_sys, rhs, args.rate, args.seconds / 2, 1,
-                                         budget, 2)
-    light = max(1.0, 0.5 * sat["solves_per_s"])
-    out["pool_8_streams_half_load"] = _serve_stream(req_sys, rhs, light, args.seconds / 2, 8,
-                                                    budget, 3)
-    out["throughput_ratio_pool_vs_one_at_a_time"] = (
-        sat["solves_per_s"] / max(out["one_at_a_time"]["solves_per_s"], 1e-9))
-    # The mixed-precision continuous-batching server on the same streams
-    # (tol: ||b - A x|| / ||b|| <= 1e-10 in FP64).
-    _serve_stream_mixed(req_sys, rhs, 5.0, 3.0, budget, 1)     # warm-up
-    mixed = _serve_stream_mixed(req_sys, rhs, args.rate, args.seconds, budget, 2)
-    out["mixed_server"] = mixed
-    out["mixed_server_half_load"] = _serve_stream_mixed(
-        req_sys, rhs, max(1.0, 0.5 * mixed["solves_per_s"]), args.seconds / 2, budget, 3)
-    out["throughput_ratio_mixed_server_vs_one_at_a_time"] = (
-        mixed["solves_per_s"] / max(out["one_at_a_time"]["solves_per_s"], 1e-9))
-    out["throughput_ratio_mixed_server_vs_pool"] = (
-        mixed["solves_per_s"] / max(sat["solves_per_s"], 1e-9))
+    parts = set(args.parts.split(",")) if args.parts != "all" else {"pool", "mixed"}
+    if "pool" in parts:
+        _serve_stream(req_sys, rhs, 5.0, 3.0, 8, budget, 1)          # warm-up
+        sat = _serve_stream(req_sys, rhs, args.rate, args.seconds, 8, budget, 2)
+        out["pool_8_streams"] = sat
+        out["one_at_a_time"] = _serve_stream(req_sys, rhs, args.rate, args.seconds / 2, 1,
+                                             budget, 2)
+        light = max(1.0, 0.5 * sat["solves_per_s"])
+        out["pool_8_streams_half_load"] = _serve_stream(req_sys, rhs, light, args.seconds / 2,
+                                                        8, budget, 3)
+        out["throughput_ratio_pool_vs_one_at_a_time"] = (
+            sat["solves_per_s"] / max(out["one_at_a_time"]["solves_per_s"], 1e-9))
+    if "mixed" in parts:
+        # The mixed-precision continuous-batching server on the same streams
+        # (tol: ||b - A x|| / ||b|| <= 1e-10 in FP64).
+        _serve_stream_mixed(req_sys, rhs, 5.0, 3.0, budget, 1)     # warm-up
+        mixed = _serve_stream_mixed(req_sys, rhs, args.rate, args.seconds, budget, 2)
+        out["mixed_server"] = mixed
+        out["mixed_server_half_load"] = _serve_stream_mixed(
+            req_sys, rhs, max(1.0, 0.5 * mixed["solves_per_s"]), args.seconds / 2, budget, 3)
+    if "pool" in parts and "mixed" in parts:
+        out["throughput_ratio_mixed_server_vs_one_at_a_time"] = (
+            mixed["solves_per_s"] / max(out["one_at_a_time"]["solves_per_s"], 1e-9))
+        out["throughput_ratio_mixed_server_vs_pool"] = (
+            mixed["solves_per_s"] / max(sat["solves_per_s"], 1e-9))
     print(json.dumps(out), flush=True)
 
 

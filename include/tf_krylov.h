@@ -241,7 +241,15 @@ enum tf_sys_status {
 int tf_batch_create(tf_ctx ctx, const tf_batch_opts* opts, tf_batch* out);
 int tf_batch_destroy(tf_batch b);
 /* Copy one system in (host arrays; x0 may be NULL for zeros).  Returns
- * TF_ERR_BUSY when the memory budget or the slots are exhausted. */
+ * TF_ERR_BUSY when the memory budget or the slots are exhausted.
+ * Systems with the same structure share one device copy of it (as a CFD
+ * time loop solves one mesh's matrix again and again with new values): the
+ * engine keeps a prepared structure (0-based CSR, renumbering, tiles) keyed
+ * by the row/col/dia addresses, n, nnz and a hash of row, dia and every
+ * 16th column index; its device copy stays resident after its systems
+ * retire and is dropped, least recently used first, when a new system
+ * needs the space.  Arrays changed in place between calls must change in
+ * those hashed entries, or be passed at other addresses. */
 int tf_batch_add(tf_batch b, int n, int64_t nnz, const int* row, const int* col,
                  const int* dia, const double* val, const double* rhs,
                  const double* x0, double tol, int maxit, int* sys);
@@ -288,12 +296,25 @@ int tf_batch_trace(tf_batch b, tf_batch_sweep* out, int cap, int* count);
  * batch was not created for profiling. */
 int tf_batch_kernel_ms(tf_batch b, double* ms8);
 int tf_batch_info(tf_batch b, int* sweeps, int* work_items, size_t* free_bytes);
+/* Where the time of tf_batch_add / tf_batch_add_many went, in milliseconds
+ * over all adds so far: host preparation (conversion, checks, renumbering,
+ * tiling) summed over the systems -- on worker threads for add_many, so it
+ * can exceed the wall time --, the admitting thread's wait for prepared
+ * systems, and admission (arena allocation and the copies to the device).
+ * Any pointer may be NULL. */
+int tf_batch_upload_ms(tf_batch b, double* prep_ms, double* wait_ms, double* admit_ms);
 
-/* Continuous batching: a worker thread admits queued requests whenever the
- * memory budget and slots allow, runs sweeps over everything admitted,
- * and retires finished systems; requests arriving while others run join at
- * the next sweep.  Submit copies the system; wait blocks until done and
- * reports end-to-end and queueing latency in milliseconds. */
+/* Continuous batching: queued requests are admitted in arrival order
+ * whenever the memory budget and slots allow, their copies made on a
+ * stream of their own while the sweeps run; every sweep iterates all
+ * admitted systems; finished systems leave at the end of their sweep and
+ * their results are copied out on a third stream.  Requests arriving while
+ * others run join at the next sweep after their copies land.  Submit
+ * copies the system (its values and right-hand side; the structure is
+ * prepared once and shared by every request with the same row/col/dia
+ * arrays -- same addresses, sizes and contents, see tf_batch_add); wait
+ * blocks until done and reports end-to-end and queueing latency in
+ * milliseconds. */
 int tf_server_create(tf_ctx ctx, const tf_batch_opts* opts, tf_server* out);
 int tf_server_submit(tf_server s, int n, int64_t nnz, const int* row,
                      const int* col, const int* dia, const double* val,
@@ -310,6 +331,14 @@ int tf_server_stats(tf_server s, long long* admitted, long long* completed,
  * TF_ERR_BUSY when the request had already finished (its result stands),
  * or TF_ERR_ARG for an unknown or collected id.  No reference counterpart. */
 int tf_server_cancel(tf_server s, int64_t req);
+/* Where the server's time went, in milliseconds since it was created, by
+ * thread: ms5[0] host preparation of submitted systems (summed over the
+ * submitting threads; a structure already prepared for an earlier request
+ * is not prepared again), ms5[1] the admission thread (reservations and
+ * uploads on its own stream), ms5[2] and ms5[3] the worker thread (commits
+ * and work-list rebuilds; sweeps from launch to the state read back), and
+ * ms5[4] the collector thread (results copied out, retirements). */
+int tf_server_timing(tf_server s, double* ms5);
 int tf_server_destroy(tf_server s);
 
 /* ---------------------------------------------------------------------------

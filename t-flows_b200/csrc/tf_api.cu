@@ -230,14 +230,12 @@ size_t tf_matrix_bytes(int n_cells, int64_t nnz) {
          up((size_t)tf::kPatMax * (tf::kPatMaxLen + 1) * 4) + 2048;
 }
 
-namespace {
-
 // Row patterns of the first ni rows: pat[i] names the offset sequence
 // (col_j - i over the row's entries, in storage order).  Returns the number
 // of patterns, or 0 when there are more than kPatMax of them or a row is
 // longer than kPatMaxLen (then the CSR columns are used).
-int find_row_patterns(const std::vector<int>& row0, const std::vector<int>& col0, int ni,
-                      std::vector<unsigned char>& pat, std::vector<int>& tab) {
+int tf_find_row_patterns(const std::vector<int>& row0, const std::vector<int>& col0, int ni,
+                         std::vector<unsigned char>& pat, std::vector<int>& tab) {
   using tf::kPatMax;
   using tf::kPatMaxLen;
   std::vector<int> offs((size_t)kPatMax * kPatMaxLen, 0), lens;
@@ -276,6 +274,9 @@ int find_row_patterns(const std::vector<int>& row0, const std::vector<int>& col0
   std::copy(lens.begin(), lens.end(), tab.begin() + (size_t)np * kPatMaxLen);
   return np;
 }
+
+namespace {
+
 
 // Largest nnz of any tile of `rows` consecutive rows among the first ni.
 // Variable tiles: consecutive rows, at most kTileRows / kTileNnzCap of the
@@ -483,7 +484,7 @@ int matrix_create_impl(tf_ctx_s* ctx, int n_cells, int n_own, int64_t nnz, const
     if (fixed != tf::kTileNone && !getenv("TF_NO_ROW_PATTERNS")) {
       std::vector<unsigned char> pat;
       std::vector<int> tab;
-      const int np = find_row_patterns(row0, col0, n_own, pat, tab);
+      const int np = tf_find_row_patterns(row0, col0, n_own, pat, tab);
       if (np > 0) {
         st = dev_alloc(ctx, &m->d_pat, pat.size());
         if (st == TF_OK) st = dev_alloc(ctx, &m->d_pat_tab, tab.size());

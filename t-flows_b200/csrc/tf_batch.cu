@@ -54,6 +54,7 @@
 #include <condition_variable>
 #include <deque>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -86,7 +87,10 @@ constexpr int kKernels = 8;
 template <typename V>
 struct SysDev {
   const int* row;       // n+1, 0-based
-  const int* col;       // nnz, 0-based local
+  const int* col;       // nnz, 0-based local (null with row patterns)
+  const unsigned char* pat;   // row patterns: one byte per row (else null)
+  const int* tab;             // their offsets, [npat][kPatMaxLen]
+  int npat;
   const double* val;    // FP64 values
   const float* val32;   // FP32 copy (use_val32)
   const int* tiles;     // ntiles+1 row boundaries
@@ -99,6 +103,7 @@ struct SysDev {
   V* q;
   V* dinv;
   double* tile_tot;     // ntiles * kPartQ: per-tile totals
+  double* chunk_tot;    // n_fin_chunks * kPartQ: chunk totals (finishing kernels)
   double* warp_part;    // FP32 values: ntiles * kWarps * kPartQ per-warp partials
   unsigned* tile_cnt;   // FP32 values: ntiles, warps of a tile that have reported
   int n, ntiles;
@@ -111,6 +116,8 @@ struct SysState {
   double rr, rr_ru, bnorm2, res_true;
   int status, iter, first, need_ru;
   int n_ru, iter_ru;   // refinements so far; iteration of the last one
+  unsigned fin_cnt;    // chunks of a finishing kernel that have reported
+  int pad;
 };
 
 struct Work {
@@ -129,6 +136,12 @@ struct RuList {
   int* count;
 };
 
+// An item of the finishing kernels: chunk `chunk` (kFinTiles tile totals)
+// of system `sys`.
+struct FinItem {
+  int sys, chunk;
+};
+
 struct BatchArgs {
   const void* desc;       // SysDev<V>*
   SysState* st;
@@ -136,8 +149,11 @@ struct BatchArgs {
   const int* nwork;
   double ru_delta2;
   RuList ru;
-  const int* sys;         // the systems of the work list (finishing kernels)
-  const int* nsys;
+  const FinItem* fin;     // the finishing kernels' items
+  const int* nfin;
+  unsigned* gate_cnt;     // CTAs of kb_beta that are done (the last opens the gate)
+  cudaGraphConditionalHandle ru_gate;   // the refinement kernels' IF node
+  int use_gate;           // 0: launched directly (no graph), the kernels always run
 };
 
 __device__ __forceinline__ bool active(const SysState& s) { return s.status == kActive; }
@@ -352,37 +368,86 @@ __global__ void __launch_bounds__(256, ew_min_blocks<V>(2)) kb_update(BatchArgs 
   }
 }
 
-// The finishing kernels: one CTA of kFinThreads per listed system (a
-// grid-stride loop over the system list).
+// The finishing kernels: one CTA of kFinThreads per item (a grid-stride
+// loop over the list), an item being a chunk of kFinTiles tile totals of a
+// system; a system of more than one chunk is finished by the CTA of its
+// last chunk to report.
 constexpr int kFinThreads = 256;
+constexpr int kFinPer = 8;                          // tile totals per thread
+constexpr int kFinTiles = kFinThreads * kFinPer;    // per item
 
-// A system's totals from its tile totals: thread t adds tiles t,
-// t + kFinThreads, ... in turn, each warp sums its lanes (butterfly), and
-// every warp then sums the warps' results in warp order, so all threads
-// hold the same bits.  The order depends only on the system's tiling.
-// Whole CTA (two barriers).
-template <int NQ, typename V>
-__device__ __forceinline__ void sum_tiles(const SysDev<V>& d, double (&v)[NQ]) {
+__host__ __device__ __forceinline__ int fin_chunks(int ntiles) {
+  return (ntiles + kFinTiles - 1) / kFinTiles;
+}
+
+// v (every thread) = the CTA's sum of w: each warp sums its lanes
+// (butterfly), then every warp sums the warps' results in warp order.
+template <int NQ>
+__device__ __forceinline__ void cta_sum(double (&w)[NQ], double (&v)[NQ]) {
   constexpr int kW = kFinThreads / 32;
   __shared__ double part[NQ][kW];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double acc[NQ];
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
-#pragma unroll 4
-  for (int t = threadIdx.x; t < d.ntiles; t += kFinThreads)
-#pragma unroll
-    for (int q = 0; q < NQ; ++q)
-      acc[q] = __dadd_rn(acc[q], __ldcg(d.tile_tot + (size_t)t * kPartQ + q));
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
-    acc[q] = warp_sum(acc[q]);
-    if (lane == 0) part[q][warp] = acc[q];
+    const double s = warp_sum(w[q]);
+    if (lane == 0) part[q][warp] = s;
   }
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < NQ; ++q) v[q] = warp_sum(lane < kW ? part[q][lane] : 0.0);
-  __syncthreads();   // part is reused by the next system
+  __syncthreads();   // part is reused
+}
+
+// A system's totals from its tile totals, chunk by chunk: the CTA of item
+// (sys, chunk) loads the chunk's tile totals (thread t takes tiles t,
+// t + kFinThreads, ..., all loads issued before the first add) and sums
+// them with cta_sum; a one-chunk system is done here.  Otherwise the chunk
+// total is stored and the chunk's CTA reports on the system's counter; the
+// last to report sums the chunk totals in chunk order.  The order depends
+// only on the system's tiling.  Returns true (CTA-uniform) in the CTA that
+// holds the system's totals in v.
+template <int NQ, typename V>
+__device__ bool finish_sum(const SysDev<V>& d, unsigned* cnt, int chunk, double (&v)[NQ]) {
+  __shared__ int last_sh;
+  const int t0 = chunk * kFinTiles, t1 = min(d.ntiles, t0 + kFinTiles);
+  double ld[kFinPer][NQ];
+#pragma unroll
+  for (int k = 0; k < kFinPer; ++k) {
+    const int t = t0 + (int)threadIdx.x + k * kFinThreads;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+      ld[k][q] = t < t1 ? __ldcg(d.tile_tot + (size_t)t * kPartQ + q) : 0.0;
+  }
+  double w[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    w[q] = 0.0;
+#pragma unroll
+    for (int k = 0; k < kFinPer; ++k) w[q] = __dadd_rn(w[q], ld[k][q]);
+  }
+  cta_sum<NQ>(w, v);
+  const int nch = fin_chunks(d.ntiles);
+  if (nch == 1) return true;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) d.chunk_tot[(size_t)chunk * kPartQ + q] = v[q];
+    __threadfence();
+    last_sh = atomicAdd(cnt, 1u) == (unsigned)nch - 1;
+  }
+  __syncthreads();
+  const bool last = last_sh;
+  __syncthreads();   // last_sh is reused
+  if (!last) return false;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) w[q] = 0.0;
+  for (int c = threadIdx.x; c < nch; c += kFinThreads)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+      w[q] = __dadd_rn(w[q], __ldcg(d.chunk_tot + (size_t)c * kPartQ + q));
+  cta_sum<NQ>(w, v);
+  if (threadIdx.x == 0) *cnt = 0u;   // ready for the next finishing kernel
+  return true;
 }
 
 // Per system after kb_update: rho, beta, the iteration count and the
@@ -392,14 +457,15 @@ template <typename V>
 __global__ void __launch_bounds__(kFinThreads) kb_beta(BatchArgs a) {
   const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
   __shared__ int base_sh;
-  const int ns = *a.nsys;
-  for (int k = blockIdx.x; k < ns; k += gridDim.x) {
-    const int sys = a.sys[k];
+  const int nf = *a.nfin;
+  for (int k = blockIdx.x; k < nf; k += gridDim.x) {
+    const FinItem it = a.fin[k];
+    const int sys = it.sys;
     SysState& s = a.st[sys];
     if (!active(s)) continue;   // CTA-uniform
     const SysDev<V>& d = D[sys];
     double v[2];
-    sum_tiles<2>(d, v);
+    if (!finish_sum<2>(d, &s.fin_cnt, it.chunk, v)) continue;
     if (threadIdx.x == 0) {
       int base = -1;
       s.rho_old = s.rho;
@@ -429,6 +495,20 @@ __global__ void __launch_bounds__(kFinThreads) kb_beta(BatchArgs a) {
         a.ru.items[base + t] = Work{sys, t, d.tiles[t], d.tiles[t + 1],
                                     d.row[d.tiles[t]], d.row[d.tiles[t + 1]]};
   }
+  // The last CTA opens the refinement kernels' gate when any system is due
+  // an update (or was admitted and waits for its first residual).
+  if (a.use_gate) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (atomicAdd(a.gate_cnt, 1u) == gridDim.x - 1) {
+        *a.gate_cnt = 0u;
+        __threadfence();
+        const int due = *(volatile int*)a.ru.count;
+        cudaGraphSetConditional(a.ru_gate, due > 0 ? 1u : 0u);
+      }
+    }
+  }
 }
 
 // Per system after kb_spmv: alpha = rho / p.q (breakdown when p.q <= 0 or
@@ -436,13 +516,13 @@ __global__ void __launch_bounds__(kFinThreads) kb_beta(BatchArgs a) {
 template <typename V>
 __global__ void __launch_bounds__(kFinThreads) kb_alpha(BatchArgs a) {
   const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
-  const int ns = *a.nsys;
-  for (int k = blockIdx.x; k < ns; k += gridDim.x) {
-    const int sys = a.sys[k];
-    SysState& s = a.st[sys];
+  const int nf = *a.nfin;
+  for (int k = blockIdx.x; k < nf; k += gridDim.x) {
+    const FinItem it = a.fin[k];
+    SysState& s = a.st[it.sys];
     if (!active(s)) continue;   // CTA-uniform
     double v[1];
-    sum_tiles<1>(D[sys], v);
+    if (!finish_sum<1>(D[it.sys], &s.fin_cnt, it.chunk, v)) continue;
     if (threadIdx.x == 0) {
       if (!(v[0] > 0.0)) s.status = kBreakdown;
       else s.alpha = __ddiv_rn(s.rho, v[0]);
@@ -541,6 +621,7 @@ struct SpmvWork {
 // which items have nothing to do in this launch.
 template <typename V, int KIND>
 struct BatchTiles {
+  static constexpr bool kRowPatterns = true;   // structured systems' tiles
   const SysDev<V>* D;
   const SysState* st;
   const Work* work;
@@ -552,6 +633,9 @@ struct BatchTiles {
     TileDesc t;
     t.row = d.row;
     t.col = d.col;
+    t.pat = d.pat;
+    t.tab = d.tab;
+    t.npat = d.npat;
     t.val = d.val;
     t.r0 = w.r0;
     t.r1 = w.r1;
@@ -745,14 +829,14 @@ __global__ void __launch_bounds__(kCsr2RedThreads, 2) kb_ru_res(BatchArgs a) {
 template <typename V>
 __global__ void __launch_bounds__(kFinThreads) kb_ru_finish(BatchArgs a) {
   const SysDev<V>* D = static_cast<const SysDev<V>*>(a.desc);
-  const int ns = *a.nsys;
-  for (int k = blockIdx.x; k < ns; k += gridDim.x) {
-    const int sys = a.sys[k];
-    SysState& s = a.st[sys];
+  const int nf = *a.nfin;
+  for (int k = blockIdx.x; k < nf; k += gridDim.x) {
+    const FinItem it = a.fin[k];
+    SysState& s = a.st[it.sys];
     if (!(s.status == kInit || (s.status == kActive && s.need_ru))) continue;   // CTA-uniform
     double v[3];
-    sum_tiles<3>(D[sys], v);
-    if (threadIdx.x == 0) res_finish(s, D[sys], v);
+    if (!finish_sum<3>(D[it.sys], &s.fin_cnt, it.chunk, v)) continue;
+    if (threadIdx.x == 0) res_finish(s, D[it.sys], v);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) *a.ru.count = 0;
 }
@@ -809,148 +893,209 @@ struct Arena {
   }
 };
 
-// Host copy of one system, converted and tiled, ready to upload.
-struct HostSys {
+// ---------------------------------------------------------------------------
+// Host preparation
+// ---------------------------------------------------------------------------
+// A matrix structure as the engine iterates it: 0-based CSR (renumbered by
+// reverse Cuthill-McKee when the caller's numbering scatters the gathers;
+// every row keeps its entries in storage order, so row sums are those of
+// the caller's matrix) and its row tiles.  Once a system using it is
+// admitted, one device copy in the arena serves every system with the same
+// structure; the engine keeps it resident after they retire (a structure
+// cache keyed by the caller's arrays) until the memory is needed.
+struct Structure {
   int n = 0;
   long long nnz = 0;
-  std::vector<int> row, col, dia, tiles;
-  std::vector<double> val, b, x0;
-  std::vector<float> val32;
-  std::vector<int> perm;   // renumbered: row i here is row perm[i] of the caller's
-  double tol = 1e-10;
-  int maxit = 10000;
+  std::vector<int> row, dia;   // 0-based, n + 1 + 8 and n + 8
+  std::vector<int> col;        // 0-based, nnz + 8; freed once on the device
+  std::vector<int> tiles;      // row boundaries of the tiles
+  std::vector<int> tile_j;     // entry boundaries of the tiles (row[tiles[t]])
+  std::vector<int> perm;       // renumbered: row i is the caller's row perm[i]
+  // Row patterns (npat > 0): on the device these replace the columns.
+  int npat = 0;
+  std::vector<unsigned char> pat;
+  std::vector<int> tab;
+  // engine lock from here on
+  int ready = 0;               // 0 being prepared, 1 prepared, < 0 -(its error status)
+  bool resident = false;       // a device copy exists (or is being uploaded)
+  size_t off = 0, bytes = 0, o_row = 0, o_col = 0, o_dia = 0, o_tiles = 0, o_pat = 0,
+         o_tab = 0;
+  int users = 0;               // admitted systems reading the device copy
+  uint64_t last_use = 0;       // eviction order: least recently used first
+  int ntiles() const { return (int)tiles.size() - 1; }
 };
 
-int prepare_host_impl(HostSys& h, int n, long long nnz, const int* row, const int* col,
-                      const int* dia, const double* val, const double* b, const double* x0,
-                      double tol, int maxit, int use_val32) {
-  if (n < 1 || nnz < n || !row || !col || !dia || !val || !b) return TF_ERR_ARG;
+// The structure cache's key: the caller's arrays (addresses and sizes) and
+// a 64-bit FNV-1a hash of row and dia and of every 16th column index (and
+// the last 16).  A structure changed in place at the same addresses in
+// those entries is seen as new.
+struct StructKey {
+  const int* row;
+  const int* col;
+  const int* dia;
+  int n;
+  long long nnz;
+  uint64_t hash;
+  bool operator<(const StructKey& o) const {
+    return std::tie(row, col, dia, n, nnz, hash) <
+           std::tie(o.row, o.col, o.dia, o.n, o.nnz, o.hash);
+  }
+};
+
+inline uint64_t fnv1a(uint64_t h, const int* p, long long count, long long step) {
+  for (long long i = 0; i < count; i += step) {
+    h ^= (uint32_t)p[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+StructKey struct_key(int n, long long nnz, const int* row, const int* col, const int* dia) {
+  uint64_t h = 1469598103934665603ull;
+  h = fnv1a(h, row, (long long)n + 1, 1);
+  h = fnv1a(h, dia, n, 1);
+  h = fnv1a(h, col, nnz, 16);
+  const long long tail = std::min<long long>(nnz, 16);
+  h = fnv1a(h, col + (nnz - tail), tail, 1);
+  return StructKey{row, col, dia, n, nnz, h};
+}
+
+// Checks the caller's 1-based Matrix_Type structure, converts it, renumbers
+// a scattered numbering, cuts the tiles and, with want_patterns, replaces
+// the columns by row patterns where every row fits one of kPatMax patterns
+// (structured hex blocks: 1 byte per row instead of 4 per entry).
+int prepare_structure(Structure& S, int n, long long nnz, const int* row, const int* col,
+                      const int* dia, bool want_patterns) {
+  if (n < 1 || nnz < n || !row || !col || !dia) return TF_ERR_ARG;
   if (row[0] != 1 || (long long)row[n] - 1 != nnz) return TF_ERR_LAYOUT;
-  h.n = n;
-  h.nnz = nnz;
-  h.tol = tol;
-  h.maxit = maxit;
-  h.row.resize((size_t)n + 1 + 8);
-  h.col.resize((size_t)nnz + 8);
-  h.dia.resize((size_t)n + 8);
-  for (int i = 0; i <= n; ++i) h.row[i] = row[i] - 1;
-  for (size_t i = n + 1; i < h.row.size(); ++i) h.row[i] = h.row[n];
+  S.n = n;
+  S.nnz = nnz;
+  S.row.resize((size_t)n + 1 + 8);
+  S.col.resize((size_t)nnz + 8);
+  S.dia.resize((size_t)n + 8);
+  for (int i = 0; i <= n; ++i) S.row[i] = row[i] - 1;
+  for (size_t i = n + 1; i < S.row.size(); ++i) S.row[i] = S.row[n];
   for (long long j = 0; j < nnz; ++j) {
     if (col[j] < 1 || col[j] > n) return TF_ERR_LAYOUT;
-    h.col[j] = col[j] - 1;
+    S.col[j] = col[j] - 1;
   }
   for (int i = 0; i < n; ++i) {
-    if (h.row[i + 1] < h.row[i]) return TF_ERR_LAYOUT;
+    if (S.row[i + 1] < S.row[i]) return TF_ERR_LAYOUT;
     const int d = dia[i] - 1;
-    if (d < h.row[i] || d >= h.row[i + 1] || h.col[d] != i) return TF_ERR_LAYOUT;
-    h.dia[i] = d;
+    if (d < S.row[i] || d >= S.row[i + 1] || S.col[d] != i) return TF_ERR_LAYOUT;
+    S.dia[i] = d;
   }
-  // Scattered numbering: renumber by reverse Cuthill-McKee, each row keeping
-  // its entries (and values) in storage order (the same row sums; see
-  // tf_renumber.cu).
-  bool have_val = false;
-  h.perm.clear();
+  // Scattered numbering: renumber by reverse Cuthill-McKee (see
+  // tf_renumber.cu); kept when it cuts the gathered lines by 20 %.
+  S.perm.clear();
   if (n >= kRenumberMinRows && !getenv("TF_NO_RENUMBER")) {
-    const double before = tf_gather_lines_per_warp(h.row.data(), h.col.data(), n, 0);
+    const double before = tf_gather_lines_per_warp(S.row.data(), S.col.data(), n, 0);
     if (before > kRenumberLines) {
       std::vector<int> order, inv(n);
-      tf_rcm_order(h.row, h.col, n, order);
+      tf_rcm_order(S.row, S.col, n, order);
       for (int i = 0; i < n; ++i) inv[order[i]] = i;
-      std::vector<int> row2(h.row.size()), col2(h.col.size(), 0), dia2(h.dia.size(), 0);
-      std::vector<double> val2((size_t)nnz + 8, 0.0);
+      std::vector<int> row2(S.row.size()), col2(S.col.size(), 0), dia2(S.dia.size(), 0);
       row2[0] = 0;
       for (int i = 0; i < n; ++i) {
-        const int o = order[i], js = h.row[o], len = h.row[o + 1] - js;
+        const int o = order[i], js = S.row[o], len = S.row[o + 1] - js;
         const int r = row2[i];
-        for (int k = 0; k < len; ++k) {
-          col2[r + k] = inv[h.col[js + k]];
-          val2[r + k] = val[js + k];
-        }
-        dia2[i] = r + (h.dia[o] - js);
+        for (int k = 0; k < len; ++k) col2[r + k] = inv[S.col[js + k]];
+        dia2[i] = r + (S.dia[o] - js);
         row2[i + 1] = r + len;
       }
       for (size_t i = n + 1; i < row2.size(); ++i) row2[i] = row2[n];
       if (tf_gather_lines_per_warp(row2.data(), col2.data(), n, 0) <= 0.8 * before) {
-        h.row.swap(row2);
-        h.col.swap(col2);
-        h.dia.swap(dia2);
-        h.perm.swap(order);
-        h.val.swap(val2);
-        have_val = true;
+        S.row.swap(row2);
+        S.col.swap(col2);
+        S.dia.swap(dia2);
+        S.perm.swap(order);
       }
     }
   }
   // tiles: <= kRows rows and <= kNnzCap entries each
-  h.tiles.clear();
-  h.tiles.push_back(0);
+  S.tiles.clear();
+  S.tiles.push_back(0);
   int r0 = 0;
   while (r0 < n) {
     int r1 = r0;
-    while (r1 < n && r1 - r0 < kRows && h.row[r1 + 1] - h.row[r0] <= kNnzCap) ++r1;
+    while (r1 < n && r1 - r0 < kRows && S.row[r1 + 1] - S.row[r0] <= kNnzCap) ++r1;
     if (r1 == r0) return TF_ERR_LAYOUT;   // one row longer than a tile stage
     // A tile cut short by its entry cap between kRows/2 and kRows rows is
     // trimmed to kRows/2, so the streamer can give each row 2 threads;
     // shorter tiles keep their rows (2 or 4 threads per row as they are:
     // halving them would double the per-tile costs).
     if (r1 < n && r1 - r0 > kRows / 2 && r1 - r0 < kRows) r1 = r0 + kRows / 2;
-    h.tiles.push_back(r1);
+    S.tiles.push_back(r1);
     r0 = r1;
   }
-  if (!have_val) {
+  S.tile_j.resize(S.tiles.size());
+  for (size_t t = 0; t < S.tiles.size(); ++t) S.tile_j[t] = S.row[S.tiles[t]];
+  S.npat = want_patterns ? tf_find_row_patterns(S.row, S.col, n, S.pat, S.tab) : 0;
+  if (S.npat == 0) {
+    S.pat.clear();
+    S.tab.clear();
+  }
+  return TF_OK;
+}
+
+// One system ready to upload: its structure (shared) and its values,
+// right-hand side and start vector in the structure's row order.
+struct HostSys {
+  std::shared_ptr<Structure> st;
+  StructKey key{};
+  int n = 0;
+  long long nnz = 0;
+  std::vector<double> val, b, x0;
+  std::vector<float> val32;
+  double tol = 1e-10;
+  int maxit = 10000;
+};
+
+// The per-system arrays of h in S's order (val permuted row by row with the
+// structure when it was renumbered).
+int prepare_values(HostSys& h, const Structure& S, const int* row, const double* val,
+                   const double* b, const double* x0, int use_val32) {
+  if (!val || !b) return TF_ERR_ARG;
+  const int n = S.n;
+  const long long nnz = S.nnz;
+  h.n = n;
+  h.nnz = nnz;
+  if (S.perm.empty()) {
     h.val.assign(val, val + nnz);
     h.val.resize((size_t)nnz + 8, 0.0);
+    h.b.assign(b, b + n);
+    if (x0) h.x0.assign(x0, x0 + n);
+    else h.x0.assign(n, 0.0);
+  } else {
+    h.val.assign((size_t)nnz + 8, 0.0);
+    h.b.resize(n);
+    h.x0.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+      const int o = S.perm[i];
+      const long long js = row[o] - 1, len = row[o + 1] - row[o];
+      std::copy(val + js, val + js + len, h.val.begin() + S.row[i]);
+      h.b[i] = b[o];
+      if (x0) h.x0[i] = x0[o];
+    }
   }
   if (use_val32) {
     h.val32.resize((size_t)nnz + 8);
     for (long long j = 0; j < nnz + 8; ++j) h.val32[j] = (float)h.val[j];
   }
-  if (h.perm.empty()) {
-    h.b.assign(b, b + n);
-    if (x0) h.x0.assign(x0, x0 + n);
-    else h.x0.assign(n, 0.0);
-  } else {
-    h.b.resize(n);
-    h.x0.assign(n, 0.0);
-    for (int i = 0; i < n; ++i) {
-      h.b[i] = b[h.perm[i]];
-      if (x0) h.x0[i] = x0[h.perm[i]];
-    }
-  }
   return TF_OK;
 }
 
-// prepare_host_impl without exceptions across the C ABI: a host
-// allocation that fails is TF_ERR_OOM.
-int prepare_host(HostSys& h, int n, long long nnz, const int* row, const int* col,
-                 const int* dia, const double* val, const double* b, const double* x0,
-                 double tol, int maxit, int use_val32) {
-  try {
-    return prepare_host_impl(h, n, nnz, row, col, dia, val, b, x0, tol, maxit, use_val32);
-  } catch (const std::bad_alloc&) {
-    h = HostSys();
-    return TF_ERR_OOM;
-  } catch (const std::length_error&) {
-    h = HostSys();
-    return TF_ERR_OOM;
-  }
-}
-
-// Byte layout of one system's segment.
+// Byte layout of one system's own segment (its structure lives in a
+// segment of its own, shared).
 struct Layout {
-  size_t row, col, dia, tiles, val, val32, b, x, xlo, r, p, q, dinv, tile_tot, warp_part,
-      tile_cnt, total;
+  size_t val, val32, b, x, xlo, r, p, q, dinv, tile_tot, chunk_tot, warp_part, tile_cnt, total;
 };
 
-Layout layout_for(const HostSys& h, size_t vsz, int use_val32) {
+Layout layout_for(const HostSys& h, int ntiles, size_t vsz, int use_val32) {
   Layout L{};
   size_t o = 0;
   auto take = [&](size_t bytes) { size_t r = o; o = Arena::up(o + bytes); return r; };
   const size_t n8 = (size_t)h.n + 8;
-  const int ntiles = (int)h.tiles.size() - 1;
-  L.row = take(h.row.size() * 4);
-  L.col = take(h.col.size() * 4);
-  L.dia = take(h.dia.size() * 4);
-  L.tiles = take(h.tiles.size() * 4);
   L.val = take(h.val.size() * 8);
   L.val32 = use_val32 ? take(h.val32.size() * 4) : 0;
   L.b = take(n8 * 8);
@@ -961,6 +1106,7 @@ Layout layout_for(const HostSys& h, size_t vsz, int use_val32) {
   L.q = take(n8 * vsz);
   L.dinv = take(n8 * vsz);
   L.tile_tot = take((size_t)ntiles * kPartQ * 8);
+  L.chunk_tot = take((size_t)fin_chunks(ntiles) * kPartQ * 8);
   if (use_val32) {   // the FP32-value SpMV's per-warp partials
     L.warp_part = take((size_t)ntiles * kWarps * kPartQ * 8);
     L.tile_cnt = take((size_t)ntiles * 4);
@@ -970,14 +1116,20 @@ Layout layout_for(const HostSys& h, size_t vsz, int use_val32) {
 }
 
 struct Slot {
-  int used = 0;
+  int used = 0;            // 1: admitted; 2: reserved, its copies in flight;
+                           // 3: out of the work list, its result being copied out
   size_t off = 0, bytes = 0;
   int n = 0, ntiles = 0;
   double done_ms = -1.0;   // wall time from tf_batch_run's start to completion
   Layout L{};
-  std::vector<int> tiles;  // row boundaries of the tiles (host copy)
-  std::vector<int> tile_j; // entry boundaries of the tiles (row[tiles[t]])
-  std::vector<int> perm;   // renumbered system: device row i is caller row perm[i]
+  std::shared_ptr<Structure> st;
+};
+
+// A slot and arena space held for a system whose copies are in flight.
+struct Reservation {
+  int slot = -1;
+  bool new_struct = false;   // this system uploads its structure
+  Layout L{};
 };
 
 }  // namespace tfb
@@ -1001,15 +1153,17 @@ struct tf_batch_s {
   int* d_nwork = nullptr;
   Work* d_ru = nullptr;          // refinement work list (same capacity)
   int* d_ru_count = nullptr;
-  int* d_sys = nullptr;          // the systems of the work list
-  int* d_nsys = nullptr;
-  std::vector<int> h_sys;
+  FinItem* d_fin = nullptr;      // the finishing kernels' items
+  int* d_nfin = nullptr;
+  unsigned* d_gate_cnt = nullptr;
+  int fin_cap = 0;
+  std::vector<FinItem> h_fin;
   int work_cap = 0;
   std::vector<Work> h_work, h_ru;
   int nwork = 0;
   long long work_rows = 0, work_nnz = 0;   // rows and entries of the listed systems
   cudaGraphExec_t sweep = nullptr;
-  int grid_pupdate = 1, grid_update = 1, grid_fold = 1, grid_tile = 1, grid_sys = 1;
+  int grid_pupdate = 1, grid_update = 1, grid_fold = 1, grid_tile = 1, grid_fin = 1;
   int sweeps = 0;
   long long total_iters = 0;
   // Per sweep of the last tf_batch_run (tf_batch_sweep): systems running at
@@ -1017,6 +1171,9 @@ struct tf_batch_s {
   // wall time of the sweep (launch to state read), kernel times (profiling).
   std::vector<tf_batch_sweep> trace;
   double sweep_kms[kKernels] = {};   // the last profiled sweep's kernel times
+  // Upload time over all adds (tf_batch_upload_ms): host preparation summed
+  // over the systems, the admitting thread's wait for it, and admission.
+  double up_prep_ms = 0.0, up_wait_ms = 0.0, up_admit_ms = 0.0;
 
   ~tf_batch_s() {
     cudaSetDevice(ctx->device);
@@ -1024,7 +1181,7 @@ struct tf_batch_s {
     if (sweep) cudaGraphExecDestroy(sweep);
     if (arena.base) cudaFree(arena.base);
     for (void* p : {d_desc, (void*)d_state, (void*)d_work, (void*)d_nwork, (void*)d_ru,
-                    (void*)d_ru_count, (void*)d_sys, (void*)d_nsys})
+                    (void*)d_ru_count, (void*)d_fin, (void*)d_nfin, (void*)d_gate_cnt})
       if (p) cudaFree(p);
     if (h_state) cudaFreeHost(h_state);
   }
@@ -1035,36 +1192,52 @@ struct tf_batch_s {
   static size_t smem_rows32() { return TileLayout<kRows, kNnzCap, float, kStages>::kSmemBytes; }
 
   BatchArgs args() const {
-    return BatchArgs{d_desc, d_state, d_work, d_nwork, opts.ru_delta * opts.ru_delta,
-                     RuList{d_ru, d_ru_count}, d_sys, d_nsys};
+    return BatchArgs{d_desc,     d_state, d_work, d_nwork, opts.ru_delta * opts.ru_delta,
+                     RuList{d_ru, d_ru_count}, d_fin, d_nfin, d_gate_cnt, 0, 0};
   }
 
-  // The kernels of one iteration (the order of tf_batch_kernel_ms).  ev
-  // (profiling only): events recorded before each kernel and after the last.
+  // The kernels of an iteration, in launch order (tf_batch_kernel_ms).
+  struct Launch {
+    const void* fn;
+    int grid, block;
+    size_t smem;
+  };
   template <typename V>
-  void launch_iteration(cudaStream_t s, const BatchArgs& a, cudaEvent_t* ev = nullptr) {
+  std::vector<Launch> iteration_kernels() const {
+    const void* spmv = opts.val_fp32         ? (const void*)kb_spmv<V, float, 0>
+                       : opts.two_phase_rows ? (const void*)kb_spmv<V, double, 0>
+                                             : (const void*)kb_spmv<V, double, -1>;
+    const int spmv_block = opts.val_fp32 ? kRows : kCsr2RedThreads;
+    const size_t spmv_smem = opts.val_fp32 ? smem_rows32() : smem_csr2();
+    const void* ru_res = opts.two_phase_rows ? (const void*)kb_ru_res<V, 0>
+                                             : (const void*)kb_ru_res<V, -1>;
+    return {{(const void*)kb_pupdate<V>, grid_pupdate, 256, 0},
+            {spmv, grid_tile, spmv_block, spmv_smem},
+            {(const void*)kb_alpha<V>, grid_fin, kFinThreads, 0},
+            {(const void*)kb_update<V>, grid_update, 256, 0},
+            {(const void*)kb_beta<V>, grid_fin, kFinThreads, 0},
+            {(const void*)kb_ru_fold<V>, grid_fold, 256, 0},
+            {ru_res, grid_tile, kCsr2RedThreads, smem_csr2()},
+            {(const void*)kb_ru_finish<V>, grid_fin, kFinThreads, 0}};
+  }
+  // The last three (fold, FP64 residual, test) run only when a system is
+  // due a refinement: in the sweep graph they sit in an IF node that
+  // kb_beta's last CTA opens.
+  static constexpr int kFirstRuKernel = 5;
+
+  // Direct launches of one iteration (profiling: ev receives an event before
+  // each kernel and after the last).
+  template <typename V>
+  int launch_iteration(cudaStream_t s, const BatchArgs& a, cudaEvent_t* ev) {
+    const std::vector<Launch> ks = iteration_kernels<V>();
     int e = 0;
-    auto mark = [&]() { if (ev) cudaEventRecord(ev[e++], s); };
-    mark();
-    kb_pupdate<V><<<grid_pupdate, 256, 0, s>>>(a);
-    mark();
-    if (opts.val_fp32) kb_spmv<V, float, 0><<<grid_tile, kRows, smem_rows32(), s>>>(a);
-    else if (opts.two_phase_rows) kb_spmv<V, double, 0><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
-    else kb_spmv<V, double, -1><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
-    mark();
-    kb_alpha<V><<<grid_sys, kFinThreads, 0, s>>>(a);
-    mark();
-    kb_update<V><<<grid_update, 256, 0, s>>>(a);
-    mark();
-    kb_beta<V><<<grid_sys, kFinThreads, 0, s>>>(a);
-    mark();
-    kb_ru_fold<V><<<grid_fold, 256, 0, s>>>(a);
-    mark();
-    if (opts.two_phase_rows) kb_ru_res<V, 0><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
-    else kb_ru_res<V, -1><<<grid_tile, kCsr2RedThreads, smem_csr2(), s>>>(a);
-    mark();
-    kb_ru_finish<V><<<grid_sys, kFinThreads, 0, s>>>(a);
-    mark();
+    for (const Launch& k : ks) {
+      if (ev) cudaEventRecord(ev[e++], s);
+      void* kp[] = {const_cast<BatchArgs*>(&a)};
+      TF_CUDA_TRY(cudaLaunchKernel(k.fn, dim3(k.grid), dim3(k.block), kp, k.smem, s));
+    }
+    if (ev) cudaEventRecord(ev[e], s);
+    return TF_OK;
   }
 
   // Profiling (TF_BATCH_PROFILE set when the batch was created): sweeps run
@@ -1079,10 +1252,10 @@ struct tf_batch_s {
     std::vector<cudaEvent_t> ev(kEv * opts.sweep_iters);
     for (auto& e : ev) TF_CUDA_TRY(cudaEventCreate(&e));
     for (int it = 0; it < opts.sweep_iters; ++it) {
-      if (vsz == 4) launch_iteration<float>(s, a, &ev[kEv * it]);
-      else launch_iteration<double>(s, a, &ev[kEv * it]);
+      const int st = vsz == 4 ? launch_iteration<float>(s, a, &ev[kEv * it])
+                              : launch_iteration<double>(s, a, &ev[kEv * it]);
+      if (st != TF_OK) return st;
     }
-    TF_CUDA_TRY(cudaGetLastError());
     TF_CUDA_TRY(cudaMemcpyAsync(h_state, d_state, (size_t)max_sys * sizeof(SysState),
                                 cudaMemcpyDeviceToHost, s));
     TF_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1124,7 +1297,7 @@ struct tf_batch_s {
     if (st == TF_OK) st = resident((const void*)kb_update<V>, &grid_update);
     if (st == TF_OK) st = resident((const void*)kb_ru_fold<V>, &grid_fold);
     if (st != TF_OK) return st;
-    grid_sys = std::max(1, std::min(max_sys, ctx->sm_count * 8));   // one CTA per system
+    grid_fin = ctx->sm_count * 4;
     return TF_OK;
   }
 
@@ -1133,19 +1306,57 @@ struct tf_batch_s {
       cudaGraphExecDestroy(sweep);
       sweep = nullptr;
     }
-    cudaStream_t s = ctx->stream;
-    const BatchArgs a = args();
     cudaGraph_t g = nullptr;
-    TF_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    for (int it = 0; it < opts.sweep_iters; ++it) {
-      if (vsz == 4) launch_iteration<float>(s, a);
-      else launch_iteration<double>(s, a);
-    }
-    cudaError_t e = cudaStreamEndCapture(s, &g);
-    TF_CUDA_TRY(e);
-    e = cudaGraphInstantiate(&sweep, g, 0);
+    TF_CUDA_TRY(cudaGraphCreate(&g, 0));
+    const int st = vsz == 4 ? add_sweep_nodes<float>(g) : add_sweep_nodes<double>(g);
+    cudaError_t e = cudaSuccess;
+    if (st == TF_OK) e = cudaGraphInstantiate(&sweep, g, 0);
     cudaGraphDestroy(g);
+    if (st != TF_OK) return st;
     TF_CUDA_TRY(e);
+    return TF_OK;
+  }
+
+  // A sweep as a graph: per iteration pupdate -> spmv -> alpha -> update ->
+  // beta -> IF(gate){ fold -> residual -> test }, each iteration's IF node
+  // with a conditional handle of its own (kb_beta of that iteration sets it).
+  template <typename V>
+  int add_sweep_nodes(cudaGraph_t g) {
+    const std::vector<Launch> ks = iteration_kernels<V>();
+    auto add = [](cudaGraph_t gr, const Launch& k, const BatchArgs* a, cudaGraphNode_t dep,
+                  cudaGraphNode_t* out) {
+      cudaKernelNodeParams p{};
+      p.func = const_cast<void*>(k.fn);
+      p.gridDim = dim3(k.grid);
+      p.blockDim = dim3(k.block);
+      p.sharedMemBytes = (unsigned)k.smem;
+      void* kp[] = {const_cast<BatchArgs*>(a)};
+      p.kernelParams = kp;
+      return cudaGraphAddKernelNode(out, gr, dep ? &dep : nullptr, dep ? 1 : 0, &p);
+    };
+    cudaGraphNode_t dep = nullptr;
+    for (int it = 0; it < opts.sweep_iters; ++it) {
+      BatchArgs a = args();
+      cudaError_t e = cudaGraphConditionalHandleCreate(&a.ru_gate, g, 0,
+                                                       cudaGraphCondAssignDefault);
+      a.use_gate = 1;
+      for (int k = 0; k < kFirstRuKernel && e == cudaSuccess; ++k) e = add(g, ks[k], &a, dep, &dep);
+      cudaGraphNodeParams cp{};
+      if (e == cudaSuccess) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = a.ru_gate;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&dep, g, &dep, 1, &cp);
+      }
+      cudaGraphNode_t bdep = nullptr;
+      for (int k = kFirstRuKernel; k < kKernels && e == cudaSuccess; ++k)
+        e = add(cp.conditional.phGraph_out[0], ks[k], &a, bdep, &bdep);
+      if (e != cudaSuccess) {
+        tf_set_last_cuda_error(e, "batch sweep graph", __FILE__, __LINE__);
+        return TF_ERR_CUDA;
+      }
+    }
     return TF_OK;
   }
 
@@ -1183,54 +1394,246 @@ struct tf_batch_s {
     TF_CUDA_TRY(cudaMemset(d_nwork, 0, sizeof(int)));
     TF_CUDA_TRY(cudaMalloc((void**)&d_ru_count, sizeof(int)));
     TF_CUDA_TRY(cudaMemset(d_ru_count, 0, sizeof(int)));
-    TF_CUDA_TRY(cudaMalloc((void**)&d_sys, (size_t)max_sys * sizeof(int)));
-    TF_CUDA_TRY(cudaMalloc((void**)&d_nsys, sizeof(int)));
-    TF_CUDA_TRY(cudaMemset(d_nsys, 0, sizeof(int)));
+    TF_CUDA_TRY(cudaMalloc((void**)&d_nfin, sizeof(int)));
+    TF_CUDA_TRY(cudaMemset(d_nfin, 0, sizeof(int)));
+    TF_CUDA_TRY(cudaMalloc((void**)&d_gate_cnt, sizeof(unsigned)));
+    TF_CUDA_TRY(cudaMemset(d_gate_cnt, 0, sizeof(unsigned)));
     st = (vsz == 4) ? setup_kernels<float>() : setup_kernels<double>();
     if (st != TF_OK) return st;
     return build_sweep();
   }
 
-  // Upload a prepared system into a free slot; TF_ERR_BUSY if no slot or
-  // no arena space (the caller may retry after other systems retire).
-  int admit(const HostSys& h, int* out_slot) {
+  // ---- admission: prepare, reserve, upload, commit ----
+  // The engine lock guards slots, the arena and the structure cache; the
+  // server's admission thread reserves and uploads while its worker thread
+  // sweeps, commits and retires.
+  std::mutex emu;
+  std::map<StructKey, std::shared_ptr<Structure>> scache;
+  uint64_t tick = 0;
+
+  std::condition_variable scv;   // a structure's preparation finished
+
+  // Drops cached structures that are prepared but neither on the device
+  // nor held by a queued system.  Engine lock held.
+  void purge_unused() {
+    for (auto it = scache.begin(); it != scache.end();)
+      if (it->second->ready != 0 && !it->second->resident && it->second.use_count() == 1)
+        it = scache.erase(it);
+      else
+        ++it;
+  }
+
+  // A system's host copy: its structure from the cache (prepared once for
+  // all the systems that share it, even while the first of them is still
+  // being prepared), else prepared here; then its values.  Host allocation
+  // failures are TF_ERR_OOM.
+  int prepare(HostSys& h, int n, long long nnz, const int* row, const int* col, const int* dia,
+              const double* val, const double* b, const double* x0, double tol, int maxit) {
+    try {
+      if (n < 1 || nnz < n || !row || !col || !dia || !val || !b) return TF_ERR_ARG;
+      h.key = struct_key(n, nnz, row, col, dia);
+      const bool patterns =
+          !opts.two_phase_rows && !opts.val_fp32 && !getenv("TF_NO_ROW_PATTERNS");
+      std::shared_ptr<Structure> S;
+      bool mine = false;
+      {
+        std::unique_lock<std::mutex> lk(emu);
+        purge_unused();
+        auto it = scache.find(h.key);
+        if (it != scache.end()) {
+          S = it->second;
+          scv.wait(lk, [&] { return S->ready != 0; });
+          if (S->ready < 0) return -S->ready;
+        } else {
+          S = std::make_shared<Structure>();
+          scache[h.key] = S;
+          mine = true;
+        }
+      }
+      if (mine) {
+        int st;
+        try {
+          st = prepare_structure(*S, n, nnz, row, col, dia, patterns);
+        } catch (const std::bad_alloc&) {
+          st = TF_ERR_OOM;
+        } catch (const std::length_error&) {
+          st = TF_ERR_OOM;
+        }
+        std::lock_guard<std::mutex> lk(emu);
+        S->ready = st == TF_OK ? 1 : -st;
+        if (st != TF_OK) {
+          auto it = scache.find(h.key);
+          if (it != scache.end() && it->second == S) scache.erase(it);
+        }
+        scv.notify_all();
+        if (st != TF_OK) return st;
+      }
+      h.st = std::move(S);
+      h.tol = tol;
+      h.maxit = maxit;
+      return prepare_values(h, *h.st, row, val, b, x0, opts.val_fp32);
+    } catch (const std::bad_alloc&) {
+      h = HostSys();
+      return TF_ERR_OOM;
+    } catch (const std::length_error&) {
+      h = HostSys();
+      return TF_ERR_OOM;
+    }
+  }
+
+  // Byte layout of a structure's device copy (columns or row patterns).
+  static size_t struct_layout(Structure& S) {
+    size_t o = 0;
+    auto take = [&](size_t bytes) { size_t r = o; o = Arena::up(o + bytes); return r; };
+    S.o_row = take(S.row.size() * 4);
+    S.o_col = S.npat ? 0 : take(((size_t)S.nnz + 8) * 4);
+    S.o_dia = take(S.dia.size() * 4);
+    S.o_tiles = take(S.tiles.size() * 4);
+    S.o_pat = S.npat ? take(S.pat.size()) : 0;
+    S.o_tab = S.npat ? take(S.tab.size() * 4) : 0;
+    return o;
+  }
+
+  // Evicts the least recently used resident structure that no system and
+  // no queued request uses; false when there is none.  Engine lock held.
+  bool evict_one() {
+    auto victim = scache.end();
+    for (auto it = scache.begin(); it != scache.end(); ++it)
+      if (it->second->resident && it->second->users == 0 && it->second.use_count() == 1 &&
+          (victim == scache.end() || it->second->last_use < victim->second->last_use))
+        victim = it;
+    if (victim == scache.end()) return false;
+    Structure& S = *victim->second;
+    arena.release(S.off, S.bytes);
+    S.resident = false;
+    scache.erase(victim);
+    return true;
+  }
+
+  // A slot and arena space for h (and for its structure when no device copy
+  // is resident); TF_ERR_BUSY when none is free now.  Engine lock held.
+  int reserve(HostSys& h, Reservation* rv) {
     int slot = -1;
     for (int i = 0; i < max_sys; ++i)
       if (!slots[i].used) { slot = i; break; }
     if (slot < 0) return TF_ERR_BUSY;
-    const Layout L = layout_for(h, vsz, opts.val_fp32);
-    size_t off = 0;
-    if (!arena.alloc(L.total, &off)) return TF_ERR_BUSY;
-    cudaStream_t s = ctx->stream;
-    char* base = arena.base + off;
-    auto up = [&](size_t o, const void* src, size_t bytes) {
-      return cudaMemcpyAsync(base + o, src, bytes, cudaMemcpyHostToDevice, s);
+    if (!h.st->resident) {   // uploaded meanwhile by a system with the same structure?
+      auto it = scache.find(h.key);
+      if (it != scache.end()) h.st = it->second;
+    }
+    Structure& S = *h.st;
+    const int ntiles = S.ntiles();
+    const Layout L = layout_for(h, ntiles, vsz, opts.val_fp32);
+    size_t soff = 0, sb = 0, off = 0;
+    const bool new_struct = !S.resident;
+    if (new_struct) sb = struct_layout(S);
+    // Both segments, or neither: on failure evict one unused structure and
+    // try both again (evicting before the retry, not between the two
+    // allocations, keeps the freed space in one piece where it can be).
+    for (;;) {
+      bool ok = !new_struct || arena.alloc(sb, &soff);
+      if (ok && !arena.alloc(L.total, &off)) {
+        if (new_struct) arena.release(soff, sb);
+        ok = false;
+      }
+      if (ok) break;
+      if (!evict_one()) return TF_ERR_BUSY;
+    }
+    if (new_struct) {
+      S.off = soff;
+      S.bytes = sb;
+      S.resident = true;
+      scache[h.key] = h.st;
+    }
+    S.users += 1;
+    S.last_use = ++tick;
+    Slot& sl = slots[slot];
+    sl = Slot{};
+    sl.used = 2;
+    sl.off = off;
+    sl.bytes = L.total;
+    sl.n = h.n;
+    sl.ntiles = ntiles;
+    sl.L = L;
+    sl.st = h.st;
+    rv->slot = slot;
+    rv->new_struct = new_struct;
+    rv->L = L;
+    return TF_OK;
+  }
+
+  // Gives a reservation back (its copies failed or its request went away).
+  // Engine lock held.
+  void unreserve(const Reservation& rv) {
+    Slot& sl = slots[rv.slot];
+    Structure& S = *sl.st;
+    S.users -= 1;
+    if (rv.new_struct) {   // the copy never landed: prepared, not resident, again
+      arena.release(S.off, S.bytes);
+      S.resident = false;
+    }
+    arena.release(sl.off, sl.bytes);
+    sl = Slot{};
+  }
+
+  // The copies of a reserved system (and of its structure when new) on
+  // stream s.  No lock: the reservation's slot and segments are this
+  // caller's until it commits or gives them back.
+  int upload(const HostSys& h, const Reservation& rv, cudaStream_t s) {
+    const Slot& sl = slots[rv.slot];
+    const Structure& S = *sl.st;
+    const Layout& L = rv.L;
+    char* base = arena.base + sl.off;
+    auto up = [&](char* dst, const void* src, size_t bytes) {
+      return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
     };
     const size_t n8 = (size_t)h.n + 8;
-    cudaError_t e = up(L.row, h.row.data(), h.row.size() * 4);
-    if (e == cudaSuccess) e = up(L.col, h.col.data(), h.col.size() * 4);
-    if (e == cudaSuccess) e = up(L.dia, h.dia.data(), h.dia.size() * 4);
-    if (e == cudaSuccess) e = up(L.tiles, h.tiles.data(), h.tiles.size() * 4);
-    if (e == cudaSuccess) e = up(L.val, h.val.data(), h.val.size() * 8);
-    if (e == cudaSuccess && opts.val_fp32) e = up(L.val32, h.val32.data(), h.val32.size() * 4);
-    if (e == cudaSuccess) e = up(L.b, h.b.data(), (size_t)h.n * 8);
-    if (e == cudaSuccess) e = up(L.x, h.x0.data(), (size_t)h.n * 8);
+    cudaError_t e = cudaSuccess;
+    if (rv.new_struct) {
+      char* sbase = arena.base + S.off;
+      e = up(sbase + S.o_row, S.row.data(), S.row.size() * 4);
+      if (e == cudaSuccess && !S.npat) e = up(sbase + S.o_col, S.col.data(), S.col.size() * 4);
+      if (e == cudaSuccess) e = up(sbase + S.o_dia, S.dia.data(), S.dia.size() * 4);
+      if (e == cudaSuccess) e = up(sbase + S.o_tiles, S.tiles.data(), S.tiles.size() * 4);
+      if (e == cudaSuccess && S.npat) e = up(sbase + S.o_pat, S.pat.data(), S.pat.size());
+      if (e == cudaSuccess && S.npat) e = up(sbase + S.o_tab, S.tab.data(), S.tab.size() * 4);
+    }
+    if (e == cudaSuccess) e = up(base + L.val, h.val.data(), h.val.size() * 8);
+    if (e == cudaSuccess && opts.val_fp32)
+      e = up(base + L.val32, h.val32.data(), h.val32.size() * 4);
+    if (e == cudaSuccess) e = up(base + L.b, h.b.data(), (size_t)h.n * 8);
+    if (e == cudaSuccess) e = up(base + L.x, h.x0.data(), (size_t)h.n * 8);
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.xlo, 0, n8 * vsz, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.p, 0, n8 * vsz, s);
     if (e == cudaSuccess && opts.val_fp32)
-      e = cudaMemsetAsync(base + L.tile_cnt, 0, (h.tiles.size() - 1) * 4, s);
+      e = cudaMemsetAsync(base + L.tile_cnt, 0, (size_t)sl.ntiles * 4, s);
     if (e != cudaSuccess) {
-      arena.release(off, L.total);
       tf_set_last_cuda_error(e, "batch admit copies", __FILE__, __LINE__);
       return TF_ERR_CUDA;
     }
-    const int ntiles = (int)h.tiles.size() - 1;
+    return TF_OK;
+  }
+
+  // Makes an uploaded system part of the batch: its descriptor and state
+  // (on the engine's stream, ahead of the next sweep).  The copies of the
+  // reservation must have completed.  Engine lock held.
+  int commit(const HostSys& h, const Reservation& rv) {
+    Slot& sl = slots[rv.slot];
+    Structure& S = *sl.st;
+    if (rv.new_struct) std::vector<int>().swap(S.col);   // the device copy is complete
+    const Layout& L = rv.L;
+    char* base = arena.base + sl.off;
+    char* sbase = arena.base + S.off;
+    cudaStream_t s = ctx->stream;
     auto fill = [&](auto& d) {
       using VV = std::remove_pointer_t<decltype(d.xlo)>;
-      d.row = (const int*)(base + L.row);
-      d.col = (const int*)(base + L.col);
-      d.dia = (const int*)(base + L.dia);
-      d.tiles = (const int*)(base + L.tiles);
+      d.row = (const int*)(sbase + S.o_row);
+      d.col = S.npat ? nullptr : (const int*)(sbase + S.o_col);
+      d.pat = S.npat ? (const unsigned char*)(sbase + S.o_pat) : nullptr;
+      d.tab = S.npat ? (const int*)(sbase + S.o_tab) : nullptr;
+      d.npat = S.npat;
+      d.dia = (const int*)(sbase + S.o_dia);
+      d.tiles = (const int*)(sbase + S.o_tiles);
       d.val = (const double*)(base + L.val);
       d.val32 = opts.val_fp32 ? (const float*)(base + L.val32) : nullptr;
       d.b = (const double*)(base + L.b);
@@ -1241,47 +1644,74 @@ struct tf_batch_s {
       d.q = (VV*)(base + L.q);
       d.dinv = (VV*)(base + L.dinv);
       d.tile_tot = (double*)(base + L.tile_tot);
+      d.chunk_tot = (double*)(base + L.chunk_tot);
       d.warp_part = opts.val_fp32 ? (double*)(base + L.warp_part) : nullptr;
       d.tile_cnt = opts.val_fp32 ? (unsigned*)(base + L.tile_cnt) : nullptr;
       d.n = h.n;
-      d.ntiles = ntiles;
+      d.ntiles = sl.ntiles;
       d.maxit = h.maxit;
       d.use_val32 = opts.val_fp32;
       d.tol = h.tol;
     };
     SysState ss{};
     ss.status = kInit;
+    cudaError_t e;
     if (vsz == 4) {
       SysDev<float> d{};
       fill(d);
-      e = cudaMemcpyAsync((SysDev<float>*)d_desc + slot, &d, sizeof d, cudaMemcpyHostToDevice, s);
+      e = cudaMemcpyAsync((SysDev<float>*)d_desc + rv.slot, &d, sizeof d,
+                          cudaMemcpyHostToDevice, s);
     } else {
       SysDev<double> d{};
       fill(d);
-      e = cudaMemcpyAsync((SysDev<double>*)d_desc + slot, &d, sizeof d, cudaMemcpyHostToDevice, s);
+      e = cudaMemcpyAsync((SysDev<double>*)d_desc + rv.slot, &d, sizeof d,
+                          cudaMemcpyHostToDevice, s);
     }
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(d_state + slot, &ss, sizeof ss, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // host buffers may go away
+      e = cudaMemcpyAsync(d_state + rv.slot, &ss, sizeof ss, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) {
-      arena.release(off, L.total);
+      unreserve(rv);
       tf_set_last_cuda_error(e, "batch admit descriptors", __FILE__, __LINE__);
       return TF_ERR_CUDA;
     }
-    Slot& sl = slots[slot];
     sl.used = 1;
-    sl.off = off;
-    sl.bytes = L.total;
-    sl.n = h.n;
-    sl.ntiles = ntiles;
-    sl.L = L;
-    sl.tiles = h.tiles;
-    sl.perm = h.perm;
-    sl.tile_j.resize(h.tiles.size());
-    for (size_t t = 0; t < h.tiles.size(); ++t) sl.tile_j[t] = h.row[h.tiles[t]];
-    h_state[slot] = ss;
-    *out_slot = slot;
+    h_state[rv.slot] = ss;
     return TF_OK;
+  }
+
+  // Reserve, upload and commit on the engine's stream, synchronously (the
+  // batch API); TF_ERR_BUSY if no slot or no arena space.
+  int admit(HostSys& h, int* out_slot) {
+    Reservation rv;
+    int st;
+    {
+      std::lock_guard<std::mutex> lk(emu);
+      st = reserve(h, &rv);
+    }
+    if (st != TF_OK) return st;
+    st = upload(h, rv, ctx->stream);
+    if (st == TF_OK) {
+      const cudaError_t e = cudaStreamSynchronize(ctx->stream);   // host buffers may go away
+      if (e != cudaSuccess) {
+        tf_set_last_cuda_error(e, "batch admit copies", __FILE__, __LINE__);
+        st = TF_ERR_CUDA;
+      }
+    }
+    std::lock_guard<std::mutex> lk(emu);
+    if (st != TF_OK) {
+      unreserve(rv);
+      return st;
+    }
+    st = commit(h, rv);
+    if (st == TF_OK) {
+      const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+      if (e != cudaSuccess) {
+        tf_set_last_cuda_error(e, "batch admit descriptors", __FILE__, __LINE__);
+        return TF_ERR_CUDA;
+      }
+      *out_slot = rv.slot;
+    }
+    return st;
   }
 
   // Work list = every tile of every system that still iterates; the
@@ -1289,17 +1719,17 @@ struct tf_batch_s {
   int rebuild_work() {
     h_work.clear();
     h_ru.clear();
-    h_sys.clear();
+    h_fin.clear();
     work_rows = work_nnz = 0;
     for (int i = 0; i < max_sys; ++i) {
-      if (!slots[i].used) continue;
+      if (slots[i].used != 1) continue;
       const int stt = h_state[i].status;
       if (stt != kInit && stt != kActive) continue;
-      const std::vector<int>& tl = slots[i].tiles;
-      const std::vector<int>& tj = slots[i].tile_j;
+      const std::vector<int>& tl = slots[i].st->tiles;
+      const std::vector<int>& tj = slots[i].st->tile_j;
       work_rows += slots[i].n;
       work_nnz += tj[slots[i].ntiles];
-      h_sys.push_back(i);
+      for (int c = 0; c < fin_chunks(slots[i].ntiles); ++c) h_fin.push_back(FinItem{i, c});
       for (int t = 0; t < slots[i].ntiles; ++t) {
         const Work wk{i, t, tl[t], tl[t + 1], tj[t], tj[t + 1]};
         h_work.push_back(wk);
@@ -1307,15 +1737,20 @@ struct tf_batch_s {
       }
     }
     nwork = (int)h_work.size();
-    if (nwork > work_cap) {
+    const int nfin = (int)h_fin.size();
+    if (nwork > work_cap || nfin > fin_cap) {
       if (d_work) cudaFree(d_work);
       if (d_ru) cudaFree(d_ru);
+      if (d_fin) cudaFree(d_fin);
       d_work = nullptr;
       d_ru = nullptr;
+      d_fin = nullptr;
       work_cap = std::max(nwork, 2 * work_cap);
+      fin_cap = std::max(nfin, 2 * fin_cap);
       TF_CUDA_TRY(cudaMalloc((void**)&d_work, (size_t)work_cap * sizeof(Work)));
       TF_CUDA_TRY(cudaMalloc((void**)&d_ru, (size_t)work_cap * sizeof(Work)));
-      int st = build_sweep();   // the graph holds the work-list pointers
+      TF_CUDA_TRY(cudaMalloc((void**)&d_fin, (size_t)fin_cap * sizeof(FinItem)));
+      int st = build_sweep();   // the graph holds the lists' pointers
       if (st != TF_OK) return st;
     }
     cudaStream_t s = ctx->stream;
@@ -1327,11 +1762,10 @@ struct tf_batch_s {
       TF_CUDA_TRY(cudaMemcpyAsync(d_ru, h_ru.data(), (size_t)nru * sizeof(Work),
                                   cudaMemcpyHostToDevice, s));
     TF_CUDA_TRY(cudaMemcpyAsync(d_nwork, &nwork, sizeof(int), cudaMemcpyHostToDevice, s));
-    const int nsys = (int)h_sys.size();
-    if (nsys)
-      TF_CUDA_TRY(cudaMemcpyAsync(d_sys, h_sys.data(), (size_t)nsys * sizeof(int),
+    if (nfin)
+      TF_CUDA_TRY(cudaMemcpyAsync(d_fin, h_fin.data(), (size_t)nfin * sizeof(FinItem),
                                   cudaMemcpyHostToDevice, s));
-    TF_CUDA_TRY(cudaMemcpyAsync(d_nsys, &nsys, sizeof(int), cudaMemcpyHostToDevice, s));
+    TF_CUDA_TRY(cudaMemcpyAsync(d_nfin, &nfin, sizeof(int), cudaMemcpyHostToDevice, s));
     TF_CUDA_TRY(cudaMemcpyAsync(d_ru_count, &nru, sizeof(int), cudaMemcpyHostToDevice, s));
     TF_CUDA_TRY(cudaStreamSynchronize(s));
     return TF_OK;
@@ -1352,7 +1786,8 @@ struct tf_batch_s {
   int n_running() const {
     int c = 0;
     for (int i = 0; i < max_sys; ++i)
-      if (slots[i].used && (h_state[i].status == kInit || h_state[i].status == kActive)) ++c;
+      if (slots[i].used == 1 && (h_state[i].status == kInit || h_state[i].status == kActive))
+        ++c;
     return c;
   }
 
@@ -1378,7 +1813,7 @@ struct tf_batch_s {
       trace.push_back(rec);
       const double ms = std::chrono::duration<double, std::milli>(te - t0).count();
       for (int i = 0; i < max_sys; ++i)
-        if (slots[i].used && slots[i].done_ms < 0.0 && h_state[i].status != kInit &&
+        if (slots[i].used == 1 && slots[i].done_ms < 0.0 && h_state[i].status != kInit &&
             h_state[i].status != kActive)
           slots[i].done_ms = ms;
       const int now = n_running();
@@ -1391,25 +1826,34 @@ struct tf_batch_s {
     return TF_OK;
   }
 
-  int fetch_x(int slot, double* x) {
+  // x of a finished system in the caller's numbering, copied on stream s
+  // (the engine's stream by default).
+  int fetch_x(int slot, double* x, cudaStream_t s = nullptr) {
+    if (!s) s = ctx->stream;
     const Slot& sl = slots[slot];
-    if (sl.perm.empty()) {
+    const std::vector<int>& perm = sl.st->perm;
+    if (perm.empty()) {
       TF_CUDA_TRY(cudaMemcpyAsync(x, arena.base + sl.off + sl.L.x, (size_t)sl.n * 8,
-                                  cudaMemcpyDeviceToHost, ctx->stream));
-      TF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+                                  cudaMemcpyDeviceToHost, s));
+      TF_CUDA_TRY(cudaStreamSynchronize(s));
       return TF_OK;
     }
     std::vector<double> tmp((size_t)sl.n);
     TF_CUDA_TRY(cudaMemcpyAsync(tmp.data(), arena.base + sl.off + sl.L.x, (size_t)sl.n * 8,
-                                cudaMemcpyDeviceToHost, ctx->stream));
-    TF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    for (int i = 0; i < sl.n; ++i) x[sl.perm[i]] = tmp[i];
+                                cudaMemcpyDeviceToHost, s));
+    TF_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int i = 0; i < sl.n; ++i) x[perm[i]] = tmp[i];
     return TF_OK;
   }
 
+  // A finished or removed system gives its slot and segment back; its
+  // structure stays resident for later systems until the space is needed.
+  // Engine lock held by callers that share the engine between threads.
   void retire(int slot) {
     Slot& sl = slots[slot];
-    if (!sl.used) return;
+    if (sl.used != 1 && sl.used != 3) return;
+    sl.st->users -= 1;
+    sl.st->last_use = ++tick;
     arena.release(sl.off, sl.bytes);
     sl = Slot{};
     h_state[slot].status = kFree;
@@ -1448,10 +1892,16 @@ extern "C" int tf_batch_add(tf_batch bt, int n, int64_t nnz, const int* row, con
   TF_API_BEGIN
   if (!bt || !sys) return TF_ERR_ARG;
   HostSys h;
-  int st = prepare_host(h, n, nnz, row, col, dia, val, b, x0, tol, maxit, bt->opts.val_fp32);
+  const auto t0 = std::chrono::steady_clock::now();
+  int st = bt->prepare(h, n, nnz, row, col, dia, val, b, x0, tol, maxit);
+  const auto t1 = std::chrono::steady_clock::now();
+  bt->up_prep_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
   if (st != TF_OK) return st;
   TF_CUDA_TRY(cudaSetDevice(bt->ctx->device));
-  return bt->admit(h, sys);
+  st = bt->admit(h, sys);
+  bt->up_admit_ms += std::chrono::duration<double, std::milli>(
+                         std::chrono::steady_clock::now() - t1).count();
+  return st;
   TF_API_END
 }
 
@@ -1482,6 +1932,7 @@ extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int
   std::condition_variable cv_ready, cv_room;
   int next = 0, admitted = 0;
   bool stop = false;
+  double prep_ms = 0.0, wait_ms = 0.0, admit_ms = 0.0;
   auto worker = [&]() {
     for (;;) {
       int i;
@@ -1491,14 +1942,19 @@ extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int
         if (stop || next >= count) return;
         i = next++;
       }
+      const auto t0 = std::chrono::steady_clock::now();
       const int r = tf_guarded([&] {
-        return prepare_host(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
-                            x0 ? x0[i] : nullptr, tol[i], maxit[i], bt->opts.val_fp32);
+        return bt->prepare(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
+                           x0 ? x0[i] : nullptr, tol[i], maxit[i]);
       });
+      const double ms =
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+              .count();
       {
         std::lock_guard<std::mutex> lk(mu);
         st[i] = r;
         ready[i] = 1;
+        prep_ms += ms;
       }
       cv_ready.notify_all();
     }
@@ -1512,18 +1968,23 @@ extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int
   const bool inline_prep = pool.empty();
   int result = TF_OK;
   for (int i = 0; i < count; ++i) {
+    const auto t0 = std::chrono::steady_clock::now();
     if (inline_prep) {
       st[i] = tf_guarded([&] {
-        return prepare_host(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
-                            x0 ? x0[i] : nullptr, tol[i], maxit[i], bt->opts.val_fp32);
+        return bt->prepare(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
+                           x0 ? x0[i] : nullptr, tol[i], maxit[i]);
       });
     } else {
       std::unique_lock<std::mutex> lk(mu);
       cv_ready.wait(lk, [&] { return ready[i] != 0; });
     }
+    const auto t1 = std::chrono::steady_clock::now();
     int r = st[i];
     if (r == TF_OK) r = tf_guarded([&] { return bt->admit(hs[i], &sys[i]); });
     hs[i] = HostSys();   // its host copy is on the device now
+    const auto t2 = std::chrono::steady_clock::now();
+    (inline_prep ? prep_ms : wait_ms) += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    admit_ms += std::chrono::duration<double, std::milli>(t2 - t1).count();
     {
       std::lock_guard<std::mutex> lk(mu);
       admitted = i + 1;
@@ -1541,7 +2002,21 @@ extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int
   }
   cv_room.notify_all();
   for (auto& t : pool) t.join();
+  bt->up_prep_ms += prep_ms;
+  bt->up_wait_ms += wait_ms;
+  bt->up_admit_ms += admit_ms;
   return result;
+  TF_API_END
+}
+
+extern "C" int tf_batch_upload_ms(tf_batch bt, double* prep_ms, double* wait_ms,
+                                  double* admit_ms) {
+  TF_API_BEGIN
+  if (!bt) return TF_ERR_ARG;
+  if (prep_ms) *prep_ms = bt->up_prep_ms;
+  if (wait_ms) *wait_ms = bt->up_wait_ms;
+  if (admit_ms) *admit_ms = bt->up_admit_ms;
+  return TF_OK;
   TF_API_END
 }
 
@@ -1557,7 +2032,7 @@ extern "C" int tf_batch_result(tf_batch bt, int sys, double* x, int* iters,
                                double* true_rel_res, int* status, int* n_updates,
                                double* done_ms) {
   TF_API_BEGIN
-  if (!bt || sys < 0 || sys >= bt->max_sys || !bt->slots[sys].used) return TF_ERR_ARG;
+  if (!bt || sys < 0 || sys >= bt->max_sys || bt->slots[sys].used != 1) return TF_ERR_ARG;
   const SysState& s = bt->h_state[sys];
   if (done_ms) *done_ms = bt->slots[sys].done_ms;
   if (iters) *iters = s.iter;
@@ -1589,7 +2064,7 @@ extern "C" int tf_batch_trace(tf_batch bt, tf_batch_sweep* out, int cap, int* co
 
 extern "C" int tf_batch_remove(tf_batch bt, int sys) {
   TF_API_BEGIN
-  if (!bt || sys < 0 || sys >= bt->max_sys || !bt->slots[sys].used) return TF_ERR_ARG;
+  if (!bt || sys < 0 || sys >= bt->max_sys || bt->slots[sys].used != 1) return TF_ERR_ARG;
   bt->retire(sys);
   return TF_OK;
   TF_API_END
@@ -1613,7 +2088,10 @@ using Clock = std::chrono::steady_clock;
 
 struct Request {
   int64_t id = 0;
-  HostSys h;
+  int n = 0;
+  HostSys h;            // host copy until its upload has landed
+  Reservation rv;       // slot and arena space once reserved
+  cudaEvent_t ev = nullptr;   // the upload's completion (copy stream)
   Clock::time_point t_submit, t_admit, t_done;
   int slot = -1;
   int status = 0;       // SysStatus at completion, or an error code (< 0)
@@ -1621,83 +2099,202 @@ struct Request {
   double res = 0.0;
   std::vector<double> x;
   bool done = false;
-  bool cancel = false;  // set by tf_server_cancel while the request runs
+  bool cancel = false;  // set by tf_server_cancel while the request is staged or runs
 };
 }  // namespace
 
+// Continuous batching with four kinds of threads:
+//   submitting threads  prepare a request's host copy (its structure shared
+//                       through the engine's cache) and queue it;
+//   the admission thread takes queued requests in arrival order, reserves
+//                       a slot and arena space when memory allows and
+//                       uploads them on a copy stream of its own, so the
+//                       copies overlap the sweeps;
+//   the worker thread   commits requests whose copies have landed (their
+//                       descriptors go ahead of the next sweep), runs the
+//                       sweeps, and takes finished and cancelled requests
+//                       out of the work list;
+//   the collector       copies their results out on a stream of its own
+//                       and retires them, which frees space for the
+//                       admission thread.
 struct tf_server_s {
   tf_batch_s eng;
-  std::mutex mu;
-  std::condition_variable cv_work, cv_done;
-  std::deque<std::shared_ptr<Request>> queue;
+  cudaStream_t copy_stream = nullptr, fetch_stream = nullptr;
+  std::mutex mu;   // everything below (the engine's own state: eng.emu)
+  std::condition_variable cv_work, cv_done, cv_admit, cv_collect;
+  std::deque<std::shared_ptr<Request>> queue;    // prepared, waiting for space
+  std::deque<std::shared_ptr<Request>> staged;   // reserved, copies in flight
+  std::deque<std::shared_ptr<Request>> finishing;   // out of the work list, to collect
   std::map<int64_t, std::shared_ptr<Request>> live;     // submitted, not yet collected
-  std::map<int, std::shared_ptr<Request>> by_slot;      // admitted, running
+  std::map<int, std::shared_ptr<Request>> by_slot;      // running (worker thread)
+  int n_running = 0;        // by_slot.size(), readable by the admission thread
+  uint64_t retire_gen = 0;  // counts retirements (the admission thread waits on it)
   int64_t next_id = 1;
   bool stop = false;
   int error = TF_OK;
-  std::thread worker;
+  std::thread worker, admitter, collector;
   // stats
   long long admitted = 0, completed = 0, rejected = 0;
   int peak_running = 0;
+  // Wall time (ms) by activity (tf_server_timing): preparation on the
+  // submitting threads (summed), the admission thread's reservations and
+  // uploads, the worker thread's commits and work-list rebuilds, its
+  // sweeps (launch to state read), and the collector's result copies and
+  // retirements.
+  double t_ms[5] = {0, 0, 0, 0, 0};
+  static double ms_since(Clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+  }
+
+  // Ends a request that never ran (lock mu held).
+  void fail(const std::shared_ptr<Request>& r, int status) {
+    r->status = -status;
+    r->t_done = Clock::now();
+    r->done = true;
+    r->h = HostSys();
+    cv_done.notify_all();
+  }
+
+  void admit_loop() {
+    cudaSetDevice(eng.ctx->device);
+    for (;;) {
+      std::shared_ptr<Request> r;
+      uint64_t gen;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_admit.wait(lk, [&] { return stop || !queue.empty(); });
+        if (stop) return;
+        r = queue.front();
+        gen = retire_gen;
+      }
+      const auto t0 = Clock::now();
+      Reservation rv;
+      int st = tf_guarded([&] {
+        std::lock_guard<std::mutex> el(eng.emu);
+        return eng.reserve(r->h, &rv);
+      });
+      if (st == TF_ERR_BUSY) {
+        std::unique_lock<std::mutex> lk(mu);
+        t_ms[1] += ms_since(t0);
+        if (n_running == 0 && staged.empty() && retire_gen == gen) {
+          // Nothing runs or lands that could free space: it never fits.
+          if (!queue.empty() && queue.front() == r) {
+            queue.pop_front();
+            ++rejected;
+            fail(r, TF_ERR_OOM);
+          }
+          continue;
+        }
+        cv_admit.wait(lk, [&] { return stop || retire_gen != gen; });
+        continue;
+      }
+      cudaEvent_t ev = nullptr;
+      if (st == TF_OK) st = tf_guarded([&] { return eng.upload(r->h, rv, copy_stream); });
+      if (st == TF_OK) {
+        cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(ev, copy_stream);
+        if (e != cudaSuccess) {
+          tf_set_last_cuda_error(e, "server upload event", __FILE__, __LINE__);
+          st = TF_ERR_CUDA;
+        }
+      }
+      bool give_back = false;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        t_ms[1] += ms_since(t0);
+        if (queue.empty() || queue.front() != r) {   // cancelled meanwhile
+          give_back = (st == TF_OK || rv.slot >= 0);
+        } else {
+          queue.pop_front();
+          if (st != TF_OK) {
+            give_back = rv.slot >= 0;
+            fail(r, st);
+          } else {
+            r->rv = rv;
+            r->ev = ev;
+            ev = nullptr;
+            staged.push_back(r);
+            cv_work.notify_one();
+          }
+        }
+      }
+      if (give_back) {   // after its copies: the space must not be reused under them
+        cudaStreamSynchronize(copy_stream);
+        std::lock_guard<std::mutex> el(eng.emu);
+        eng.unreserve(rv);
+      }
+      if (ev) cudaEventDestroy(ev);
+    }
+  }
 
   void loop() {
     cudaSetDevice(eng.ctx->device);
     for (;;) {
-      std::vector<std::shared_ptr<Request>> incoming;
+      std::vector<std::shared_ptr<Request>> ready;
+      std::shared_ptr<Request> wait_for;
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv_work.wait(lk, [&] { return stop || !queue.empty() || !by_slot.empty(); });
+        cv_work.wait(lk, [&] { return stop || !staged.empty() || !by_slot.empty(); });
         if (stop) return;
-      }
-      // Admit from the queue in arrival order while memory and slots allow.
-      bool changed = false;
-      for (;;) {
-        std::shared_ptr<Request> r;
-        {
-          std::lock_guard<std::mutex> lk(mu);
-          if (queue.empty()) break;
-          r = queue.front();
+        while (!staged.empty() && cudaEventQuery(staged.front()->ev) == cudaSuccess) {
+          ready.push_back(staged.front());
+          staged.pop_front();
         }
-        int slot = -1;
-        const int st = tf_guarded([&] { return eng.admit(r->h, &slot); });
-        if (st == TF_ERR_BUSY) {
-          if (by_slot.empty()) {   // cannot ever fit: fail the request
-            std::lock_guard<std::mutex> lk(mu);
-            if (queue.empty() || queue.front() != r) continue;   // cancelled meanwhile
-            queue.pop_front();
-            r->status = -TF_ERR_OOM;
-            r->done = true;
-            r->t_done = Clock::now();
-            ++rejected;
-            cv_done.notify_all();
-            continue;
+        if (ready.empty() && by_slot.empty()) wait_for = staged.front();
+      }
+      if (wait_for) {   // nothing to sweep: wait for the next upload to land
+        cudaEventSynchronize(wait_for->ev);
+        continue;
+      }
+      auto t0 = Clock::now();
+      bool changed = false;
+      for (auto& r : ready) {
+        cudaEventDestroy(r->ev);
+        r->ev = nullptr;
+        int st;
+        {
+          std::lock_guard<std::mutex> el(eng.emu);
+          if (r->cancel) {
+            eng.unreserve(r->rv);
+            st = TF_ERR_CANCELLED;
+          } else {
+            st = tf_guarded([&] { return eng.commit(r->h, r->rv); });
           }
-          break;
         }
         std::lock_guard<std::mutex> lk(mu);
-        if (queue.empty() || queue.front() != r) {   // cancelled while being admitted
-          if (st == TF_OK) eng.retire(slot);
+        if (st != TF_OK) {   // its reservation was given back
+          fail(r, st);
+          ++retire_gen;
+          cv_admit.notify_all();
           continue;
         }
-        queue.pop_front();
-        if (st != TF_OK) {
-          r->status = -st;
-          r->done = true;
-          r->t_done = Clock::now();
-          cv_done.notify_all();
-          continue;
-        }
-        r->slot = slot;
+        r->slot = r->rv.slot;
         r->t_admit = Clock::now();
-        by_slot[slot] = r;
+        r->h = HostSys();   // on the device now
+        by_slot[r->slot] = r;
+        n_running = (int)by_slot.size();
         ++admitted;
         changed = true;
       }
-      if (by_slot.empty()) continue;
+      if (by_slot.empty()) {
+        std::lock_guard<std::mutex> lk(mu);
+        t_ms[2] += ms_since(t0);
+        continue;
+      }
       peak_running = std::max(peak_running, (int)by_slot.size());
       int st = TF_OK;
-      if (changed) st = tf_guarded([&] { return eng.rebuild_work(); });
+      if (changed)
+        st = tf_guarded([&] {
+          std::lock_guard<std::mutex> el(eng.emu);
+          return eng.rebuild_work();
+        });
+      const auto t1 = Clock::now();
       if (st == TF_OK) st = tf_guarded([&] { return eng.run_sweep(); });
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        t_ms[2] += std::chrono::duration<double, std::milli>(t1 - t0).count();
+        t_ms[3] += ms_since(t1);
+      }
       if (st != TF_OK) {
         std::lock_guard<std::mutex> lk(mu);
         error = st;
@@ -1706,10 +2303,14 @@ struct tf_server_s {
           kv.second->done = true;
         }
         by_slot.clear();
+        n_running = 0;
         cv_done.notify_all();
         continue;
       }
-      // Retire finished systems, and cancelled ones that have not finished.
+      t0 = Clock::now();
+      // Finished systems, and cancelled ones that have not finished, leave
+      // the work list now; the collector copies their results out and
+      // retires them.
       std::vector<int> fin, cancelled;
       {
         std::lock_guard<std::mutex> lk(mu);
@@ -1719,34 +2320,67 @@ struct tf_server_s {
           else if (kv.second->cancel) cancelled.push_back(kv.first);
         }
       }
-      for (int slot : cancelled) {
-        auto r = by_slot[slot];
-        std::lock_guard<std::mutex> lk(mu);
-        r->status = -TF_ERR_CANCELLED;
-        r->t_done = Clock::now();
-        r->done = true;
-        eng.retire(slot);
-        by_slot.erase(slot);
-        cv_done.notify_all();
-      }
+      if (fin.empty() && cancelled.empty()) continue;
+      st = tf_guarded([&] {
+        std::lock_guard<std::mutex> el(eng.emu);
+        for (int slot : fin) eng.slots[slot].used = 3;
+        for (int slot : cancelled) eng.slots[slot].used = 3;
+        return eng.rebuild_work();
+      });
+      std::lock_guard<std::mutex> lk(mu);
+      if (st != TF_OK) error = st;
       for (int slot : fin) {
         auto r = by_slot[slot];
         const SysState& ss = eng.h_state[slot];
-        r->x.resize(r->h.n);
-        eng.fetch_x(slot, r->x.data());
-        std::lock_guard<std::mutex> lk(mu);
         r->status = ss.status;
         r->iters = ss.iter;
         r->n_ru = ss.n_ru;
         r->res = ss.res_true;
-        r->t_done = Clock::now();
-        r->done = true;
-        eng.retire(slot);
         by_slot.erase(slot);
-        ++completed;
-        cv_done.notify_all();
+        finishing.push_back(r);
       }
-      if (!fin.empty() || !cancelled.empty()) eng.rebuild_work();
+      for (int slot : cancelled) {
+        auto r = by_slot[slot];
+        r->status = -TF_ERR_CANCELLED;
+        by_slot.erase(slot);
+        finishing.push_back(r);
+      }
+      n_running = (int)by_slot.size();
+      t_ms[2] += ms_since(t0);
+      cv_collect.notify_one();
+    }
+  }
+
+  void collect_loop() {
+    cudaSetDevice(eng.ctx->device);
+    for (;;) {
+      std::shared_ptr<Request> r;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_collect.wait(lk, [&] { return stop || !finishing.empty(); });
+        if (stop) return;
+        r = finishing.front();
+        finishing.pop_front();
+      }
+      const auto t0 = Clock::now();
+      int st = TF_OK;
+      if (r->status >= 0) {
+        r->x.resize(r->n);
+        st = tf_guarded([&] { return eng.fetch_x(r->slot, r->x.data(), fetch_stream); });
+      }
+      {
+        std::lock_guard<std::mutex> el(eng.emu);
+        eng.retire(r->slot);
+      }
+      std::lock_guard<std::mutex> lk(mu);
+      if (st != TF_OK) r->status = -st;
+      r->t_done = Clock::now();
+      r->done = true;
+      if (r->status >= 0) ++completed;
+      ++retire_gen;
+      t_ms[4] += ms_since(t0);
+      cv_admit.notify_all();
+      cv_done.notify_all();
     }
   }
 };
@@ -1756,12 +2390,22 @@ extern "C" int tf_server_create(tf_ctx ctx, const tf_batch_opts* opts, tf_server
   if (!ctx || !out) return TF_ERR_ARG;
   *out = nullptr;
   auto* s = new tf_server_s();
-  const int st = s->eng.init(ctx, opts);
+  int st = s->eng.init(ctx, opts);
+  if (st == TF_OK) {
+    cudaError_t e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->fetch_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      tf_set_last_cuda_error(e, "server copy stream", __FILE__, __LINE__);
+      st = TF_ERR_CUDA;
+    }
+  }
   if (st != TF_OK) {
     delete s;
     return st;
   }
   s->worker = std::thread([s] { s->loop(); });
+  s->admitter = std::thread([s] { s->admit_loop(); });
+  s->collector = std::thread([s] { s->collect_loop(); });
   *out = s;
   return TF_OK;
   TF_API_END
@@ -1774,17 +2418,19 @@ extern "C" int tf_server_submit(tf_server sv, int n, int64_t nnz, const int* row
   TF_API_BEGIN
   if (!sv || !req) return TF_ERR_ARG;
   auto r = std::make_shared<Request>();
-  const int st = prepare_host(r->h, n, nnz, row, col, dia, val, b, x0, tol, maxit,
-                              sv->eng.opts.val_fp32);
+  const auto t0 = Clock::now();
+  const int st = sv->eng.prepare(r->h, n, nnz, row, col, dia, val, b, x0, tol, maxit);
   if (st != TF_OK) return st;
+  r->n = n;
   std::lock_guard<std::mutex> lk(sv->mu);
+  sv->t_ms[0] += tf_server_s::ms_since(t0);
   if (sv->stop) return TF_ERR_CANCELLED;
   r->id = sv->next_id++;
   r->t_submit = Clock::now();
   sv->queue.push_back(r);
   sv->live[r->id] = r;
   *req = r->id;
-  sv->cv_work.notify_one();
+  sv->cv_admit.notify_one();
   return TF_OK;
   TF_API_END
 }
@@ -1831,7 +2477,7 @@ extern "C" int tf_server_cancel(tf_server sv, int64_t req) {
       sv->cv_done.notify_all();
       return TF_OK;
     }
-  r->cancel = true;                           // admitted: retired after this sweep
+  r->cancel = true;   // staged: given back at commit; running: retired after this sweep
   sv->cv_work.notify_one();
   return TF_OK;
   TF_API_END
@@ -1850,6 +2496,15 @@ extern "C" int tf_server_stats(tf_server sv, long long* admitted, long long* com
   TF_API_END
 }
 
+extern "C" int tf_server_timing(tf_server sv, double* ms5) {
+  TF_API_BEGIN
+  if (!sv || !ms5) return TF_ERR_ARG;
+  std::lock_guard<std::mutex> lk(sv->mu);
+  for (int k = 0; k < 5; ++k) ms5[k] = sv->t_ms[k];
+  return TF_OK;
+  TF_API_END
+}
+
 extern "C" int tf_server_destroy(tf_server sv) {
   TF_API_BEGIN
   if (!sv) return TF_ERR_ARG;
@@ -1862,9 +2517,21 @@ extern "C" int tf_server_destroy(tf_server sv) {
         kv.second->done = true;
       }
     sv->cv_work.notify_all();
+    sv->cv_admit.notify_all();
+    sv->cv_collect.notify_all();
     sv->cv_done.notify_all();
   }
   if (sv->worker.joinable()) sv->worker.join();
+  if (sv->admitter.joinable()) sv->admitter.join();
+  if (sv->collector.joinable()) sv->collector.join();
+  cudaSetDevice(sv->eng.ctx->device);
+  for (cudaStream_t st : {sv->copy_stream, sv->fetch_stream})
+    if (st) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+  for (auto& r : sv->staged)
+    if (r->ev) cudaEventDestroy(r->ev);
   delete sv;
   return TF_OK;
   TF_API_END

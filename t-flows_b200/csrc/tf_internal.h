@@ -213,6 +213,13 @@ int tf_solve_resident(tf_matrix_s* m, int prec, int miter, double tol, const dou
 int tf_dev_alloc_bytes(tf_ctx_s* ctx, void** p, size_t bytes);
 // Renumbering (tf_renumber.cu)
 double tf_gather_lines_per_warp(const int* row, const int* col, int n, int base);
+// Row patterns of the first ni rows of a 0-based CSR: pat[i] (ni + 32
+// bytes) names row i's offset sequence (col_j - i over its entries, in
+// storage order), tab holds the sequences ([npat][kPatMaxLen], then the
+// npat lengths).  Returns npat, or 0 when more than kPatMax patterns or a
+// row longer than kPatMaxLen would be needed.
+int tf_find_row_patterns(const std::vector<int>& row0, const std::vector<int>& col0, int ni,
+                         std::vector<unsigned char>& pat, std::vector<int>& tab);
 void tf_rcm_order(const std::vector<int>& row0, const std::vector<int>& col0, int n,
                   std::vector<int>& order);
 int tf_renumber_in(tf_matrix_s* m);

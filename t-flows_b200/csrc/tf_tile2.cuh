@@ -51,6 +51,7 @@
 //                                     warp has parked tile it (tile_end)
 #pragma once
 #include "tf_common.cuh"
+#include "tf_tile.cuh"   // kPatMaxLen: the row-pattern table's row length
 
 namespace tf {
 
@@ -67,6 +68,13 @@ struct TileDesc {
   const void* aux0;   // handed to op.begin through the stage (e.g. x, y vectors)
   void* aux1;
   int aux2, aux3;
+  // Row-pattern tile (warp-group consumers of a source with kRowPatterns
+  // only): the rows' pattern bytes and the pattern table ([npat][kPatMaxLen]
+  // offsets, npat <= kPatMax) are staged instead of the columns,
+  // col = i + tab[pat(i)][k].
+  const unsigned char* pat = nullptr;
+  const int* tab = nullptr;
+  int npat = 0;
 };
 
 // What op.begin receives about its tile (copied by the producer into the
@@ -77,6 +85,11 @@ struct TileAux {
   int i2, i3;
 };
 
+// The staged pattern table follows the pattern bytes of a stage's column
+// region, at this byte offset (a multiple of 16).
+template <int ROWCAP>
+__host__ __device__ constexpr int pat_tab_offset() { return ((ROWCAP + 32 + 15) / 16) * 16; }
+
 template <int ROWCAP, int NNZCAP, int STAGES>
 struct Csr2Layout {
   static constexpr size_t kValBytes = (((NNZCAP + 4) * 8 + 127) / 128) * 128;
@@ -85,7 +98,11 @@ struct Csr2Layout {
   static constexpr size_t kStageBytes = kValBytes + kColBytes + kRowBytes;
   static constexpr size_t kBarOffset = STAGES * kStageBytes;   // full[S], empty[S]
   static constexpr size_t kMetaOffset = kBarOffset + 16 * STAGES;
-  static constexpr int kMetaInts = 16;   // 0-8 tile, 9-10 aux ints, 12-15 aux pointers
+  // 0-8 tile, 9-10 aux ints, 11 row patterns (their count), 12-15 aux pointers
+  static constexpr int kMetaInts = 16;
+  static_assert((size_t)pat_tab_offset<ROWCAP>() + kPatMax * kPatMaxLen * 4 <=
+                    (size_t)(NNZCAP + 8) * 4,
+                "a stage's column region holds the pattern bytes and table");
   // parked[2], freed[2]: the reducer warp's hand-over (after the abort flag)
   static constexpr size_t kRedBarOffset = kMetaOffset + 4 * kMetaInts * STAGES + 16;
   static constexpr size_t kSmemBytes = kRedBarOffset + 4 * 8;
@@ -120,8 +137,27 @@ __device__ __forceinline__ bool consumer_bar_or(bool v) {
 // the one-thread-per-row sum in storage order, bit for bit; no barrier
 // joins the consumer warps, so each warp moves on as soon as its rows are
 // done.  Rows of any length up to the tile's entry cap are handled.
-template <int G, class Op>
-__device__ __forceinline__ void wg_rows(Op& op, const double* prod, const int* cc,
+// Columns of a staged CSR tile: entry q of the row starting at staged
+// entry js.
+struct CsrCols {
+  const int* cc;
+  __device__ __forceinline__ const int* row(int, int js) const { return cc + js; }
+  __device__ __forceinline__ int col(const int* rc, int, int q) const { return rc[q]; }
+};
+// Columns of a staged row-pattern tile: row i's offsets from its pattern
+// byte and the pattern table, both staged.
+struct PatCols {
+  const unsigned char* sp;   // pattern bytes, sp[i - b0]
+  int b0;
+  const int* tab;            // [npat][kPatMaxLen]
+  __device__ __forceinline__ const int* row(int i, int) const {
+    return tab + (int)sp[i - b0] * kPatMaxLen;
+  }
+  __device__ __forceinline__ int col(const int* rc, int i, int q) const { return i + rc[q]; }
+};
+
+template <int G, class Op, class Cols>
+__device__ __forceinline__ void wg_rows(Op& op, const double* prod, const Cols& cols,
                                         const int* sr, int p0, int r0, int r1, int j0,
                                         int warp, int lane, int nwarps) {
   constexpr int kRpw = 32 / G;   // rows per warp pass
@@ -131,9 +167,11 @@ __device__ __forceinline__ void wg_rows(Op& op, const double* prod, const int* c
   for (int rb = r0 + warp * kRpw; rb < r1; rb += nwarps * kRpw) {
     const int i = rb + grp;
     int js = 0, len = 0;
+    const int* rc = nullptr;
     if (i < r1) {
       js = sr[i - p0] - j0;
       len = sr[i + 1 - p0] - j0 - js;
+      rc = cols.row(i, js);
     }
     const int maxlen = __reduce_max_sync(0xffffffffu, len);
     double acc = (i < r1) ? op.row_init(i) : 0.0;
@@ -142,7 +180,7 @@ __device__ __forceinline__ void wg_rows(Op& op, const double* prod, const int* c
 #pragma unroll
       for (int u = 0; u < kU; ++u) {
         const int q = k0 + u * G + g;
-        pr[u] = (q < len) ? __dmul_rn(prod[js + q], op.gather(cc[js + q])) : 0.0;
+        pr[u] = (q < len) ? __dmul_rn(prod[js + q], op.gather(cols.col(rc, i, q))) : 0.0;
       }
 #pragma unroll
       for (int u = 0; u < kU; ++u) {
@@ -160,6 +198,18 @@ __device__ __forceinline__ void wg_rows(Op& op, const double* prod, const int* c
     if (g == 0 && i < r1) op.row_done(i, acc);
   }
 }
+
+// Whether a tile source may hand out row-pattern tiles (S::kRowPatterns);
+// sources without the member never do, and their streamers carry no
+// pattern code.
+template <class S, class = void>
+struct tile_patterns {
+  static constexpr bool value = false;
+};
+template <class S>
+struct tile_patterns<S, decltype((void)S::kRowPatterns)> {
+  static constexpr bool value = S::kRowPatterns;
+};
 
 // G = -1: the group width is picked per tile from its mean row length
 // (the same for every warp of the CTA), for sources whose tiles mix short
@@ -182,6 +232,7 @@ __device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLi
   uint64_t* parked = reinterpret_cast<uint64_t*>(tf_smem + L::kRedBarOffset);
   uint64_t* freed = parked + 2;
   constexpr bool kRed = Op::kReducer;
+  constexpr bool kPat = G != 0 && tile_patterns<S>::value;
   int* meta = reinterpret_cast<int*>(tf_smem + L::kMetaOffset);
   volatile int* abort_flag = meta + L::kMetaInts * STAGES;
   auto sval = [&](int s) { return reinterpret_cast<double*>(tf_smem + s * L::kStageBytes); };
@@ -245,16 +296,25 @@ __device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLi
           mbar_arrive_expect_tx(&full[s], 0);
           continue;
         }
+        const bool pat = kPat && d.pat != nullptr && d.npat > 0;
         const int a0 = d.j0 & ~1, a1 = (d.j1 + 1) & ~1;
-        const int c0 = d.j0 & ~3, c1 = (d.j1 + 3) & ~3;
+        // the columns' (or the pattern bytes') first staged element
+        const int c0 = pat ? (d.r0 & ~15) : (d.j0 & ~3);
+        const int c1 = pat ? ((d.r1 + 15) & ~15) : ((d.j1 + 3) & ~3);
         const int p0 = d.r0 & ~3, p1 = (d.r1 + 1 + 3) & ~3;
         m[0] = a0; m[1] = c0; m[2] = p0; m[3] = d.r0; m[4] = d.r1; m[5] = d.j0; m[6] = d.j1;
+        m[11] = pat ? d.npat : 0;
         const unsigned bv = (unsigned)(a1 - a0) * 8u;
-        const unsigned bc = (unsigned)(c1 - c0) * 4u;
+        const unsigned bc = (unsigned)(c1 - c0) * (pat ? 1u : 4u);
         const unsigned br = (unsigned)(p1 - p0) * 4u;
-        mbar_arrive_expect_tx(&full[s], bv + bc + br);
+        const unsigned bt = pat ? (unsigned)d.npat * kPatMaxLen * 4u : 0u;
+        mbar_arrive_expect_tx(&full[s], bv + bc + br + bt);
         if (bv) bulk_g2s(sval(s), d.val + a0, bv, &full[s]);
-        if (bc) bulk_g2s(scol(s), d.col + c0, bc, &full[s]);
+        if (bc && pat) bulk_g2s(scol(s), d.pat + c0, bc, &full[s]);
+        else if (bc) bulk_g2s(scol(s), d.col + c0, bc, &full[s]);
+        if (bt)
+          bulk_g2s(reinterpret_cast<unsigned char*>(scol(s)) + pat_tab_offset<ROWCAP>(), d.tab,
+                   bt, &full[s]);
         bulk_g2s(srow(s), d.row + p0, br, &full[s]);
       }
       for (int k = (issued > STAGES ? issued - STAGES : 0); k < issued; ++k)
@@ -295,16 +355,29 @@ __device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLi
                           *reinterpret_cast<void* const*>(m + 14), m[9], m[10]};
         op.begin(k, aux);
         const double* prod = sval(s) + (j0 - a0);
-        const int* cc = scol(s) + (j0 - c0);
-        if constexpr (G > 0) {
-          wg_rows<G>(op, prod, cc, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
-        } else {
-          switch (tile_group_width(r1 - r0, m[6] - j0)) {
-            case 1: wg_rows<1>(op, prod, cc, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps); break;
-            case 2: wg_rows<2>(op, prod, cc, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps); break;
-            default: wg_rows<4>(op, prod, cc, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+        auto rows = [&](const auto& cols) {
+          if constexpr (G > 0) {
+            wg_rows<G>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+          } else {
+            switch (tile_group_width(r1 - r0, m[6] - j0)) {
+              case 1: wg_rows<1>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps); break;
+              case 2: wg_rows<2>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps); break;
+              default: wg_rows<4>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+            }
+          }
+        };
+        bool done = false;
+        if constexpr (kPat) {
+          if (m[11]) {   // rows of at most kPatMaxLen entries: one lane per row
+            const unsigned char* sp = reinterpret_cast<const unsigned char*>(scol(s));
+            wg_rows<1>(op, prod,
+                       PatCols{sp, c0,
+                               reinterpret_cast<const int*>(sp + pat_tab_offset<ROWCAP>())},
+                       srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+            done = true;
           }
         }
+        if (!done) rows(CsrCols{scol(s) + (j0 - c0)});
         if constexpr (!kRed) op.tile_end(it);
       }
       if constexpr (kRed) {

@@ -43,6 +43,7 @@ def _lib():
     L.tf_batch_trace.argtypes = [_vp, ctypes.POINTER(SweepRec), ctypes.c_int, ip]
     L.tf_batch_kernel_ms.argtypes = [_vp, dp]
     L.tf_batch_info.argtypes = [_vp, ip, ip, ctypes.POINTER(ctypes.c_size_t)]
+    L.tf_batch_upload_ms.argtypes = [_vp, dp, dp, dp]
     L.tf_server_create.argtypes = [_vp, ctypes.POINTER(BatchOpts), ctypes.POINTER(_vp)]
     L.tf_server_submit.argtypes = [_vp, ctypes.c_int, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp,
                                    _vp, ctypes.c_double, ctypes.c_int,
@@ -52,6 +53,7 @@ def _lib():
                                   ctypes.POINTER(ctypes.c_longlong), ip, ip]
     L.tf_server_destroy.argtypes = [_vp]
     L.tf_server_cancel.argtypes = [_vp, ctypes.c_int64]
+    L.tf_server_timing.argtypes = [_vp, dp]
     L._tf_batch_bound = True
     return L
 
@@ -163,6 +165,15 @@ class Batch:
                                            ctypes.byref(fb)), "tf_batch_info")
         return dict(sweeps=sw.value, work_items=wi.value, free_bytes=fb.value)
 
+    def upload_ms(self):
+        """{prep, wait, admit}: milliseconds over all adds so far (host
+        preparation summed over systems, the admitting thread's wait for it,
+        admission with the copies to the device)."""
+        v = [ctypes.c_double() for _ in range(3)]
+        native._check(self.L.tf_batch_upload_ms(self.h, *[ctypes.byref(x) for x in v]),
+                      "tf_batch_upload_ms")
+        return dict(zip(("prep", "wait", "admit"), (x.value for x in v)))
+
     def close(self):
         if getattr(self, "h", None):
             self.L.tf_batch_destroy(self.h)
@@ -209,6 +220,13 @@ class Server:
                                      ctypes.byref(sw))
         return dict(admitted=a.value, completed=c.value, peak_running=pk.value,
                     sweeps=sw.value, error=err)
+
+    def timing(self):
+        """Milliseconds by activity since creation (tf_server_timing)."""
+        out = (ctypes.c_double * 5)()
+        native._check(self.L.tf_server_timing(self.h, out), "tf_server_timing")
+        return dict(zip(("prepare", "admit", "rebuild", "sweeps", "retire"),
+                        (round(v, 1) for v in out)))
 
     def close(self):
         if getattr(self, "h", None):

@@ -241,6 +241,150 @@ def test_server_continuous_batching(gpu_ctx):
         srv.close()
 
 
+def test_batch_row_patterns_equal_csr_columns(gpu_ctx, monkeypatch):
+    """Structured systems stream row patterns (one byte per row) instead of
+    their columns; every row sum, and so every iterate, is the same bit for
+    bit (TF_NO_ROW_PATTERNS keeps the columns)."""
+    sysl = mixed_systems()
+    out = []
+    for no_pat in (False, True):
+        if no_pat:
+            monkeypatch.setenv("TF_NO_ROW_PATTERNS", "1")
+        b = batch.Batch(gpu_ctx, mem_budget=1 << 30)
+        try:
+            free0 = b.info()["free_bytes"]
+            ids = [b.add(s) for s in sysl]
+            used = free0 - b.info()["free_bytes"]
+            b.run()
+            out.append((used, [b.result(i) for i in ids]))
+        finally:
+            b.close()
+    (used_pat, r_pat), (used_csr, r_csr) = out
+    for a, c in zip(r_pat, r_csr):
+        assert a["status"] == c["status"] == "converged"
+        assert a["iters"] == c["iters"] and np.array_equal(a["x"], c["x"])
+    hex_nnz = sum(s.nnz for s in sysl if "-hex-" in s.name)
+    assert used_csr - used_pat >= 3 * hex_nnz   # the hex systems' columns stay home
+
+
+def _with_values(s, seed):
+    """s with the same structure arrays (the same memory) and new values and
+    right-hand side: every off-diagonal a_ij scaled by f_i f_j (seeded; a
+    symmetric matrix stays symmetric), the diagonal kept dominant."""
+    import copy
+    rng = np.random.default_rng(seed)
+    t = copy.copy(s)
+    val = s.val.copy()
+    row0 = s.csr.row - 1
+    col0 = s.csr.col - 1
+    f = rng.uniform(0.7, 1.3, s.n)
+    for i in range(s.n):
+        js, je = row0[i], row0[i + 1]
+        d = s.csr.dia[i] - 1
+        off = np.array([j for j in range(js, je) if j != d], dtype=np.int64)
+        if off.size:
+            val[off] *= f[i] * f[col0[off]]
+            val[d] = max(val[d], 1.05 * np.abs(val[off]).sum())
+    t.val = val
+    t.b = rng.uniform(-1.0, 1.0, s.n)
+    return t
+
+
+def test_shared_structure_equals_separate_structures(gpu_ctx):
+    """Systems that share one structure (the same caller arrays) use one
+    device copy of it; each result equals the same system in a batch of
+    its own, where its structure is uploaded anew."""
+    base = [systems.small_hex(14, seed=31, kind="pressure", ratio=1.02),
+            lattice_poly(12000, 32)]
+    variants = [_with_values(s, 100 + k) for s in base for k in range(3)]
+    alone = []
+    for v in variants:
+        b = batch.Batch(gpu_ctx, mem_budget=1 << 28)
+        try:
+            i = b.add(v)
+            b.run()
+            alone.append(b.result(i))
+        finally:
+            b.close()
+    b = batch.Batch(gpu_ctx, mem_budget=1 << 29)
+    try:
+        free0 = b.info()["free_bytes"]
+        ids = [b.add(v) for v in variants]
+        used_shared = free0 - b.info()["free_bytes"]
+        b.run()
+        for v, i, a in zip(variants, ids, alone):
+            r = b.result(i)
+            assert r["status"] == "converged" and _true_rel(v, r["x"]) <= 1.01 * TOL
+            assert r["iters"] == a["iters"] and np.array_equal(r["x"], a["x"])
+    finally:
+        b.close()
+    # One structure copy (4 B per entry and ~8 per row) per base system, not
+    # one per variant; each variant adds its values, vectors and tile sums.
+    own = sum(8 * v.nnz + 40 * v.n + (8 << 10) for v in variants)
+    shared = sum(4 * s.nnz + 12 * s.n + (8 << 10) for s in base)
+    assert sum(8 * v.nnz for v in variants) < used_shared <= own + shared
+
+
+def test_resident_structures_are_evicted_when_space_is_needed(gpu_ctx):
+    """A retired system's structure stays on the device for later systems
+    with the same structure, and gives its space up when a new structure
+    needs it."""
+    a = systems.small_hex(30, seed=41, kind="pressure")
+    c = systems.small_hex(30, seed=42, kind="pressure", ratio=1.03)
+    # Room for one structure (4 B per entry, ~8 per row) and one system's own
+    # arrays (8 per entry, ~36 per row), not for a second structure.
+    b = batch.Batch(gpu_ctx, mem_budget=12 * a.nnz + 44 * a.n + (64 << 10))
+    try:
+        i = b.add(a)
+        b.run()
+        ra = b.result(i)
+        b.remove(i)
+        i = b.add(_with_values(a, 7))      # same structure: reuses the resident copy
+        b.run()
+        assert b.result(i)["status"] == "converged"
+        b.remove(i)
+        i = b.add(c)                       # new structure: evicts the old one
+        b.run()
+        rc = b.result(i)
+        assert rc["status"] == "converged" and _true_rel(c, rc["x"]) <= 1.01 * TOL
+        b.remove(i)
+        i = b.add(a)                       # the first again, uploaded anew
+        b.run()
+        r = b.result(i)
+        assert r["iters"] == ra["iters"] and np.array_equal(r["x"], ra["x"])
+    finally:
+        b.close()
+
+
+def test_server_shared_structures(gpu_ctx):
+    """Requests that share a structure but not values (a CFD time loop)
+    each equal the same system solved alone."""
+    base = systems.small_hex(16, seed=51, kind="pressure", ratio=1.02)
+    variants = [_with_values(base, 200 + k) for k in range(6)]
+    ref = []
+    for v in variants:
+        b = batch.Batch(gpu_ctx, mem_budget=1 << 28)
+        try:
+            i = b.add(v)
+            b.run()
+            ref.append(b.result(i))
+        finally:
+            b.close()
+    srv = batch.Server(gpu_ctx, mem_budget=1 << 28, sweep_iters=4)
+    try:
+        rids = [srv.submit(v) for v in variants * 2]
+        for k, rid in enumerate(rids):
+            r = srv.wait(rid)
+            want = ref[k % len(variants)]
+            assert r["status"] == "converged"
+            assert r["iters"] == want["iters"] and np.array_equal(r["x"], want["x"])
+        t = srv.timing()
+        assert set(t) == {"prepare", "admit", "rebuild", "sweeps", "retire"}
+        assert t["sweeps"] > 0
+    finally:
+        srv.close()
+
+
 def test_server_cancel_running_and_queued(gpu_ctx):
     """A running request is retired at the end of its sweep and its slot
     reused; a queued one is dropped; a finished one keeps its result."""
