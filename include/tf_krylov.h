@@ -335,8 +335,9 @@ int tf_server_cancel(tf_server s, int64_t req);
  * thread: ms5[0] host preparation of submitted systems (summed over the
  * submitting threads; a structure already prepared for an earlier request
  * is not prepared again), ms5[1] the admission thread (reservations and
- * uploads on its own stream), ms5[2] and ms5[3] the worker thread (commits
- * and work-list rebuilds; sweeps from launch to the state read back), and
+ * uploads on its own stream), ms5[2] and ms5[3] the worker thread (host
+ * work: commits, building and uploading the next work list, launching the
+ * next sweep behind the one in flight; waits for the sweep in flight), and
  * ms5[4] the collector thread (results copied out, retirements). */
 int tf_server_timing(tf_server s, double* ms5);
 int tf_server_destroy(tf_server s);

@@ -111,6 +111,11 @@ struct SysDev {
   double tol;
 };
 
+// Bytes of one slot's descriptor staging (either iterate type).
+constexpr size_t kDescBytes =
+    ((sizeof(SysDev<double>) > sizeof(SysDev<float>) ? sizeof(SysDev<double>)
+                                                      : sizeof(SysDev<float>)) + 63) / 64 * 64;
+
 struct SysState {
   double rho, rho_old, beta, alpha;
   double rr, rr_ru, bnorm2, res_true;
@@ -1116,8 +1121,8 @@ Layout layout_for(const HostSys& h, int ntiles, size_t vsz, int use_val32) {
 }
 
 struct Slot {
-  int used = 0;            // 1: admitted; 2: reserved, its copies in flight;
-                           // 3: out of the work list, its result being copied out
+  int used = 0;            // 1: admitted; 2: reserved, its copies in flight
+  int listed = 0;          // in a work list already (its first residual is queued)
   size_t off = 0, bytes = 0;
   int n = 0, ntiles = 0;
   double done_ms = -1.0;   // wall time from tf_batch_run's start to completion
@@ -1148,21 +1153,39 @@ struct tf_batch_s {
   std::vector<Slot> slots;
   void* d_desc = nullptr;           // SysDev<V>[max_sys]
   SysState* d_state = nullptr;
-  SysState* h_state = nullptr;      // pinned mirror
-  Work* d_work = nullptr;
-  int* d_nwork = nullptr;
-  Work* d_ru = nullptr;          // refinement work list (same capacity)
-  int* d_ru_count = nullptr;
-  FinItem* d_fin = nullptr;      // the finishing kernels' items
-  int* d_nfin = nullptr;
+  SysState* h_state = nullptr;      // the latest known state of every slot
   unsigned* d_gate_cnt = nullptr;
-  int fin_cap = 0;
-  std::vector<FinItem> h_fin;
-  int work_cap = 0;
-  std::vector<Work> h_work, h_ru;
-  int nwork = 0;
-  long long work_rows = 0, work_nnz = 0;   // rows and entries of the listed systems
-  cudaGraphExec_t sweep = nullptr;
+  // Staging of the descriptors and initial states of committed systems
+  // (pinned, one entry per slot: copies ahead of a running sweep stay
+  // asynchronous).
+  unsigned char* h_desc_stage = nullptr;
+  SysState* h_init_stage = nullptr;
+
+  // A work list -- the (system, tile) items, the refinement items of new
+  // systems, the finishing kernels' items -- with its device buffers,
+  // pinned host buffers and the sweep graph bound to them.  The batch API
+  // uses one; the server alternates two, building and uploading the next
+  // sweep's list while the current sweep runs.
+  struct ListSet {
+    Work* d_work = nullptr;
+    Work* d_ru = nullptr;          // refinement work list (same capacity)
+    FinItem* d_fin = nullptr;
+    int* d_cnt = nullptr;          // work items, refinement items, finishing items
+    int work_cap = 0, fin_cap = 0;
+    Work* h_work = nullptr;        // pinned staging of the lists
+    Work* h_ru = nullptr;
+    FinItem* h_fin = nullptr;
+    int* h_cnt = nullptr;
+    int h_work_cap = 0, h_ru_cap = 0, h_fin_cap = 0;
+    SysState* h_state = nullptr;   // pinned: every slot's state after this list's last sweep
+    cudaGraphExec_t graph = nullptr;
+    cudaEvent_t done = nullptr;    // this list's last sweep, state copy included
+    std::vector<int> slots;        // the systems listed
+    int nwork = 0, nru = 0, nfin = 0;
+    long long rows = 0, nnz = 0;   // rows and entries of the listed systems
+  };
+  ListSet ls[2];
+  int nwork = 0;                   // items of the last list built
   int grid_pupdate = 1, grid_update = 1, grid_fold = 1, grid_tile = 1, grid_fin = 1;
   int sweeps = 0;
   long long total_iters = 0;
@@ -1178,12 +1201,20 @@ struct tf_batch_s {
   ~tf_batch_s() {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    if (sweep) cudaGraphExecDestroy(sweep);
+    for (ListSet& L : ls) {
+      if (L.graph) cudaGraphExecDestroy(L.graph);
+      if (L.done) cudaEventDestroy(L.done);
+      for (void* p : {(void*)L.d_work, (void*)L.d_ru, (void*)L.d_fin, (void*)L.d_cnt})
+        if (p) cudaFree(p);
+      for (void* p : {(void*)L.h_work, (void*)L.h_ru, (void*)L.h_fin, (void*)L.h_cnt,
+                      (void*)L.h_state})
+        if (p) cudaFreeHost(p);
+    }
     if (arena.base) cudaFree(arena.base);
-    for (void* p : {d_desc, (void*)d_state, (void*)d_work, (void*)d_nwork, (void*)d_ru,
-                    (void*)d_ru_count, (void*)d_fin, (void*)d_nfin, (void*)d_gate_cnt})
+    for (void* p : {d_desc, (void*)d_state, (void*)d_gate_cnt})
       if (p) cudaFree(p);
-    if (h_state) cudaFreeHost(h_state);
+    for (void* p : {(void*)h_state, (void*)h_desc_stage, (void*)h_init_stage})
+      if (p) cudaFreeHost(p);
   }
 
   // Shared memory of the tile kernels: the producer-warp streamer (FP64
@@ -1191,9 +1222,9 @@ struct tf_batch_s {
   static size_t smem_csr2() { return Csr2Layout<kRows, kNnzCap, kStages>::kSmemBytes; }
   static size_t smem_rows32() { return TileLayout<kRows, kNnzCap, float, kStages>::kSmemBytes; }
 
-  BatchArgs args() const {
-    return BatchArgs{d_desc,     d_state, d_work, d_nwork, opts.ru_delta * opts.ru_delta,
-                     RuList{d_ru, d_ru_count}, d_fin, d_nfin, d_gate_cnt, 0, 0};
+  BatchArgs args(const ListSet& L) const {
+    return BatchArgs{d_desc,      d_state,       L.d_work, L.d_cnt, opts.ru_delta * opts.ru_delta,
+                     RuList{L.d_ru, L.d_cnt + 1}, L.d_fin, L.d_cnt + 2, d_gate_cnt, 0, 0};
   }
 
   // The kernels of an iteration, in launch order (tf_batch_kernel_ms).
@@ -1247,7 +1278,8 @@ struct tf_batch_s {
   double kern_ms[kKernels] = {};
   int run_sweep_profiled() {
     cudaStream_t s = ctx->stream;
-    const BatchArgs a = args();
+    ListSet& L = ls[0];
+    const BatchArgs a = args(L);
     constexpr int kEv = kKernels + 1;
     std::vector<cudaEvent_t> ev(kEv * opts.sweep_iters);
     for (auto& e : ev) TF_CUDA_TRY(cudaEventCreate(&e));
@@ -1256,9 +1288,10 @@ struct tf_batch_s {
                               : launch_iteration<double>(s, a, &ev[kEv * it]);
       if (st != TF_OK) return st;
     }
-    TF_CUDA_TRY(cudaMemcpyAsync(h_state, d_state, (size_t)max_sys * sizeof(SysState),
+    TF_CUDA_TRY(cudaMemcpyAsync(L.h_state, d_state, (size_t)max_sys * sizeof(SysState),
                                 cudaMemcpyDeviceToHost, s));
     TF_CUDA_TRY(cudaStreamSynchronize(s));
+    merge_state(L);
     for (int k = 0; k < kKernels; ++k) sweep_kms[k] = 0.0;
     for (int it = 0; it < opts.sweep_iters; ++it)
       for (int k = 0; k < kKernels; ++k) {
@@ -1301,27 +1334,37 @@ struct tf_batch_s {
     return TF_OK;
   }
 
-  int build_sweep() {
-    if (sweep) {
-      cudaGraphExecDestroy(sweep);
-      sweep = nullptr;
+  // The sweep graph of list set L (it holds L's buffers), ending with the
+  // copy of every slot's state into L.h_state.
+  int build_sweep(ListSet& L) {
+    if (L.graph) {
+      cudaGraphExecDestroy(L.graph);
+      L.graph = nullptr;
     }
     cudaGraph_t g = nullptr;
     TF_CUDA_TRY(cudaGraphCreate(&g, 0));
-    const int st = vsz == 4 ? add_sweep_nodes<float>(g) : add_sweep_nodes<double>(g);
+    cudaGraphNode_t last = nullptr;
+    int st = vsz == 4 ? add_sweep_nodes<float>(g, L, &last) : add_sweep_nodes<double>(g, L, &last);
     cudaError_t e = cudaSuccess;
-    if (st == TF_OK) e = cudaGraphInstantiate(&sweep, g, 0);
+    if (st == TF_OK) {
+      cudaGraphNode_t cp = nullptr;
+      e = cudaGraphAddMemcpyNode1D(&cp, g, &last, 1, L.h_state, d_state,
+                                   (size_t)max_sys * sizeof(SysState), cudaMemcpyDeviceToHost);
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&L.graph, g, 0);
+      if (e != cudaSuccess) {
+        tf_set_last_cuda_error(e, "batch sweep graph", __FILE__, __LINE__);
+        st = TF_ERR_CUDA;
+      }
+    }
     cudaGraphDestroy(g);
-    if (st != TF_OK) return st;
-    TF_CUDA_TRY(e);
-    return TF_OK;
+    return st;
   }
 
   // A sweep as a graph: per iteration pupdate -> spmv -> alpha -> update ->
   // beta -> IF(gate){ fold -> residual -> test }, each iteration's IF node
   // with a conditional handle of its own (kb_beta of that iteration sets it).
   template <typename V>
-  int add_sweep_nodes(cudaGraph_t g) {
+  int add_sweep_nodes(cudaGraph_t g, const ListSet& L, cudaGraphNode_t* last) {
     const std::vector<Launch> ks = iteration_kernels<V>();
     auto add = [](cudaGraph_t gr, const Launch& k, const BatchArgs* a, cudaGraphNode_t dep,
                   cudaGraphNode_t* out) {
@@ -1336,7 +1379,7 @@ struct tf_batch_s {
     };
     cudaGraphNode_t dep = nullptr;
     for (int it = 0; it < opts.sweep_iters; ++it) {
-      BatchArgs a = args();
+      BatchArgs a = args(L);
       cudaError_t e = cudaGraphConditionalHandleCreate(&a.ru_gate, g, 0,
                                                        cudaGraphCondAssignDefault);
       a.use_gate = 1;
@@ -1357,6 +1400,7 @@ struct tf_batch_s {
         return TF_ERR_CUDA;
       }
     }
+    *last = dep;
     return TF_OK;
   }
 
@@ -1390,17 +1434,24 @@ struct tf_batch_s {
     TF_CUDA_TRY(cudaMemset(d_state, 0, (size_t)max_sys * sizeof(SysState)));
     TF_CUDA_TRY(cudaMallocHost((void**)&h_state, (size_t)max_sys * sizeof(SysState)));
     memset(h_state, 0, (size_t)max_sys * sizeof(SysState));
-    TF_CUDA_TRY(cudaMalloc((void**)&d_nwork, sizeof(int)));
-    TF_CUDA_TRY(cudaMemset(d_nwork, 0, sizeof(int)));
-    TF_CUDA_TRY(cudaMalloc((void**)&d_ru_count, sizeof(int)));
-    TF_CUDA_TRY(cudaMemset(d_ru_count, 0, sizeof(int)));
-    TF_CUDA_TRY(cudaMalloc((void**)&d_nfin, sizeof(int)));
-    TF_CUDA_TRY(cudaMemset(d_nfin, 0, sizeof(int)));
+    TF_CUDA_TRY(cudaMallocHost((void**)&h_desc_stage, (size_t)max_sys * kDescBytes));
+    TF_CUDA_TRY(cudaMallocHost((void**)&h_init_stage, (size_t)max_sys * sizeof(SysState)));
+    for (ListSet& L : ls) {
+      TF_CUDA_TRY(cudaMalloc((void**)&L.d_cnt, 4 * sizeof(int)));
+      TF_CUDA_TRY(cudaMemset(L.d_cnt, 0, 4 * sizeof(int)));
+      TF_CUDA_TRY(cudaMallocHost((void**)&L.h_cnt, 4 * sizeof(int)));
+      TF_CUDA_TRY(cudaMallocHost((void**)&L.h_state, (size_t)max_sys * sizeof(SysState)));
+      TF_CUDA_TRY(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
+    }
     TF_CUDA_TRY(cudaMalloc((void**)&d_gate_cnt, sizeof(unsigned)));
     TF_CUDA_TRY(cudaMemset(d_gate_cnt, 0, sizeof(unsigned)));
     st = (vsz == 4) ? setup_kernels<float>() : setup_kernels<double>();
     if (st != TF_OK) return st;
-    return build_sweep();
+    for (ListSet& L : ls) {
+      st = build_sweep(L);
+      if (st != TF_OK) return st;
+    }
+    return TF_OK;
   }
 
   // ---- admission: prepare, reserve, upload, commit ----
@@ -1615,7 +1666,8 @@ struct tf_batch_s {
   }
 
   // Makes an uploaded system part of the batch: its descriptor and state
-  // (on the engine's stream, ahead of the next sweep).  The copies of the
+  // (on the engine's stream, asynchronously from the slot's pinned staging,
+  // ahead of the next sweep launched there).  The copies of the
   // reservation must have completed.  Engine lock held.
   int commit(const HostSys& h, const Reservation& rv) {
     Slot& sl = slots[rv.slot];
@@ -1653,16 +1705,20 @@ struct tf_batch_s {
       d.use_val32 = opts.val_fp32;
       d.tol = h.tol;
     };
-    SysState ss{};
+    SysState& ss = h_init_stage[rv.slot];
+    ss = SysState{};
     ss.status = kInit;
     cudaError_t e;
+    void* stage = h_desc_stage + (size_t)rv.slot * kDescBytes;
     if (vsz == 4) {
-      SysDev<float> d{};
+      SysDev<float>& d = *static_cast<SysDev<float>*>(stage);
+      d = SysDev<float>{};
       fill(d);
       e = cudaMemcpyAsync((SysDev<float>*)d_desc + rv.slot, &d, sizeof d,
                           cudaMemcpyHostToDevice, s);
     } else {
-      SysDev<double> d{};
+      SysDev<double>& d = *static_cast<SysDev<double>*>(stage);
+      d = SysDev<double>{};
       fill(d);
       e = cudaMemcpyAsync((SysDev<double>*)d_desc + rv.slot, &d, sizeof d,
                           cudaMemcpyHostToDevice, s);
@@ -1714,71 +1770,119 @@ struct tf_batch_s {
     return st;
   }
 
-  // Work list = every tile of every system that still iterates; the
-  // refinement list starts with the tiles of systems not yet initialised.
-  int rebuild_work() {
-    h_work.clear();
-    h_ru.clear();
-    h_fin.clear();
-    work_rows = work_nnz = 0;
-    for (int i = 0; i < max_sys; ++i) {
-      if (slots[i].used != 1) continue;
-      const int stt = h_state[i].status;
-      if (stt != kInit && stt != kActive) continue;
-      const std::vector<int>& tl = slots[i].st->tiles;
-      const std::vector<int>& tj = slots[i].st->tile_j;
-      work_rows += slots[i].n;
-      work_nnz += tj[slots[i].ntiles];
-      for (int c = 0; c < fin_chunks(slots[i].ntiles); ++c) h_fin.push_back(FinItem{i, c});
-      for (int t = 0; t < slots[i].ntiles; ++t) {
-        const Work wk{i, t, tl[t], tl[t + 1], tj[t], tj[t + 1]};
-        h_work.push_back(wk);
-        if (stt == kInit) h_ru.push_back(wk);
-      }
-    }
-    nwork = (int)h_work.size();
-    const int nfin = (int)h_fin.size();
-    if (nwork > work_cap || nfin > fin_cap) {
-      if (d_work) cudaFree(d_work);
-      if (d_ru) cudaFree(d_ru);
-      if (d_fin) cudaFree(d_fin);
-      d_work = nullptr;
-      d_ru = nullptr;
-      d_fin = nullptr;
-      work_cap = std::max(nwork, 2 * work_cap);
-      fin_cap = std::max(nfin, 2 * fin_cap);
-      TF_CUDA_TRY(cudaMalloc((void**)&d_work, (size_t)work_cap * sizeof(Work)));
-      TF_CUDA_TRY(cudaMalloc((void**)&d_ru, (size_t)work_cap * sizeof(Work)));
-      TF_CUDA_TRY(cudaMalloc((void**)&d_fin, (size_t)fin_cap * sizeof(FinItem)));
-      int st = build_sweep();   // the graph holds the lists' pointers
-      if (st != TF_OK) return st;
-    }
-    cudaStream_t s = ctx->stream;
-    const int nru = (int)h_ru.size();
-    if (nwork)
-      TF_CUDA_TRY(cudaMemcpyAsync(d_work, h_work.data(), (size_t)nwork * sizeof(Work),
-                                  cudaMemcpyHostToDevice, s));
-    if (nru)
-      TF_CUDA_TRY(cudaMemcpyAsync(d_ru, h_ru.data(), (size_t)nru * sizeof(Work),
-                                  cudaMemcpyHostToDevice, s));
-    TF_CUDA_TRY(cudaMemcpyAsync(d_nwork, &nwork, sizeof(int), cudaMemcpyHostToDevice, s));
-    if (nfin)
-      TF_CUDA_TRY(cudaMemcpyAsync(d_fin, h_fin.data(), (size_t)nfin * sizeof(FinItem),
-                                  cudaMemcpyHostToDevice, s));
-    TF_CUDA_TRY(cudaMemcpyAsync(d_nfin, &nfin, sizeof(int), cudaMemcpyHostToDevice, s));
-    TF_CUDA_TRY(cudaMemcpyAsync(d_ru_count, &nru, sizeof(int), cudaMemcpyHostToDevice, s));
-    TF_CUDA_TRY(cudaStreamSynchronize(s));
+  // Grows a pinned buffer (contents dropped) to at least n elements.
+  template <typename T>
+  static int grow_pinned(T** p, int* cap, int n) {
+    if (n <= *cap) return TF_OK;
+    if (*p) cudaFreeHost(*p);
+    *p = nullptr;
+    *cap = std::max(n, 2 * *cap);
+    TF_CUDA_TRY(cudaMallocHost((void**)p, (size_t)*cap * sizeof(T)));
     return TF_OK;
   }
 
-  // One sweep (sweep_iters iterations), then refresh the host state mirror.
+  // Fills list set L: every tile of every admitted system that still
+  // iterates (skip[slot] != 0 leaves a system out); the refinement list
+  // starts with the tiles of systems not yet initialised.  Grows L's
+  // buffers (and rebuilds its graph) when needed, which requires L's last
+  // sweep to have finished.  Engine lock held when threads share the engine.
+  int build_list(ListSet& L, const std::vector<char>* skip = nullptr) {
+    int nw = 0, nr = 0, nf = 0;
+    L.slots.clear();
+    L.rows = L.nnz = 0;
+    for (int i = 0; i < max_sys; ++i) {
+      if (slots[i].used != 1 || (skip && (*skip)[i])) continue;
+      const int stt = h_state[i].status;
+      if (stt != kInit && stt != kActive) continue;
+      L.slots.push_back(i);
+      nw += slots[i].ntiles;
+      if (stt == kInit && !slots[i].listed) nr += slots[i].ntiles;
+      nf += fin_chunks(slots[i].ntiles);
+      L.rows += slots[i].n;
+      L.nnz += slots[i].st->tile_j[slots[i].ntiles];
+    }
+    int st = grow_pinned(&L.h_work, &L.h_work_cap, std::max(nw, 1));
+    if (st == TF_OK) st = grow_pinned(&L.h_ru, &L.h_ru_cap, std::max(nr, 1));
+    if (st == TF_OK) st = grow_pinned(&L.h_fin, &L.h_fin_cap, std::max(nf, 1));
+    if (st != TF_OK) return st;
+    if (nw > L.work_cap || nf > L.fin_cap) {
+      for (void* p : {(void*)L.d_work, (void*)L.d_ru, (void*)L.d_fin})
+        if (p) cudaFree(p);
+      L.d_work = nullptr;
+      L.d_ru = nullptr;
+      L.d_fin = nullptr;
+      L.work_cap = std::max(nw, 2 * L.work_cap);
+      L.fin_cap = std::max(nf, 2 * L.fin_cap);
+      TF_CUDA_TRY(cudaMalloc((void**)&L.d_work, (size_t)L.work_cap * sizeof(Work)));
+      TF_CUDA_TRY(cudaMalloc((void**)&L.d_ru, (size_t)L.work_cap * sizeof(Work)));
+      TF_CUDA_TRY(cudaMalloc((void**)&L.d_fin, (size_t)L.fin_cap * sizeof(FinItem)));
+      st = build_sweep(L);   // the graph holds the lists' pointers
+      if (st != TF_OK) return st;
+    }
+    int w = 0, r = 0, f = 0;
+    for (int i : L.slots) {
+      const std::vector<int>& tl = slots[i].st->tiles;
+      const std::vector<int>& tj = slots[i].st->tile_j;
+      // A new system's first residual is queued once, with its first list:
+      // a list built while that sweep is still in flight sees the system's
+      // state as new too, and must not queue it again (the refinement
+      // kernels would then fold and recompute its tiles twice, concurrently).
+      const bool init = h_state[i].status == kInit && !slots[i].listed;
+      slots[i].listed = 1;
+      for (int t = 0; t < slots[i].ntiles; ++t) {
+        const Work wk{i, t, tl[t], tl[t + 1], tj[t], tj[t + 1]};
+        L.h_work[w++] = wk;
+        if (init) L.h_ru[r++] = wk;
+      }
+      for (int c = 0; c < fin_chunks(slots[i].ntiles); ++c) L.h_fin[f++] = FinItem{i, c};
+    }
+    L.nwork = nw;
+    L.nru = nr;
+    L.nfin = nf;
+    nwork = nw;
+    return TF_OK;
+  }
+
+  // Copies L's lists to the device on stream s (asynchronously: from pinned
+  // memory, ahead of the sweep launched after them).
+  int upload_list(ListSet& L, cudaStream_t s) {
+    if (L.nwork)
+      TF_CUDA_TRY(cudaMemcpyAsync(L.d_work, L.h_work, (size_t)L.nwork * sizeof(Work),
+                                  cudaMemcpyHostToDevice, s));
+    if (L.nru)
+      TF_CUDA_TRY(cudaMemcpyAsync(L.d_ru, L.h_ru, (size_t)L.nru * sizeof(Work),
+                                  cudaMemcpyHostToDevice, s));
+    if (L.nfin)
+      TF_CUDA_TRY(cudaMemcpyAsync(L.d_fin, L.h_fin, (size_t)L.nfin * sizeof(FinItem),
+                                  cudaMemcpyHostToDevice, s));
+    L.h_cnt[0] = L.nwork;
+    L.h_cnt[1] = L.nru;
+    L.h_cnt[2] = L.nfin;
+    TF_CUDA_TRY(cudaMemcpyAsync(L.d_cnt, L.h_cnt, 3 * sizeof(int), cudaMemcpyHostToDevice, s));
+    return TF_OK;
+  }
+
+  // The listed systems' state after L's sweep (slots not in the list keep
+  // theirs: they may have been committed since the sweep was launched).
+  void merge_state(const ListSet& L) {
+    for (int i : L.slots) h_state[i] = L.h_state[i];
+  }
+
+  // The batch API's list: set 0, built and uploaded ahead of the next sweep.
+  int rebuild_work() {
+    int st = build_list(ls[0]);
+    if (st == TF_OK) st = upload_list(ls[0], ctx->stream);
+    return st;
+  }
+
+  // One sweep (sweep_iters iterations) of set 0, then refresh the host state.
   int run_sweep() {
     if (profile) return run_sweep_profiled();
-    cudaStream_t s = ctx->stream;
-    TF_CUDA_TRY(cudaGraphLaunch(sweep, s));
-    TF_CUDA_TRY(cudaMemcpyAsync(h_state, d_state, (size_t)max_sys * sizeof(SysState),
-                                cudaMemcpyDeviceToHost, s));
-    TF_CUDA_TRY(cudaStreamSynchronize(s));
+    ListSet& L = ls[0];
+    TF_CUDA_TRY(cudaGraphLaunch(L.graph, ctx->stream));
+    TF_CUDA_TRY(cudaEventRecord(L.done, ctx->stream));
+    TF_CUDA_TRY(cudaEventSynchronize(L.done));
+    merge_state(L);
     ++sweeps;
     return TF_OK;
   }
@@ -1805,8 +1909,8 @@ struct tf_batch_s {
       tf_batch_sweep rec{};
       rec.active = running;
       rec.items = nwork;
-      rec.rows = work_rows;
-      rec.nnz = work_nnz;
+      rec.rows = ls[0].rows;
+      rec.nnz = ls[0].nnz;
       rec.ms = std::chrono::duration<double, std::milli>(te - ts).count();
       if (profile)
         for (int k = 0; k < kKernels; ++k) rec.kernel_ms[k] = sweep_kms[k];
@@ -1851,7 +1955,7 @@ struct tf_batch_s {
   // Engine lock held by callers that share the engine between threads.
   void retire(int slot) {
     Slot& sl = slots[slot];
-    if (sl.used != 1 && sl.used != 3) return;
+    if (sl.used != 1) return;
     sl.st->users -= 1;
     sl.st->last_use = ++tick;
     arena.release(sl.off, sl.bytes);
@@ -2138,9 +2242,9 @@ struct tf_server_s {
   int peak_running = 0;
   // Wall time (ms) by activity (tf_server_timing): preparation on the
   // submitting threads (summed), the admission thread's reservations and
-  // uploads, the worker thread's commits and work-list rebuilds, its
-  // sweeps (launch to state read), and the collector's result copies and
-  // retirements.
+  // uploads, the worker thread's host work (commits, lists, launches) and
+  // its waits for the sweep in flight, and the collector's result copies
+  // and retirements.
   double t_ms[5] = {0, 0, 0, 0, 0};
   static double ms_since(Clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
@@ -2227,27 +2331,43 @@ struct tf_server_s {
     }
   }
 
+  // The worker: sweeps back to back, two work lists alternating.  While
+  // sweep k runs, the next list is built from the systems admitted so far
+  // (committed ones included, finished ones left out), uploaded and sweep
+  // k + 1 launched behind it; then the worker waits for sweep k, reads its
+  // state and takes the systems it finished (or that were cancelled) out
+  // of the lists.  Those are still in sweep k + 1's list (built before they
+  // were seen), where they are skipped; they go to the collector once sweep
+  // k + 1 has ended, so no sweep in flight refers to their memory when it
+  // is released.
   void loop() {
     cudaSetDevice(eng.ctx->device);
+    cudaStream_t s = eng.ctx->stream;
+    std::vector<char> out(eng.max_sys, 0);          // left out of the lists
+    std::vector<std::shared_ptr<Request>> leaving;  // out of the next list, still in the one in flight
+    int cur = 0;
+    bool inflight = false;
     for (;;) {
       std::vector<std::shared_ptr<Request>> ready;
       std::shared_ptr<Request> wait_for;
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv_work.wait(lk, [&] { return stop || !staged.empty() || !by_slot.empty(); });
-        if (stop) return;
+        cv_work.wait(lk, [&] {
+          return stop || !staged.empty() || !by_slot.empty() || inflight || !leaving.empty();
+        });
+        if (stop) break;
         while (!staged.empty() && cudaEventQuery(staged.front()->ev) == cudaSuccess) {
           ready.push_back(staged.front());
           staged.pop_front();
         }
-        if (ready.empty() && by_slot.empty()) wait_for = staged.front();
+        if (ready.empty() && by_slot.empty() && !inflight && leaving.empty())
+          wait_for = staged.front();
       }
       if (wait_for) {   // nothing to sweep: wait for the next upload to land
         cudaEventSynchronize(wait_for->ev);
         continue;
       }
       auto t0 = Clock::now();
-      bool changed = false;
       for (auto& r : ready) {
         cudaEventDestroy(r->ev);
         r->ev = nullptr;
@@ -2271,30 +2391,51 @@ struct tf_server_s {
         r->slot = r->rv.slot;
         r->t_admit = Clock::now();
         r->h = HostSys();   // on the device now
+        out[r->slot] = 0;
         by_slot[r->slot] = r;
         n_running = (int)by_slot.size();
         ++admitted;
-        changed = true;
-      }
-      if (by_slot.empty()) {
-        std::lock_guard<std::mutex> lk(mu);
-        t_ms[2] += ms_since(t0);
-        continue;
       }
       peak_running = std::max(peak_running, (int)by_slot.size());
+      // Launch the next sweep behind the one in flight.
+      const int nxt = inflight ? (cur ^ 1) : cur;
+      bool launched = false;
       int st = TF_OK;
-      if (changed)
+      if (!by_slot.empty()) {
+        tf_batch_s::ListSet& L = eng.ls[nxt];
         st = tf_guarded([&] {
           std::lock_guard<std::mutex> el(eng.emu);
-          return eng.rebuild_work();
+          return eng.build_list(L, &out);
         });
-      const auto t1 = Clock::now();
-      if (st == TF_OK) st = tf_guarded([&] { return eng.run_sweep(); });
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        t_ms[2] += std::chrono::duration<double, std::milli>(t1 - t0).count();
-        t_ms[3] += ms_since(t1);
+        if (st == TF_OK && L.nwork > 0) {
+          st = eng.upload_list(L, s);
+          if (st == TF_OK) {
+            cudaError_t e = cudaGraphLaunch(L.graph, s);
+            if (e == cudaSuccess) e = cudaEventRecord(L.done, s);
+            if (e != cudaSuccess) {
+              tf_set_last_cuda_error(e, "server sweep", __FILE__, __LINE__);
+              st = TF_ERR_CUDA;
+            }
+          }
+          launched = st == TF_OK;
+        }
       }
+      const auto t1 = Clock::now();
+      // Wait for the sweep in flight and read its state.
+      std::vector<int> fin, cancelled;
+      if (st == TF_OK && inflight) {
+        tf_batch_s::ListSet& L = eng.ls[cur];
+        const cudaError_t e = cudaEventSynchronize(L.done);
+        if (e != cudaSuccess) {
+          tf_set_last_cuda_error(e, "server sweep", __FILE__, __LINE__);
+          st = TF_ERR_CUDA;
+        } else {
+          std::lock_guard<std::mutex> el(eng.emu);
+          eng.merge_state(L);
+          ++eng.sweeps;
+        }
+      }
+      const auto t2 = Clock::now();
       if (st != TF_OK) {
         std::lock_guard<std::mutex> lk(mu);
         error = st;
@@ -2305,50 +2446,58 @@ struct tf_server_s {
         by_slot.clear();
         n_running = 0;
         cv_done.notify_all();
+        inflight = false;
         continue;
       }
-      t0 = Clock::now();
-      // Finished systems, and cancelled ones that have not finished, leave
-      // the work list now; the collector copies their results out and
-      // retires them.
-      std::vector<int> fin, cancelled;
-      {
-        std::lock_guard<std::mutex> lk(mu);
+      std::lock_guard<std::mutex> lk(mu);
+      // Systems left out of the list just launched are in no sweep now.
+      if (inflight && !leaving.empty()) {
+        for (auto& r : leaving) finishing.push_back(r);
+        leaving.clear();
+        cv_collect.notify_one();
+      }
+      if (inflight) {
         for (auto& kv : by_slot) {
-          const int s = eng.h_state[kv.first].status;
-          if (s != kInit && s != kActive) fin.push_back(kv.first);
+          const int ss = eng.h_state[kv.first].status;
+          if (ss != kInit && ss != kActive) fin.push_back(kv.first);
           else if (kv.second->cancel) cancelled.push_back(kv.first);
         }
+        for (int slot : fin) {
+          auto r = by_slot[slot];
+          const SysState& ss = eng.h_state[slot];
+          r->status = ss.status;
+          r->iters = ss.iter;
+          r->n_ru = ss.n_ru;
+          r->res = ss.res_true;
+        }
+        for (int slot : cancelled) by_slot[slot]->status = -TF_ERR_CANCELLED;
+        for (int slot : fin) {
+          out[slot] = 1;
+          leaving.push_back(by_slot[slot]);
+          by_slot.erase(slot);
+        }
+        for (int slot : cancelled) {
+          out[slot] = 1;
+          leaving.push_back(by_slot[slot]);
+          by_slot.erase(slot);
+        }
+        n_running = (int)by_slot.size();
       }
-      if (fin.empty() && cancelled.empty()) continue;
-      st = tf_guarded([&] {
-        std::lock_guard<std::mutex> el(eng.emu);
-        for (int slot : fin) eng.slots[slot].used = 3;
-        for (int slot : cancelled) eng.slots[slot].used = 3;
-        return eng.rebuild_work();
-      });
-      std::lock_guard<std::mutex> lk(mu);
-      if (st != TF_OK) error = st;
-      for (int slot : fin) {
-        auto r = by_slot[slot];
-        const SysState& ss = eng.h_state[slot];
-        r->status = ss.status;
-        r->iters = ss.iter;
-        r->n_ru = ss.n_ru;
-        r->res = ss.res_true;
-        by_slot.erase(slot);
-        finishing.push_back(r);
+      if (launched) {
+        cur = nxt;
+        inflight = true;
+      } else {
+        inflight = false;
+        // Nothing in flight: whatever is leaving is in no sweep.
+        for (auto& r : leaving) finishing.push_back(r);
+        if (!leaving.empty()) cv_collect.notify_one();
+        leaving.clear();
       }
-      for (int slot : cancelled) {
-        auto r = by_slot[slot];
-        r->status = -TF_ERR_CANCELLED;
-        by_slot.erase(slot);
-        finishing.push_back(r);
-      }
-      n_running = (int)by_slot.size();
-      t_ms[2] += ms_since(t0);
-      cv_collect.notify_one();
+      t_ms[2] += std::chrono::duration<double, std::milli>(t1 - t0).count() + ms_since(t2);
+      t_ms[3] += std::chrono::duration<double, std::milli>(t2 - t1).count();
     }
+    // Stopping: let the sweeps end before the engine goes away.
+    cudaStreamSynchronize(s);
   }
 
   void collect_loop() {
