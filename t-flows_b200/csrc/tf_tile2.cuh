@@ -131,9 +131,10 @@ __device__ __forceinline__ bool consumer_bar_or(bool v) {
 // Warp-group consumers (G = 1, 2, 4 or 8; G = 0 selects the two-phase
 // consumers above).  Each warp takes 32/G rows of the staged tile at a
 // time, G lanes per row: lane g of a row's group forms the products of
-// the row's entries g, g+G, g+2G, ... of a 16-entry chunk (16/G gathers in
-// flight per lane), and the group's first lane adds the 16 products in
-// entry order, fetched by warp shuffles, before the next chunk.  The sum is
+// the row's entries g, g+G, g+2G, ... of a chunk of CHUNK entries (CHUNK/G
+// gathers in flight per lane), and the group's first lane adds the
+// chunk's products in entry order, fetched by warp shuffles, before the
+// next chunk.  The sum is
 // the one-thread-per-row sum in storage order, bit for bit; no barrier
 // joins the consumer warps, so each warp moves on as soon as its rows are
 // done.  Rows of any length up to the tile's entry cap are handled.
@@ -156,12 +157,13 @@ struct PatCols {
   __device__ __forceinline__ int col(const int* rc, int i, int q) const { return i + rc[q]; }
 };
 
-template <int G, class Op, class Cols>
+template <int G, int CHUNK, class Op, class Cols>
 __device__ __forceinline__ void wg_rows(Op& op, const double* prod, const Cols& cols,
                                         const int* sr, int p0, int r0, int r1, int j0,
                                         int warp, int lane, int nwarps) {
   constexpr int kRpw = 32 / G;   // rows per warp pass
-  constexpr int kU = 16 / G;     // products per lane per 16-entry chunk
+  constexpr int kChunk = CHUNK;  // entries per chunk (see wg_chunk)
+  constexpr int kU = kChunk / G;  // products per lane per chunk
   const int grp = lane / G, g = lane & (G - 1);
   const int gbase = lane & ~(G - 1);
   for (int rb = r0 + warp * kRpw; rb < r1; rb += nwarps * kRpw) {
@@ -175,7 +177,7 @@ __device__ __forceinline__ void wg_rows(Op& op, const double* prod, const Cols& 
     }
     const int maxlen = __reduce_max_sync(0xffffffffu, len);
     double acc = (i < r1) ? op.row_init(i) : 0.0;
-    for (int k0 = 0; k0 < maxlen; k0 += 16) {
+    for (int k0 = 0; k0 < maxlen; k0 += kChunk) {
       double pr[kU];
 #pragma unroll
       for (int u = 0; u < kU; ++u) {
@@ -210,6 +212,15 @@ template <class S>
 struct tile_patterns<S, decltype((void)S::kRowPatterns)> {
   static constexpr bool value = S::kRowPatterns;
 };
+
+// Entries per chunk for one lane per row: every slot of a chunk costs its
+// instructions even when predicated off, and on short rows (hex: 7
+// entries) this path is issue-bound, so tiles of at most 8 entries per row
+// on average take chunks of 8; longer rows keep 16 (their second chunk's
+// gathers would otherwise wait for the first chunk's sum).
+__device__ __forceinline__ bool wg_short_rows(int rows, int entries) {
+  return entries <= 8 * rows;
+}
 
 // G = -1: the group width is picked per tile from its mean row length
 // (the same for every warp of the CTA), for sources whose tiles mix short
@@ -355,14 +366,23 @@ __device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLi
                           *reinterpret_cast<void* const*>(m + 14), m[9], m[10]};
         op.begin(k, aux);
         const double* prod = sval(s) + (j0 - a0);
+        const bool short_rows = wg_short_rows(r1 - r0, m[6] - j0);
+        auto one_lane = [&](const auto& cols) {
+          if (short_rows)
+            wg_rows<1, 8>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+          else
+            wg_rows<1, 16>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+        };
         auto rows = [&](const auto& cols) {
-          if constexpr (G > 0) {
-            wg_rows<G>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+          if constexpr (G == 1) {
+            one_lane(cols);
+          } else if constexpr (G > 0) {
+            wg_rows<G, 16>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
           } else {
             switch (tile_group_width(r1 - r0, m[6] - j0)) {
-              case 1: wg_rows<1>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps); break;
-              case 2: wg_rows<2>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps); break;
-              default: wg_rows<4>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+              case 1: one_lane(cols); break;
+              case 2: wg_rows<2, 16>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps); break;
+              default: wg_rows<4, 16>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
             }
           }
         };
@@ -370,10 +390,8 @@ __device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLi
         if constexpr (kPat) {
           if (m[11]) {   // rows of at most kPatMaxLen entries: one lane per row
             const unsigned char* sp = reinterpret_cast<const unsigned char*>(scol(s));
-            wg_rows<1>(op, prod,
-                       PatCols{sp, c0,
-                               reinterpret_cast<const int*>(sp + pat_tab_offset<ROWCAP>())},
-                       srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+            one_lane(PatCols{sp, c0,
+                             reinterpret_cast<const int*>(sp + pat_tab_offset<ROWCAP>())});
             done = true;
           }
         }
