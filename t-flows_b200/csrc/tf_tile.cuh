@@ -212,21 +212,25 @@ struct PatTable {
 };
 
 // One row of a row-pattern tile for operators with per-row hooks
-// (kRowOps: gather / row_init / combine / row_done): all of the row's
-// (at most kPatMaxLen) gathers are issued before the first product is
-// added, so a thread keeps its row's loads in flight together; the sum is
-// the one-entry-at-a-time sum in storage order, bit for bit.
+// (kRowOps: gather / row_init / combine / row_done): the row's gathers are
+// issued eight at a time before their products are added, so a thread
+// keeps a hex row's (at most 7) loads in flight together; the sum is the
+// one-entry-at-a-time sum in storage order, bit for bit.  Eight slots, not
+// kPatMaxLen: every slot costs its instructions even when predicated off,
+// and on hex rows this loop is issue-bound.
 template <class Op>
 __device__ __forceinline__ void pat_row(Op& op, int i, const double* v, const int* off,
                                         int len) {
   double acc = op.row_init(i);
-  double pr[kPatMaxLen];
+  for (int u0 = 0; u0 < len; u0 += 8) {
+    double pr[8];
 #pragma unroll
-  for (int u = 0; u < kPatMaxLen; ++u)
-    pr[u] = (u < len) ? __dmul_rn(v[u], op.gather(i + off[u])) : 0.0;
+    for (int u = 0; u < 8; ++u)
+      pr[u] = (u0 + u < len) ? __dmul_rn(v[u0 + u], op.gather(i + off[u0 + u])) : 0.0;
 #pragma unroll
-  for (int u = 0; u < kPatMaxLen; ++u)
-    if (u < len) acc = op.combine(acc, pr[u]);
+    for (int u = 0; u < 8; ++u)
+      if (u0 + u < len) acc = op.combine(acc, pr[u]);
+  }
   op.row_done(i, acc);
 }
 
