@@ -255,9 +255,10 @@ int tf_batch_add(tf_batch b, int n, int64_t nnz, const int* row, const int* col,
                  const double* x0, double tol, int maxit, int* sys);
 /* Several systems at once (array i holds system i's arguments of
  * tf_batch_add; x0 may be NULL, or x0[i] NULL for zeros).  The host
- * preparation runs on `threads` threads (0: one per hardware thread, at
- * most 64), holding at most 2 x threads prepared host copies at a time;
- * systems are admitted in order, so sys[] and the results equal count calls
+ * preparation and the copies to the device run on `threads` threads (0:
+ * one per hardware thread, at most 64; each copies on a stream of its own),
+ * holding at most 2 x threads prepared host copies at a time; slots and
+ * space are reserved in order, so sys[] and the results equal count calls
  * of tf_batch_add.  On an error the systems before the failing one stay
  * added (sys[i] >= 0), the rest get sys[i] = -1.  No reference counterpart
  * (the reference solves one system per call). */
@@ -299,8 +300,9 @@ int tf_batch_info(tf_batch b, int* sweeps, int* work_items, size_t* free_bytes);
 /* Where the time of tf_batch_add / tf_batch_add_many went, in milliseconds
  * over all adds so far: host preparation (conversion, checks, renumbering,
  * tiling) summed over the systems -- on worker threads for add_many, so it
- * can exceed the wall time --, the admitting thread's wait for prepared
- * systems, and admission (arena allocation and the copies to the device).
+ * can exceed the wall time --, the reserving thread's wait for prepared
+ * systems, and admission (reservations, and the copies to the device summed
+ * over the threads that make them).
  * Any pointer may be NULL. */
 int tf_batch_upload_ms(tf_batch b, double* prep_ms, double* wait_ms, double* admit_ms);
 

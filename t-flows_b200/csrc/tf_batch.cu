@@ -1130,6 +1130,51 @@ struct Slot {
   std::shared_ptr<Structure> st;
 };
 
+// Copies from pageable host memory through two pinned buffers in turn: a
+// thread fills one while the DMA of the other runs, so host-to-device
+// copies run at the DMA rate instead of the driver's staged pageable rate,
+// and several threads copying at once do not serialise on its staging.
+struct Stager {
+  static constexpr size_t kBytes = (size_t)8 << 20;   // per buffer
+  unsigned char* buf[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};   // the last DMA from each buffer
+  int k = 0;
+  int init() {
+    for (int j = 0; j < 2; ++j) {
+      TF_CUDA_TRY(cudaMallocHost((void**)&buf[j], kBytes));
+      TF_CUDA_TRY(cudaEventCreateWithFlags(&done[j], cudaEventDisableTiming));
+    }
+    return TF_OK;
+  }
+  ~Stager() {
+    for (int j = 0; j < 2; ++j) {
+      if (done[j]) {
+        cudaEventSynchronize(done[j]);
+        cudaEventDestroy(done[j]);
+      }
+      if (buf[j]) cudaFreeHost(buf[j]);
+    }
+  }
+  cudaError_t copy(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    const unsigned char* from = static_cast<const unsigned char*>(src);
+    unsigned char* to = static_cast<unsigned char*>(dst);
+    while (bytes) {
+      const size_t c = std::min(bytes, kBytes);
+      cudaError_t e = cudaEventSynchronize(done[k]);   // its last DMA has drained
+      if (e != cudaSuccess) return e;
+      memcpy(buf[k], from, c);
+      e = cudaMemcpyAsync(to, buf[k], c, cudaMemcpyHostToDevice, s);
+      if (e == cudaSuccess) e = cudaEventRecord(done[k], s);
+      if (e != cudaSuccess) return e;
+      k ^= 1;
+      from += c;
+      to += c;
+      bytes -= c;
+    }
+    return cudaSuccess;
+  }
+};
+
 // A slot and arena space held for a system whose copies are in flight.
 struct Reservation {
   int slot = -1;
@@ -1186,6 +1231,28 @@ struct tf_batch_s {
   };
   ListSet ls[2];
   int nwork = 0;                   // items of the last list built
+
+  // Pinned staging for uploads, kept for later calls (one per copying thread).
+  std::mutex stager_mu;
+  std::vector<std::unique_ptr<Stager>> stagers;
+  std::unique_ptr<Stager> take_stager() {
+    {
+      std::lock_guard<std::mutex> lk(stager_mu);
+      if (!stagers.empty()) {
+        std::unique_ptr<Stager> p = std::move(stagers.back());
+        stagers.pop_back();
+        return p;
+      }
+    }
+    std::unique_ptr<Stager> p(new Stager());
+    if (p->init() != TF_OK) return nullptr;   // copies go without staging then
+    return p;
+  }
+  void give_stager(std::unique_ptr<Stager> p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(stager_mu);
+    stagers.push_back(std::move(p));
+  }
   int grid_pupdate = 1, grid_update = 1, grid_fold = 1, grid_tile = 1, grid_fin = 1;
   int sweeps = 0;
   long long total_iters = 0;
@@ -1628,15 +1695,18 @@ struct tf_batch_s {
   }
 
   // The copies of a reserved system (and of its structure when new) on
-  // stream s.  No lock: the reservation's slot and segments are this
-  // caller's until it commits or gives them back.
-  int upload(const HostSys& h, const Reservation& rv, cudaStream_t s) {
+  // stream s, through `stager`'s pinned buffers when given.  No lock: the
+  // reservation's slot and segments are this caller's until it commits or
+  // gives them back.
+  int upload(const HostSys& h, const Reservation& rv, cudaStream_t s,
+             Stager* stager = nullptr) {
     const Slot& sl = slots[rv.slot];
     const Structure& S = *sl.st;
     const Layout& L = rv.L;
     char* base = arena.base + sl.off;
     auto up = [&](char* dst, const void* src, size_t bytes) {
-      return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+      return stager ? stager->copy(dst, src, bytes, s)
+                    : cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
     };
     const size_t n8 = (size_t)h.n + 8;
     cudaError_t e = cudaSuccess;
@@ -2010,10 +2080,11 @@ extern "C" int tf_batch_add(tf_batch bt, int n, int64_t nnz, const int* row, con
 }
 
 // Several systems in one call: the host preparation (conversion,
-// renumbering, tiling) runs on `threads` worker threads (0: one per
-// hardware thread) while this thread admits the prepared systems in order,
-// so slots, results and errors are those of tf_batch_add called for each
-// system in turn.  At most 2 x threads prepared systems wait for admission.
+// renumbering, tiling) and the copies to the device run on `threads`
+// worker threads (0: one per hardware thread), each copying on a stream of
+// its own; this thread reserves slots and space in order, so slots,
+// results and errors are those of tf_batch_add called for each system in
+// turn.  At most 2 x threads prepared systems wait for their copies.
 extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int64_t* nnz,
                                  const int* const* row, const int* const* col,
                                  const int* const* dia, const double* const* val,
@@ -2029,86 +2100,142 @@ extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int
   int nt = threads > 0 ? threads : (int)std::thread::hardware_concurrency();
   nt = std::max(1, std::min(std::min(nt, count), 64));
   const int window = 2 * nt;
+  using clk = std::chrono::steady_clock;
+  auto ms_since = [](clk::time_point t0) {
+    return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+  };
   std::vector<HostSys> hs(count);
+  std::vector<Reservation> rv(count);
   std::vector<int> st(count, TF_OK);
   std::vector<char> ready(count, 0);
+  std::deque<int> upq;   // reserved, waiting for their copies
   std::mutex mu;
-  std::condition_variable cv_ready, cv_room;
-  int next = 0, admitted = 0;
-  bool stop = false;
+  std::condition_variable cv;
+  int next = 0, reserved = 0, copied = 0;
+  bool stop_prep = false, stop_all = false;
+  int copy_err = TF_OK;
   double prep_ms = 0.0, wait_ms = 0.0, admit_ms = 0.0;
+  auto prepare = [&](int i) {
+    const auto t0 = clk::now();
+    const int r = tf_guarded([&] {
+      return bt->prepare(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
+                         x0 ? x0[i] : nullptr, tol[i], maxit[i]);
+    });
+    const double ms = ms_since(t0);
+    std::lock_guard<std::mutex> lk(mu);
+    st[i] = r;
+    ready[i] = 1;
+    prep_ms += ms;
+  };
+  // The copies of reserved system i on stream s, then its commit.
+  auto copy_in = [&](int i, cudaStream_t s, Stager* stager) {
+    const auto t0 = clk::now();
+    int r = tf_guarded([&] { return bt->upload(hs[i], rv[i], s, stager); });
+    if (r == TF_OK) {
+      const cudaError_t e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) {
+        tf_set_last_cuda_error(e, "batch admit copies", __FILE__, __LINE__);
+        r = TF_ERR_CUDA;
+      }
+    }
+    {
+      std::lock_guard<std::mutex> el(bt->emu);
+      if (r == TF_OK) r = tf_guarded([&] { return bt->commit(hs[i], rv[i]); });
+      else bt->unreserve(rv[i]);
+    }
+    hs[i] = HostSys();   // on the device now
+    std::lock_guard<std::mutex> lk(mu);
+    if (r == TF_OK) sys[i] = rv[i].slot;
+    else if (copy_err == TF_OK) copy_err = r;
+    ++copied;
+    admit_ms += ms_since(t0);
+  };
   auto worker = [&]() {
+    cudaSetDevice(bt->ctx->device);
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) s = nullptr;
+    std::unique_ptr<Stager> stager = bt->take_stager();
     for (;;) {
-      int i;
+      int i = -1;
+      bool up = false;
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv_room.wait(lk, [&] { return stop || next >= count || next < admitted + window; });
-        if (stop || next >= count) return;
-        i = next++;
+        cv.wait(lk, [&] {
+          return stop_all || !upq.empty() ||
+                 (!stop_prep && next < count && next < copied + window);
+        });
+        if (!upq.empty()) {
+          i = upq.front();
+          upq.pop_front();
+          up = true;
+        } else if (!stop_prep && next < count && next < copied + window) {
+          i = next++;
+        } else {
+          break;   // stop_all
+        }
       }
-      const auto t0 = std::chrono::steady_clock::now();
-      const int r = tf_guarded([&] {
-        return bt->prepare(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
-                           x0 ? x0[i] : nullptr, tol[i], maxit[i]);
-      });
-      const double ms =
-          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
-              .count();
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        st[i] = r;
-        ready[i] = 1;
-        prep_ms += ms;
-      }
-      cv_ready.notify_all();
+      if (up) copy_in(i, s ? s : bt->ctx->stream, stager.get());
+      else prepare(i);
+      cv.notify_all();
     }
+    if (s) cudaStreamSynchronize(s);
+    bt->give_stager(std::move(stager));
+    if (s) cudaStreamDestroy(s);
   };
   std::vector<std::thread> pool;
   try {
     for (int t = 0; t < nt; ++t) pool.emplace_back(worker);
   } catch (const std::system_error&) {
-    // fewer workers than asked for (none: this thread prepares each system)
+    // fewer workers than asked for (none: this thread does everything)
   }
-  const bool inline_prep = pool.empty();
+  const bool inline_work = pool.empty();
   int result = TF_OK;
   for (int i = 0; i < count; ++i) {
-    const auto t0 = std::chrono::steady_clock::now();
-    if (inline_prep) {
-      st[i] = tf_guarded([&] {
-        return bt->prepare(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
-                           x0 ? x0[i] : nullptr, tol[i], maxit[i]);
-      });
+    const auto t0 = clk::now();
+    if (inline_work) {
+      prepare(i);
     } else {
       std::unique_lock<std::mutex> lk(mu);
-      cv_ready.wait(lk, [&] { return ready[i] != 0; });
+      cv.wait(lk, [&] { return ready[i] != 0; });
     }
-    const auto t1 = std::chrono::steady_clock::now();
+    const auto t1 = clk::now();
     int r = st[i];
-    if (r == TF_OK) r = tf_guarded([&] { return bt->admit(hs[i], &sys[i]); });
-    hs[i] = HostSys();   // its host copy is on the device now
-    const auto t2 = std::chrono::steady_clock::now();
-    (inline_prep ? prep_ms : wait_ms) += std::chrono::duration<double, std::milli>(t1 - t0).count();
-    admit_ms += std::chrono::duration<double, std::milli>(t2 - t1).count();
+    if (r == TF_OK) {
+      std::lock_guard<std::mutex> el(bt->emu);
+      r = tf_guarded([&] { return bt->reserve(hs[i], &rv[i]); });
+    }
     {
       std::lock_guard<std::mutex> lk(mu);
-      admitted = i + 1;
-      if (r != TF_OK) stop = true;
+      wait_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
+      admit_ms += ms_since(t1);
+      if (r == TF_OK) {
+        ++reserved;
+        if (!inline_work) upq.push_back(i);
+      } else {
+        stop_prep = true;
+      }
     }
-    cv_room.notify_all();
+    cv.notify_all();
+    if (inline_work && r == TF_OK) copy_in(i, bt->ctx->stream, nullptr);
     if (r != TF_OK) {
+      hs[i] = HostSys();
       result = r;
       break;
     }
   }
   {
-    std::lock_guard<std::mutex> lk(mu);
-    stop = true;
+    std::unique_lock<std::mutex> lk(mu);
+    stop_prep = true;
+    cv.wait(lk, [&] { return copied == reserved; });
+    stop_all = true;
   }
-  cv_room.notify_all();
+  cv.notify_all();
   for (auto& t : pool) t.join();
+  TF_CUDA_TRY(cudaStreamSynchronize(bt->ctx->stream));   // the commits' descriptors
   bt->up_prep_ms += prep_ms;
   bt->up_wait_ms += wait_ms;
   bt->up_admit_ms += admit_ms;
+  if (result == TF_OK) result = copy_err;
   return result;
   TF_API_END
 }
@@ -2261,6 +2388,7 @@ struct tf_server_s {
 
   void admit_loop() {
     cudaSetDevice(eng.ctx->device);
+    std::unique_ptr<Stager> stager = eng.take_stager();
     for (;;) {
       std::shared_ptr<Request> r;
       uint64_t gen;
@@ -2293,7 +2421,8 @@ struct tf_server_s {
         continue;
       }
       cudaEvent_t ev = nullptr;
-      if (st == TF_OK) st = tf_guarded([&] { return eng.upload(r->h, rv, copy_stream); });
+      if (st == TF_OK)
+        st = tf_guarded([&] { return eng.upload(r->h, rv, copy_stream, stager.get()); });
       if (st == TF_OK) {
         cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventRecord(ev, copy_stream);
