@@ -283,6 +283,9 @@ typedef struct tf_batch_sweep {
   int active;            /* systems iterating when the sweep was launched */
   int items;             /* work items (row tiles) in its list */
   int64_t rows, nnz;     /* rows and entries of those systems */
+  double iter_bytes;     /* their inner iteration's algorithmic bytes: 12 per
+                            entry (8 per entry and 1 per row with row
+                            patterns), 4 per row pointer, 13 iterate vectors */
   double ms;             /* wall time, launch to the state read back */
   double kernel_ms[8];   /* TF_BATCH_PROFILE only (else 0): the sweep's time in
                             the eight kernels of tf_batch_kernel_ms */

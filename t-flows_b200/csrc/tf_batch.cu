@@ -1228,6 +1228,7 @@ struct tf_batch_s {
     std::vector<int> slots;        // the systems listed
     int nwork = 0, nru = 0, nfin = 0;
     long long rows = 0, nnz = 0;   // rows and entries of the listed systems
+    double bytes = 0.0;            // their inner iteration's algorithmic bytes
   };
   ListSet ls[2];
   int nwork = 0;                   // items of the last list built
@@ -1860,6 +1861,7 @@ struct tf_batch_s {
     int nw = 0, nr = 0, nf = 0;
     L.slots.clear();
     L.rows = L.nnz = 0;
+    L.bytes = 0.0;
     for (int i = 0; i < max_sys; ++i) {
       if (slots[i].used != 1 || (skip && (*skip)[i])) continue;
       const int stt = h_state[i].status;
@@ -1869,7 +1871,13 @@ struct tf_batch_s {
       if (stt == kInit && !slots[i].listed) nr += slots[i].ntiles;
       nf += fin_chunks(slots[i].ntiles);
       L.rows += slots[i].n;
-      L.nnz += slots[i].st->tile_j[slots[i].ntiles];
+      const long long e = slots[i].st->tile_j[slots[i].ntiles];
+      L.nnz += e;
+      // An inner iteration's algorithmic bytes: the matrix (8 per value and
+      // 4 per column, or 1 per row with row patterns; 4 per row pointer) and
+      // 13 iterate vectors (p gathered and read, q, r, x-correction, 1/d).
+      L.bytes += (double)e * (slots[i].st->npat ? 8.0 : 12.0) +
+                 (double)slots[i].n * ((slots[i].st->npat ? 1.0 : 0.0) + 4.0 + 13.0 * vsz);
     }
     int st = grow_pinned(&L.h_work, &L.h_work_cap, std::max(nw, 1));
     if (st == TF_OK) st = grow_pinned(&L.h_ru, &L.h_ru_cap, std::max(nr, 1));
@@ -1981,6 +1989,7 @@ struct tf_batch_s {
       rec.items = nwork;
       rec.rows = ls[0].rows;
       rec.nnz = ls[0].nnz;
+      rec.iter_bytes = ls[0].bytes;
       rec.ms = std::chrono::duration<double, std::milli>(te - ts).count();
       if (profile)
         for (int k = 0; k < kKernels; ++k) rec.kernel_ms[k] = sweep_kms[k];

@@ -19,7 +19,8 @@ class BatchOpts(ctypes.Structure):
 class SweepRec(ctypes.Structure):
     """tf_batch_sweep: one sweep of a tf_batch_run."""
     _fields_ = [("active", ctypes.c_int), ("items", ctypes.c_int),
-                ("rows", ctypes.c_int64), ("nnz", ctypes.c_int64), ("ms", ctypes.c_double),
+                ("rows", ctypes.c_int64), ("nnz", ctypes.c_int64),
+                ("iter_bytes", ctypes.c_double), ("ms", ctypes.c_double),
                 ("kernel_ms", ctypes.c_double * 8)]
 
 
@@ -144,7 +145,8 @@ class Batch:
         recs = (SweepRec * max(n, 1))()
         native._check(self.L.tf_batch_trace(self.h, recs, n, ctypes.byref(cnt)),
                       "tf_batch_trace")
-        return [dict(active=r.active, items=r.items, rows=r.rows, nnz=r.nnz, ms=r.ms,
+        return [dict(active=r.active, items=r.items, rows=r.rows, nnz=r.nnz,
+                     iter_bytes=r.iter_bytes, ms=r.ms,
                      kernel_ms=dict(zip(KERNELS, list(r.kernel_ms))))
                 for r in recs[:n]]
 

@@ -182,6 +182,8 @@ def test_batch_trace_records(gpu_ctx, profiled, monkeypatch):
         assert tr[0]["active"] == len(sysl)
         assert tr[0]["rows"] == sum(s.n for s in sysl)
         assert tr[0]["nnz"] == sum(s.nnz for s in sysl)
+        nnz, rows = tr[0]["nnz"], tr[0]["rows"]
+        assert 8 * nnz + 56 * rows <= tr[0]["iter_bytes"] <= 12 * nnz + 57 * rows
         assert all(t["ms"] > 0 and t["items"] > 0 for t in tr)
         assert all(a["active"] >= c["active"] and a["rows"] >= c["rows"]
                    for a, c in zip(tr, tr[1:]))
