@@ -65,6 +65,9 @@ def parse():
                     help="batched: comma list of mixed, fp64_batched, mixed_two_phase, drop_in, "
                          "streams, pool; served: pool, mixed (default all)")
     ap.add_argument("--rate", type=float, default=200.0, help="served: arrivals per second")
+    ap.add_argument("--max-running", default="0",
+                    help="served: comma list of the mixed server's system slots to run "
+                         "(0: as many as requests outstanding)")
     ap.add_argument("--seconds", type=float, default=60.0, help="served: window length")
     ap.add_argument("--iters", type=int, default=30, help="iters: Cg iterations per solve")
     ap.add_argument("--mesh", default="hex", choices=["hex", "poly-lattice", "poly-delaunay"],
@@ -401,7 +404,7 @@ def _serve_stream(req_sys, rhs, rate, seconds, workers, budget, seed, max_outsta
 
 
 def _serve_stream_mixed(req_sys, rhs, rate, seconds, budget, seed, max_outstanding=256,
-                        submit_threads=8):
+                        submit_threads=8, max_running=0):
     """The same Poisson stream into the continuous-batching server
     (tf_server_*: the mixed-precision engine, requests admitted into free
     slots between sweeps, Krylov state resident).  Submission copies and
@@ -417,7 +420,11 @@ def _serve_stream_mixed(req_sys, rhs, rate, seconds, budget, seed, max_outstandi
     sizes = np.array([s.n for s in req_sys])
     kinds = np.array([s.solver for s in req_sys])
     ctx = native.Context(0)
-    srv = batch.Server(ctx, mem_budget=budget, max_systems=max_outstanding + 8,
+    # max_running: the server's system slots (0: every outstanding request
+    # can be admitted); fewer slots keep large requests from being spread
+    # over a crowded sweep, at the price of waits in the queue.
+    srv = batch.Server(ctx, mem_budget=budget,
+                       max_systems=max_running if max_running > 0 else max_outstanding + 8,
                        sweep_iters=8)
     results, lock = [], threading.Lock()
     state = {"outstanding": 0}
@@ -524,10 +531,17 @@ def run_served(args):
         # The mixed-precision continuous-batching server on the same streams
         # (tol: ||b - A x|| / ||b|| <= 1e-10 in FP64).
         _serve_stream_mixed(req_sys, rhs, 5.0, 3.0, budget, 1)     # warm-up
-        mixed = _serve_stream_mixed(req_sys, rhs, args.rate, args.seconds, budget, 2)
-        out["mixed_server"] = mixed
+        for k, cap in enumerate(int(c) for c in args.max_running.split(",")):
+            tag = "" if k == 0 else f"_max_running_{cap}"
+            mixed_k = _serve_stream_mixed(req_sys, rhs, args.rate, args.seconds, budget, 2,
+                                          max_running=cap)
+            mixed_k["max_running"] = cap
+            out["mixed_server" + tag] = mixed_k
+            if k == 0:
+                mixed = mixed_k
         out["mixed_server_half_load"] = _serve_stream_mixed(
-            req_sys, rhs, max(1.0, 0.5 * mixed["solves_per_s"]), args.seconds / 2, budget, 3)
+            req_sys, rhs, max(1.0, 0.5 * mixed["solves_per_s"]), args.seconds / 2, budget, 3,
+            max_running=int(args.max_running.split(",")[0]))
     if "pool" in parts and "mixed" in parts:
         out["throughput_ratio_mixed_server_vs_one_at_a_time"] = (
             mixed["solves_per_s"] / max(out["one_at_a_time"]["solves_per_s"], 1e-9))

@@ -1051,23 +1051,32 @@ struct HostSys {
   int n = 0;
   long long nnz = 0;
   std::vector<double> val, b, x0;
+  const double* val_in = nullptr;   // the caller's values, used in place (borrowed)
   std::vector<float> val32;
   double tol = 1e-10;
   int maxit = 10000;
+  const double* values() const { return val_in ? val_in : val.data(); }
 };
 
 // The per-system arrays of h in S's order (val permuted row by row with the
-// structure when it was renumbered).
+// structure when it was renumbered).  borrow: the caller's values stay
+// where they are until the upload (a structure in the caller's numbering
+// needs no copy of them).
 int prepare_values(HostSys& h, const Structure& S, const int* row, const double* val,
-                   const double* b, const double* x0, int use_val32) {
+                   const double* b, const double* x0, int use_val32, bool borrow) {
   if (!val || !b) return TF_ERR_ARG;
   const int n = S.n;
   const long long nnz = S.nnz;
   h.n = n;
   h.nnz = nnz;
+  h.val_in = nullptr;
   if (S.perm.empty()) {
-    h.val.assign(val, val + nnz);
-    h.val.resize((size_t)nnz + 8, 0.0);
+    if (borrow && !use_val32) {
+      h.val_in = val;
+    } else {
+      h.val.assign(val, val + nnz);
+      h.val.resize((size_t)nnz + 8, 0.0);
+    }
     h.b.assign(b, b + n);
     if (x0) h.x0.assign(x0, x0 + n);
     else h.x0.assign(n, 0.0);
@@ -1101,8 +1110,8 @@ Layout layout_for(const HostSys& h, int ntiles, size_t vsz, int use_val32) {
   size_t o = 0;
   auto take = [&](size_t bytes) { size_t r = o; o = Arena::up(o + bytes); return r; };
   const size_t n8 = (size_t)h.n + 8;
-  L.val = take(h.val.size() * 8);
-  L.val32 = use_val32 ? take(h.val32.size() * 4) : 0;
+  L.val = take(((size_t)h.nnz + 8) * 8);
+  L.val32 = use_val32 ? take(((size_t)h.nnz + 8) * 4) : 0;
   L.b = take(n8 * 8);
   L.x = take(n8 * 8);
   L.xlo = take(n8 * vsz);
@@ -1546,8 +1555,11 @@ struct tf_batch_s {
   // all the systems that share it, even while the first of them is still
   // being prepared), else prepared here; then its values.  Host allocation
   // failures are TF_ERR_OOM.
+  // borrow: val stays the caller's until the upload (calls that upload
+  // before returning).
   int prepare(HostSys& h, int n, long long nnz, const int* row, const int* col, const int* dia,
-              const double* val, const double* b, const double* x0, double tol, int maxit) {
+              const double* val, const double* b, const double* x0, double tol, int maxit,
+              bool borrow = false) {
     try {
       if (n < 1 || nnz < n || !row || !col || !dia || !val || !b) return TF_ERR_ARG;
       h.key = struct_key(n, nnz, row, col, dia);
@@ -1590,7 +1602,7 @@ struct tf_batch_s {
       h.st = std::move(S);
       h.tol = tol;
       h.maxit = maxit;
-      return prepare_values(h, *h.st, row, val, b, x0, opts.val_fp32);
+      return prepare_values(h, *h.st, row, val, b, x0, opts.val_fp32, borrow);
     } catch (const std::bad_alloc&) {
       h = HostSys();
       return TF_ERR_OOM;
@@ -1720,9 +1732,9 @@ struct tf_batch_s {
       if (e == cudaSuccess && S.npat) e = up(sbase + S.o_pat, S.pat.data(), S.pat.size());
       if (e == cudaSuccess && S.npat) e = up(sbase + S.o_tab, S.tab.data(), S.tab.size() * 4);
     }
-    if (e == cudaSuccess) e = up(base + L.val, h.val.data(), h.val.size() * 8);
+    if (e == cudaSuccess) e = up(base + L.val, h.values(), (size_t)h.nnz * 8);
     if (e == cudaSuccess && opts.val_fp32)
-      e = up(base + L.val32, h.val32.data(), h.val32.size() * 4);
+      e = up(base + L.val32, h.val32.data(), (size_t)h.nnz * 4);
     if (e == cudaSuccess) e = up(base + L.b, h.b.data(), (size_t)h.n * 8);
     if (e == cudaSuccess) e = up(base + L.x, h.x0.data(), (size_t)h.n * 8);
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.xlo, 0, n8 * vsz, s);
@@ -2076,7 +2088,7 @@ extern "C" int tf_batch_add(tf_batch bt, int n, int64_t nnz, const int* row, con
   if (!bt || !sys) return TF_ERR_ARG;
   HostSys h;
   const auto t0 = std::chrono::steady_clock::now();
-  int st = bt->prepare(h, n, nnz, row, col, dia, val, b, x0, tol, maxit);
+  int st = bt->prepare(h, n, nnz, row, col, dia, val, b, x0, tol, maxit, true);
   const auto t1 = std::chrono::steady_clock::now();
   bt->up_prep_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
   if (st != TF_OK) return st;
@@ -2128,7 +2140,7 @@ extern "C" int tf_batch_add_many(tf_batch bt, int count, const int* n, const int
     const auto t0 = clk::now();
     const int r = tf_guarded([&] {
       return bt->prepare(hs[i], n[i], nnz[i], row[i], col[i], dia[i], val[i], rhs[i],
-                         x0 ? x0[i] : nullptr, tol[i], maxit[i]);
+                         x0 ? x0[i] : nullptr, tol[i], maxit[i], true);
     });
     const double ms = ms_since(t0);
     std::lock_guard<std::mutex> lk(mu);
