@@ -65,9 +65,9 @@ def parse():
                     help="batched: comma list of mixed, fp64_batched, mixed_two_phase, drop_in, "
                          "streams, pool; served: pool, mixed (default all)")
     ap.add_argument("--rate", type=float, default=200.0, help="served: arrivals per second")
-    ap.add_argument("--max-running", default="0",
+    ap.add_argument("--max-running", default="96",
                     help="served: comma list of the mixed server's system slots to run "
-                         "(0: as many as requests outstanding)")
+                         "(0: as many as requests outstanding); the first is the headline")
     ap.add_argument("--seconds", type=float, default=60.0, help="served: window length")
     ap.add_argument("--iters", type=int, default=30, help="iters: Cg iterations per solve")
     ap.add_argument("--mesh", default="hex", choices=["hex", "poly-lattice", "poly-delaunay"],
