@@ -249,7 +249,11 @@ int tf_batch_destroy(tf_batch b);
  * 16th column index; its device copy stays resident after its systems
  * retire and is dropped, least recently used first, when a new system
  * needs the space.  Arrays changed in place between calls must change in
- * those hashed entries, or be passed at other addresses. */
+ * those hashed entries, or be passed at other addresses.  A structure whose
+ * rows fit at most 64 column-offset patterns (structured hex blocks) is
+ * stored as one pattern byte per row instead of its columns (the
+ * environment variable TF_NO_ROW_PATTERNS keeps the columns; the same bits
+ * either way).  The values are read in place until the call returns. */
 int tf_batch_add(tf_batch b, int n, int64_t nnz, const int* row, const int* col,
                  const int* dia, const double* val, const double* rhs,
                  const double* x0, double tol, int maxit, int* sys);

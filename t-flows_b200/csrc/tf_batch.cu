@@ -1311,7 +1311,10 @@ struct tf_batch_s {
     size_t smem;
   };
   template <typename V>
-  std::vector<Launch> iteration_kernels() const {
+  std::vector<Launch> iteration_kernels(const ListSet& L) const {
+    // The finishing kernels need no more CTAs than the list can hold items
+    // (a single large system has a handful).
+    const int gf = std::max(1, std::min(grid_fin, L.fin_cap));
     const void* spmv = opts.val_fp32         ? (const void*)kb_spmv<V, float, 0>
                        : opts.two_phase_rows ? (const void*)kb_spmv<V, double, 0>
                                              : (const void*)kb_spmv<V, double, -1>;
@@ -1321,12 +1324,12 @@ struct tf_batch_s {
                                              : (const void*)kb_ru_res<V, -1>;
     return {{(const void*)kb_pupdate<V>, grid_pupdate, 256, 0},
             {spmv, grid_tile, spmv_block, spmv_smem},
-            {(const void*)kb_alpha<V>, grid_fin, kFinThreads, 0},
+            {(const void*)kb_alpha<V>, gf, kFinThreads, 0},
             {(const void*)kb_update<V>, grid_update, 256, 0},
-            {(const void*)kb_beta<V>, grid_fin, kFinThreads, 0},
+            {(const void*)kb_beta<V>, gf, kFinThreads, 0},
             {(const void*)kb_ru_fold<V>, grid_fold, 256, 0},
             {ru_res, grid_tile, kCsr2RedThreads, smem_csr2()},
-            {(const void*)kb_ru_finish<V>, grid_fin, kFinThreads, 0}};
+            {(const void*)kb_ru_finish<V>, gf, kFinThreads, 0}};
   }
   // The last three (fold, FP64 residual, test) run only when a system is
   // due a refinement: in the sweep graph they sit in an IF node that
@@ -1336,8 +1339,8 @@ struct tf_batch_s {
   // Direct launches of one iteration (profiling: ev receives an event before
   // each kernel and after the last).
   template <typename V>
-  int launch_iteration(cudaStream_t s, const BatchArgs& a, cudaEvent_t* ev) {
-    const std::vector<Launch> ks = iteration_kernels<V>();
+  int launch_iteration(cudaStream_t s, const BatchArgs& a, const ListSet& L, cudaEvent_t* ev) {
+    const std::vector<Launch> ks = iteration_kernels<V>(L);
     int e = 0;
     for (const Launch& k : ks) {
       if (ev) cudaEventRecord(ev[e++], s);
@@ -1361,8 +1364,8 @@ struct tf_batch_s {
     std::vector<cudaEvent_t> ev(kEv * opts.sweep_iters);
     for (auto& e : ev) TF_CUDA_TRY(cudaEventCreate(&e));
     for (int it = 0; it < opts.sweep_iters; ++it) {
-      const int st = vsz == 4 ? launch_iteration<float>(s, a, &ev[kEv * it])
-                              : launch_iteration<double>(s, a, &ev[kEv * it]);
+      const int st = vsz == 4 ? launch_iteration<float>(s, a, L, &ev[kEv * it])
+                              : launch_iteration<double>(s, a, L, &ev[kEv * it]);
       if (st != TF_OK) return st;
     }
     TF_CUDA_TRY(cudaMemcpyAsync(L.h_state, d_state, (size_t)max_sys * sizeof(SysState),
@@ -1442,7 +1445,7 @@ struct tf_batch_s {
   // with a conditional handle of its own (kb_beta of that iteration sets it).
   template <typename V>
   int add_sweep_nodes(cudaGraph_t g, const ListSet& L, cudaGraphNode_t* last) {
-    const std::vector<Launch> ks = iteration_kernels<V>();
+    const std::vector<Launch> ks = iteration_kernels<V>(L);
     auto add = [](cudaGraph_t gr, const Launch& k, const BatchArgs* a, cudaGraphNode_t dep,
                   cudaGraphNode_t* out) {
       cudaKernelNodeParams p{};
