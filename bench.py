@@ -79,7 +79,7 @@ def parse():
     ap.add_argument("--rcm", action="store_true",
                     help="spmv: renumber the cells by reverse Cuthill-McKee first")
     ap.add_argument("--mode", default="solve",
-                    choices=["solve", "spmv", "iters", "multi", "poly", "batched", "served",
+                    choices=["solve", "spmv", "iters", "multi", "poly", "single", "batched", "served",
                              "icc"],
                     help="spmv: only the pressure matrix and `--steps` SpMV launches "
                          "(the small case profiled with ncu); iters: `--steps` Cg solves "
@@ -754,7 +754,8 @@ def run_poly_system(args):
     A = sps.csr_matrix((s.val, s.csr.col - 1, s.csr.row - 1), shape=(s.n, s.n))
     rel = lambda x: float(np.linalg.norm(s.b - A @ x) / np.linalg.norm(s.b))  # noqa: E731
     ctx = native.Context(0)
-    out = {"mode": "poly", "mesh": args.mesh, "n": s.n, "nnz": s.nnz, "gen_s": gen}
+    out = {"mode": "poly", "mesh": "poly-lattice" if args.mesh == "poly-lattice" else "poly-delaunay",
+           "n": s.n, "nnz": s.nnz, "gen_s": gen}
     # FP64 drop-in.  Its stopping test is the reference's NRMS, which on a
     # mesh with widely varying cell sizes differs from the true relative
     # residual by orders of magnitude: tol is calibrated (tightened until
@@ -794,6 +795,30 @@ def run_poly_system(args):
         out[label] = {"ms": t_run * 1e3, "iters": res[0]["iters"], "true_rel": res[0]["rel"],
                       "status": res[0]["status"], "refinements": res[0]["n_updates"],
                       "mcell_iters_per_s": s.n * res[0]["iters"] / t_run / 1e6}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
+def run_single_hex(args):
+    """One large hex Poisson system (--size^3, stretched 1.02 toward the y
+    walls, seed 5) in the batch engine with FP32 iterates and in the FP64
+    drop-in, both to ||b - A x|| / ||b|| <= 1e-10: time per iteration (the
+    case profiled for the batch SpMV; a small batch warms the engine up)."""
+    from tflows_b200 import native, systems
+    s = systems.small_hex(args.size, seed=5, kind="pressure", ratio=1.02, tol=1e-10,
+                          miter=100000)
+    ctx = native.Context(0)
+    _batch_solve(ctx, [systems.small_hex(8, seed=1, kind="pressure")], vec_fp32=True)
+    t_add, t_run, res, info = _batch_solve(ctx, [s], vec_fp32=True)
+    out = {"mode": "single", "mesh": "hex", "n": s.n, "nnz": s.nnz,
+           "batch_mixed": {"ms": t_run * 1e3, "iters": res[0]["iters"],
+                           "us_per_iteration": t_run * 1e6 / res[0]["iters"],
+                           "true_rel": res[0]["rel"], "kernel_ms": info.get("kernel_ms")}}
+    if not os.environ.get("TF_BATCH_PROFILE"):
+        _drop_in_solve_times(ctx, [systems.small_hex(8, seed=1, kind="pressure")], 1e-10)
+        ms, it, rel = _drop_in_solve_times(ctx, [s], 1e-10)[0]
+        out["fp64_drop_in"] = {"ms": ms, "iters": it, "us_per_iteration": ms * 1e3 / it,
+                               "true_rel": rel}
     print(json.dumps(out), flush=True)
     ctx.close()
 
@@ -978,6 +1003,9 @@ def main():
         return
     if args.mode == "poly":
         run_poly_system(args)
+        return
+    if args.mode == "single":
+        run_single_hex(args)
         return
     if args.mode == "batched":
         run_batched(args)
