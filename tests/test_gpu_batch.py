@@ -108,6 +108,9 @@ def test_batch_add_many_equals_adds(gpu_ctx, threads):
         b = batch.Batch(gpu_ctx, mem_budget=1 << 30)
         try:
             ids = b.add_many(sysl, threads=threads) if many else [b.add(s) for s in sysl]
+            up = b.upload_ms()
+            assert set(up) == {"prep", "wait", "admit"}
+            assert up["prep"] > 0.0 and up["admit"] > 0.0 and up["wait"] >= 0.0
             b.run()
             out.append((ids, [b.result(i) for i in ids]))
         finally:
