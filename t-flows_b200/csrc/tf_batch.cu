@@ -2383,6 +2383,7 @@ struct tf_server_s {
   std::map<int64_t, std::shared_ptr<Request>> live;     // submitted, not yet collected
   std::map<int, std::shared_ptr<Request>> by_slot;      // running (worker thread)
   int n_running = 0;        // by_slot.size(), readable by the admission thread
+  int n_releasing = 0;      // finished or cancelled, their memory not yet released
   uint64_t retire_gen = 0;  // counts retirements (the admission thread waits on it)
   int64_t next_id = 1;
   bool stop = false;
@@ -2432,8 +2433,9 @@ struct tf_server_s {
       if (st == TF_ERR_BUSY) {
         std::unique_lock<std::mutex> lk(mu);
         t_ms[1] += ms_since(t0);
-        if (n_running == 0 && staged.empty() && retire_gen == gen) {
-          // Nothing runs or lands that could free space: it never fits.
+        if (n_running == 0 && staged.empty() && n_releasing == 0 && retire_gen == gen) {
+          // Nothing runs, lands or is being released that could free space:
+          // it never fits.
           if (!queue.empty() && queue.front() == r) {
             queue.pop_front();
             ++rejected;
@@ -2634,6 +2636,7 @@ struct tf_server_s {
           leaving.push_back(by_slot[slot]);
           by_slot.erase(slot);
         }
+        n_releasing += (int)(fin.size() + cancelled.size());
         n_running = (int)by_slot.size();
       }
       if (launched) {
@@ -2679,6 +2682,7 @@ struct tf_server_s {
       r->t_done = Clock::now();
       r->done = true;
       if (r->status >= 0) ++completed;
+      --n_releasing;
       ++retire_gen;
       t_ms[4] += ms_since(t0);
       cv_admit.notify_all();
