@@ -79,8 +79,8 @@ def parse():
     ap.add_argument("--rcm", action="store_true",
                     help="spmv: renumber the cells by reverse Cuthill-McKee first")
     ap.add_argument("--mode", default="solve",
-                    choices=["solve", "spmv", "iters", "multi", "poly", "single", "batched", "served",
-                             "icc"],
+                    choices=["solve", "spmv", "iters", "multi", "poly", "single", "batched",
+                             "served", "icc"],
                     help="spmv: only the pressure matrix and `--steps` SpMV launches "
                          "(the small case profiled with ncu); iters: `--steps` Cg solves "
                          "of exactly `--iters` iterations on the pressure matrix (launch "
@@ -754,8 +754,8 @@ def run_poly_system(args):
     A = sps.csr_matrix((s.val, s.csr.col - 1, s.csr.row - 1), shape=(s.n, s.n))
     rel = lambda x: float(np.linalg.norm(s.b - A @ x) / np.linalg.norm(s.b))  # noqa: E731
     ctx = native.Context(0)
-    out = {"mode": "poly", "mesh": "poly-lattice" if args.mesh == "poly-lattice" else "poly-delaunay",
-           "n": s.n, "nnz": s.nnz, "gen_s": gen}
+    mesh = "poly-lattice" if args.mesh == "poly-lattice" else "poly-delaunay"
+    out = {"mode": "poly", "mesh": mesh, "n": s.n, "nnz": s.nnz, "gen_s": gen}
     # FP64 drop-in.  Its stopping test is the reference's NRMS, which on a
     # mesh with widely varying cell sizes differs from the true relative
     # residual by orders of magnitude: tol is calibrated (tightened until

@@ -2499,7 +2499,8 @@ struct tf_server_s {
     cudaSetDevice(eng.ctx->device);
     cudaStream_t s = eng.ctx->stream;
     std::vector<char> out(eng.max_sys, 0);          // left out of the lists
-    std::vector<std::shared_ptr<Request>> leaving;  // out of the next list, still in the one in flight
+    // out of the next list, still in the one in flight
+    std::vector<std::shared_ptr<Request>> leaving;
     int cur = 0;
     bool inflight = false;
     for (;;) {

@@ -381,8 +381,11 @@ __device__ bool stream_csr2(S& src, Op& op, unsigned long long wait_ns = kWaitLi
           } else {
             switch (tile_group_width(r1 - r0, m[6] - j0)) {
               case 1: one_lane(cols); break;
-              case 2: wg_rows<2, 16>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps); break;
-              default: wg_rows<4, 16>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+              case 2:
+                wg_rows<2, 16>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
+                break;
+              default:
+                wg_rows<4, 16>(op, prod, cols, srow(s), p0, r0, r1, j0, warp, lane, kConsWarps);
             }
           }
         };
