@@ -65,3 +65,32 @@ def test_null_arguments_rejected(lib):
     assert lib.tf_batch_add_many(None, 0, None, None, None, None, None, None, None, None,
                                  None, None, 0, None) == 3
     assert lib.tf_batch_run(None) == 3
+
+
+def header_prototypes():
+    """{name: number of parameters} of every function the header declares."""
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(tf_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", txt, flags=re.S):
+        args = m.group(2).strip()
+        out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_bindings_pass_as_many_arguments_as_the_header_declares(lib):
+    """Every argtypes list set by the Python bindings has the length of the
+    C prototype (a mismatch would pass garbage through the ABI)."""
+    from tflows_b200 import batch, pool
+    batch._lib()
+    pool._lib()
+    protos = header_prototypes()
+    checked = 0
+    for name, nargs in protos.items():
+        fn = getattr(lib, name, None)
+        argtypes = getattr(fn, "argtypes", None) if fn is not None else None
+        if argtypes is None:
+            continue
+        assert len(argtypes) == nargs, (name, len(argtypes), nargs)
+        checked += 1
+    assert checked >= 40
